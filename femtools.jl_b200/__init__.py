@@ -1,0 +1,15 @@
+"""femtools_b200 — sm_100a backend for FEMTools.jl's dynamic-relaxation solvers.
+
+Host-side mirror of the reference's Stokes/thermal DR API (solve!, solve_coupled!,
+the assemble_* kernels) over the C ABI of libfemtools_b200 (include/femtools_b200.h).
+The directory name is not an importable identifier; load it by path (see
+tests/conftest.py) under the module name `femtools_b200`.
+"""
+from . import _abi  # noqa: F401
+from . import mesh  # noqa: F401
+from . import problem  # noqa: F401
+from .mesh import structured_mixed_mesh, element_tables, MixedMesh  # noqa: F401
+from .problem import StokesMaterial, DruckerPrager, DirichletBoundaryCondition  # noqa: F401
+
+__all__ = ["structured_mixed_mesh", "element_tables", "MixedMesh", "StokesMaterial", "DruckerPrager",
+           "DirichletBoundaryCondition"]

@@ -1,0 +1,334 @@
+/*
+ * femtools_b200.h — C ABI of libfemtools_b200, the sm_100a backend for the
+ * matrix-free dynamic-relaxation (DR) Stokes and thermal-diffusion solvers of
+ * FEMTools.jl.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (FEMB200_OK on success) and never synchronises the device: work is queued on
+ * the stream set with femb200_set_stream (the legacy default stream if none),
+ * and a call that must read a scalar back (a convergence check) synchronises
+ * that stream only.
+ *
+ * Conventions, identical to the Julia arrays the reference hands to its
+ * KernelAbstractions kernels, so a Julia caller passes `pointer(::CuArray)`:
+ *   - arrays are column-major; connectivities are 1-based int32;
+ *   - `el2n` is nv × nels, `dofsP` and `el2nP` are np × nels;
+ *   - `geo_v` is nels × nq × (dim·dim + 1): the inverse Jacobian (column-major)
+ *     followed by |det J|·ω at each velocity quadrature point
+ *     (QuadraturePointGeometry, src/mesh/mesh.jl:467); `geo_P` is nels × nq;
+ *   - vector fields are separate component arrays (VectorField3D), stresses are
+ *     the six assembler-order components (xx, yy, zz, xy, xz, yz)
+ *     (src/stokes/types/stokes_types.jl:316-318), or (xx, yy, xy) in 2-D;
+ *   - integration-point arrays (stress history, P_old, viscosity) are nq × nels.
+ *
+ * The library owns only scratch (reduction buffers and iteration scalars);
+ * every state array belongs to the caller.
+ */
+#ifndef FEMTOOLS_B200_H
+#define FEMTOOLS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+    FEMB200_OK = 0,
+    FEMB200_EINVAL = 1,        /* bad argument (sizes, layouts, null pointers) */
+    FEMB200_ECUDA = 2,         /* a CUDA runtime call failed */
+    FEMB200_ENOMEM = 3,        /* scratch allocation failed */
+    FEMB200_ENOTCONV = 4,      /* solve did not converge (throw_on_failure) */
+    FEMB200_ENAN = 5,          /* NaN detected in a convergence check */
+    FEMB200_EKABOOM = 6,       /* error above 1e10 in a convergence check */
+    FEMB200_ELAMBDA = 7,       /* preconditioner produced an invalid lambda_max */
+    FEMB200_EUNSUPPORTED = 8,  /* element/option combination not implemented */
+    FEMB200_ENONFINITE = 9     /* non-finite thermal residual in a coupled solve */
+};
+
+/* ---- enumerations -------------------------------------------------------- */
+enum { FEMB200_F64 = 0, FEMB200_F32 = 1 };
+
+/* Phase layouts (src/utils.jl:70-74): a per-node vector indexed through the
+ * connectivity, one phase per cell (a 1 × nels matrix), or one phase per
+ * element-local node (an n × nels matrix). */
+enum { FEMB200_PHASE_NODAL = 0, FEMB200_PHASE_CELL = 1, FEMB200_PHASE_ELEMENT_NODE = 2 };
+
+/* Layout of an auxiliary field: absent, nq × nels at integration points, or
+ * nodal (interpolated with the shape functions). */
+enum { FEMB200_FIELD_NONE = 0, FEMB200_FIELD_IP = 1, FEMB200_FIELD_NODAL = 2 };
+
+/* Arithmetic of the DR sweeps. FP64 is the reference algorithm; MIXED runs the
+ * residual and update sweeps in FP32 inside an FP64 defect-correction loop. */
+enum { FEMB200_PRECISION_FP64 = 0, FEMB200_PRECISION_MIXED = 1 };
+
+#define FEMB200_MAX_PHASES 16
+
+/* ---- problem description ------------------------------------------------- */
+
+/* Per-phase Stokes material (StokesMaterial, src/stokes/types/stokes_types.jl:19)
+ * and Drucker-Prager parameters (DruckerPrager, stokes_types.jl:388). Host data. */
+typedef struct femb200_stokes_material {
+    int32_t nphases;
+    double eta[FEMB200_MAX_PHASES];
+    double eta_b[FEMB200_MAX_PHASES];
+    double G[FEMB200_MAX_PHASES];
+    double alpha[FEMB200_MAX_PHASES];
+    double rho0[FEMB200_MAX_PHASES];
+    double K[FEMB200_MAX_PHASES];
+    double g[3];
+    double Tref;
+    int32_t plastic;                 /* 0: no yield model; 1: DruckerPrager */
+    double cos_phi[FEMB200_MAX_PHASES];
+    double sin_phi[FEMB200_MAX_PHASES];
+    double sin_psi[FEMB200_MAX_PHASES];
+    double C[FEMB200_MAX_PHASES];
+    double eta_reg[FEMB200_MAX_PHASES];
+    double Kb[FEMB200_MAX_PHASES];
+    /* Pressure-scaling viscosity (the `scaling_viscosity` keyword of solve!,
+     * src/stokes/solvers/DR.jl:309); used only when use_scaling_eta != 0. */
+    int32_t use_scaling_eta;
+    double scaling_eta[FEMB200_MAX_PHASES];
+} femb200_stokes_material;
+
+/* Mesh, state and boundary data of one StokesDR solve. Pointers are device
+ * pointers for libfemtools_b200 (host pointers for the CPU oracle); every
+ * floating-point array has the type given by `dtype` except the geometry,
+ * whose type is `geo_dtype` (the reference's geometry_precision). */
+typedef struct femb200_stokes_problem {
+    int32_t dim;          /* 2 (plane strain, Q9/P1-disc) or 3 (Hex27/P1-disc) */
+    int32_t nv, np, nq;   /* 9,3,9 or 27,4,27 */
+    int32_t dtype;        /* FEMB200_F64 or FEMB200_F32 */
+    int32_t geo_dtype;
+    int64_t nels, nnodes, nnodesP;
+
+    /* mesh */
+    const int32_t* el2n;
+    const int32_t* dofsP;
+    const int32_t* el2nP;
+    const void* geo_v;
+    const void* geo_P;
+
+    /* velocity-node state (dim components each, length nnodes) */
+    void* v[3];
+    void* rate[3];        /* ∂v∂τ */
+    void* Rv[3];
+    void* Rv0[3];
+    void* dRdv[3];        /* ∂Rv∂v: Jacobian L1 row sums */
+    void* PC[3];          /* |diag| preconditioner */
+
+    /* pressure-DoF state (length nnodesP) */
+    void* P;
+    void* P0;
+    void* gammaP;
+    void* T;
+    void* T0;
+    void* Q;              /* may be NULL: no volumetric source */
+    void* Pf;             /* may be NULL: zero fluid pressure */
+    void* RP;
+    void* M_P;
+    void* Pnum;
+
+    /* phases */
+    const int32_t* phases_v;
+    int32_t phases_v_layout;
+    const int32_t* phases_P;
+    int32_t phases_P_layout;
+
+    /* stress history and output (3 or 6 components) */
+    const void* tau_old[6];
+    int32_t tau_old_layout;   /* FEMB200_FIELD_NONE / IP / NODAL */
+    void* tau[6];             /* written by femb200_store_stress (IP layout) */
+
+    /* optional overrides */
+    const void* P_old;        /* NULL → P0; else nodal (nnodesP) or IP */
+    int32_t P_old_layout;
+    const void* viscosity_ip; /* NULL → material eta; else nq × nels */
+    const void* body_force[3];/* NULL or assembled nodal loads */
+
+    /* Dirichlet conditions, one set per velocity component */
+    const int32_t* bc_dofs[3];
+    const void* bc_vals[3];
+    int64_t bc_n[3];
+
+    femb200_stokes_material mat;
+} femb200_stokes_problem;
+
+/* Iteration controls of solve!/solve_stokes_dyrel! (src/stokes/solvers/DR.jl:302-387). */
+typedef struct femb200_stokes_controls {
+    double dt;
+    double pressure_factor;   /* γfact of the pressure scaling (default 50) */
+    double tolerance;         /* ϵ_tol (default 1e-6) */
+    int64_t max_iterations;   /* total_iterMax (default 50 000) */
+    int64_t check_interval;   /* ncheck (default 50) */
+    int64_t iter_max;         /* iterMax per Powell–Hestenes step (default 50 000) */
+    int64_t max_ph_iterations;/* default 1000 */
+    double rel_drop0;         /* default 1e-2 */
+    int32_t freeze_jacobian;  /* -1: default (plastic == 0) */
+    int32_t finite_K;         /* storage modulus K instead of ηb */
+    int32_t assemble_scaling; /* 1: solve! (assemble M_P, γP first); 0: solve_stokes_dyrel! */
+    int32_t throw_on_failure; /* nonzero: return FEMB200_ENOTCONV when not converged */
+    int32_t precision;        /* FEMB200_PRECISION_FP64 / MIXED */
+    double cfl_v;             /* CFL_v (default 0.98) */
+    double c_fact;            /* default 0.9 */
+    /* Optional history of every convergence check, 4 + dim doubles per entry:
+     * (iter, err_v, err_P, unused, err_v_components[dim]). */
+    double* history;
+    int64_t history_capacity;
+    /* Mixed precision: FP32 inner sweeps run until their residual drops by
+     * this factor before each FP64 defect-correction step (default 1e-3). */
+    double mixed_inner_drop;
+} femb200_stokes_controls;
+
+typedef struct femb200_stokes_stats {
+    int64_t itPH;
+    int64_t iter;
+    double err, err_abs, err_rel, err_v, err_P;
+    int32_t converged;
+    int32_t reached_total_iter;
+    double lambda_max;
+    double lambda_max_gershgorin;
+    int64_t jacobian_assemblies;
+    int64_t history_len;
+    double err_T;
+    int64_t thermal_iterations;
+    int64_t defect_corrections;   /* mixed precision: outer FP64 corrections */
+} femb200_stokes_stats;
+
+/* Thermal diffusion (ThermalDiffusionDR, src/heat_diffusion/types/heat_diffusion_types.jl:90). */
+typedef struct femb200_thermal_problem {
+    int32_t dim, nv, nq, dtype, geo_dtype;
+    int64_t nels, nnodes;
+    const int32_t* el2n;
+    const void* geo;          /* nels × nq × (dim·dim + 1) */
+    void* T; void* T0; void* rate; void* R; void* R0; void* dRdT; void* PC;
+    void* P; void* source;
+    const void* source_ip;    /* optional nq × nels heat source (shear heating Φ) */
+    const int32_t* phases; int32_t phases_layout;
+    const int32_t* bc_dofs; const void* bc_vals; int64_t bc_n;
+    int32_t nphases;
+    double k[FEMB200_MAX_PHASES], Cp[FEMB200_MAX_PHASES], rho0[FEMB200_MAX_PHASES];
+    double alpha[FEMB200_MAX_PHASES], K[FEMB200_MAX_PHASES];
+    double cfl, c_fact, eps;  /* CFL (0.98), c_fact (0.9), ϵ (1e-6) */
+} femb200_thermal_problem;
+
+typedef struct femb200_thermal_controls {
+    double dt;
+    double Tref;
+    double tolerance;         /* relative ‖R‖/‖R⁰‖ */
+    int64_t max_iterations;   /* default 10 000 */
+    int64_t check_interval;   /* default 100 */
+    int32_t throw_on_failure;
+} femb200_thermal_controls;
+
+typedef struct femb200_thermal_stats {
+    int32_t converged;
+    int64_t iterations;
+    double residual;
+} femb200_thermal_stats;
+
+/* ---- handle -------------------------------------------------------------- */
+typedef struct femb200_handle femb200_handle;
+
+/* Create a handle on the current CUDA device. Replaces the implicit backend
+ * state of KA.get_backend(mesh.coords) (src/stokes/solvers/DR.jl:255). */
+int femb200_create(femb200_handle** out);
+int femb200_destroy(femb200_handle* h);
+/* Queue all work on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Replaces CUDA.stream() of the Julia CUDABackend. */
+int femb200_set_stream(femb200_handle* h, void* stream);
+/* Message of the last failure on this handle (also the reference's error text). */
+const char* femb200_last_error(const femb200_handle* h);
+/* Build information: compiled architecture and version string. */
+const char* femb200_version(void);
+
+/* ---- Stokes element sweeps ------------------------------------------------ */
+
+/* assemble_pressure_residual_kernel! (src/stokes/assemblers/pressure_residual.jl:256):
+ * RP ← Σ_e ∫ N (−∇·v − (P−P_old)/(ηb Δt) + α(T−T0)/Δt + Q) dΩ, element-private DoFs.
+ * `finite_K` selects K instead of ηb as the storage modulus. */
+int femb200_pressure_residual(femb200_handle* h, const femb200_stokes_problem* p,
+                              double dt, int32_t finite_K);
+
+/* assemble_momentum_residual_kernel! (src/stokes/assemblers/momentum_residuals.jl:417):
+ * Rv ← Σ_e ∫ ∇N·(τ − (P + Pnum) I) − N ρ g dΩ with the visco-elasto-plastic stress
+ * of src/stokes/assemblers/rheology.jl. `with_pnum` = 0 passes Pnum = nothing. */
+int femb200_momentum_residual(femb200_handle* h, const femb200_stokes_problem* p,
+                              double dt, int32_t with_pnum);
+
+/* One fused DR residual sweep: the pressure residual, Pnum = γP·RP/M_P
+ * (src/stokes/solvers/DR.jl:665-684) and the momentum residual in one pass. */
+int femb200_stokes_residuals(femb200_handle* h, const femb200_stokes_problem* p,
+                             double dt, int32_t finite_K);
+
+/* update_stokes_velocity! (src/stokes/helpers.jl:52): per component,
+ * rate ← β·rate + Rv/PC; v ← v + alpha·rate (alpha already signed). */
+int femb200_velocity_update(femb200_handle* h, const femb200_stokes_problem* p,
+                            const double* beta, const double* alpha);
+
+/* apply_dirichlet! (src/dynamic_relaxation/solver.jl:152): x[dofs[i]] ← vals[i]
+ * (vals == NULL → 0). dtype as in the problem. */
+int femb200_apply_dirichlet(femb200_handle* h, void* x, const int32_t* dofs,
+                            const void* vals, int64_t n, int32_t dtype);
+
+/* assemble_augmented_momentum_jacobian_matrices_atomix!
+ * (src/stokes/assemblers/momentum_residuals.jl:998): L1 row sums of the augmented
+ * element Jacobian into dRdv and |diagonal| of the same-direction block into PC. */
+int femb200_jacobian_diagnostics(femb200_handle* h, const femb200_stokes_problem* p,
+                                 double dt, int32_t finite_K);
+
+/* assemble_viscosity_weighted_pressure_scaling! (src/stokes/assemblers/pressure_scaling.jl:118):
+ * M_P = Σ N² dΩ, γP = Σ N² γ_eff dΩ / M_P. */
+int femb200_pressure_scaling(femb200_handle* h, const femb200_stokes_problem* p,
+                             double gamma_fact, double dt, int32_t finite_K);
+
+/* update_stokes_current_stress! (src/stokes/solvers/DR.jl:820): integration-point
+ * stresses of the current v, P into p->tau (nq × nels each). */
+int femb200_store_stress(femb200_handle* h, const femb200_stokes_problem* p, double dt);
+
+/* ---- Stokes solves --------------------------------------------------------- */
+
+/* solve! / solve_stokes_dyrel! (src/stokes/solvers/DR.jl:302, :241, core :348-802).
+ * With controls->assemble_scaling the pressure mass and scale are assembled first,
+ * as solve! does. Returns FEMB200_ENOTCONV when the solve did not converge and
+ * controls->throw_on_failure is set; FEMB200_ENAN / FEMB200_EKABOOM /
+ * FEMB200_ELAMBDA on the reference's error paths. */
+int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p,
+                         const femb200_stokes_controls* c, femb200_stokes_stats* stats);
+
+/* ---- thermal diffusion ---------------------------------------------------- */
+
+/* assemble_diffusion_matrices_atomix! (src/heat_diffusion/assembly/residual_atomics.jl:10)
+ * with element_residual / element_jacobian (src/heat_diffusion/assembly/residual.jl:7,30). */
+int femb200_thermal_residual(femb200_handle* h, const femb200_thermal_problem* t,
+                             double dt, double Tref, int32_t compute_jacobian);
+
+/* solve!(::ThermalDiffusionDR, …) (src/heat_diffusion/solvers/DR.jl:50 →
+ * src/dynamic_relaxation/solver.jl:61). */
+int femb200_solve_thermal(femb200_handle* h, const femb200_thermal_problem* t,
+                          const femb200_thermal_controls* c, femb200_thermal_stats* stats);
+
+/* _transfer_temperature! (src/stokes/solvers/DR.jl:44): T_P[dofsP[i]] = T[el2nP[i]]. */
+int femb200_transfer_temperature(femb200_handle* h, void* T_P, const void* T,
+                                 const int32_t* dofsP, const int32_t* el2nP,
+                                 int64_t n, int32_t dtype);
+
+/* assemble_shear_heating! (src/stokes/assemblers/shear_heating.jl:18):
+ * Φ = τ:(ε̇ − ε̇_el) at every velocity quadrature point into phi (nq × nels). */
+int femb200_shear_heating(femb200_handle* h, const femb200_stokes_problem* p,
+                          double dt, void* phi);
+
+/* solve_coupled! (src/stokes/solvers/DR.jl:89): one thermal DR iteration per inner
+ * Stokes iteration; `shear_heating` adds Φ to the heat source. */
+int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t,
+                          const femb200_stokes_problem* p,
+                          const femb200_stokes_controls* c, double Tref,
+                          int32_t shear_heating, void* phi_scratch,
+                          femb200_stokes_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEMTOOLS_B200_H */

@@ -1,0 +1,264 @@
+"""Test-side binding of the CPU oracle (oracle/_build/liboracle.so).
+
+The oracle is test infrastructure: the parity checker of libfemtools_b200. This
+module builds host (numpy) problems with the same struct packing the product
+uses, so a test can hand one problem to both implementations.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from conftest import fem
+
+abi = fem._abi
+problem = fem.problem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+
+_P = C.POINTER
+_vp = C.c_void_p
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            import subprocess
+            subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+        L = C.CDLL(ORACLE_SO)
+        sig = {
+            "orc_last_error": (C.c_char_p, []),
+            "orc_num_threads": (C.c_int, []),
+            "orc_set_num_threads": (None, [C.c_int]),
+            "orc_tables": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp]),
+            "orc_structured_mesh": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "orc_geometry": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
+            "orc_pressure_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
+            "orc_momentum_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
+            "orc_stokes_residuals": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
+            "orc_jacobian_diagnostics": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
+            "orc_pressure_scaling": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_double, C.c_int32]),
+            "orc_store_stress": (C.c_int, [_P(abi.StokesProblemC), C.c_double]),
+            "orc_solve_stokes": (C.c_int, [_P(abi.StokesProblemC), _P(abi.StokesControlsC), _P(abi.StokesStatsC)]),
+            "orc_thermal_residual": (C.c_int, [_P(abi.ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
+            "orc_solve_thermal": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.ThermalControlsC), _P(abi.ThermalStatsC)]),
+            "orc_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64]),
+            "orc_shear_heating": (C.c_int, [_P(abi.StokesProblemC), C.c_double, _vp]),
+            "orc_solve_coupled": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.StokesProblemC), _P(abi.StokesControlsC),
+                                            C.c_double, C.c_int32, _vp, _P(abi.StokesStatsC)]),
+            "orc_element_custom": (C.c_int, [C.c_int] * 4 + [_vp] * 15 + [_P(abi.StokesMaterialC), C.c_double,
+                                                                              C.c_int32, _vp, _vp, _vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    if a is None:
+        return 0
+    assert isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"], "oracle arrays must be contiguous numpy"
+    return a.ctypes.data
+
+
+def check(rc):
+    if rc != 0:
+        raise abi.FemB200Error(rc, lib().orc_last_error().decode())
+
+
+class HostStokes:
+    """numpy mirror of a StokesDR state plus its packed problem for the oracle."""
+
+    def __init__(self, mesh, material, plastic=None, phases_v=None, phases_v_layout=abi.PHASE_NODAL,
+                 phases_P=None, phases_P_layout=abi.PHASE_NODAL, stress=True, scaling_eta=None):
+        self.mesh = mesh
+        self.material = material
+        self.plastic = plastic
+        dim, nn, nP = mesh.dim, mesh.nnodes, mesh.nnodesP
+        z = lambda n: np.zeros(n)
+        self.v = [z(nn) for _ in range(dim)]
+        self.rate = [z(nn) for _ in range(dim)]
+        self.Rv = [z(nn) for _ in range(dim)]
+        self.Rv0 = [z(nn) for _ in range(dim)]
+        self.dRdv = [z(nn) for _ in range(dim)]
+        self.PC = [z(nn) for _ in range(dim)]
+        for name in ("P", "P0", "gammaP", "T", "T0", "Q", "Pf", "RP", "M_P", "Pnum"):
+            setattr(self, name, z(nP))
+        nt = 6 if dim == 3 else 3
+        nqe = mesh.nq * mesh.nels
+        self.tau_old = [z(nqe) for _ in range(nt)] if stress else None
+        self.tau = [z(nqe) for _ in range(nt)] if stress else None
+        self.phases_v = phases_v if phases_v is not None else np.ones(nn, dtype=np.int32)
+        self.phases_v_layout = phases_v_layout if phases_v is not None else abi.PHASE_NODAL
+        self.phases_P = phases_P if phases_P is not None else np.ones(nP, dtype=np.int32)
+        self.phases_P_layout = phases_P_layout if phases_P is not None else abi.PHASE_NODAL
+        self.P_old = None
+        self.P_old_layout = abi.FIELD_NODAL
+        self.viscosity_ip = None
+        self.body_force = None
+        self.scaling_eta = scaling_eta
+        self.mesh_arrays = {
+            "dim": dim, "nels": mesh.nels, "nnodes": nn, "nnodesP": nP,
+            "el2n": np.ascontiguousarray(mesh.el2n), "dofsP": np.ascontiguousarray(mesh.dofsP),
+            "el2nP": np.ascontiguousarray(mesh.el2nP),
+            "geo_v": np.ascontiguousarray(mesh.geo_v), "geo_P": np.ascontiguousarray(mesh.geo_P),
+        }
+        self.bcs = [None] * dim
+
+    def set_bc(self, comps):
+        """comps: one (dofs, vals) pair per velocity component."""
+        self.bcs = [(np.ascontiguousarray(d, dtype=np.int32), np.ascontiguousarray(v, dtype=np.float64))
+                    for d, v in comps]
+
+    def state(self):
+        return {
+            "v": self.v, "rate": self.rate, "Rv": self.Rv, "Rv0": self.Rv0, "dRdv": self.dRdv, "PC": self.PC,
+            "P": self.P, "P0": self.P0, "gammaP": self.gammaP, "T": self.T, "T0": self.T0, "Q": self.Q,
+            "Pf": self.Pf, "RP": self.RP, "M_P": self.M_P, "Pnum": self.Pnum,
+            "phases_v": self.phases_v, "phases_v_layout": self.phases_v_layout,
+            "phases_P": self.phases_P, "phases_P_layout": self.phases_P_layout,
+            "tau_old": self.tau_old, "tau": self.tau,
+            "tau_old_layout": abi.FIELD_IP if self.tau_old is not None else abi.FIELD_NONE,
+            "P_old": self.P_old, "P_old_layout": self.P_old_layout,
+            "viscosity_ip": self.viscosity_ip, "body_force": self.body_force,
+        }
+
+    def struct(self):
+        s = abi.StokesProblemC()
+        mat = problem.material_struct(self.material, self.plastic, self.scaling_eta)
+        problem.fill_stokes_problem(s, self.mesh_arrays, self.state(), mat, self.bcs, ptr)
+        self._s = s
+        return s
+
+    # ---- oracle calls ----
+    def pressure_scaling(self, gamma_fact, dt, finite_K=False):
+        check(lib().orc_pressure_scaling(C.byref(self.struct()), gamma_fact, dt, int(finite_K)))
+
+    def pressure_residual(self, dt, finite_K=False):
+        check(lib().orc_pressure_residual(C.byref(self.struct()), dt, int(finite_K)))
+
+    def momentum_residual(self, dt, with_pnum=False):
+        check(lib().orc_momentum_residual(C.byref(self.struct()), dt, int(with_pnum)))
+
+    def stokes_residuals(self, dt, finite_K=False):
+        check(lib().orc_stokes_residuals(C.byref(self.struct()), dt, int(finite_K)))
+
+    def jacobian_diagnostics(self, dt, finite_K=False):
+        check(lib().orc_jacobian_diagnostics(C.byref(self.struct()), dt, int(finite_K)))
+
+    def store_stress(self, dt):
+        check(lib().orc_store_stress(C.byref(self.struct()), dt))
+
+    def shear_heating(self, dt):
+        phi = np.zeros(self.mesh.nq * self.mesh.nels)
+        check(lib().orc_shear_heating(C.byref(self.struct()), dt, ptr(phi)))
+        return phi
+
+    def solve(self, history_capacity=0, **kw):
+        hist = np.zeros((history_capacity, 4 + self.mesh.dim)) if history_capacity else None
+        c = problem.controls_struct(history=hist, **kw)
+        st = abi.StokesStatsC()
+        rc = lib().orc_solve_stokes(C.byref(self.struct()), C.byref(c), C.byref(st))
+        check(rc)
+        out = problem.stats_dict(st)
+        if hist is not None:
+            out["history"] = hist[: st.history_len]
+        return out
+
+
+def element_custom(dim, N, dNdx, dOmega, NP, v, P, material, dt=1.0, P0=None, T=None, T0=None, Q=None,
+                   Pnum=None, phv=None, php=None, tau_old=None, P0_ip=None, plastic=None, finite_K=False):
+    """One synthetic element through the oracle (the reference's element unit-test setup)."""
+    N = np.ascontiguousarray(N, dtype=np.float64)
+    nq, nv = N.shape
+    NP = np.ascontiguousarray(NP, dtype=np.float64)
+    npd = NP.shape[1]
+    arr = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    iarr = lambda x: None if x is None else np.ascontiguousarray(x, dtype=np.int32)
+    m = problem.material_struct(material, plastic)
+    R = np.zeros(dim * nv)
+    RP = np.zeros(npd)
+    ntau = 6 if dim == 3 else 3
+    tau = np.zeros(nq * ntau)
+    args = [arr(dNdx), arr(dOmega), NP, arr(v), arr(P), arr(P0), arr(T), arr(T0), arr(Q), arr(Pnum),
+            iarr(phv), iarr(php), arr(tau_old), arr(P0_ip)]
+    keep = [N] + args
+    rc = lib().orc_element_custom(dim, nv, npd, nq, ptr(N), *[ptr(a) for a in args], C.byref(m), dt,
+                                  int(finite_K), ptr(R), ptr(RP), ptr(tau))
+    del keep
+    check(rc)
+    return R.reshape(dim, nv), RP, tau.reshape(nq, ntau)
+
+
+class HostThermal:
+    """numpy mirror of a ThermalDiffusionDR state (heat_diffusion_types.jl:90-132)."""
+
+    def __init__(self, mesh, k=(1.0,), Cp=(1.0,), rho0=(1.0,), alpha=(0.0,), K=(np.inf,), phases=None,
+                 cfl=0.98, c_fact=0.9, eps=1e-6):
+        self.mesh = mesh
+        nn = mesh.nnodes
+        for name in ("T", "T0", "rate", "R", "R0", "dRdT", "PC", "P", "source"):
+            setattr(self, name, np.zeros(nn))
+        self.phases = np.ones(nn, dtype=np.int32) if phases is None else phases
+        self.mat = dict(k=k, Cp=Cp, rho0=rho0, alpha=alpha, K=K)
+        self.cfl, self.c_fact, self.eps = cfl, c_fact, eps
+        self.source_ip = None
+        self.bc = (np.zeros(0, dtype=np.int32), np.zeros(0))
+        self.el2n = np.ascontiguousarray(mesh.el2n)
+        self.geo = np.ascontiguousarray(mesh.geo_v)
+
+    def set_bc(self, dofs, vals):
+        self.bc = (np.ascontiguousarray(dofs, dtype=np.int32), np.ascontiguousarray(vals, dtype=np.float64))
+
+    def struct(self):
+        t = abi.ThermalProblemC()
+        t.dim, t.dtype, t.geo_dtype = self.mesh.dim, abi.F64, abi.F64
+        t.nv, t.nq = (27, 27) if self.mesh.dim == 3 else (9, 9)
+        t.nels, t.nnodes = self.mesh.nels, self.mesh.nnodes
+        t.el2n, t.geo = ptr(self.el2n), ptr(self.geo)
+        for name in ("T", "T0", "rate", "R", "R0", "dRdT", "PC", "P", "source"):
+            setattr(t, name, ptr(getattr(self, name)))
+        t.source_ip = ptr(self.source_ip)
+        t.phases, t.phases_layout = ptr(self.phases), abi.PHASE_NODAL
+        t.bc_dofs, t.bc_vals, t.bc_n = ptr(self.bc[0]), ptr(self.bc[1]), len(self.bc[0])
+        n = len(self.mat["k"])
+        t.nphases = n
+        for name, fill in (("k", 1.0), ("Cp", 1.0), ("rho0", 1.0), ("alpha", 0.0), ("K", np.inf)):
+            arr = getattr(t, name)
+            vals = self.mat[name]
+            for i in range(abi.MAX_PHASES):
+                arr[i] = vals[i] if i < n else fill
+        t.cfl, t.c_fact, t.eps = self.cfl, self.c_fact, self.eps
+        self._t = t
+        return t
+
+    def residual(self, dt, Tref, jac=False):
+        check(lib().orc_thermal_residual(C.byref(self.struct()), dt, Tref, int(jac)))
+
+    def solve(self, dt, Tref=273.0, tolerance=None, max_iterations=10_000, check_interval=100, throw_on_failure=True):
+        c = abi.ThermalControlsC()
+        c.dt, c.Tref = dt, Tref
+        c.tolerance = self.eps if tolerance is None else tolerance
+        c.max_iterations, c.check_interval, c.throw_on_failure = max_iterations, check_interval, int(throw_on_failure)
+        st = abi.ThermalStatsC()
+        check(lib().orc_solve_thermal(C.byref(self.struct()), C.byref(c), C.byref(st)))
+        return {"converged": bool(st.converged), "iterations": st.iterations, "residual": st.residual}
+
+
+def solve_coupled(thermal: HostThermal, stokes: HostStokes, Tref=273.0, shear_heating=False, history_capacity=0, **kw):
+    phi = np.zeros(stokes.mesh.nq * stokes.mesh.nels) if shear_heating else None
+    c = problem.controls_struct(**kw)
+    st = abi.StokesStatsC()
+    t = thermal.struct()
+    rc = lib().orc_solve_coupled(C.byref(t), C.byref(stokes.struct()), C.byref(c), Tref, int(shear_heating),
+                                 ptr(phi), C.byref(st))
+    check(rc)
+    return problem.stats_dict(st), phi
