@@ -13,3 +13,10 @@ from .problem import StokesMaterial, DruckerPrager, DirichletBoundaryCondition  
 
 __all__ = ["structured_mixed_mesh", "element_tables", "MixedMesh", "StokesMaterial", "DruckerPrager",
            "DirichletBoundaryCondition"]
+
+from . import solver  # noqa: E402,F401
+from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, solve_coupled,  # noqa: E402,F401
+                     solve_thermal, assemble_pressure_residual, assemble_momentum_residual,
+                     assemble_stokes_residuals, assemble_augmented_momentum_jacobian,
+                     assemble_viscosity_weighted_pressure_scaling, update_stokes_current_stress,
+                     assemble_shear_heating, assemble_thermal_residual)

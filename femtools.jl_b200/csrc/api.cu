@@ -1,0 +1,929 @@
+// api.cu — the C ABI of libfemtools_b200 (include/femtools_b200.h): handle,
+// constant-memory set-up, kernel dispatch and the device-resident dynamic-
+// relaxation drivers (the host side of _solve_stokes_dyrel!, DR.jl:348-802, and
+// solve_dynamic_relaxation!, dynamic_relaxation/solver.jl:61-122).
+//
+// All state stays on the device; a convergence check reads back a handful of
+// reduced scalars (one stream synchronisation per check, as the reference's
+// host norms do) and the iteration scalars α, β are passed by value.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace femb {
+__constant__ DevStokesMaterial c_mat;
+__constant__ DevTables c_tab;
+}  // namespace femb
+
+using namespace femb;
+
+struct femb200_handle {
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    double* d_partials = nullptr;
+    size_t partials_cap = 0;    // doubles
+    double* h_partials = nullptr;
+    size_t h_partials_cap = 0;
+    uint8_t* d_mask = nullptr;
+    size_t mask_cap = 0;
+    uint8_t* d_tmask = nullptr;
+    size_t tmask_cap = 0;
+    std::string err;
+    bool tables_ready = false;
+};
+
+namespace {
+
+#define CK(...)                                                                                   \
+    do {                                                                                          \
+        cudaError_t e_ = (__VA_ARGS__);                                                           \
+        if (e_ != cudaSuccess) {                                                                  \
+            h->err = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #__VA_ARGS__;  \
+            return FEMB200_ECUDA;                                                                 \
+        }                                                                                         \
+    } while (0)
+
+#define RC(...)                          \
+    do {                                 \
+        int r_ = (__VA_ARGS__);          \
+        if (r_ != FEMB200_OK) return r_; \
+    } while (0)
+
+inline double line_N(double x, int node) {
+    if (node == -1) return x * (x - 1) * 0.5;
+    if (node == 0) return 1 - x * x;
+    return x * (x + 1) * 0.5;
+}
+inline double line_dN(double x, int node) {
+    if (node == -1) return x - 0.5;
+    if (node == 0) return -2 * x;
+    return x + 0.5;
+}
+
+// Hex27 / Q9 local node coordinates (src/elements/shape_functions.jl:414-442, :268-278).
+const int H27[27][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1}, {1, -1, 1}, {1, 1, 1},
+                        {-1, 1, 1},   {0, -1, -1}, {1, 0, -1}, {0, 1, -1}, {-1, 0, -1}, {0, -1, 1}, {1, 0, 1},
+                        {0, 1, 1},    {-1, 0, 1},  {-1, -1, 0}, {1, -1, 0}, {1, 1, 0},  {-1, 1, 0}, {0, 0, -1},
+                        {0, -1, 0},   {1, 0, 0},   {0, 1, 0},   {-1, 0, 0}, {0, 0, 1},  {0, 0, 0}};
+const int Q9[9][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}, {0, -1}, {1, 0}, {0, 1}, {-1, 0}, {0, 0}};
+
+DevTables build_tables() {
+    DevTables t;
+    std::memset(&t, 0, sizeof(t));
+    const double a = std::sqrt(3.0 / 5.0);
+    const double pts[3] = {-a, 0.0, a};
+    const double wts[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    const int nodes1[3] = {-1, 0, 1};
+    for (int q = 0; q < 3; ++q) {
+        t.qx[q] = pts[q];
+        t.w1[q] = wts[q];
+        for (int i = 0; i < 3; ++i) { t.B[q][i] = line_N(pts[q], nodes1[i]); t.Dd[q][i] = line_dN(pts[q], nodes1[i]); }
+    }
+    for (int a3 = 0; a3 < 27; ++a3) t.tn3[(H27[a3][0] + 1) + 3 * (H27[a3][1] + 1) + 9 * (H27[a3][2] + 1)] = a3;
+    for (int a2 = 0; a2 < 9; ++a2) t.tn2[(Q9[a2][0] + 1) + 3 * (Q9[a2][1] + 1)] = a2;
+    for (int q = 0; q < 27; ++q) {
+        const int qx = q % 3, qy = (q / 3) % 3, qz = q / 9;
+        const double x[3] = {pts[qx], pts[qy], pts[qz]};
+        t.w3[q] = wts[qx] * wts[qy] * wts[qz];
+        double s = 0;
+        for (int n = 0; n < 27; ++n) {
+            double l[3], dl[3];
+            for (int d = 0; d < 3; ++d) { l[d] = line_N(x[d], H27[n][d]); dl[d] = line_dN(x[d], H27[n][d]); }
+            t.N3[q][n] = l[0] * l[1] * l[2];
+            t.dN3[q][n][0] = dl[0] * l[1] * l[2];
+            t.dN3[q][n][1] = l[0] * dl[1] * l[2];
+            t.dN3[q][n][2] = l[0] * l[1] * dl[2];
+            s += t.N3[q][n];
+        }
+        t.sumN3[q] = s;
+        t.NP3[q][0] = 1 - x[0] - x[1] - x[2];
+        t.NP3[q][1] = x[0]; t.NP3[q][2] = x[1]; t.NP3[q][3] = x[2];
+    }
+    const double w2[9] = {25.0 / 81, 40.0 / 81, 25.0 / 81, 40.0 / 81, 64.0 / 81, 40.0 / 81, 25.0 / 81, 40.0 / 81, 25.0 / 81};
+    for (int q = 0; q < 9; ++q) {
+        const double x[2] = {pts[q % 3], pts[q / 3]};
+        t.w2[q] = w2[q];
+        double s = 0;
+        for (int n = 0; n < 9; ++n) {
+            double l[2], dl[2];
+            for (int d = 0; d < 2; ++d) { l[d] = line_N(x[d], Q9[n][d]); dl[d] = line_dN(x[d], Q9[n][d]); }
+            t.N2[q][n] = l[0] * l[1];
+            t.dN2[q][n][0] = dl[0] * l[1];
+            t.dN2[q][n][1] = l[0] * dl[1];
+            s += t.N2[q][n];
+        }
+        t.sumN2[q] = s;
+        t.NP2[q][0] = 1 - x[0] - x[1];
+        t.NP2[q][1] = x[0]; t.NP2[q][2] = x[1];
+    }
+    return t;
+}
+
+int ensure_tables(femb200_handle* h) {
+    if (h->tables_ready) return FEMB200_OK;
+    static DevTables host_tab = build_tables();
+    CK(cudaMemcpyToSymbolAsync(c_tab, &host_tab, sizeof(DevTables), 0, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->tables_ready = true;
+    return FEMB200_OK;
+}
+
+// Constant-memory material of one call. `finite_K` selects K as the storage
+// modulus of the continuity residual and of the pressure scaling (DR.jl:419, :325).
+int upload_material(femb200_handle* h, const femb200_stokes_material& m, int finite_K) {
+    if (m.nphases < 1 || m.nphases > FEMB200_MAX_PHASES) { h->err = "nphases must lie in 1:16"; return FEMB200_EINVAL; }
+    static thread_local DevStokesMaterial d;   // host staging must outlive the async copy
+    std::memset(&d, 0, sizeof(d));
+    d.nphases = m.nphases;
+    d.plastic = m.plastic;
+    bool all_inf = true;
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) {
+        d.eta[i] = m.eta[i];
+        d.eta_scaling[i] = m.use_scaling_eta ? m.scaling_eta[i] : m.eta[i];
+        d.invG[i] = 1.0 / m.G[i];
+        d.alpha[i] = m.alpha[i];
+        d.rho0[i] = m.rho0[i];
+        d.beta[i] = 1.0 / m.K[i];
+        d.bulk[i] = finite_K ? m.K[i] : m.eta_b[i];
+        d.inv_Kscale[i] = 1.0 / d.bulk[i];
+        if (i < m.nphases && !std::isinf(d.bulk[i])) all_inf = false;
+        d.cos_phi[i] = m.cos_phi[i]; d.sin_phi[i] = m.sin_phi[i]; d.sin_psi[i] = m.sin_psi[i];
+        d.C[i] = m.C[i]; d.eta_reg[i] = m.eta_reg[i]; d.Kb[i] = m.Kb[i];
+    }
+    d.all_bulk_inf = all_inf;
+    for (int i = 0; i < 3; ++i) d.g[i] = m.g[i];
+    d.Tref = m.Tref;
+    CK(cudaMemcpyToSymbolAsync(c_mat, &d, sizeof(d), 0, cudaMemcpyHostToDevice, h->stream));
+    // the staging buffer is reused by the next call: make this copy complete first
+    CK(cudaStreamSynchronize(h->stream));
+    return FEMB200_OK;
+}
+
+int check_problem(femb200_handle* h, const femb200_stokes_problem* p) {
+    if (!h) return FEMB200_EINVAL;
+    if (!p) { h->err = "null problem"; return FEMB200_EINVAL; }
+    const bool h27 = p->dim == 3 && p->nv == 27 && p->np == 4 && p->nq == 27;
+    const bool q9 = p->dim == 2 && p->nv == 9 && p->np == 3 && p->nq == 9;
+    if (!h27 && !q9) { h->err = "libfemtools_b200 supports Hex27/P1-disc (3-D) and Q9/P1-disc (2-D) meshes"; return FEMB200_EUNSUPPORTED; }
+    if ((p->dtype != FEMB200_F64 && p->dtype != FEMB200_F32) || (p->geo_dtype != FEMB200_F64 && p->geo_dtype != FEMB200_F32)) {
+        h->err = "dtype must be FEMB200_F64 or FEMB200_F32"; return FEMB200_EINVAL;
+    }
+    if (p->nels <= 0 || p->nnodes <= 0 || p->nnodesP <= 0) { h->err = "empty mesh"; return FEMB200_EINVAL; }
+    if (!p->el2n || !p->dofsP || !p->geo_v || !p->geo_P || !p->P) { h->err = "mesh arrays and P are required"; return FEMB200_EINVAL; }
+    for (int c = 0; c < p->dim; ++c)
+        if (!p->v[c]) { h->err = "velocity components are required"; return FEMB200_EINVAL; }
+    return FEMB200_OK;
+}
+
+int red_blocks(femb200_handle* h, int64_t n) {
+    int64_t b = (n + NODE_THREADS - 1) / NODE_THREADS;
+    b = std::min<int64_t>(b, (int64_t)h->num_sms * 4);
+    return (int)std::max<int64_t>(b, 1);
+}
+
+int ensure_partials(femb200_handle* h, size_t blocks) {
+    const size_t need = blocks * RED_SLOTS;
+    if (need > h->partials_cap) {
+        if (h->d_partials) cudaFree(h->d_partials);
+        if (h->h_partials) cudaFreeHost(h->h_partials);
+        h->d_partials = nullptr; h->h_partials = nullptr;
+        CK(cudaMalloc(&h->d_partials, need * sizeof(double)));
+        CK(cudaMallocHost(&h->h_partials, need * sizeof(double)));
+        h->partials_cap = need;
+    }
+    return FEMB200_OK;
+}
+
+// Copy block partials back and sum each slot in block order (deterministic).
+int fetch_sums(femb200_handle* h, int blocks, int nslots, double* out) {
+    CK(cudaMemcpyAsync(h->h_partials, h->d_partials, (size_t)blocks * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < nslots; ++s) {
+        double t = 0;
+        for (int b = 0; b < blocks; ++b) t += h->h_partials[(size_t)b * RED_SLOTS + s];
+        out[s] = t;
+    }
+    return FEMB200_OK;
+}
+
+template <class T>
+int sumsq(femb200_handle* h, const T* x, const T* div, int64_t n, double& out) {
+    const int b = red_blocks(h, n);
+    RC(ensure_partials(h, b));
+    CK(launch_sumsq<T>(x, div, n, h->d_partials, b, h->stream));
+    return fetch_sums(h, b, 1, &out);
+}
+
+// _checked_λmax (src/utils.jl:152-158)
+template <class T>
+int checked_lmax(femb200_handle* h, const T* J, const T* PC, int64_t n, const char* label, double& out) {
+    const int b = red_blocks(h, n);
+    RC(ensure_partials(h, b));
+    CK(launch_ratio_max<T>(J, PC, n, h->d_partials, b, h->stream));
+    CK(cudaMemcpyAsync(h->h_partials, h->d_partials, (size_t)b * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double m = -INFINITY; bool nan = false;
+    for (int i = 0; i < b; ++i) { m = std::max(m, h->h_partials[(size_t)i * RED_SLOTS]); nan = nan || h->h_partials[(size_t)i * RED_SLOTS + 1] != 0; }
+    if (nan) m = NAN;
+    if (!(std::isfinite(m) && m > 0)) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "%s preconditioner produced invalid λmax = %g; check for zero or non-finite preconditioner entries", label, m);
+        h->err = buf;
+        return FEMB200_ELAMBDA;
+    }
+    out = m;
+    return FEMB200_OK;
+}
+
+template <class T, class TG>
+H27Args<T, TG> residual_args(const femb200_stokes_problem* p, double dt) {
+    H27Args<T, TG> a;
+    std::memset(&a, 0, sizeof(a));
+    a.el2n = p->el2n; a.dofsP = p->dofsP;
+    a.geo_v = static_cast<const TG*>(p->geo_v); a.geo_P = static_cast<const TG*>(p->geo_P);
+    for (int c = 0; c < 3; ++c) { a.v[c] = static_cast<const T*>(p->v[c]); a.Rv[c] = static_cast<T*>(p->Rv[c]); }
+    a.P = static_cast<const T*>(p->P);
+    const bool ip = p->P_old && p->P_old_layout == FEMB200_FIELD_IP;
+    a.P0 = static_cast<const T*>(p->P_old && !ip ? p->P_old : p->P0);
+    a.P_old_ip = ip ? static_cast<const T*>(p->P_old) : nullptr;
+    a.temp = static_cast<const T*>(p->T); a.temp0 = static_cast<const T*>(p->T0);
+    a.Q = static_cast<const T*>(p->Q); a.Pf = static_cast<const T*>(p->Pf);
+    a.gammaP = static_cast<const T*>(p->gammaP); a.MP = static_cast<const T*>(p->M_P);
+    a.RP = static_cast<T*>(p->RP);
+    a.phv = p->phases_v; a.phv_layout = p->phases_v_layout;
+    a.php = p->phases_P; a.php_layout = p->phases_P_layout;
+    const int nt = p->dim == 3 ? 6 : 3;
+    for (int c = 0; c < 6; ++c)
+        a.told[c] = (p->tau_old_layout == FEMB200_FIELD_IP && c < nt) ? static_cast<const T*>(p->tau_old[c]) : nullptr;
+    a.eta_ip = static_cast<const T*>(p->viscosity_ip);
+    a.nels = p->nels;
+    a.dt = (T)dt;
+    return a;
+}
+
+template <class T, class TG>
+int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H27Args<T, TG>& a) {
+    if (a.do_momentum)
+        for (int c = 0; c < p->dim; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(T) * p->nnodes, h->stream));
+    if (p->dim == 3) CK(launch_hex27_residual<T, TG>(a, h->num_sms, h->stream));
+    else CK(launch_q9_residual<T, TG>(a, h->stream));
+    return FEMB200_OK;
+}
+
+// Residual sweep: RP (+ Pnum) and, optionally, Rv.
+template <class T, class TG>
+int residual_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt, int with_pnum, int do_momentum,
+                   int write_RP) {
+    H27Args<T, TG> a = residual_args<T, TG>(p, dt);
+    a.with_pnum = with_pnum;
+    a.do_momentum = do_momentum;
+    a.write_RP = write_RP;
+    a.Pnum_out = with_pnum ? static_cast<T*>(p->Pnum) : nullptr;
+    if (!with_pnum && !write_RP && !do_momentum) return FEMB200_OK;
+    if ((write_RP || with_pnum) && !p->RP) { h->err = "RP is required"; return FEMB200_EINVAL; }
+    if (with_pnum && (!p->gammaP || !p->M_P)) { h->err = "γP and M_P are required for Pnum"; return FEMB200_EINVAL; }
+    if (do_momentum)
+        for (int c = 0; c < p->dim; ++c)
+            if (!p->Rv[c]) { h->err = "Rv is required"; return FEMB200_EINVAL; }
+    return launch_residual<T, TG>(h, p, a);
+}
+
+template <class T, class TG>
+int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt) {
+    H27JacArgs<T, TG> a;
+    std::memset(&a, 0, sizeof(a));
+    a.el2n = p->el2n; a.dofsP = p->dofsP;
+    a.geo_v = static_cast<const TG*>(p->geo_v); a.geo_P = static_cast<const TG*>(p->geo_P);
+    for (int c = 0; c < 3; ++c) {
+        a.v[c] = static_cast<const T*>(p->v[c]);
+        a.dRdv[c] = static_cast<T*>(p->dRdv[c]); a.PC[c] = static_cast<T*>(p->PC[c]);
+    }
+    a.P = static_cast<const T*>(p->P); a.P0 = static_cast<const T*>(p->P0);
+    a.temp = static_cast<const T*>(p->T); a.temp0 = static_cast<const T*>(p->T0);
+    a.Pf = static_cast<const T*>(p->Pf);
+    a.gammaP = static_cast<const T*>(p->gammaP); a.MP = static_cast<const T*>(p->M_P);
+    a.phv = p->phases_v; a.phv_layout = p->phases_v_layout;
+    a.php = p->phases_P; a.php_layout = p->phases_P_layout;
+    const int nt = p->dim == 3 ? 6 : 3;
+    for (int c = 0; c < 6; ++c)
+        a.told[c] = (p->tau_old_layout == FEMB200_FIELD_IP && c < nt) ? static_cast<const T*>(p->tau_old[c]) : nullptr;
+    a.eta_ip = static_cast<const T*>(p->viscosity_ip);
+    a.nels = p->nels;
+    a.dt = (T)dt;
+    for (int c = 0; c < p->dim; ++c) {
+        if (!p->dRdv[c] || !p->PC[c]) { h->err = "dRdv and PC are required"; return FEMB200_EINVAL; }
+        CK(cudaMemsetAsync(p->dRdv[c], 0, sizeof(T) * p->nnodes, h->stream));
+        CK(cudaMemsetAsync(p->PC[c], 0, sizeof(T) * p->nnodes, h->stream));
+    }
+    if (!p->gammaP || !p->M_P) { h->err = "γP and M_P are required by the augmented Jacobian"; return FEMB200_EINVAL; }
+    if (p->dim == 3) CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
+    else CK(launch_q9_jacobian<T, TG>(a, h->stream));
+    return FEMB200_OK;
+}
+
+template <class T, class TG>
+int pressure_scaling_impl(femb200_handle* h, const femb200_stokes_problem* p, double gfact, double dt) {
+    if (!p->M_P || !p->gammaP) { h->err = "M_P and γP are required"; return FEMB200_EINVAL; }
+    CK(cudaMemsetAsync(p->M_P, 0, sizeof(T) * p->nnodesP, h->stream));
+    CK(cudaMemsetAsync(p->gammaP, 0, sizeof(T) * p->nnodesP, h->stream));
+    const bool use_ip = p->viscosity_ip && !p->mat.use_scaling_eta;
+    CK(launch_pressure_scaling<T, TG>(p->dim, p->el2n, p->dofsP, static_cast<const TG*>(p->geo_P), p->phases_v,
+                                      p->phases_v_layout, static_cast<const T*>(p->viscosity_ip), use_ip ? 1 : 0,
+                                      static_cast<T*>(p->M_P), static_cast<T*>(p->gammaP), p->nels, p->nnodesP, (T)gfact,
+                                      (T)dt, h->stream));
+    return FEMB200_OK;
+}
+
+int build_mask(femb200_handle* h, const femb200_stokes_problem* p) {
+    const size_t n = (size_t)p->nnodes;
+    if (n > h->mask_cap) {
+        if (h->d_mask) cudaFree(h->d_mask);
+        h->d_mask = nullptr;
+        CK(cudaMalloc(&h->d_mask, n));
+        h->mask_cap = n;
+    }
+    CK(cudaMemsetAsync(h->d_mask, 0, n, h->stream));
+    for (int c = 0; c < p->dim; ++c)
+        if (p->bc_n[c] > 0) CK(launch_build_mask(h->d_mask, p->bc_dofs[c], p->bc_n[c], c, h->stream));
+    return FEMB200_OK;
+}
+
+inline double julia_eps(double x) { x = std::fabs(x); return std::nextafter(x, INFINITY) - x; }
+
+void cheb(double dtau, double lmin, double c_fact, double& a, double& b) {
+    const double c = 2 * std::sqrt(lmin) * c_fact;
+    a = 2 * dtau * dtau / (2 + c * dtau);
+    b = (2 - c * dtau) / (2 + c * dtau);
+}
+
+// Coupled thermal state (DR.jl:604-663).
+struct Coupled {
+    femb200_thermal_problem* t;
+    double Tref;
+    void* phi;
+};
+
+template <class T, class TG>
+int thermal_assemble(femb200_handle* h, const femb200_thermal_problem* t, double dt, double Tref, bool jac,
+                     const void* src_ip) {
+    ThermalArgs<T, TG> a;
+    std::memset(&a, 0, sizeof(a));
+    a.dim = t->dim; a.el2n = t->el2n; a.geo = static_cast<const TG*>(t->geo);
+    a.Tn = static_cast<const T*>(t->T); a.T0 = static_cast<const T*>(t->T0); a.P = static_cast<const T*>(t->P);
+    a.src = static_cast<const T*>(t->source); a.src_ip = static_cast<const T*>(src_ip);
+    a.ph = t->phases; a.ph_layout = t->phases_layout;
+    a.R = static_cast<T*>(t->R); a.dRdT = static_cast<T*>(t->dRdT); a.PC = static_cast<T*>(t->PC);
+    a.nels = t->nels; a.dt = (T)dt; a.Tref = (T)Tref; a.jac = jac ? 1 : 0;
+    CK(cudaMemsetAsync(t->R, 0, sizeof(T) * t->nnodes, h->stream));
+    if (jac) {
+        CK(cudaMemsetAsync(t->dRdT, 0, sizeof(T) * t->nnodes, h->stream));
+        CK(cudaMemsetAsync(t->PC, 0, sizeof(T) * t->nnodes, h->stream));
+    }
+    CK(launch_thermal<T, TG>(a, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+int upload_thermal_material(femb200_handle* h, const femb200_thermal_problem* t) {
+    static thread_local DevThermalMaterial d;
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) {
+        d.k[i] = t->k[i]; d.Cp[i] = t->Cp[i]; d.rho0[i] = t->rho0[i]; d.alpha[i] = t->alpha[i]; d.beta[i] = 1.0 / t->K[i];
+    }
+    CK(cudaMemcpyToSymbolAsync(c_tmat, &d, sizeof(d), 0, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FEMB200_OK;
+}
+
+int build_tmask(femb200_handle* h, const femb200_thermal_problem* t) {
+    const size_t n = (size_t)t->nnodes;
+    if (n > h->tmask_cap) {
+        if (h->d_tmask) cudaFree(h->d_tmask);
+        h->d_tmask = nullptr;
+        CK(cudaMalloc(&h->d_tmask, n));
+        h->tmask_cap = n;
+    }
+    CK(cudaMemsetAsync(h->d_tmask, 0, n, h->stream));
+    if (t->bc_n > 0) CK(launch_build_mask(h->d_tmask, t->bc_dofs, t->bc_n, 0, h->stream));
+    return FEMB200_OK;
+}
+
+// One thermal DR iteration of the coupled loop, and its check (DR.jl:604-663).
+struct ThermalIter {
+    int64_t iter = 0;
+    double err = INFINITY, a = 0, b = 0, lmax = 0, nr0 = 0;
+    bool converged = false;
+};
+
+template <class T, class TG>
+int shear_heating_impl(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi);
+
+template <class T, class TG>
+int thermal_coupled_step(femb200_handle* h, Coupled& cp, ThermalIter& ti, const femb200_stokes_problem* p, int64_t nout,
+                         double dt) {
+    femb200_thermal_problem* t = cp.t;
+    const int64_t n = t->nnodes;
+    ++ti.iter;
+    const bool check = ti.iter == 1 || ti.iter % nout == 0;
+    if (check) CK(launch_copy<T>(static_cast<T*>(t->R0), static_cast<const T*>(t->R), n, h->stream));
+    RC((thermal_assemble<T, TG>(h, t, dt, cp.Tref, check, cp.phi)));
+    if (check) {
+        // the Dirichlet rows of R are zeroed by the update kernel below; λmax reads J and PC only
+        RC(checked_lmax<T>(h, static_cast<const T*>(t->dRdT), static_cast<const T*>(t->PC), n, "thermal diffusion", ti.lmax));
+    }
+    CK(launch_thermal_update<T>(static_cast<T*>(t->T), static_cast<T*>(t->rate), static_cast<T*>(t->R),
+                                static_cast<const T*>(t->PC), h->d_tmask, n, ti.a, ti.b, h->stream));
+    if (t->bc_n > 0) CK(launch_dirichlet<T>(static_cast<T*>(t->T), t->bc_dofs, static_cast<const T*>(t->bc_vals), t->bc_n, h->stream));
+    CK(launch_transfer_temperature<T>(static_cast<T*>(p->T), static_cast<const T*>(t->T), p->dofsP, p->el2nP,
+                                      (int64_t)p->np * p->nels, h->stream));
+    if (check) {
+        const double dtau = 2 / std::sqrt(ti.lmax) * t->cfl;
+        const int b = red_blocks(h, n);
+        RC(ensure_partials(h, b));
+        CK(launch_lmin_sums<T>(static_cast<const T*>(t->rate), static_cast<const T*>(t->R), static_cast<const T*>(t->R0),
+                               static_cast<const T*>(t->PC), n, dtau, h->d_partials, b, h->stream));
+        double s[3];
+        RC(fetch_sums(h, b, 3, s));
+        const double nr = std::sqrt(s[2]);
+        if (ti.iter == 1) ti.nr0 = std::max(nr, julia_eps(nr));
+        ti.err = nr / ti.nr0;
+        if (!std::isfinite(ti.err)) {
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "non-finite thermal residual at coupled iteration %lld", (long long)ti.iter);
+            h->err = buf;
+            return FEMB200_ENONFINITE;
+        }
+        const double lmin = (ti.iter == 1 || s[0] == 0) ? 0.0 : std::fabs(s[1]) / s[0];
+        cheb(dtau, lmin, t->c_fact, ti.a, ti.b);
+        ti.converged = ti.err < t->eps;
+        if (cp.phi) RC((shear_heating_impl<T, TG>(h, p, dt, cp.phi)));
+    }
+    return FEMB200_OK;
+}
+
+template <class T, class TG>
+int shear_heating_impl(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) {
+    H27Args<T, TG> a = residual_args<T, TG>(p, dt);
+    a.phi = static_cast<T*>(phi);
+    a.do_momentum = 0; a.write_RP = 0; a.with_pnum = 0;
+    if (p->dim == 3) CK(launch_hex27_residual<T, TG>(a, h->num_sms, h->stream));
+    else CK(launch_q9_residual<T, TG>(a, h->stream));
+    return FEMB200_OK;
+}
+
+// _solve_stokes_dyrel! (src/stokes/solvers/DR.jl:348-802), device-resident.
+template <class T, class TG>
+int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
+                femb200_stokes_stats* st, Coupled* cp) {
+    const int D = p->dim;
+    const int64_t nn = p->nnodes, nP = p->nnodesP;
+    const double dt = c->dt;
+    const int finite_K = c->finite_K;
+    const bool freeze = c->freeze_jacobian < 0 ? (p->mat.plastic == 0) : (c->freeze_jacobian != 0);
+    const int64_t nout = c->check_interval > 0 ? c->check_interval : 50;
+    const double cfl = c->cfl_v > 0 ? c->cfl_v : 0.98, cf = c->c_fact > 0 ? c->c_fact : 0.9;
+    static const char* labels[3] = {"stokes vx", "stokes vy", "stokes vz"};
+    std::memset(st, 0, sizeof(*st));
+    for (int k = 0; k < D; ++k)
+        if (!p->rate[k] || !p->Rv0[k] || !p->Rv[k] || !p->PC[k] || !p->dRdv[k]) { h->err = "DR work arrays are required"; return FEMB200_EINVAL; }
+    if (!p->RP || !p->M_P || !p->gammaP || !p->Pnum) { h->err = "RP, M_P, γP and Pnum are required"; return FEMB200_EINVAL; }
+
+    RC(upload_material(h, p->mat, finite_K));
+    RC(build_mask(h, p));
+    for (int k = 0; k < D; ++k) {
+        CK(cudaMemsetAsync(p->rate[k], 0, sizeof(T) * nn, h->stream));
+        CK(cudaMemsetAsync(p->Rv0[k], 0, sizeof(T) * nn, h->stream));
+    }
+    RC((jacobian_sweep<T, TG>(h, p, dt)));
+    double lmax[3] = {0, 0, 0};
+    for (int k = 0; k < D; ++k)
+        RC(checked_lmax<T>(h, static_cast<const T*>(p->dRdv[k]), static_cast<const T*>(p->PC[k]), nn, labels[k], lmax[k]));
+    double lmax_g = *std::max_element(lmax, lmax + D);
+    int64_t jac_assemblies = 1;
+    double alpha[3] = {0, 0, 0}, beta[3] = {0, 0, 0}, dtau[3];
+    for (int k = 0; k < D; ++k) { dtau[k] = 2 / std::sqrt(lmax[k]) * cfl; cheb(dtau[k], 0.0, cf, alpha[k], beta[k]); }
+
+    double err_min = INFINITY, eps = c->tolerance;
+    double err = 2 * eps, err_abs = INFINITY, err_rel = INFINITY;
+    double err_v0 = 1.0, err_P0 = 1.0, err_v00 = 1.0, err_v = INFINITY, err_P = INFINITY;
+    int64_t iter = 0, itPH_done = 0, hist = 0;
+    bool converged = false;
+    double rel_drop = c->rel_drop0;
+    const double sq_nn = std::sqrt((double)nn), sq_nP = std::sqrt((double)nP);
+    auto push_hist = [&](double it, double ev, double eP, const double* comps) {
+        if (c->history && hist < c->history_capacity) {
+            double* hh = c->history + hist * (4 + D);
+            hh[0] = it; hh[1] = ev; hh[2] = eP; hh[3] = 0;
+            for (int k = 0; k < D; ++k) hh[4 + k] = comps[k];
+        }
+        ++hist;
+    };
+
+    ThermalIter ti;
+    bool thermal_converged = cp == nullptr;
+    if (cp) {
+        RC(upload_thermal_material(h, cp->t));
+        RC(build_tmask(h, cp->t));
+        CK(cudaMemsetAsync(cp->t->rate, 0, sizeof(T) * cp->t->nnodes, h->stream));
+        CK(cudaMemsetAsync(cp->t->R0, 0, sizeof(T) * cp->t->nnodes, h->stream));
+        if (cp->phi) RC((shear_heating_impl<T, TG>(h, p, dt, cp->phi)));
+    }
+
+    const int nb = red_blocks(h, nn);
+    RC(ensure_partials(h, std::max(nb, red_blocks(h, nP))));
+
+    auto apply_bc_R = [&]() -> int {
+        for (int k = 0; k < D; ++k) {
+            if (p->body_force[k]) CK(launch_sub<T>(static_cast<T*>(p->Rv[k]), static_cast<const T*>(p->body_force[k]), nn, h->stream));
+            if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(static_cast<T*>(p->Rv[k]), p->bc_dofs[k], nullptr, p->bc_n[k], h->stream));
+        }
+        return FEMB200_OK;
+    };
+
+    for (int64_t itPH = 1; itPH <= c->max_ph_iterations; ++itPH) {
+        itPH_done = itPH;
+        RC((residual_sweep<T, TG>(h, p, dt, 0, 1, 1)));
+        RC(apply_bc_R());
+        double sP;
+        RC(sumsq<T>(h, static_cast<const T*>(p->RP), static_cast<const T*>(p->M_P), nP, sP));
+        err_P = std::sqrt(sP) / sq_nP;
+        double comps[3] = {0, 0, 0};
+        err_v = 0;
+        for (int k = 0; k < D; ++k) {
+            double s;
+            RC(sumsq<T>(h, static_cast<const T*>(p->Rv[k]), (const T*)nullptr, nn, s));
+            comps[k] = std::sqrt(s) / (2 * sq_nn);
+            err_v = std::max(err_v, std::sqrt(s));
+        }
+        err_v /= 2 * sq_nn;
+        push_hist((double)iter, err_v, err_P, comps);
+        if (itPH == 1) { err_P0 = err_P + julia_eps(err_P); err_v0 = err_v + julia_eps(err_v); }
+        else if (itPH == 2) err_P0 = err_P + julia_eps(err_P);
+        const double err_v_rel = err_v / err_v0, err_P_rel = err_P / err_P0;
+        err_abs = std::max(err_v, err_P);
+        err_rel = std::max(err_v_rel, err_P_rel);
+        err = std::min(err_abs, err_rel);
+        if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_ENAN; }
+        if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_EKABOOM; }
+        if (err < eps && thermal_converged) { converged = true; break; }
+        if (err > err_min * 1.05) rel_drop = std::max(rel_drop * 0.1, 1.0e-3);
+        err_min = std::min(err_min, err);
+        const double eps_vel = err * rel_drop;
+        int64_t itPT = 0;
+        while ((err > eps_vel || !thermal_converged) && itPT <= c->iter_max) {
+            ++itPT; ++iter;
+            const bool do_check = iter % nout == 0;
+            if (do_check)
+                for (int k = 0; k < D; ++k) CK(launch_copy<T>(static_cast<T*>(p->Rv0[k]), static_cast<const T*>(p->Rv[k]), nn, h->stream));
+            if (cp) {
+                RC((thermal_coupled_step<T, TG>(h, *cp, ti, p, nout, dt)));
+                thermal_converged = ti.converged;
+            }
+            RC((residual_sweep<T, TG>(h, p, dt, 1, 1, 1)));
+            RC(apply_bc_R());
+            NodeArgs<T> na;
+            std::memset(&na, 0, sizeof(na));
+            for (int k = 0; k < 3; ++k) {
+                na.v[k] = static_cast<T*>(p->v[k]); na.rate[k] = static_cast<T*>(p->rate[k]);
+                na.Rv[k] = static_cast<T*>(p->Rv[k]); na.Rv0[k] = static_cast<T*>(p->Rv0[k]);
+                na.PC[k] = static_cast<const T*>(p->PC[k]);
+                na.alpha[k] = -alpha[k]; na.beta[k] = beta[k]; na.lam_step[k] = alpha[k];
+            }
+            na.mask = h->d_mask; na.n = nn; na.dim = D;
+            na.reduce = do_check ? 1 : 0;
+            na.partials = h->d_partials;
+            CK(launch_node_update<T>(na, nb, h->stream));
+            for (int k = 0; k < D; ++k)
+                if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(static_cast<T*>(p->v[k]), p->bc_dofs[k], static_cast<const T*>(p->bc_vals[k]), p->bc_n[k], h->stream));
+            if (do_check) {
+                double s[RED_SLOTS];
+                RC(fetch_sums(h, nb, RED_SLOTS, s));
+                double ev = 0, cmp[3] = {0, 0, 0};
+                for (int k = 0; k < D; ++k) { ev = std::max(ev, std::sqrt(s[3 * k])); cmp[k] = std::sqrt(s[3 * k]) / (2 * sq_nn); }
+                ev /= 2 * sq_nn;
+                if (iter == nout) err_v00 = ev + julia_eps(ev);
+                err = ev <= eps ? ev : std::max(ev / err_v00, ev);
+                if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_ENAN; }
+                if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_EKABOOM; }
+                if (c->history) {
+                    double sPc;
+                    RC(sumsq<T>(h, static_cast<const T*>(p->RP), static_cast<const T*>(p->M_P), nP, sPc));
+                    push_hist((double)iter, ev, std::sqrt(sPc) / sq_nP, cmp);
+                } else {
+                    ++hist;
+                }
+                double lmin[3];
+                for (int k = 0; k < D; ++k) lmin[k] = s[3 * k + 1] == 0 ? 0.0 : std::fabs(s[3 * k + 2]) / s[3 * k + 1];
+                if (!freeze) {
+                    ++jac_assemblies;
+                    RC((jacobian_sweep<T, TG>(h, p, dt)));
+                    for (int k = 0; k < D; ++k)
+                        RC(checked_lmax<T>(h, static_cast<const T*>(p->dRdv[k]), static_cast<const T*>(p->PC[k]), nn, labels[k], lmax[k]));
+                    lmax_g = *std::max_element(lmax, lmax + D);
+                }
+                for (int k = 0; k < D; ++k) { dtau[k] = 2 / std::sqrt(lmax[k]) * cfl; cheb(dtau[k], lmin[k], cf, alpha[k], beta[k]); }
+            }
+            if (iter > c->max_iterations) break;
+        }
+        CK(launch_pressure_update<T>(static_cast<T*>(p->P), static_cast<const T*>(p->gammaP), static_cast<const T*>(p->RP),
+                                     static_cast<const T*>(p->M_P), nP, h->stream));
+        if (iter > c->max_iterations) break;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    st->itPH = itPH_done; st->iter = iter; st->err = err; st->err_abs = err_abs; st->err_rel = err_rel;
+    st->err_v = err_v; st->err_P = err_P; st->converged = converged; st->reached_total_iter = iter > c->max_iterations;
+    st->lambda_max = *std::max_element(lmax, lmax + D); st->lambda_max_gershgorin = lmax_g;
+    st->jacobian_assemblies = jac_assemblies;
+    st->history_len = c->history ? std::min<int64_t>(hist, c->history_capacity) : 0;
+    st->err_T = cp ? ti.err : 0.0; st->thermal_iterations = ti.iter;
+    return FEMB200_OK;
+}
+
+int finish_solve(femb200_handle* h, const femb200_stokes_controls* c, femb200_stokes_stats* st) {
+    if (!st->converged && c->throw_on_failure) {
+        char b[256];
+        std::snprintf(b, sizeof b, "Stokes solve did not converge after %lld iterations (residual = %g, tolerance = %g)",
+                      (long long)st->iter, st->err_abs, c->tolerance);
+        h->err = b;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
+}
+
+// dtype dispatch
+template <template <class, class> class F, class... Args>
+int dispatch(const femb200_stokes_problem* p, Args&&... args) {
+    if (p->dtype == FEMB200_F64 && p->geo_dtype == FEMB200_F64) return F<double, double>::run(args...);
+    if (p->dtype == FEMB200_F32 && p->geo_dtype == FEMB200_F32) return F<float, float>::run(args...);
+    if (p->dtype == FEMB200_F64 && p->geo_dtype == FEMB200_F32) return F<double, float>::run(args...);
+    return F<float, double>::run(args...);
+}
+
+template <class T, class TG> struct DoResidual {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, int with_pnum, int do_momentum, int write_RP) {
+        return residual_sweep<T, TG>(h, p, dt, with_pnum, do_momentum, write_RP);
+    }
+};
+template <class T, class TG> struct DoMomentum {
+    // assemble_momentum_residual_kernel! with the caller's Pnum array (or none).
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, int with_pnum) {
+        H27Args<T, TG> a = residual_args<T, TG>(p, dt);
+        a.do_momentum = 1; a.write_RP = 0; a.with_pnum = with_pnum;
+        a.Pnum_in = with_pnum ? static_cast<const T*>(p->Pnum) : nullptr;
+        return launch_residual<T, TG>(h, p, a);
+    }
+};
+template <class T, class TG> struct DoJacobian {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt) { return jacobian_sweep<T, TG>(h, p, dt); }
+};
+template <class T, class TG> struct DoScaling {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double g, double dt) { return pressure_scaling_impl<T, TG>(h, p, g, dt); }
+};
+template <class T, class TG> struct DoStore {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt) {
+        H27Args<T, TG> a = residual_args<T, TG>(p, dt);
+        const int nt = p->dim == 3 ? 6 : 3;
+        for (int c = 0; c < nt; ++c) {
+            if (!p->tau[c]) { h->err = "tau output components are required"; return FEMB200_EINVAL; }
+            a.tau_store[c] = static_cast<T*>(p->tau[c]);
+        }
+        a.do_momentum = 1; a.write_RP = 0; a.with_pnum = 0;
+        a.eta_ip = nullptr;   // update_stokes_current_stress! uses dr.η (DR.jl:890)
+        return launch_residual<T, TG>(h, p, a);
+    }
+};
+template <class T, class TG> struct DoShear {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) { return shear_heating_impl<T, TG>(h, p, dt, phi); }
+};
+template <class T, class TG> struct DoSolve {
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c, femb200_stokes_stats* st, Coupled* cp) {
+        if (c->assemble_scaling) {
+            RC(upload_material(h, p->mat, c->finite_K));
+            RC((pressure_scaling_impl<T, TG>(h, p, c->pressure_factor, c->dt)));
+        }
+        RC((solve_dyrel<T, TG>(h, p, c, st, cp)));
+        return FEMB200_OK;
+    }
+};
+
+int check_controls(femb200_handle* h, const femb200_stokes_controls* c) {
+    if (!c) { h->err = "null controls"; return FEMB200_EINVAL; }
+    if (!(c->dt > 0)) { h->err = "dt must be positive"; return FEMB200_EINVAL; }
+    if (c->check_interval <= 0) { h->err = "check_interval must be positive"; return FEMB200_EINVAL; }
+    if (c->precision != FEMB200_PRECISION_FP64) { h->err = "this build runs the FP64 DR path only"; return FEMB200_EUNSUPPORTED; }
+    return FEMB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int femb200_create(femb200_handle** out) {
+    if (!out) return FEMB200_EINVAL;
+    femb200_handle* h = new femb200_handle();
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (e != cudaSuccess) {
+        delete h;
+        *out = nullptr;
+        return FEMB200_ECUDA;
+    }
+    int rc = ensure_tables(h);
+    if (rc) { delete h; *out = nullptr; return rc; }
+    *out = h;
+    return FEMB200_OK;
+}
+
+int femb200_destroy(femb200_handle* h) {
+    if (!h) return FEMB200_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->d_partials) cudaFree(h->d_partials);
+    if (h->h_partials) cudaFreeHost(h->h_partials);
+    if (h->d_mask) cudaFree(h->d_mask);
+    if (h->d_tmask) cudaFree(h->d_tmask);
+    delete h;
+    return FEMB200_OK;
+}
+
+int femb200_set_stream(femb200_handle* h, void* stream) {
+    if (!h) return FEMB200_EINVAL;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return FEMB200_OK;
+}
+
+const char* femb200_last_error(const femb200_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+const char* femb200_version(void) { return "libfemtools_b200 0.1 (sm_100a)"; }
+
+int femb200_pressure_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, finite_K));
+    return dispatch<DoResidual>(p, h, p, dt, 0, 0, 1);
+}
+
+int femb200_momentum_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t with_pnum) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, 0));
+    if (with_pnum && !p->Pnum) { h->err = "Pnum is required"; return FEMB200_EINVAL; }
+    return dispatch<DoMomentum>(p, h, p, dt, (int)with_pnum);
+}
+
+int femb200_stokes_residuals(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, finite_K));
+    return dispatch<DoResidual>(p, h, p, dt, 1, 1, 1);
+}
+
+int femb200_velocity_update(femb200_handle* h, const femb200_stokes_problem* p, const double* beta, const double* alpha) {
+    RC(check_problem(h, p));
+    if (!beta || !alpha) { h->err = "alpha and beta are required"; return FEMB200_EINVAL; }
+    auto go = [&](auto tag) -> int {
+        using T = decltype(tag);
+        NodeArgs<T> na;
+        std::memset(&na, 0, sizeof(na));
+        for (int k = 0; k < 3; ++k) {
+            na.v[k] = static_cast<T*>(p->v[k]); na.rate[k] = static_cast<T*>(p->rate[k]);
+            na.Rv[k] = static_cast<T*>(p->Rv[k]); na.PC[k] = static_cast<const T*>(p->PC[k]);
+            na.alpha[k] = k < p->dim ? alpha[k] : 0; na.beta[k] = k < p->dim ? beta[k] : 0;
+        }
+        na.mask = nullptr; na.n = p->nnodes; na.dim = p->dim; na.reduce = 0;
+        CK(launch_node_update<T>(na, red_blocks(h, p->nnodes), h->stream));
+        return FEMB200_OK;
+    };
+    return p->dtype == FEMB200_F64 ? go(double()) : go(float());
+}
+
+int femb200_apply_dirichlet(femb200_handle* h, void* x, const int32_t* dofs, const void* vals, int64_t n, int32_t dtype) {
+    if (!h) return FEMB200_EINVAL;
+    if (n == 0) return FEMB200_OK;
+    if (!x || !dofs) { h->err = "x and dofs are required"; return FEMB200_EINVAL; }
+    if (dtype == FEMB200_F64) CK(launch_dirichlet<double>(static_cast<double*>(x), dofs, static_cast<const double*>(vals), n, h->stream));
+    else CK(launch_dirichlet<float>(static_cast<float*>(x), dofs, static_cast<const float*>(vals), n, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_jacobian_diagnostics(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, finite_K));
+    return dispatch<DoJacobian>(p, h, p, dt);
+}
+
+int femb200_pressure_scaling(femb200_handle* h, const femb200_stokes_problem* p, double gamma_fact, double dt, int32_t finite_K) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, finite_K));
+    return dispatch<DoScaling>(p, h, p, gamma_fact, dt);
+}
+
+int femb200_store_stress(femb200_handle* h, const femb200_stokes_problem* p, double dt) {
+    RC(check_problem(h, p));
+    RC(upload_material(h, p->mat, 0));
+    return dispatch<DoStore>(p, h, p, dt);
+}
+
+int femb200_shear_heating(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) {
+    RC(check_problem(h, p));
+    if (!phi) { h->err = "phi is required"; return FEMB200_EINVAL; }
+    RC(upload_material(h, p->mat, 0));
+    return dispatch<DoShear>(p, h, p, dt, phi);
+}
+
+int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
+                         femb200_stokes_stats* st) {
+    RC(check_problem(h, p));
+    RC(check_controls(h, c));
+    if (!st) { h->err = "null stats"; return FEMB200_EINVAL; }
+    RC(dispatch<DoSolve>(p, h, p, c, st, (Coupled*)nullptr));
+    return finish_solve(h, c, st);
+}
+
+int femb200_transfer_temperature(femb200_handle* h, void* TP, const void* Tn, const int32_t* dofsP, const int32_t* el2nP,
+                                 int64_t n, int32_t dtype) {
+    if (!h) return FEMB200_EINVAL;
+    if (dtype == FEMB200_F64) CK(launch_transfer_temperature<double>(static_cast<double*>(TP), static_cast<const double*>(Tn), dofsP, el2nP, n, h->stream));
+    else CK(launch_transfer_temperature<float>(static_cast<float*>(TP), static_cast<const float*>(Tn), dofsP, el2nP, n, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_thermal_residual(femb200_handle* h, const femb200_thermal_problem* t, double dt, double Tref, int32_t jac) {
+    if (!h || !t) return FEMB200_EINVAL;
+    RC(ensure_tables(h));
+    RC(upload_thermal_material(h, t));
+    if (t->dtype == FEMB200_F64) return thermal_assemble<double, double>(h, t, dt, Tref, jac != 0, t->source_ip);
+    return thermal_assemble<float, float>(h, t, dt, Tref, jac != 0, t->source_ip);
+}
+
+int femb200_solve_thermal(femb200_handle* h, const femb200_thermal_problem* t, const femb200_thermal_controls* c,
+                          femb200_thermal_stats* st) {
+    if (!h || !t || !c || !st) return FEMB200_EINVAL;
+    if (t->dtype != FEMB200_F64 || t->geo_dtype != FEMB200_F64) { h->err = "the thermal solver runs in FP64"; return FEMB200_EUNSUPPORTED; }
+    using T = double;
+    RC(upload_thermal_material(h, t));
+    RC(build_tmask(h, t));
+    const int64_t n = t->nnodes;
+    double a = 0, b = 0, nr0 = 0, last = NAN, lmax = 0;
+    const int nbk = red_blocks(h, n);
+    RC(ensure_partials(h, nbk));
+    for (int64_t it = 1; it <= c->max_iterations; ++it) {
+        const bool dj = (it % c->check_interval == 0) || it == 1;
+        if (dj) CK(launch_copy<T>(static_cast<T*>(t->R0), static_cast<const T*>(t->R), n, h->stream));
+        RC((thermal_assemble<T, T>(h, t, c->dt, c->Tref, dj, t->source_ip)));
+        if (dj) RC(checked_lmax<T>(h, static_cast<const T*>(t->dRdT), static_cast<const T*>(t->PC), n, "thermal diffusion", lmax));
+        CK(launch_thermal_update<T>(static_cast<T*>(t->T), static_cast<T*>(t->rate), static_cast<T*>(t->R),
+                                    static_cast<const T*>(t->PC), h->d_tmask, n, a, b, h->stream));
+        if (t->bc_n > 0) CK(launch_dirichlet<T>(static_cast<T*>(t->T), t->bc_dofs, static_cast<const T*>(t->bc_vals), t->bc_n, h->stream));
+        if (dj) {
+            const double dtau = 2 / std::sqrt(lmax) * t->cfl;
+            CK(launch_lmin_sums<T>(static_cast<const T*>(t->rate), static_cast<const T*>(t->R), static_cast<const T*>(t->R0),
+                                   static_cast<const T*>(t->PC), n, dtau, h->d_partials, nbk, h->stream));
+            double s[3];
+            RC(fetch_sums(h, nbk, 3, s));
+            const double nr = std::sqrt(s[2]);
+            if (it == 1) nr0 = std::max(nr, julia_eps(nr));
+            if (std::isnan(nr / nr0)) { char bb[64]; std::snprintf(bb, sizeof bb, "NaNs at PT iter %lld", (long long)it); h->err = bb; return FEMB200_ENAN; }
+            const double lmin = (it == 1 || s[0] == 0) ? 0.0 : std::fabs(s[1]) / s[0];
+            cheb(dtau, lmin, t->c_fact, a, b);
+            last = nr / nr0;
+            if (last < c->tolerance) { st->converged = 1; st->iterations = it; st->residual = last; return FEMB200_OK; }
+        }
+    }
+    st->converged = 0; st->iterations = c->max_iterations; st->residual = last;
+    if (c->throw_on_failure) {
+        char bb[256];
+        std::snprintf(bb, sizeof bb, "Thermal diffusion DR solver did not converge after %lld pseudo-transient iterations (relative residual = %g)",
+                      (long long)c->max_iterations, last);
+        h->err = bb;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
+}
+
+int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t, const femb200_stokes_problem* p,
+                          const femb200_stokes_controls* c, double Tref, int32_t shear_heating, void* phi_scratch,
+                          femb200_stokes_stats* st) {
+    RC(check_problem(h, p));
+    RC(check_controls(h, c));
+    if (!t || !st) { h->err = "thermal problem and stats are required"; return FEMB200_EINVAL; }
+    if (t->nnodes != p->nnodes) { h->err = "thermal mesh nodes must match the Stokes velocity-node layout"; return FEMB200_EINVAL; }
+    if (t->dtype != p->dtype) { h->err = "thermal and Stokes states must share a precision"; return FEMB200_EINVAL; }
+    if (shear_heating && !phi_scratch) { h->err = "shear heating needs an nq × nels scratch array"; return FEMB200_EINVAL; }
+    const int64_t ntr = (int64_t)p->np * p->nels;
+    if (p->dtype == FEMB200_F64) {
+        CK(launch_transfer_temperature<double>(static_cast<double*>(p->T), static_cast<const double*>(t->T), p->dofsP, p->el2nP, ntr, h->stream));
+        CK(launch_transfer_temperature<double>(static_cast<double*>(p->T0), static_cast<const double*>(t->T0), p->dofsP, p->el2nP, ntr, h->stream));
+        if (shear_heating) CK(cudaMemsetAsync(phi_scratch, 0, sizeof(double) * p->nq * p->nels, h->stream));
+    } else {
+        CK(launch_transfer_temperature<float>(static_cast<float*>(p->T), static_cast<const float*>(t->T), p->dofsP, p->el2nP, ntr, h->stream));
+        CK(launch_transfer_temperature<float>(static_cast<float*>(p->T0), static_cast<const float*>(t->T0), p->dofsP, p->el2nP, ntr, h->stream));
+        if (shear_heating) CK(cudaMemsetAsync(phi_scratch, 0, sizeof(float) * p->nq * p->nels, h->stream));
+    }
+    Coupled cp{t, Tref, shear_heating ? phi_scratch : nullptr};
+    RC(dispatch<DoSolve>(p, h, p, c, st, &cp));
+    return finish_solve(h, c, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,152 @@
+// hex27.cuh — sum-factorised Hex27/P1-disc element machinery.
+//
+// Mapping: a warp processes three elements at a time; lanes 0..26 form three
+// groups of nine ("line threads"), lanes 27..31 idle. Thread m = m1 + 3·m2 of a
+// group owns one tensor line of the 3×3×3 node/quadrature grid, so every 1-D
+// contraction of the tensor-product basis runs in registers and only the
+// re-orientation between directions goes through shared memory (warp-local,
+// ordered by __syncwarp). This replaces the reference's thread-per-element
+// loops over 27 quadrature points × 27 nodes (momentum_residuals.jl:231-256)
+// with ~1/3 of the floating-point work.
+//
+// Orientation of the owned line per stage:
+//   gather / scatter : x-line (·, m1, m2)  — contiguous node runs in memory
+//   after stage Y    : y-line (m1, ·, m2)
+//   quadrature stage : z-line (m1, m2, ·)  — quadrature points q = m1 + 3m2 + 9qz
+#pragma once
+#include "common.cuh"
+
+namespace femb {
+
+constexpr int H27_ELEM_SMEM = 540;   // scalars of stage scratch per element
+
+FEMB_D int tidx(int i, int j, int k) { return i + 3 * j + 9 * k; }
+
+template <class T>
+struct Tab1D {
+    T B[3][3], Dd[3][3];
+    FEMB_D void load() {
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) { B[q][i] = (T)c_tab.B[q][i]; Dd[q][i] = (T)c_tab.Dd[q][i]; }
+    }
+};
+
+// Reference gradients of the three velocity components at the three quadrature
+// points of the owned z-line. v[c][i]: node values on the owned x-line.
+// Output g[c][d][qz], d = ξ, η, ζ.
+template <class T>
+FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m2, T g[3][3][3]) {
+    // stage X: contract x (thread owns x-line (·, m1, m2))
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            T x0 = t.B[q][0] * v[c][0] + t.B[q][1] * v[c][1] + t.B[q][2] * v[c][2];
+            T x1 = t.Dd[q][0] * v[c][0] + t.Dd[q][1] * v[c][1] + t.Dd[q][2] * v[c][2];
+            E[(c * 2 + 0) * 27 + tidx(q, m1, m2)] = x0;
+            E[(c * 2 + 1) * 27 + tidx(q, m1, m2)] = x1;
+        }
+    __syncwarp();
+    // stage Y: thread owns y-line (qx = m1, ·, k = m2)
+    T* E1 = E + 162;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T X0[3], X1[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) { X0[j] = E[(c * 2 + 0) * 27 + tidx(m1, j, m2)]; X1[j] = E[(c * 2 + 1) * 27 + tidx(m1, j, m2)]; }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            E1[(c * 3 + 0) * 27 + tidx(m1, q, m2)] = t.B[q][0] * X1[0] + t.B[q][1] * X1[1] + t.B[q][2] * X1[2];
+            E1[(c * 3 + 1) * 27 + tidx(m1, q, m2)] = t.Dd[q][0] * X0[0] + t.Dd[q][1] * X0[1] + t.Dd[q][2] * X0[2];
+            E1[(c * 3 + 2) * 27 + tidx(m1, q, m2)] = t.B[q][0] * X0[0] + t.B[q][1] * X0[1] + t.B[q][2] * X0[2];
+        }
+    }
+    __syncwarp();
+    // stage Z: thread owns z-line (qx = m1, qy = m2, ·)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T A[3], Bv[3], Cv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            A[k] = E1[(c * 3 + 0) * 27 + tidx(m1, m2, k)];
+            Bv[k] = E1[(c * 3 + 1) * 27 + tidx(m1, m2, k)];
+            Cv[k] = E1[(c * 3 + 2) * 27 + tidx(m1, m2, k)];
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            g[c][0][q] = t.B[q][0] * A[0] + t.B[q][1] * A[1] + t.B[q][2] * A[2];
+            g[c][1][q] = t.B[q][0] * Bv[0] + t.B[q][1] * Bv[1] + t.B[q][2] * Bv[2];
+            g[c][2][q] = t.Dd[q][0] * Cv[0] + t.Dd[q][1] * Cv[1] + t.Dd[q][2] * Cv[2];
+        }
+    }
+    __syncwarp();
+}
+
+// Transposed contraction: nodal residual R[c][ix] on the owned x-line from the
+// reference-frame fluxes F[c][d][qz] and the body-force density beta[qz]
+// (R_c(a) = Σ_q Σ_d ∂_d N_a(q) F_cd(q) − g_c Σ_q N_a(q) β(q)).
+template <class T>
+FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3], const T gvec[3], T* E,
+                          int m1, int m2, T R[3][3]) {
+    // Z^T: thread owns z-line (qx = m1, qy = m2)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            E[(c * 3 + 0) * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * F[c][0][0] + t.B[1][iz] * F[c][0][1] + t.B[2][iz] * F[c][0][2];
+            E[(c * 3 + 1) * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * F[c][1][0] + t.B[1][iz] * F[c][1][1] + t.B[2][iz] * F[c][1][2];
+            E[(c * 3 + 2) * 27 + tidx(m1, m2, iz)] = t.Dd[0][iz] * F[c][2][0] + t.Dd[1][iz] * F[c][2][1] + t.Dd[2][iz] * F[c][2][2];
+        }
+#pragma unroll
+    for (int iz = 0; iz < 3; ++iz)
+        E[9 * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
+    __syncwarp();
+    // Y^T: thread owns y-line (qx = m1, ·, iz = m2)
+    T* E1 = E + 270;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T TA[3], TB[3], TC[3];
+#pragma unroll
+        for (int qy = 0; qy < 3; ++qy) {
+            TA[qy] = E[(c * 3 + 0) * 27 + tidx(m1, qy, m2)];
+            TB[qy] = E[(c * 3 + 1) * 27 + tidx(m1, qy, m2)];
+            TC[qy] = E[(c * 3 + 2) * 27 + tidx(m1, qy, m2)];
+        }
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            E1[(c * 2 + 0) * 27 + tidx(m1, iy, m2)] = t.B[0][iy] * TA[0] + t.B[1][iy] * TA[1] + t.B[2][iy] * TA[2];
+            E1[(c * 2 + 1) * 27 + tidx(m1, iy, m2)] = (t.Dd[0][iy] * TB[0] + t.Dd[1][iy] * TB[1] + t.Dd[2][iy] * TB[2]) +
+                                                       (t.B[0][iy] * TC[0] + t.B[1][iy] * TC[1] + t.B[2][iy] * TC[2]);
+        }
+    }
+    {
+        T TD[3];
+#pragma unroll
+        for (int qy = 0; qy < 3; ++qy) TD[qy] = E[9 * 27 + tidx(m1, qy, m2)];
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) E1[6 * 27 + tidx(m1, iy, m2)] = t.B[0][iy] * TD[0] + t.B[1][iy] * TD[1] + t.B[2][iy] * TD[2];
+    }
+    __syncwarp();
+    // X^T: thread owns x-line (·, iy = m1, iz = m2)
+    T UD[3];
+#pragma unroll
+    for (int qx = 0; qx < 3; ++qx) UD[qx] = E1[6 * 27 + tidx(qx, m1, m2)];
+    T body[3];
+#pragma unroll
+    for (int ix = 0; ix < 3; ++ix) body[ix] = t.B[0][ix] * UD[0] + t.B[1][ix] * UD[1] + t.B[2][ix] * UD[2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T UA[3], UB[3];
+#pragma unroll
+        for (int qx = 0; qx < 3; ++qx) { UA[qx] = E1[(c * 2 + 0) * 27 + tidx(qx, m1, m2)]; UB[qx] = E1[(c * 2 + 1) * 27 + tidx(qx, m1, m2)]; }
+#pragma unroll
+        for (int ix = 0; ix < 3; ++ix)
+            R[c][ix] = (t.Dd[0][ix] * UA[0] + t.Dd[1][ix] * UA[1] + t.Dd[2][ix] * UA[2]) +
+                       (t.B[0][ix] * UB[0] + t.B[1][ix] * UB[1] + t.B[2][ix] * UB[2]) - gvec[c] * body[ix];
+    }
+    __syncwarp();
+}
+
+}  // namespace femb

@@ -1,0 +1,323 @@
+// jacobian3d.cu — augmented momentum-Jacobian diagnostics for Hex27/P1-disc.
+//
+// Restates assemble_augmented_momentum_jacobian_matrices_atomix!
+// (src/stokes/assemblers/momentum_residuals.jl:998-1117): per element, the
+// Jacobian of the momentum residual with Pnum = γP·RP(v)/M_P formed inline,
+// evaluated with the element-max viscosity η_pc; its L1 row sums over all
+// direction blocks go to dRdv and the |diagonal| of the same-direction block to
+// PC. The reference differentiates with ForwardDiff; here each of the 81 columns
+// is the exact directional derivative of the same expressions (the linearised
+// Maxwell stress and Drucker–Prager return, rheology.jl:441-472), pushed through
+// the sum-factorised transposed contraction. Line threads own fixed rows, so the
+// row sums accumulate in registers without cross-thread reduction.
+#include "kernels.cuh"
+#include "hex27.cuh"
+
+namespace femb {
+
+constexpr int JAC_THREADS = 64;                // 2 warps, 6 elements per block
+constexpr int JAC_GEO = 27 * 11;               // J⁻¹ (9), dΩ, dΩ_P per point
+constexpr int JAC_BP = 4 * 81;                 // ∂RP_p/∂v_(b,j)
+constexpr int JAC_ELEM = H27_ELEM_SMEM + JAC_GEO + JAC_BP;
+
+template <class T, class TG>
+__global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<T, TG> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_ok = lane < 27;
+    const int s = lane_ok ? lane / 9 : 0, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 3 + s) * JAC_ELEM;
+    T* GEO = E + H27_ELEM_SMEM;
+    T* BP = GEO + JAC_GEO;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 3 * JAC_ELEM) + (warp * 3 + s) * 28;
+
+    Tab1D<T> tb; tb.load();
+    const T dt = a.dt;
+    const bool plastic = c_mat.plastic != 0;
+    const T EPS2 = eps2<T>();
+    const T zero3[3] = {T(0), T(0), T(0)};
+
+    const int64_t stride = (int64_t)gridDim.x * wpb * 3;
+    for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
+        const int64_t e = base + s;
+        const bool act = lane_ok && e < a.nels;
+        const int64_t ec = act ? e : 0;
+
+        int node[3];
+        T v[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            node[i] = act ? __ldg(a.el2n + 27 * ec + c_tab.tn3[tidx(i, m1, m2)]) - 1 : 0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c][i] = act ? ld(a.v[c] + node[i]) : T(0);
+        }
+        // phases: always staged so that the element maximum can be formed
+        int p0 = 0;
+        bool uniform = true;
+        if (a.phv_layout == FEMB200_PHASE_CELL || !a.phv) {
+            p0 = a.phv ? (act ? __ldg(a.phv + ec) - 1 : 0) : 0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) PH[tidx(i, m1, m2)] = p0;
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int li = c_tab.tn3[tidx(i, m1, m2)];
+                PH[tidx(i, m1, m2)] = act ? phase_of(a.phv, a.phv_layout, (int64_t)node[i] + 1, li, ec, 27) : 0;
+            }
+            __syncwarp();
+            p0 = PH[0];
+            bool same = PH[tidx(0, m1, m2)] == p0 && PH[tidx(1, m1, m2)] == p0 && PH[tidx(2, m1, m2)] == p0;
+            const unsigned bal = __ballot_sync(0xffffffffu, same || !lane_ok);
+            uniform = ((bal >> (s * 9)) & 0x1ffu) == 0x1ffu;
+        }
+        int dof[4];
+        T Pl[4], Pfl[4], gam[4], MPl[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            dof[p] = act ? __ldg(a.dofsP + 4 * ec + p) - 1 : 0;
+            Pl[p] = act ? ld(a.P + dof[p]) : T(0);
+            Pfl[p] = (act && a.Pf) ? ld(a.Pf + dof[p]) : T(0);
+            gam[p] = (act && a.gammaP) ? ld(a.gammaP + dof[p]) : T(0);
+            MPl[p] = (act && a.MP) ? ld(a.MP + dof[p]) : T(1);
+        }
+        // geometry of all 27 points of the element into shared memory
+#pragma unroll
+        for (int qz = 0; qz < 3; ++qz) {
+            const int q = tidx(m1, m2, qz);
+            const TG* G = a.geo_v + ((int64_t)ec * 27 + q) * 10;
+#pragma unroll
+            for (int r = 0; r < 10; ++r) GEO[q * 11 + r] = act ? (T)ld(G + r) : T(0);
+            GEO[q * 11 + 10] = act ? (T)ld(a.geo_P + (int64_t)ec * 27 + q) : T(0);
+        }
+        // element-max viscosity η_pc (_element_max_phase_property, momentum_residuals.jl:36-44)
+        T eta_pc;
+        bool eta_scalar = false;
+        if (a.eta_ip) {
+            T mx = T(-INFINITY);
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) mx = fmax(mx, act ? ld(a.eta_ip + ec * 27 + tidx(m1, m2, qz)) : T(-INFINITY));
+            E[460 + m] = mx;
+            __syncwarp();
+            mx = E[460];
+            for (int t = 1; t < 9; ++t) mx = fmax(mx, E[460 + t]);
+            __syncwarp();
+            eta_pc = mx;
+            eta_scalar = true;
+        } else {
+            T mx = (T)c_mat.eta[PH[0]];
+            for (int t = 1; t < 27; ++t) mx = fmax(mx, (T)c_mat.eta[PH[t]]);
+            eta_pc = mx;
+        }
+
+        T g[3][3][3];
+        h27_gradient(tb, v, E, m1, m2, g);
+
+        // primal state at the owned points with η_pc
+        T pe[3], plam[3], ptt[3][6], ptII[3], ptIIs[3], pden[3];
+#pragma unroll
+        for (int qz = 0; qz < 3; ++qz) {
+            const int q = tidx(m1, m2, qz);
+            const T* Ji = GEO + q * 11;
+            T gq[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) gq[c][k] = g[c][0][qz] * Ji[0 + 3 * k] + g[c][1][qz] * Ji[1 + 3 * k] + g[c][2][qz] * Ji[2 + 3 * k];
+            const T sN = (T)c_tab.sumN3[q];
+            T invG, cphi = 0, sphi = 0, spsi = 0, C = 0, ereg = 0, Kb = 0;
+            if (uniform) {
+                invG = (T)c_mat.invG[p0] * sN;
+                if (plastic) {
+                    cphi = (T)c_mat.cos_phi[p0] * sN; sphi = (T)c_mat.sin_phi[p0] * sN; spsi = (T)c_mat.sin_psi[p0] * sN;
+                    C = (T)c_mat.C[p0] * sN; ereg = (T)c_mat.eta_reg[p0] * sN; Kb = (T)c_mat.Kb[p0] * sN;
+                }
+            } else {
+                invG = T(0);
+                for (int kk = 0; kk < 3; ++kk)
+                    for (int jj = 0; jj < 3; ++jj)
+                        for (int ii = 0; ii < 3; ++ii) {
+                            const T N = tb.B[m1][ii] * tb.B[m2][jj] * tb.B[qz][kk];
+                            const int p = PH[tidx(ii, jj, kk)];
+                            invG += N * (T)c_mat.invG[p];
+                            if (plastic) {
+                                cphi += N * (T)c_mat.cos_phi[p]; sphi += N * (T)c_mat.sin_phi[p];
+                                spsi += N * (T)c_mat.sin_psi[p]; C += N * (T)c_mat.C[p];
+                                ereg += N * (T)c_mat.eta_reg[p]; Kb += N * (T)c_mat.Kb[p];
+                            }
+                        }
+            }
+            const T etaq = eta_scalar ? eta_pc : eta_pc * sN;
+            const T etave = T(1) / (T(1) / etaq + invG / dt);
+            const T inv2Gdt = invG / (T(2) * dt);
+            const T tr = (gq[0][0] + gq[1][1] + gq[2][2]) / T(3);
+            const T eps_[6] = {gq[0][0] - tr, gq[1][1] - tr, gq[2][2] - tr, (gq[0][1] + gq[1][0]) / T(2),
+                               (gq[0][2] + gq[2][0]) / T(2), (gq[1][2] + gq[2][1]) / T(2)};
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const T to = (act && a.told[c]) ? ld(a.told[c] + ec * 27 + q) : T(0);
+                ptt[qz][c] = (T(2) * etave) * (eps_[c] + to * inv2Gdt);
+            }
+            pe[qz] = etave;
+            plam[qz] = T(0);
+            ptII[qz] = T(1); ptIIs[qz] = T(1); pden[qz] = T(1);
+            if (plastic) {
+                T Pq = T(0), Pfq = T(0);
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const T xi = (T)c_tab.qx[m1], et = (T)c_tab.qx[m2], ze = (T)c_tab.qx[qz];
+                    const T NP = p == 0 ? T(1) - xi - et - ze : (p == 1 ? xi : (p == 2 ? et : ze));
+                    Pq += NP * Pl[p]; Pfq += NP * Pfl[p];
+                }
+                const T Peq = a.Pf ? Pq - Pfq : Pq;
+                const T* t = ptt[qz];
+                const T tII = sqrt((t[0] * t[0] + t[1] * t[1] + t[2] * t[2]) / T(2) + t[3] * t[3] + t[4] * t[4] + t[5] * t[5] + EPS2);
+                const T Fy = tII - cphi * C - sphi * Peq;
+                const T den = etave + ereg + Kb * dt * (-spsi) * (-sphi);
+                const T lam = Fy > T(0) ? Fy / den : T(0);
+                plam[qz] = lam; ptII[qz] = tII; ptIIs[qz] = tII + EPS2; pden[qz] = den;
+            }
+        }
+
+        // ∂RP_p/∂v_(b,j) = −Σ_q NP_p(q) ∂_j N_b(q) dΩ_P(q) for every column, via the
+        // transposed contraction with a unit "pressure" flux per p.
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p) {
+            T Fp[3][3][3];
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) {
+                const int q = tidx(m1, m2, qz);
+                const T* Ji = GEO + q * 11;
+                const T xi = (T)c_tab.qx[m1], et = (T)c_tab.qx[m2], ze = (T)c_tab.qx[qz];
+                const T NP = p == 0 ? T(1) - xi - et - ze : (p == 1 ? xi : (p == 2 ? et : ze));
+                const T w = -NP * Ji[10];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) Fp[c][d][qz] = w * Ji[d + 3 * c];
+            }
+            T Rp[3][3];
+            h27_transpose(tb, Fp, zero3, zero3, E, m1, m2, Rp);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) BP[p * 81 + tidx(i, m1, m2) * 3 + c] = Rp[c][i] * gam[p] / MPl[p];
+        }
+        __syncwarp();
+
+        T rows[3][3], diag[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) { rows[c][i] = T(0); diag[c][i] = T(0); }
+
+#pragma unroll 1
+        for (int b = 0; b < 27; ++b) {
+            const int bx = b % 3, by = (b / 3) % 3, bz = b / 9;
+#pragma unroll 1
+            for (int j = 0; j < 3; ++j) {
+                const int col = b * 3 + j;
+                const T dPn0 = BP[0 * 81 + col], dPn1 = BP[1 * 81 + col], dPn2 = BP[2 * 81 + col], dPn3 = BP[3 * 81 + col];
+                T Fd[3][3][3];
+#pragma unroll
+                for (int qz = 0; qz < 3; ++qz) {
+                    const int q = tidx(m1, m2, qz);
+                    const T* Ji = GEO + q * 11;
+                    const T rx = tb.Dd[m1][bx] * tb.B[m2][by] * tb.B[qz][bz];
+                    const T ry = tb.B[m1][bx] * tb.Dd[m2][by] * tb.B[qz][bz];
+                    const T rz = tb.B[m1][bx] * tb.B[m2][by] * tb.Dd[qz][bz];
+                    T dn[3];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) dn[k] = rx * Ji[0 + 3 * k] + ry * Ji[1 + 3 * k] + rz * Ji[2 + 3 * k];
+                    // δg[i][k] = δ_ij dn[k]
+                    T dg[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) dg[i][k] = (i == j) ? dn[k] : T(0);
+                    const T tr = (dg[0][0] + dg[1][1] + dg[2][2]) / T(3);
+                    const T de[6] = {dg[0][0] - tr, dg[1][1] - tr, dg[2][2] - tr, (dg[0][1] + dg[1][0]) / T(2),
+                                     (dg[0][2] + dg[2][0]) / T(2), (dg[1][2] + dg[2][1]) / T(2)};
+                    const T two_e = T(2) * pe[qz];
+                    T dt_[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) dt_[c] = two_e * de[c];
+                    T dtau[6];
+                    if (plam[qz] > T(0)) {
+                        const T* t = ptt[qz];
+                        const T tII = ptII[qz], tIIs = ptIIs[qz];
+                        const T dtII = (t[0] * dt_[0] + t[1] * dt_[1] + t[2] * dt_[2]) / (T(2) * tII) +
+                                       (t[3] * dt_[3] + t[4] * dt_[4] + t[5] * dt_[5]) / tII;
+                        const T dlam = dtII / pden[qz];
+                        const T lam = plam[qz];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) {
+                            const T fac = c < 3 ? T(2) * tIIs : tIIs;
+                            const T mq = t[c] / fac;
+                            const T dm = dt_[c] / fac - t[c] * dtII / (fac * tIIs);
+                            dtau[c] = dt_[c] - two_e * (dlam * mq + lam * dm);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) dtau[c] = dt_[c];
+                    }
+                    const T xi = (T)c_tab.qx[m1], et = (T)c_tab.qx[m2], ze = (T)c_tab.qx[qz];
+                    const T dPn = (T(1) - xi - et - ze) * dPn0 + xi * dPn1 + et * dPn2 + ze * dPn3;
+                    const T sg[3][3] = {{dtau[0] - dPn, dtau[3], dtau[4]}, {dtau[3], dtau[1] - dPn, dtau[5]},
+                                        {dtau[4], dtau[5], dtau[2] - dPn}};
+                    const T dOq = Ji[9];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                            Fd[c][d][qz] = dOq * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
+                }
+                T dR[3][3];
+                h27_transpose(tb, Fd, zero3, zero3, E, m1, m2, dR);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        rows[c][i] += fabs(dR[c][i]);
+                        if (c == j && tidx(i, m1, m2) == b) diag[c][i] = fabs(dR[c][i]);
+                    }
+            }
+        }
+        if (act) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    atomic_add(a.dRdv[c] + node[i], rows[c][i]);
+                    atomic_add(a.PC[c] + node[i], diag[c][i]);
+                }
+        }
+        __syncwarp();
+    }
+}
+
+template <class T, class TG>
+cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st) {
+    const int wpb = JAC_THREADS / 32;
+    const size_t smem = (size_t)wpb * 3 * JAC_ELEM * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+    }
+    const int64_t groups = (args.nels + 2) / 3;
+    int64_t blocks = (groups + wpb - 1) / wpb;
+    const int64_t cap = (int64_t)num_sms * 32;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    hex27_jacobian_kernel<T, TG><<<(unsigned)blocks, JAC_THREADS, smem, st>>>(args);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_hex27_jacobian<double, double>(const H27JacArgs<double, double>&, int, cudaStream_t);
+template cudaError_t launch_hex27_jacobian<float, float>(const H27JacArgs<float, float>&, int, cudaStream_t);
+template cudaError_t launch_hex27_jacobian<double, float>(const H27JacArgs<double, float>&, int, cudaStream_t);
+template cudaError_t launch_hex27_jacobian<float, double>(const H27JacArgs<float, double>&, int, cudaStream_t);
+
+}  // namespace femb

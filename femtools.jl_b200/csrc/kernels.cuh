@@ -1,0 +1,179 @@
+// kernels.cuh — argument packs and launchers of the libfemtools_b200 kernels.
+#pragma once
+#include <limits>
+#include "common.cuh"
+
+namespace femb {
+
+constexpr int H27_THREADS = 128;   // 4 warps × 3 elements per warp
+
+template <class T, class TG>
+struct H27Args {
+    const int32_t* el2n;
+    const int32_t* dofsP;
+    const TG* geo_v;
+    const TG* geo_P;
+    const T* v[3];
+    T* Rv[3];
+    const T* P;
+    const T* P0;          // nodal P_old (or P0)
+    const T* P_old_ip;    // nq × nels P_old, or null
+    const T* temp;        // T on pressure DoFs
+    const T* temp0;
+    const T* Q;
+    const T* Pf;
+    const T* gammaP;
+    const T* MP;
+    T* RP;
+    T* Pnum_out;
+    const T* Pnum_in;     // stored Pnum read instead of γP·RP/M_P, or null
+    const int32_t* phv; int phv_layout;
+    const int32_t* php; int php_layout;
+    const T* told[6];
+    const T* eta_ip;
+    T* tau_store[6];
+    T* phi;               // shear dissipation output (nq × nels) or null
+    int64_t nels;
+    T dt;
+    int with_pnum;
+    int do_momentum;
+    int write_RP;
+};
+
+template <class T, class TG>
+cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaStream_t st);
+
+// Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
+template <class T, class TG>
+struct H27JacArgs {
+    const int32_t* el2n;
+    const int32_t* dofsP;
+    const TG* geo_v;
+    const TG* geo_P;
+    const T* v[3];
+    const T* P;
+    const T* P0;
+    const T* temp;
+    const T* temp0;
+    const T* Pf;
+    const T* gammaP;
+    const T* MP;
+    const int32_t* phv; int phv_layout;
+    const int32_t* php; int php_layout;
+    const T* told[6];
+    const T* eta_ip;
+    T* dRdv[3];
+    T* PC[3];
+    int64_t nels;
+    T dt;
+};
+
+template <class T, class TG>
+cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st);
+
+// Pressure mass and scale (pressure_scaling.jl:166-216).
+template <class T, class TG>
+cudaError_t launch_pressure_scaling(int dim, const int32_t* el2n, const int32_t* dofsP, const TG* geo_P,
+                                    const int32_t* phv, int phv_layout, const T* eta_ip, int use_eta_ip,
+                                    T* MP, T* gP, int64_t nels, int64_t nnodesP, T gfact, T dt, cudaStream_t st);
+
+// Q9/P1-disc plane-strain residual sweep (thread per element).
+template <class T, class TG>
+cudaError_t launch_q9_residual(const H27Args<T, TG>& args, cudaStream_t st);
+template <class T, class TG>
+cudaError_t launch_q9_jacobian(const H27JacArgs<T, TG>& args, cudaStream_t st);
+
+// ---- node-wise kernels -------------------------------------------------------
+
+// Scalars of the DR iteration kept on the device (α, β per component and the
+// Powell–Hestenes update factor), so launches need no host round trip.
+struct IterScalars {
+    double alpha[3];
+    double beta[3];
+};
+
+// Block-partial reductions written by the fused node sweep on check iterations.
+constexpr int RED_SLOTS = 12;   // per component: Σ R², Σ (a r)², Σ (a r)(R−R0)/PC ; + spare
+constexpr int NODE_THREADS = 256;
+
+template <class T>
+struct NodeArgs {
+    T* v[3];
+    T* rate[3];
+    T* Rv[3];
+    T* Rv0[3];
+    const T* PC[3];
+    const uint8_t* mask;   // bit c: component c constrained at this node
+    int64_t n;
+    int dim;
+    double alpha[3];       // negated Chebyshev step (v += alpha·rate)
+    double beta[3];
+    int save_R0;           // copy (masked) R into Rv0 after the update
+    int reduce;            // write block partials of the norms and λmin sums
+    double lam_step[3];    // α used in the λmin sums (DR.jl:722-724)
+    double* partials;      // gridDim.x × RED_SLOTS
+};
+
+template <class T>
+cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st);
+
+template <class T>
+cudaError_t launch_dirichlet(T* x, const int32_t* dofs, const T* vals, int64_t n, cudaStream_t st);
+
+cudaError_t launch_build_mask(uint8_t* mask, const int32_t* dofs, int64_t n, int comp, cudaStream_t st);
+
+// Σ x² over an array (block partials), and Σ (RP/M_P)².
+template <class T>
+cudaError_t launch_sumsq(const T* x, const T* div, int64_t n, double* partials, int blocks, cudaStream_t st);
+
+// P += γP·RP/M_P (DR.jl:777) and Pnum = γP·RP/M_P.
+template <class T>
+cudaError_t launch_pressure_update(T* P, const T* gP, const T* RP, const T* MP, int64_t n, cudaStream_t st);
+template <class T>
+cudaError_t launch_pnum(T* Pnum, const T* gP, const T* RP, const T* MP, int64_t n, cudaStream_t st);
+
+// max(J/PC) with NaN propagation (block partials) for _checked_λmax.
+template <class T>
+cudaError_t launch_ratio_max(const T* J, const T* PC, int64_t n, double* partials, int blocks, cudaStream_t st);
+
+template <class T>
+cudaError_t launch_sub(T* x, const T* y, int64_t n, cudaStream_t st);
+template <class T>
+cudaError_t launch_copy(T* dst, const T* src, int64_t n, cudaStream_t st);
+
+template <class T>
+cudaError_t launch_transfer_temperature(T* TP, const T* Tn, const int32_t* dofsP, const int32_t* el2nP, int64_t n,
+                                        cudaStream_t st);
+
+// Thermal diffusion element residual (+ Jacobian diagnostics).
+template <class T, class TG>
+struct ThermalArgs {
+    int dim;
+    const int32_t* el2n;
+    const TG* geo;
+    const T* Tn; const T* T0; const T* P; const T* src; const T* src_ip;
+    const int32_t* ph; int ph_layout;
+    T* R; T* dRdT; T* PC;
+    int64_t nels;
+    T dt, Tref;
+    int jac;
+};
+template <class T, class TG>
+cudaError_t launch_thermal(const ThermalArgs<T, TG>& a, int num_sms, cudaStream_t st);
+
+// Thermal DR node update: rate = R/PC + β rate; T += α rate, masked by Dirichlet.
+template <class T>
+cudaError_t launch_thermal_update(T* Tn, T* rate, T* R, const T* PC, const uint8_t* mask, int64_t n, double alpha,
+                                  double beta, cudaStream_t st);
+
+// Generic λmin sums of the thermal solver: Σ (s r)², Σ (s r)(R−R0)/PC.
+template <class T>
+cudaError_t launch_lmin_sums(const T* rate, const T* R, const T* R0, const T* PC, int64_t n, double step,
+                             double* partials, int blocks, cudaStream_t st);
+
+struct DevThermalMaterial {
+    double k[MAXPH], Cp[MAXPH], rho0[MAXPH], alpha[MAXPH], beta[MAXPH];
+};
+extern __constant__ DevThermalMaterial c_tmat;
+
+}  // namespace femb
