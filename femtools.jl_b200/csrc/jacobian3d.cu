@@ -26,11 +26,13 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
-    const int s = lane_ok ? lane / 9 : 0, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 3 + s) * JAC_ELEM;
+    // lanes 27..31 carry no element; they work in a private scratch slot (3) so
+    // their (discarded) stage writes never touch an element's shared memory.
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * JAC_ELEM;
     T* GEO = E + H27_ELEM_SMEM;
     T* BP = GEO + JAC_GEO;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 3 * JAC_ELEM) + (warp * 3 + s) * 28;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * JAC_ELEM) + (warp * 4 + s) * 28;
 
     Tab1D<T> tb; tb.load();
     const T dt = a.dt;
@@ -40,7 +42,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 
     const int64_t stride = (int64_t)gridDim.x * wpb * 3;
     for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
-        const int64_t e = base + s;
+        const int64_t e = base + (lane_ok ? s : 0);
         const bool act = lane_ok && e < a.nels;
         const int64_t ec = act ? e : 0;
 
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 template <class T, class TG>
 cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st) {
     const int wpb = JAC_THREADS / 32;
-    const size_t smem = (size_t)wpb * 3 * JAC_ELEM * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
+    const size_t smem = (size_t)wpb * 4 * JAC_ELEM * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -69,9 +69,11 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
-    const int s = lane_ok ? lane / 9 : 0, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 3 + s) * H27_ELEM_SMEM;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 3 * H27_ELEM_SMEM) + (warp * 3 + s) * 28;
+    // lanes 27..31 carry no element; they work in a private scratch slot (3) so
+    // their (discarded) stage writes never touch an element's shared memory.
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * H27_ELEM_SMEM;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * H27_ELEM_SMEM) + (warp * 4 + s) * 28;
 
     Tab1D<T> tb; tb.load();
     const T dt = a.dt;
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
 
     const int64_t stride = (int64_t)gridDim.x * wpb * 3;
     for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
-        const int64_t e = base + s;
+        const int64_t e = base + (lane_ok ? s : 0);
         const bool act = lane_ok && e < a.nels;
         const int64_t ec = act ? e : 0;   // clamped element for address formation
 
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
 template <class T, class TG>
 cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaStream_t st) {
     const int wpb = H27_THREADS / 32;
-    const size_t smem = (size_t)wpb * 3 * H27_ELEM_SMEM * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
+    const size_t smem = (size_t)wpb * 4 * H27_ELEM_SMEM * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(hex27_residual_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -210,7 +210,8 @@ def assemble_shear_heating(dr: StokesDR, dt, phi=None):
 
 def _controls(dt, **kw):
     history_capacity = kw.pop("history_capacity", 0)
-    hist = np.zeros((history_capacity, 4 + kw.pop("_dim", 3))) if history_capacity else None
+    dim = kw.pop("_dim", 3)
+    hist = np.zeros((history_capacity, 4 + dim)) if history_capacity else None
     c = prob.controls_struct(dt, history=hist, **kw)
     return c, hist
 
