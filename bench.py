@@ -1,0 +1,414 @@
+"""Benchmark: time to a 1e-8 DR solve of 3-D Hex27/Q2–P1-disc visco-elasto-plastic Stokes at 64³.
+
+One step = one `solve` (solve! of the reference, src/stokes/solvers/DR.jl:302) of the
+layered visco-elasto-plastic configuration from the same initial state to
+min(err_abs, err_rel) < 1e-8, with M_P/γP assembly, the Jacobian diagnostics every
+check and the Powell–Hestenes/DYREL loop, all inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 64] [--impl ours|reference]
+
+Prints one JSON line (rank 0). Multi-GPU runs are independent replicas (the path has
+no exchange step on one mesh): value = slowest rank's time per solve, scaling "weak".
+`--impl reference` times the CPU restatement of the reference's algorithm (the
+oracle, all host cores) on the same workload by a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "time-to-1e-8 residual, 3D Q2 Stokes 64³: chosen vs plain FP64 DR; HBM GB/s"
+
+
+def load_package():
+    import importlib.util
+    if "femtools_b200" in sys.modules:
+        return sys.modules["femtools_b200"]
+    pkg_dir = os.path.join(ROOT, "femtools.jl_b200")
+    spec = importlib.util.spec_from_file_location(
+        "femtools_b200", os.path.join(pkg_dir, "__init__.py"), submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["femtools_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def mesh_is_affine(mesh, tol=1e-12):
+    """Every element carries one J⁻¹ and |det J| at all quadrature points (the test the
+    library applies before it takes the compressed-geometry sweep)."""
+    g = mesh.geo_v
+    w = __import__("femtools_b200").mesh.element_tables(mesh.dim).w
+    c = g[:, 13:14, :]
+    sc = np.abs(c[:, :, :9]).max(axis=2, keepdims=True)
+    ok = np.all(np.abs(g[:, :, :9] - c[:, :, :9]) <= tol * sc)
+    d = g[:, :, 9] / w[None, :]
+    ok = ok and np.all(np.abs(d - d[:, 13:14]) <= tol * np.abs(d[:, 13:14]))
+    ok = ok and np.all(np.abs(mesh.geo_P - g[:, :, 9]) <= tol * np.abs(g[:, :, 9]))
+    return bool(ok)
+
+
+def residual_kernel_bytes(case, itemsize=8, geo_itemsize=8, affine=None):
+    """Algorithmic bytes of one fused residual-sweep launch: every array the sweep
+    must touch, once, at its stored precision (Rv read-modify-write counted twice).
+    On affine meshes the sweep reads one J⁻¹ and |det J| per element (80 B) instead
+    of the reference layout's per-point J⁻¹, dΩ and dΩ_P (2376 B), and the figure
+    counts what it reads."""
+    m = case.mesh
+    nels, nn, nP = m.nels, m.nnodes, m.nnodesP
+    if affine is None:
+        affine = m.dim == 3 and mesh_is_affine(m)
+    b = 0
+    b += 3 * nn * itemsize                 # v
+    b += 27 * 4 * nels + 4 * 4 * nels      # el2n, dofsP
+    if affine:
+        b += 10 * itemsize * nels          # per-element J⁻¹ and |det J|
+    else:
+        b += 27 * 10 * geo_itemsize * nels     # geo_v (J⁻¹ + dΩ per point)
+        b += 27 * geo_itemsize * nels          # geo_P
+    b += 4 * nP * itemsize                 # P, P_old, γP, M_P
+    b += 4 * nels                          # cell phase
+    b += 6 * 27 * itemsize * nels          # τ_old at integration points
+    b += 2 * nP * itemsize                 # RP, Pnum written
+    b += 2 * 3 * nn * itemsize             # Rv atomic read-modify-write
+    return b
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.proc = None
+        self.index = index
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_estimate(case, iterations, jac_assemblies, threads=None):
+    """Time-to-solution of the CPU restatement of the reference (the oracle), from a
+    bounded sample: two fused residual sweeps on the full mesh, one Jacobian-diagnostics
+    assembly on an 8³ sub-mesh scaled by the element ratio, extrapolated with the GPU
+    run's iteration and assembly counts (both implementations take the same path)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    from cases import vep_layers_case
+    L = oh.lib()
+    if threads:
+        L.orc_set_num_threads(threads)
+    cores = L.orc_num_threads()
+    hs = case.host_state(oh)
+    hs.pressure_scaling(50.0, case.dt)
+    t0 = time.perf_counter()
+    hs.stokes_residuals(case.dt)
+    hs.stokes_residuals(case.dt)
+    t_res = (time.perf_counter() - t0) / 2
+    small = vep_layers_case(n=8, seed=0)
+    hsm = small.host_state(oh)
+    hsm.pressure_scaling(50.0, small.dt)
+    t0 = time.perf_counter()
+    hsm.jacobian_diagnostics(small.dt)
+    t_jac = (time.perf_counter() - t0) * case.mesh.nels / small.mesh.nels
+    est = iterations * t_res + jac_assemblies * t_jac
+    sample = (f"2 fused residual sweeps at {case.mesh.nel} ({t_res:.3f} s each) + Jacobian diagnostics on "
+              f"8³ scaled ×{case.mesh.nels // small.mesh.nels} ({t_jac:.2f} s per assembly), extrapolated to "
+              f"{iterations} iterations and {jac_assemblies} assemblies")
+    return est, cores, sample
+
+
+def sweep_mode(args, fem, case, dr, lib, h):
+    """Kernel-level timing: K fused residual sweeps and K Jacobian assemblies."""
+    import torch
+    fem.assemble_viscosity_weighted_pressure_scaling(dr, 50.0, case.dt)
+    for _ in range(args.warmup):
+        fem.assemble_stokes_residuals(dr, case.dt)
+    fem.assemble_augmented_momentum_jacobian(dr, case.dt)
+    torch.cuda.synchronize()
+    lib.femb200_profile(h, 1)
+    for _ in range(args.steps):
+        fem.assemble_stokes_residuals(dr, case.dt)
+    for _ in range(max(1, args.steps // 10)):
+        fem.assemble_augmented_momentum_jacobian(dr, case.dt)
+    prof_ms = (C.c_double * 4)()
+    prof_n = (C.c_int64 * 4)()
+    lib.femb200_profile_read(h, prof_ms, prof_n)
+    lib.femb200_profile(h, 0)
+    nbytes = residual_kernel_bytes(case)
+    res_ms = prof_ms[0] / max(prof_n[0], 1)
+    peak, kind = measured_peaks()
+    print(json.dumps({"mode": "sweep", "n": args.n, "residual_ms": res_ms, "residual_launches": prof_n[0],
+                      "achieved_GBs": nbytes / (res_ms / 1e3) / 1e9, "frac": nbytes / (res_ms / 1e3) / 1e9 / peak,
+                      "bytes_per_launch": nbytes, "jacobian_ms": prof_ms[1] / max(prof_n[1], 1),
+                      "jacobian_launches": prof_n[1]}), flush=True)
+    return 0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    fem = load_package()
+    case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
+    iters, jacs = args.ref_iterations, args.ref_jacobians
+    times = []
+    for _ in range(args.warmup + args.steps):
+        est, cores, sample = cpu_baseline_estimate(case, iters, jacs)
+        times.append(est)
+    t = statistics.mean(times[args.warmup:])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": t, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
+                   "tolerance": 1e-8},
+        "cpu_baseline": {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--check-interval", type=int, default=100)
+    ap.add_argument("--tolerance", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iterations", type=int, default=0,
+                    help="iteration count of the GPU run used to scale the reference sample")
+    ap.add_argument("--ref-jacobians", type=int, default=0)
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep"],
+                    help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        if args.ref_iterations <= 0:
+            # the same solve's path on the GPU measured at 64³ (iterations, Jacobian assemblies)
+            prev = os.path.join(ROOT, "profiles", "bench_path.json")
+            if os.path.exists(prev):
+                d = json.load(open(prev))
+                args.ref_iterations, args.ref_jacobians = d["iterations"], d["jacobian_assemblies"]
+            else:
+                print(json.dumps({"impl": "reference", "unavailable": "no measured iteration path to scale the sample"}))
+                return 0
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    fem = load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
+    dr = case.device_state()
+    bc = case.bc_device()
+    lib, h = fem.solver._Handle.get()
+    if args.mode == "sweep":
+        return sweep_mode(args, fem, case, dr, lib, h)
+    # device-resident initial state of every step
+    init = {"v": [x.clone() for x in dr.v], "P": dr.P.clone(), "P0": dr.P0.clone(),
+            "tau_old": [x.clone() for x in dr.tau_old]}
+
+    def reset():
+        for c in range(3):
+            dr.v[c].copy_(init["v"][c])
+        dr.P.copy_(init["P"])
+        dr.P0.copy_(init["P0"])
+        for c in range(6):
+            dr.tau_old[c].copy_(init["tau_old"][c])
+
+    kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
+              max_iterations=2_000_000, iter_max=2_000_000, precision=args.precision)
+    stats = None
+    for _ in range(args.warmup):
+        reset()
+        stats = fem.solve(dr, bc, **kw)
+    barrier()
+
+    # ---- timed region: inputs resident in HBM ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    lib.femb200_profile(h, 1)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    step_stats = []
+    for _ in range(args.steps):
+        reset()
+        step_stats.append(fem.solve(dr, bc, **kw))
+    ev1.record(stream)
+    barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    prof_ms = (C.c_double * 4)()
+    prof_n = (C.c_int64 * 4)()
+    lib.femb200_profile_read(h, prof_ms, prof_n)
+    lib.femb200_profile(h, 0)
+    clocks = sampler.stop()
+    t_step = ms_total / 1e3 / args.steps
+    if world > 1:
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = tt.item()
+
+    # ---- end to end: host inputs in pinned memory, copies inside the timed region ----
+    host_in = {k: ([x.cpu().pin_memory() for x in v] if isinstance(v, list) else v.cpu().pin_memory())
+               for k, v in init.items()}
+    out_v = [torch.empty(dr.mesh.nnodes, dtype=dr.dtype).pin_memory() for _ in range(3)]
+    out_P = torch.empty(dr.mesh.nnodesP, dtype=dr.dtype).pin_memory()
+    h2d = sum(x.numel() * x.element_size() for v in host_in.values() for x in (v if isinstance(v, list) else [v]))
+    d2h = sum(x.numel() * x.element_size() for x in out_v) + out_P.numel() * out_P.element_size()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        for c in range(3):
+            dr.v[c].copy_(host_in["v"][c], non_blocking=True)
+        dr.P.copy_(host_in["P"], non_blocking=True)
+        dr.P0.copy_(host_in["P0"], non_blocking=True)
+        for c in range(6):
+            dr.tau_old[c].copy_(host_in["tau_old"][c], non_blocking=True)
+        fem.solve(dr, bc, **kw)
+        for c in range(3):
+            out_v[c].copy_(dr.v[c], non_blocking=True)
+        out_P.copy_(dr.P, non_blocking=True)
+    ev1.record(stream)
+    barrier()
+    t_e2e = ev0.elapsed_time(ev1) / 1e3 / e2e_steps
+    if world > 1:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = tt.item()
+
+    st = step_stats[-1]
+    iters = st["iter"]
+    jacs = st["jacobian_assemblies"]
+    peak, peak_kind = measured_peaks()
+    itemsize = 8 if args.precision == "fp64" else 4
+    nbytes = residual_kernel_bytes(case, itemsize=8, geo_itemsize=8)
+    res_avg_ms = prof_ms[0] / max(prof_n[0], 1)
+    achieved = nbytes / (res_avg_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "residual_traffic.json")
+    if os.path.exists(tp):
+        d = json.load(open(tp))
+        if d.get("n") == args.n and d.get("precision") == args.precision:
+            traffic = d.get("bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        est, cores, sample = cpu_baseline_estimate(case, iters, jacs)
+        cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
+        if args.n == 64 and args.precision == "fp64":
+            json.dump({"iterations": iters, "jacobian_assemblies": jacs, "itPH": st["itPH"]},
+                      open(os.path.join(ROOT, "profiles", "bench_path.json"), "w"))
+        line = {
+            "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {
+                "workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
+                "precision": args.precision, "tolerance": args.tolerance, "check_interval": args.check_interval,
+                "dt": case.dt, "iterations": iters, "itPH": st["itPH"], "jacobian_assemblies": jacs,
+                "converged": bool(st["converged"]), "err": st["err"],
+                "nels": case.mesh.nels, "nnodes": case.mesh.nnodes, "nnodesP": case.mesh.nnodesP,
+                "l2": "inputs larger than L2 (geometry alone %.0f MB)" % (case.mesh.geo_v.nbytes / 1e6),
+                "parallelism": f"replicas{world}",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "hex27_residual_pipe_kernel (fused RP + Pnum + Rv sweep, affine geometry)"
+                                   if mesh_is_affine(case.mesh) else "hex27_residual_kernel (fused RP + Pnum + Rv sweep)",
+                         "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": res_avg_ms,
+                         "launches": int(prof_n[0]), "peak_kind": peak_kind},
+            "kernel_ms": {"residual": prof_ms[0], "jacobian": prof_ms[1], "node_update": prof_ms[2],
+                          "total_timed": ms_total},
+            "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(prof_n[3]),
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -8,6 +8,7 @@ tests/conftest.py) under the module name `femtools_b200`.
 from . import _abi  # noqa: F401
 from . import mesh  # noqa: F401
 from . import problem  # noqa: F401
+from . import configs  # noqa: F401
 from .mesh import structured_mixed_mesh, element_tables, MixedMesh  # noqa: F401
 from .problem import StokesMaterial, DruckerPrager, DirichletBoundaryCondition  # noqa: F401
 

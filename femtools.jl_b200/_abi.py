@@ -143,7 +143,10 @@ SIGNATURES = {
     "femb200_solve_coupled": (C.c_int, [_vp, _P(ThermalProblemC), _P(StokesProblemC),
                                         _P(StokesControlsC), C.c_double, C.c_int32, _vp,
                                         _P(StokesStatsC)]),
+    "femb200_profile": (C.c_int, [_vp, C.c_int32]),
+    "femb200_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_int64)]),
 }
+PROF_RESIDUAL, PROF_JACOBIAN, PROF_NODE, PROF_ALL, PROF_COUNT = range(5)
 
 _lib = None
 

@@ -18,6 +18,7 @@
 namespace femb {
 __constant__ DevStokesMaterial c_mat;
 __constant__ DevTables c_tab;
+unsigned long long g_kernel_launches = 0;
 }  // namespace femb
 
 using namespace femb;
@@ -36,6 +37,20 @@ struct femb200_handle {
     size_t tmask_cap = 0;
     std::string err;
     bool tables_ready = false;
+    // profiling: event pairs per kernel class, folded into totals when the pool fills
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool[FEMB200_PROF_COUNT];
+    size_t ev_used[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
+    double prof_ms[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
+    int64_t prof_n[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
+    unsigned long long launches_at_reset = 0;
+    // compressed affine geometry (one J⁻¹, |det J| per element), rebuilt per call
+    void* d_geo_c = nullptr;
+    size_t geo_c_cap = 0;
+    int* d_flag = nullptr;
+    int* h_flag = nullptr;
+    bool geo_c_valid = false;
+    int use_pipe = 1;   // the pipelined sweep on affine meshes (0 forces the general sweep)
 };
 
 namespace {
@@ -136,7 +151,7 @@ int ensure_tables(femb200_handle* h) {
 
 // Constant-memory material of one call. `finite_K` selects K as the storage
 // modulus of the continuity residual and of the pressure scaling (DR.jl:419, :325).
-int upload_material(femb200_handle* h, const femb200_stokes_material& m, int finite_K) {
+int upload_material(femb200_handle* h, const femb200_stokes_material& m, int finite_K, double dt = 0.0) {
     if (m.nphases < 1 || m.nphases > FEMB200_MAX_PHASES) { h->err = "nphases must lie in 1:16"; return FEMB200_EINVAL; }
     static thread_local DevStokesMaterial d;   // host staging must outlive the async copy
     std::memset(&d, 0, sizeof(d));
@@ -157,6 +172,17 @@ int upload_material(femb200_handle* h, const femb200_stokes_material& m, int fin
         d.C[i] = m.C[i]; d.eta_reg[i] = m.eta_reg[i]; d.Kb[i] = m.Kb[i];
     }
     d.all_bulk_inf = all_inf;
+    d.dt_consts = dt;
+    if (dt > 0) {
+        for (int i = 0; i < FEMB200_MAX_PHASES; ++i) {
+            const double etave = 1.0 / (1.0 / d.eta[i] + d.invG[i] / dt);
+            d.u_twoe[i] = 2 * etave;
+            d.u_twoe_el[i] = 2 * etave * (d.invG[i] / (2 * dt));
+            d.u_cC[i] = d.cos_phi[i] * d.C[i];
+            d.u_inv_den[i] = 1.0 / (etave + d.eta_reg[i] + d.Kb[i] * dt * (-d.sin_psi[i]) * (-d.sin_phi[i]));
+            d.u_inv_bulkdt[i] = all_inf ? 0.0 : 1.0 / (d.bulk[i] * dt);
+        }
+    }
     for (int i = 0; i < 3; ++i) d.g[i] = m.g[i];
     d.Tref = m.Tref;
     CK(cudaMemcpyToSymbolAsync(c_mat, &d, sizeof(d), 0, cudaMemcpyHostToDevice, h->stream));
@@ -178,6 +204,40 @@ int check_problem(femb200_handle* h, const femb200_stokes_problem* p) {
     if (!p->el2n || !p->dofsP || !p->geo_v || !p->geo_P || !p->P) { h->err = "mesh arrays and P are required"; return FEMB200_EINVAL; }
     for (int c = 0; c < p->dim; ++c)
         if (!p->v[c]) { h->err = "velocity components are required"; return FEMB200_EINVAL; }
+    return FEMB200_OK;
+}
+
+// ---- profiling ----------------------------------------------------------------
+constexpr size_t PROF_PAIRS = 512;
+
+int prof_flush(femb200_handle* h, int k) {
+    if (h->ev_used[k] == 0) return FEMB200_OK;
+    CK(cudaEventSynchronize(h->ev_pool[k][2 * h->ev_used[k] - 1]));
+    for (size_t i = 0; i < h->ev_used[k]; ++i) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, h->ev_pool[k][2 * i], h->ev_pool[k][2 * i + 1]));
+        h->prof_ms[k] += ms;
+    }
+    h->ev_used[k] = 0;
+    return FEMB200_OK;
+}
+
+int prof_begin(femb200_handle* h, int k) {
+    if (!h->prof) return FEMB200_OK;
+    if (h->ev_pool[k].empty()) {
+        h->ev_pool[k].resize(2 * PROF_PAIRS);
+        for (auto& e : h->ev_pool[k]) CK(cudaEventCreate(&e));
+    }
+    if (h->ev_used[k] == PROF_PAIRS) RC(prof_flush(h, k));
+    CK(cudaEventRecord(h->ev_pool[k][2 * h->ev_used[k]], h->stream));
+    return FEMB200_OK;
+}
+
+int prof_end(femb200_handle* h, int k) {
+    if (!h->prof) return FEMB200_OK;
+    CK(cudaEventRecord(h->ev_pool[k][2 * h->ev_used[k] + 1], h->stream));
+    ++h->ev_used[k];
+    ++h->prof_n[k];
     return FEMB200_OK;
 }
 
@@ -253,7 +313,12 @@ H27Args<T, TG> residual_args(const femb200_stokes_problem* p, double dt) {
     const bool ip = p->P_old && p->P_old_layout == FEMB200_FIELD_IP;
     a.P0 = static_cast<const T*>(p->P_old && !ip ? p->P_old : p->P0);
     a.P_old_ip = ip ? static_cast<const T*>(p->P_old) : nullptr;
-    a.temp = static_cast<const T*>(p->T); a.temp0 = static_cast<const T*>(p->T0);
+    // T enters only through α (EOS density and the α∂T/∂t continuity term): with
+    // α = 0 in every phase the sweep need not read T and T0 at all.
+    bool any_alpha = false;
+    for (int i = 0; i < p->mat.nphases; ++i) any_alpha = any_alpha || p->mat.alpha[i] != 0.0;
+    a.temp = any_alpha ? static_cast<const T*>(p->T) : nullptr;
+    a.temp0 = any_alpha ? static_cast<const T*>(p->T0) : nullptr;
     a.Q = static_cast<const T*>(p->Q); a.Pf = static_cast<const T*>(p->Pf);
     a.gammaP = static_cast<const T*>(p->gammaP); a.MP = static_cast<const T*>(p->M_P);
     a.RP = static_cast<T*>(p->RP);
@@ -268,12 +333,48 @@ H27Args<T, TG> residual_args(const femb200_stokes_problem* p, double dt) {
     return a;
 }
 
+// Build the per-element affine geometry of a Hex27 problem (in the state type) and
+// report whether every element is affine. Costs one read of geo_v.
+template <class T, class TG>
+int prepare_geometry(femb200_handle* h, const femb200_stokes_problem* p) {
+    h->geo_c_valid = false;
+    if (p->dim != 3 || !h->use_pipe) return FEMB200_OK;
+    const size_t need = (size_t)p->nels * 10 * sizeof(T);
+    if (need > h->geo_c_cap) {
+        if (h->d_geo_c) cudaFree(h->d_geo_c);
+        h->d_geo_c = nullptr;
+        CK(cudaMalloc(&h->d_geo_c, need));
+        h->geo_c_cap = need;
+    }
+    if (!h->d_flag) {
+        CK(cudaMalloc(&h->d_flag, sizeof(int)));
+        CK(cudaMallocHost(&h->h_flag, sizeof(int)));
+    }
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    CK(launch_compress_geometry<TG, T>(static_cast<const TG*>(p->geo_v), static_cast<const TG*>(p->geo_P), p->nels,
+                                       static_cast<T*>(h->d_geo_c), h->d_flag, h->stream));
+    CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->geo_c_valid = *h->h_flag == 0;
+    return FEMB200_OK;
+}
+
 template <class T, class TG>
 int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H27Args<T, TG>& a) {
     if (a.do_momentum)
         for (int c = 0; c < p->dim; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(T) * p->nnodes, h->stream));
-    if (p->dim == 3) CK(launch_hex27_residual<T, TG>(a, h->num_sms, h->stream));
-    else CK(launch_q9_residual<T, TG>(a, h->stream));
+    RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
+    if (p->dim == 3 && h->geo_c_valid) {
+        H27Args<T, T> b;
+        std::memcpy(&b, &a, sizeof(b));   // identical layout; the pipelined sweep reads geometry from d_geo_c
+        b.geo_v = nullptr; b.geo_P = nullptr;
+        CK(launch_hex27_residual_pipe<T>(b, static_cast<const T*>(h->d_geo_c), h->num_sms, h->stream));
+    } else if (p->dim == 3) {
+        CK(launch_hex27_residual<T, TG>(a, h->num_sms, h->stream));
+    } else {
+        CK(launch_q9_residual<T, TG>(a, h->stream));
+    }
+    RC(prof_end(h, FEMB200_PROF_RESIDUAL));
     return FEMB200_OK;
 }
 
@@ -323,8 +424,10 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
         CK(cudaMemsetAsync(p->PC[c], 0, sizeof(T) * p->nnodes, h->stream));
     }
     if (!p->gammaP || !p->M_P) { h->err = "γP and M_P are required by the augmented Jacobian"; return FEMB200_EINVAL; }
+    RC(prof_begin(h, FEMB200_PROF_JACOBIAN));
     if (p->dim == 3) CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
     else CK(launch_q9_jacobian<T, TG>(a, h->stream));
+    RC(prof_end(h, FEMB200_PROF_JACOBIAN));
     return FEMB200_OK;
 }
 
@@ -493,7 +596,8 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
         if (!p->rate[k] || !p->Rv0[k] || !p->Rv[k] || !p->PC[k] || !p->dRdv[k]) { h->err = "DR work arrays are required"; return FEMB200_EINVAL; }
     if (!p->RP || !p->M_P || !p->gammaP || !p->Pnum) { h->err = "RP, M_P, γP and Pnum are required"; return FEMB200_EINVAL; }
 
-    RC(upload_material(h, p->mat, finite_K));
+    RC(upload_material(h, p->mat, finite_K, dt));
+    RC((prepare_geometry<T, TG>(h, p)));
     RC(build_mask(h, p));
     for (int k = 0; k < D; ++k) {
         CK(cudaMemsetAsync(p->rate[k], 0, sizeof(T) * nn, h->stream));
@@ -597,7 +701,9 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
             na.mask = h->d_mask; na.n = nn; na.dim = D;
             na.reduce = do_check ? 1 : 0;
             na.partials = h->d_partials;
+            RC(prof_begin(h, FEMB200_PROF_NODE));
             CK(launch_node_update<T>(na, nb, h->stream));
+            RC(prof_end(h, FEMB200_PROF_NODE));
             for (int k = 0; k < D; ++k)
                 if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(static_cast<T*>(p->v[k]), p->bc_dofs[k], static_cast<const T*>(p->bc_vals[k]), p->bc_n[k], h->stream));
             if (do_check) {
@@ -666,6 +772,7 @@ int dispatch(const femb200_stokes_problem* p, Args&&... args) {
 
 template <class T, class TG> struct DoResidual {
     static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, int with_pnum, int do_momentum, int write_RP) {
+        RC((prepare_geometry<T, TG>(h, p)));
         return residual_sweep<T, TG>(h, p, dt, with_pnum, do_momentum, write_RP);
     }
 };
@@ -675,6 +782,7 @@ template <class T, class TG> struct DoMomentum {
         H27Args<T, TG> a = residual_args<T, TG>(p, dt);
         a.do_momentum = 1; a.write_RP = 0; a.with_pnum = with_pnum;
         a.Pnum_in = with_pnum ? static_cast<const T*>(p->Pnum) : nullptr;
+        h->geo_c_valid = false;   // the pipelined sweep has no stored-Pnum input
         return launch_residual<T, TG>(h, p, a);
     }
 };
@@ -694,16 +802,20 @@ template <class T, class TG> struct DoStore {
         }
         a.do_momentum = 1; a.write_RP = 0; a.with_pnum = 0;
         a.eta_ip = nullptr;   // update_stokes_current_stress! uses dr.η (DR.jl:890)
+        RC((prepare_geometry<T, TG>(h, p)));
         return launch_residual<T, TG>(h, p, a);
     }
 };
 template <class T, class TG> struct DoShear {
-    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) { return shear_heating_impl<T, TG>(h, p, dt, phi); }
+    static int run(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) {
+        h->geo_c_valid = false;
+        return shear_heating_impl<T, TG>(h, p, dt, phi);
+    }
 };
 template <class T, class TG> struct DoSolve {
     static int run(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c, femb200_stokes_stats* st, Coupled* cp) {
         if (c->assemble_scaling) {
-            RC(upload_material(h, p->mat, c->finite_K));
+            RC(upload_material(h, p->mat, c->finite_K, c->dt));
             RC((pressure_scaling_impl<T, TG>(h, p, c->pressure_factor, c->dt)));
         }
         RC((solve_dyrel<T, TG>(h, p, c, st, cp)));
@@ -739,13 +851,41 @@ int femb200_create(femb200_handle** out) {
     return FEMB200_OK;
 }
 
+int femb200_profile(femb200_handle* h, int32_t enable) {
+    if (!h) return FEMB200_EINVAL;
+    for (int k = 0; k < FEMB200_PROF_COUNT; ++k) {
+        RC(prof_flush(h, k));
+        h->prof_ms[k] = 0;
+        h->prof_n[k] = 0;
+    }
+    h->prof = enable != 0;
+    h->launches_at_reset = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+    return FEMB200_OK;
+}
+
+int femb200_profile_read(femb200_handle* h, double* ms, int64_t* launches) {
+    if (!h || !ms || !launches) return FEMB200_EINVAL;
+    for (int k = 0; k < FEMB200_PROF_COUNT; ++k) {
+        RC(prof_flush(h, k));
+        ms[k] = h->prof_ms[k];
+        launches[k] = h->prof_n[k];
+    }
+    launches[FEMB200_PROF_ALL] = (int64_t)(__atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED) - h->launches_at_reset);
+    return FEMB200_OK;
+}
+
 int femb200_destroy(femb200_handle* h) {
     if (!h) return FEMB200_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int k = 0; k < FEMB200_PROF_COUNT; ++k)
+        for (auto& e : h->ev_pool[k]) cudaEventDestroy(e);
     if (h->d_partials) cudaFree(h->d_partials);
     if (h->h_partials) cudaFreeHost(h->h_partials);
     if (h->d_mask) cudaFree(h->d_mask);
     if (h->d_tmask) cudaFree(h->d_tmask);
+    if (h->d_geo_c) cudaFree(h->d_geo_c);
+    if (h->d_flag) cudaFree(h->d_flag);
+    if (h->h_flag) cudaFreeHost(h->h_flag);
     delete h;
     return FEMB200_OK;
 }
@@ -762,20 +902,20 @@ const char* femb200_version(void) { return "libfemtools_b200 0.1 (sm_100a)"; }
 
 int femb200_pressure_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, finite_K));
+    RC(upload_material(h, p->mat, finite_K, dt));
     return dispatch<DoResidual>(p, h, p, dt, 0, 0, 1);
 }
 
 int femb200_momentum_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t with_pnum) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, 0));
+    RC(upload_material(h, p->mat, 0, dt));
     if (with_pnum && !p->Pnum) { h->err = "Pnum is required"; return FEMB200_EINVAL; }
     return dispatch<DoMomentum>(p, h, p, dt, (int)with_pnum);
 }
 
 int femb200_stokes_residuals(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, finite_K));
+    RC(upload_material(h, p->mat, finite_K, dt));
     return dispatch<DoResidual>(p, h, p, dt, 1, 1, 1);
 }
 
@@ -809,26 +949,26 @@ int femb200_apply_dirichlet(femb200_handle* h, void* x, const int32_t* dofs, con
 
 int femb200_jacobian_diagnostics(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, finite_K));
+    RC(upload_material(h, p->mat, finite_K, dt));
     return dispatch<DoJacobian>(p, h, p, dt);
 }
 
 int femb200_pressure_scaling(femb200_handle* h, const femb200_stokes_problem* p, double gamma_fact, double dt, int32_t finite_K) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, finite_K));
+    RC(upload_material(h, p->mat, finite_K, dt));
     return dispatch<DoScaling>(p, h, p, gamma_fact, dt);
 }
 
 int femb200_store_stress(femb200_handle* h, const femb200_stokes_problem* p, double dt) {
     RC(check_problem(h, p));
-    RC(upload_material(h, p->mat, 0));
+    RC(upload_material(h, p->mat, 0, dt));
     return dispatch<DoStore>(p, h, p, dt);
 }
 
 int femb200_shear_heating(femb200_handle* h, const femb200_stokes_problem* p, double dt, void* phi) {
     RC(check_problem(h, p));
     if (!phi) { h->err = "phi is required"; return FEMB200_EINVAL; }
-    RC(upload_material(h, p->mat, 0));
+    RC(upload_material(h, p->mat, 0, dt));
     return dispatch<DoShear>(p, h, p, dt, phi);
 }
 

@@ -29,6 +29,12 @@ struct DevStokesMaterial {
     double g[3];
     double Tref;
     double cos_phi[MAXPH], sin_phi[MAXPH], sin_psi[MAXPH], C[MAXPH], eta_reg[MAXPH], Kb[MAXPH];
+    // Per-phase constants of an element whose nodes all carry one phase, for the
+    // Δt of the upload (valid when dt_consts == the kernel's Δt): the Maxwell
+    // viscosity ηve = 1/(1/η + 1/(GΔt)), 2ηve, 2ηve/(2GΔt), C·cosϕ, the reciprocal
+    // plastic denominator 1/(ηve + η_reg + Kb·Δt·sinΨ·sinϕ) and 1/(bulk·Δt).
+    double dt_consts;
+    double u_twoe[MAXPH], u_twoe_el[MAXPH], u_cC[MAXPH], u_inv_den[MAXPH], u_inv_bulkdt[MAXPH];
 };
 
 // Hex27 tensor tables: 1-D quadratic Lagrange values/derivatives at the 3 Gauss

@@ -22,22 +22,33 @@ constexpr int H27_ELEM_SMEM = 540;   // scalars of stage scratch per element
 
 FEMB_D int tidx(int i, int j, int k) { return i + 3 * j + 9 * k; }
 
+// 1-D basis tables read straight from constant memory: every index in the stage
+// code is a compile-time constant, so they become constant-bank operands and take
+// no registers.
 template <class T>
 struct Tab1D {
-    T B[3][3], Dd[3][3];
-    FEMB_D void load() {
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) { B[q][i] = (T)c_tab.B[q][i]; Dd[q][i] = (T)c_tab.Dd[q][i]; }
-    }
+    struct Row {
+        int q;
+        FEMB_D T operator[](int i) const { return (T)c_tab.B[q][i]; }
+    };
+    struct RowD {
+        int q;
+        FEMB_D T operator[](int i) const { return (T)c_tab.Dd[q][i]; }
+    };
+    struct TabB {
+        FEMB_D Row operator[](int q) const { return Row{q}; }
+    } B;
+    struct TabD {
+        FEMB_D RowD operator[](int q) const { return RowD{q}; }
+    } Dd;
+    FEMB_D void load() {}
 };
 
 // Reference gradients of the three velocity components at the three quadrature
 // points of the owned z-line. v[c][i]: node values on the owned x-line.
 // Output g[c][d][qz], d = ξ, η, ζ.
 template <class T>
-FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m2, T g[3][3][3]) {
+FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m2, T g[3][3][3], bool wr = true) {
     // stage X: contract x (thread owns x-line (·, m1, m2))
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -45,8 +56,10 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
         for (int q = 0; q < 3; ++q) {
             T x0 = t.B[q][0] * v[c][0] + t.B[q][1] * v[c][1] + t.B[q][2] * v[c][2];
             T x1 = t.Dd[q][0] * v[c][0] + t.Dd[q][1] * v[c][1] + t.Dd[q][2] * v[c][2];
-            E[(c * 2 + 0) * 27 + tidx(q, m1, m2)] = x0;
-            E[(c * 2 + 1) * 27 + tidx(q, m1, m2)] = x1;
+            if (wr) {
+                E[(c * 2 + 0) * 27 + tidx(q, m1, m2)] = x0;
+                E[(c * 2 + 1) * 27 + tidx(q, m1, m2)] = x1;
+            }
         }
     __syncwarp();
     // stage Y: thread owns y-line (qx = m1, ·, k = m2)
@@ -58,9 +71,14 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
         for (int j = 0; j < 3; ++j) { X0[j] = E[(c * 2 + 0) * 27 + tidx(m1, j, m2)]; X1[j] = E[(c * 2 + 1) * 27 + tidx(m1, j, m2)]; }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-            E1[(c * 3 + 0) * 27 + tidx(m1, q, m2)] = t.B[q][0] * X1[0] + t.B[q][1] * X1[1] + t.B[q][2] * X1[2];
-            E1[(c * 3 + 1) * 27 + tidx(m1, q, m2)] = t.Dd[q][0] * X0[0] + t.Dd[q][1] * X0[1] + t.Dd[q][2] * X0[2];
-            E1[(c * 3 + 2) * 27 + tidx(m1, q, m2)] = t.B[q][0] * X0[0] + t.B[q][1] * X0[1] + t.B[q][2] * X0[2];
+            const T y0 = t.B[q][0] * X1[0] + t.B[q][1] * X1[1] + t.B[q][2] * X1[2];
+            const T y1 = t.Dd[q][0] * X0[0] + t.Dd[q][1] * X0[1] + t.Dd[q][2] * X0[2];
+            const T y2 = t.B[q][0] * X0[0] + t.B[q][1] * X0[1] + t.B[q][2] * X0[2];
+            if (wr) {
+                E1[(c * 3 + 0) * 27 + tidx(m1, q, m2)] = y0;
+                E1[(c * 3 + 1) * 27 + tidx(m1, q, m2)] = y1;
+                E1[(c * 3 + 2) * 27 + tidx(m1, q, m2)] = y2;
+            }
         }
     }
     __syncwarp();
@@ -89,19 +107,26 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
 // (R_c(a) = Σ_q Σ_d ∂_d N_a(q) F_cd(q) − g_c Σ_q N_a(q) β(q)).
 template <class T>
 FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3], const T gvec[3], T* E,
-                          int m1, int m2, T R[3][3]) {
+                          int m1, int m2, T R[3][3], bool wr = true) {
     // Z^T: thread owns z-line (qx = m1, qy = m2)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int iz = 0; iz < 3; ++iz) {
-            E[(c * 3 + 0) * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * F[c][0][0] + t.B[1][iz] * F[c][0][1] + t.B[2][iz] * F[c][0][2];
-            E[(c * 3 + 1) * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * F[c][1][0] + t.B[1][iz] * F[c][1][1] + t.B[2][iz] * F[c][1][2];
-            E[(c * 3 + 2) * 27 + tidx(m1, m2, iz)] = t.Dd[0][iz] * F[c][2][0] + t.Dd[1][iz] * F[c][2][1] + t.Dd[2][iz] * F[c][2][2];
+            const T z0 = t.B[0][iz] * F[c][0][0] + t.B[1][iz] * F[c][0][1] + t.B[2][iz] * F[c][0][2];
+            const T z1 = t.B[0][iz] * F[c][1][0] + t.B[1][iz] * F[c][1][1] + t.B[2][iz] * F[c][1][2];
+            const T z2 = t.Dd[0][iz] * F[c][2][0] + t.Dd[1][iz] * F[c][2][1] + t.Dd[2][iz] * F[c][2][2];
+            if (wr) {
+                E[(c * 3 + 0) * 27 + tidx(m1, m2, iz)] = z0;
+                E[(c * 3 + 1) * 27 + tidx(m1, m2, iz)] = z1;
+                E[(c * 3 + 2) * 27 + tidx(m1, m2, iz)] = z2;
+            }
         }
 #pragma unroll
-    for (int iz = 0; iz < 3; ++iz)
-        E[9 * 27 + tidx(m1, m2, iz)] = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
+    for (int iz = 0; iz < 3; ++iz) {
+        const T zb = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
+        if (wr) E[9 * 27 + tidx(m1, m2, iz)] = zb;
+    }
     __syncwarp();
     // Y^T: thread owns y-line (qx = m1, ·, iz = m2)
     T* E1 = E + 270;
@@ -116,9 +141,13 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
         }
 #pragma unroll
         for (int iy = 0; iy < 3; ++iy) {
-            E1[(c * 2 + 0) * 27 + tidx(m1, iy, m2)] = t.B[0][iy] * TA[0] + t.B[1][iy] * TA[1] + t.B[2][iy] * TA[2];
-            E1[(c * 2 + 1) * 27 + tidx(m1, iy, m2)] = (t.Dd[0][iy] * TB[0] + t.Dd[1][iy] * TB[1] + t.Dd[2][iy] * TB[2]) +
-                                                       (t.B[0][iy] * TC[0] + t.B[1][iy] * TC[1] + t.B[2][iy] * TC[2]);
+            const T u0 = t.B[0][iy] * TA[0] + t.B[1][iy] * TA[1] + t.B[2][iy] * TA[2];
+            const T u1 = (t.Dd[0][iy] * TB[0] + t.Dd[1][iy] * TB[1] + t.Dd[2][iy] * TB[2]) +
+                         (t.B[0][iy] * TC[0] + t.B[1][iy] * TC[1] + t.B[2][iy] * TC[2]);
+            if (wr) {
+                E1[(c * 2 + 0) * 27 + tidx(m1, iy, m2)] = u0;
+                E1[(c * 2 + 1) * 27 + tidx(m1, iy, m2)] = u1;
+            }
         }
     }
     {
@@ -126,7 +155,10 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
 #pragma unroll
         for (int qy = 0; qy < 3; ++qy) TD[qy] = E[9 * 27 + tidx(m1, qy, m2)];
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy) E1[6 * 27 + tidx(m1, iy, m2)] = t.B[0][iy] * TD[0] + t.B[1][iy] * TD[1] + t.B[2][iy] * TD[2];
+        for (int iy = 0; iy < 3; ++iy) {
+            const T ub = t.B[0][iy] * TD[0] + t.B[1][iy] * TD[1] + t.B[2][iy] * TD[2];
+            if (wr) E1[6 * 27 + tidx(m1, iy, m2)] = ub;
+        }
     }
     __syncwarp();
     // X^T: thread owns x-line (·, iy = m1, iz = m2)

@@ -313,6 +313,7 @@ cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cu
     const int64_t cap = (int64_t)num_sms * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
+    count_launch();
     hex27_jacobian_kernel<T, TG><<<(unsigned)blocks, JAC_THREADS, smem, st>>>(args);
     return cudaGetLastError();
 }

@@ -5,6 +5,11 @@
 
 namespace femb {
 
+// Kernels launched by this library since the last profile reset (every launcher
+// adds one per launch); reported through femb200_profile_read.
+extern unsigned long long g_kernel_launches;
+inline void count_launch() { __atomic_fetch_add(&g_kernel_launches, 1ull, __ATOMIC_RELAXED); }
+
 constexpr int H27_THREADS = 128;   // 4 warps × 3 elements per warp
 
 template <class T, class TG>
@@ -42,6 +47,13 @@ struct H27Args {
 
 template <class T, class TG>
 cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaStream_t st);
+
+// Pipelined sweep over affine Hex27 elements with one J⁻¹, |det J| per element.
+template <class T>
+cudaError_t launch_hex27_residual_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, cudaStream_t st);
+template <class TG, class TC>
+cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t nels, TC* out, int* not_affine,
+                                     cudaStream_t st);
 
 // Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
 template <class T, class TG>

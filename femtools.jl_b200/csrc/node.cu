@@ -187,6 +187,7 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t
 
 template <class T>
 cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st) {
+    count_launch();
     node_update_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
@@ -194,48 +195,56 @@ cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st
 template <class T>
 cudaError_t launch_dirichlet(T* x, const int32_t* dofs, const T* vals, int64_t n, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
+    count_launch();
     dirichlet_kernel<T><<<nblk(n), 256, 0, st>>>(x, dofs, vals, n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_build_mask(uint8_t* mask, const int32_t* dofs, int64_t n, int comp, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
+    count_launch();
     mask_kernel<<<nblk(n), 256, 0, st>>>(mask, dofs, n, comp);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_sumsq(const T* x, const T* div, int64_t n, double* partials, int blocks, cudaStream_t st) {
+    count_launch();
     sumsq_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(x, div, n, partials);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_ratio_max(const T* J, const T* PC, int64_t n, double* partials, int blocks, cudaStream_t st) {
+    count_launch();
     ratio_max_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(J, PC, n, partials);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_pressure_update(T* P, const T* gP, const T* RP, const T* MP, int64_t n, cudaStream_t st) {
+    count_launch();
     pressure_update_kernel<T><<<nblk(n), 256, 0, st>>>(P, gP, RP, MP, n);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_pnum(T* Pn, const T* gP, const T* RP, const T* MP, int64_t n, cudaStream_t st) {
+    count_launch();
     pnum_kernel<T><<<nblk(n), 256, 0, st>>>(Pn, gP, RP, MP, n);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_sub(T* x, const T* y, int64_t n, cudaStream_t st) {
+    count_launch();
     sub_kernel<T><<<nblk(n), 256, 0, st>>>(x, y, n);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_copy(T* d, const T* s, int64_t n, cudaStream_t st) {
+    count_launch();
     copy_kernel<T><<<nblk(n), 256, 0, st>>>(d, s, n);
     return cudaGetLastError();
 }
@@ -243,6 +252,7 @@ cudaError_t launch_copy(T* d, const T* s, int64_t n, cudaStream_t st) {
 template <class T>
 cudaError_t launch_transfer_temperature(T* TP, const T* Tn, const int32_t* dofsP, const int32_t* el2nP, int64_t n,
                                         cudaStream_t st) {
+    count_launch();
     transfer_kernel<T><<<nblk(n), 256, 0, st>>>(TP, Tn, dofsP, el2nP, n);
     return cudaGetLastError();
 }
@@ -250,6 +260,7 @@ cudaError_t launch_transfer_temperature(T* TP, const T* Tn, const int32_t* dofsP
 template <class T>
 cudaError_t launch_thermal_update(T* Tn, T* rate, T* R, const T* PC, const uint8_t* mask, int64_t n, double alpha,
                                   double beta, cudaStream_t st) {
+    count_launch();
     thermal_update_kernel<T><<<nblk(n), 256, 0, st>>>(Tn, rate, R, PC, mask, n, alpha, beta);
     return cudaGetLastError();
 }
@@ -257,6 +268,7 @@ cudaError_t launch_thermal_update(T* Tn, T* rate, T* R, const T* PC, const uint8
 template <class T>
 cudaError_t launch_lmin_sums(const T* rate, const T* R, const T* R0, const T* PC, int64_t n, double step,
                              double* partials, int blocks, cudaStream_t st) {
+    count_launch();
     lmin_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(rate, R, R0, PC, n, step, partials);
     return cudaGetLastError();
 }

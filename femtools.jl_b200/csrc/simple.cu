@@ -484,24 +484,28 @@ template <class T, class TG>
 cudaError_t launch_pressure_scaling(int dim, const int32_t* el2n, const int32_t* dofsP, const TG* geo_P,
                                     const int32_t* phv, int phv_layout, const T* eta_ip, int use_eta_ip, T* MP, T* gP,
                                     int64_t nels, int64_t nnodesP, T gfact, T dt, cudaStream_t st) {
+    count_launch();
     if (dim == 3)
         pressure_scaling_kernel<3, T, TG><<<nb(nels, 128), 128, 0, st>>>(el2n, dofsP, geo_P, phv, phv_layout, eta_ip,
                                                                          use_eta_ip, MP, gP, nels, gfact, dt);
     else
         pressure_scaling_kernel<2, T, TG><<<nb(nels, 128), 128, 0, st>>>(el2n, dofsP, geo_P, phv, phv_layout, eta_ip,
                                                                          use_eta_ip, MP, gP, nels, gfact, dt);
+    count_launch();
     scaling_finalize_kernel<T><<<nb(nnodesP, 256), 256, 0, st>>>(gP, MP, nnodesP);
     return cudaGetLastError();
 }
 
 template <class T, class TG>
 cudaError_t launch_q9_residual(const H27Args<T, TG>& args, cudaStream_t st) {
+    count_launch();
     q9_residual_kernel<T, TG><<<nb(args.nels, 128), 128, 0, st>>>(args);
     return cudaGetLastError();
 }
 
 template <class T, class TG>
 cudaError_t launch_q9_jacobian(const H27JacArgs<T, TG>& args, cudaStream_t st) {
+    count_launch();
     q9_jacobian_kernel<T, TG><<<nb(args.nels, 64), 64, 0, st>>>(args);
     return cudaGetLastError();
 }
@@ -509,6 +513,7 @@ cudaError_t launch_q9_jacobian(const H27JacArgs<T, TG>& args, cudaStream_t st) {
 template <class T, class TG>
 cudaError_t launch_thermal(const ThermalArgs<T, TG>& a, int num_sms, cudaStream_t st) {
     (void)num_sms;
+    count_launch();
     if (a.dim == 3) thermal_kernel<3, T, TG><<<nb(a.nels, 64), 64, 0, st>>>(a);
     else thermal_kernel<2, T, TG><<<nb(a.nels, 128), 128, 0, st>>>(a);
     return cudaGetLastError();

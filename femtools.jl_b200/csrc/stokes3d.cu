@@ -305,6 +305,7 @@ cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaS
     const int64_t cap = (int64_t)num_sms * 16;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
+    count_launch();
     hex27_residual_kernel<T, TG><<<(unsigned)blocks, H27_THREADS, smem, st>>>(args);
     return cudaGetLastError();
 }

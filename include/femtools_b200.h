@@ -327,6 +327,21 @@ int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t,
                           int32_t shear_heating, void* phi_scratch,
                           femb200_stokes_stats* stats);
 
+/* ---- measurement (no counterpart in the reference, which has no timers) ---- */
+
+/* Kernel classes timed when profiling is on; slot FEMB200_PROF_ALL counts every
+ * kernel the library launched (its milliseconds are not measured). */
+enum { FEMB200_PROF_RESIDUAL = 0, FEMB200_PROF_JACOBIAN = 1, FEMB200_PROF_NODE = 2, FEMB200_PROF_ALL = 3,
+       FEMB200_PROF_COUNT = 4 };
+
+/* Turn per-launch CUDA-event timing of the residual sweep, the Jacobian
+ * diagnostics and the node update on (1) or off (0), and reset the totals. The
+ * events are recorded on the handle's stream around each launch. */
+int femb200_profile(femb200_handle* h, int32_t enable);
+/* Totals since the last femb200_profile(h, 1): milliseconds and launch counts per
+ * kernel class (arrays of FEMB200_PROF_COUNT). Synchronises the handle's stream. */
+int femb200_profile_read(femb200_handle* h, double* ms, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,169 +1,7 @@
-"""Seeded problem builders shared by the GPU parity tests, smoke() and bench.py.
-
-Each case holds host (numpy) inputs and can materialise them both as a device
-StokesDR (the product) and as an oracle HostStokes (the checker), so the two
-implementations see bit-identical inputs.
-"""
-from __future__ import annotations
-
-import math
-from dataclasses import dataclass, field
-from typing import Optional
-
-import numpy as np
-
+"""Test-side access to the package's seeded configurations (femtools.jl_b200/configs.py)."""
 from conftest import fem
 
-abi = fem._abi
-
-
-@dataclass
-class StokesCase:
-    mesh: object
-    material: object
-    plastic: object
-    dt: float
-    phases_v: Optional[np.ndarray] = None
-    phases_v_layout: int = abi.PHASE_NODAL
-    phases_P: Optional[np.ndarray] = None
-    phases_P_layout: int = abi.PHASE_NODAL
-    v: list = field(default_factory=list)
-    P: Optional[np.ndarray] = None
-    P0: Optional[np.ndarray] = None
-    T: Optional[np.ndarray] = None
-    T0: Optional[np.ndarray] = None
-    tau_old: Optional[list] = None
-    bc: list = field(default_factory=list)    # (dofs 1-based, vals) per component
-    gammaP: Optional[np.ndarray] = None
-    M_P: Optional[np.ndarray] = None
-    Pnum: Optional[np.ndarray] = None
-
-    def device_state(self, fem_, dtype=None, geometry_dtype=None):
-        import torch
-        dr = fem_.StokesDR(self.mesh, self.material, self.plastic, phases_v=self.phases_v,
-                           phases_v_layout=self.phases_v_layout, phases_P=self.phases_P,
-                           phases_P_layout=self.phases_P_layout, dtype=dtype, geometry_dtype=geometry_dtype)
-        for c, x in enumerate(self.v):
-            dr.v[c].copy_(dr.tensor(x))
-        for name in ("P", "P0", "T", "T0", "gammaP", "M_P", "Pnum"):
-            x = getattr(self, name)
-            if x is not None:
-                getattr(dr, name).copy_(dr.tensor(x))
-        if self.tau_old is not None:
-            for c, x in enumerate(self.tau_old):
-                dr.tau_old[c].copy_(dr.tensor(x))
-        torch.cuda.synchronize()
-        return dr
-
-    def bc_device(self):
-        return [fem.DirichletBoundaryCondition(d, v) for d, v in self.bc]
-
-    def host_state(self, oh):
-        hs = oh.HostStokes(self.mesh, self.material, self.plastic, phases_v=self.phases_v,
-                           phases_v_layout=self.phases_v_layout, phases_P=self.phases_P,
-                           phases_P_layout=self.phases_P_layout)
-        for c, x in enumerate(self.v):
-            hs.v[c][:] = x
-        for name in ("P", "P0", "T", "T0", "gammaP", "M_P", "Pnum"):
-            x = getattr(self, name)
-            if x is not None:
-                getattr(hs, name)[:] = x
-        if self.tau_old is not None:
-            for c, x in enumerate(self.tau_old):
-                hs.tau_old[c][:] = x
-        hs.set_bc(self.bc)
-        return hs
-
-
-def vep_layers_case(n=4, seed=0, dt=0.1, eta_reg=1e-2, Kb=1e2, bulk=1e2, plastic=True):
-    """3-D Hex27/P1-disc visco-elasto-plastic Stokes on the unit cube, n³ cells:
-    three horizontal layers with interfaces z1 < z2 ~ U(0.3, 0.7), per-phase
-    η = 10^U(0,3), G = 1, cohesion U(0.1, 1), ϕ = 30°, ψ = 0, ρ0 = 1, g = (0,0,−1),
-    pure-shear wall velocities vx = x − ½, vy = 0, vz = −(z − ½) (ε̇ = 1), seeded.
-
-    Fixed here (the configuration leaves them open): Δt = 0.1, η_reg = 1e-2 and
-    ηb = K = Kb = 100 (β = 0.01), the values of the reference's visco-elasto-plastic
-    shear-band example (examples/miniapps/stokes/vevp/stokes_2D_shear_bands_triangle.jl:51-76);
-    Kb must be finite because ψ = 0 makes Kb·Δt·sinΨ·sinϕ = Inf·0 otherwise."""
-    rng = np.random.default_rng(seed)
-    z1, z2 = np.sort(rng.uniform(0.3, 0.7, size=2))
-    eta = tuple(10.0 ** rng.uniform(0.0, 3.0, size=3))
-    C = tuple(rng.uniform(0.1, 1.0, size=3))
-    mesh = fem.structured_mixed_mesh(3, (n, n, n))
-    zc = fem.mesh.cell_centroids(mesh)[:, 2]
-    phase = np.where(zc < z1, 1, np.where(zc < z2, 2, 3)).astype(np.int32)
-    mat = fem.StokesMaterial(eta=eta, eta_b=(bulk,) * 3, G=(1.0,) * 3, alpha=(0.0,) * 3, rho0=(1.0,) * 3,
-                             K=(bulk,) * 3, g=(0.0, 0.0, -1.0), Tref=0.0)
-    pl = fem.DruckerPrager.from_angles((math.radians(30),) * 3, (0.0,) * 3, C, (eta_reg,) * 3, (Kb,) * 3) \
-        if plastic else None
-    x, y, z = mesh.coords.T
-    fields = [x - 0.5, np.zeros_like(y), -(z - 0.5)]
-    b = mesh.boundary_nodes
-    bc = [(b, f[b - 1].copy()) for f in fields]
-    case = StokesCase(mesh, mat, pl, dt, phases_v=phase, phases_v_layout=abi.PHASE_CELL, phases_P=phase,
-                      phases_P_layout=abi.PHASE_CELL, v=[f.copy() for f in fields],
-                      P=np.zeros(mesh.nnodesP), P0=np.zeros(mesh.nnodesP), T=np.zeros(mesh.nnodesP),
-                      T0=np.zeros(mesh.nnodesP), tau_old=[np.zeros(mesh.nq * mesh.nels) for _ in range(6)], bc=bc)
-    case.meta = dict(z1=z1, z2=z2, eta=eta, C=C)
-    return case
-
-
-def inclusion_2d_case(n=64, dt=1.0):
-    """2-D Q9/P1-disc plane-strain viscous Stokes on the unit square: circular inclusion
-    r = 0.1 at (½, ½) with η = 1e3, ρ = 1.1 in a matrix η = 1, ρ = 1; g = (0, −1); free
-    slip on all walls (vx = 0 on x ∈ {0,1}, vy = 0 on y ∈ {0,1})."""
-    mesh = fem.structured_mixed_mesh(2, (n, n))
-    c = fem.mesh.cell_centroids(mesh)
-    phase = np.where(np.hypot(c[:, 0] - 0.5, c[:, 1] - 0.5) < 0.1, 2, 1).astype(np.int32)
-    mat = fem.StokesMaterial(eta=(1.0, 1e3), eta_b=(math.inf, math.inf), G=(math.inf, math.inf), alpha=(0.0, 0.0),
-                             rho0=(1.0, 1.1), K=(math.inf, math.inf), g=(0.0, -1.0))
-    bx = fem.mesh.wall_nodes(mesh, 0)
-    by = fem.mesh.wall_nodes(mesh, 1)
-    bc = [(bx, np.zeros(len(bx))), (by, np.zeros(len(by)))]
-    return StokesCase(mesh, mat, None, dt, phases_v=phase, phases_v_layout=abi.PHASE_CELL, phases_P=phase,
-                      phases_P_layout=abi.PHASE_CELL, v=[np.zeros(mesh.nnodes)] * 2, P=np.zeros(mesh.nnodesP),
-                      P0=np.zeros(mesh.nnodesP), T=np.zeros(mesh.nnodesP), T0=np.zeros(mesh.nnodesP),
-                      tau_old=[np.zeros(mesh.nq * mesh.nels) for _ in range(3)], bc=bc)
-
-
-def random_state_case(dim=3, n=3, seed=0, phases="nodal", plastic=True, nphases=3, elastic=True):
-    """Random fields on a slightly distorted mesh for element-level parity: random v,
-    P, P0, T, T0, τ_old, γP, M_P and phases in one of the three layouts."""
-    rng = np.random.default_rng(seed)
-    mesh = fem.structured_mixed_mesh(dim, (n,) * dim)
-    # distort interior nodes (keeps elements valid) so J⁻¹ is not diagonal
-    coords = mesh.coords.copy()
-    h = 1.0 / (2 * n)
-    interior = np.all((coords > 1e-12) & (coords < 1 - 1e-12), axis=1)
-    coords[interior] += rng.uniform(-0.15 * h, 0.15 * h, size=(interior.sum(), dim))
-    geo_v, geo_P = fem.mesh.precompute_geometry(coords, mesh.el2n, fem.element_tables(dim))
-    mesh.coords, mesh.geo_v, mesh.geo_P = coords, geo_v, geo_P
-    ph = nphases
-    mat = fem.StokesMaterial(eta=tuple(10 ** rng.uniform(0, 2, ph)), eta_b=tuple(rng.uniform(5, 50, ph)),
-                             G=tuple(rng.uniform(0.5, 3, ph)) if elastic else (math.inf,) * ph,
-                             alpha=tuple(rng.uniform(0, 0.1, ph)), rho0=tuple(rng.uniform(1, 2, ph)),
-                             K=tuple(rng.uniform(10, 100, ph)), g=(0.0, -1.0) if dim == 2 else (0.0, 0.3, -1.0),
-                             Tref=0.1)
-    pl = fem.DruckerPrager.from_angles(tuple(rng.uniform(0.3, 0.6, ph)), tuple(rng.uniform(0.0, 0.2, ph)),
-                                       tuple(rng.uniform(0.05, 0.3, ph)), tuple(rng.uniform(0.01, 0.1, ph)),
-                                       tuple(rng.uniform(1, 10, ph))) if plastic else None
-    nv, npd = mesh.nv, mesh.np_
-    if phases == "nodal":
-        pv, lv = rng.integers(1, ph + 1, mesh.nnodes).astype(np.int32), abi.PHASE_NODAL
-        pp, lp = rng.integers(1, ph + 1, mesh.nnodesP).astype(np.int32), abi.PHASE_NODAL
-    elif phases == "cell":
-        pv = rng.integers(1, ph + 1, mesh.nels).astype(np.int32)
-        lv, pp, lp = abi.PHASE_CELL, pv, abi.PHASE_CELL
-    else:
-        pv, lv = rng.integers(1, ph + 1, (mesh.nels, nv)).astype(np.int32), abi.PHASE_ELEMENT_NODE
-        pp, lp = rng.integers(1, ph + 1, (mesh.nels, npd)).astype(np.int32), abi.PHASE_ELEMENT_NODE
-    nt = 6 if dim == 3 else 3
-    case = StokesCase(mesh, mat, pl, 0.7, phases_v=pv, phases_v_layout=lv, phases_P=pp, phases_P_layout=lp,
-                      v=[rng.standard_normal(mesh.nnodes) for _ in range(dim)],
-                      P=rng.standard_normal(mesh.nnodesP) * 0.3, P0=rng.standard_normal(mesh.nnodesP) * 0.3,
-                      T=rng.standard_normal(mesh.nnodesP), T0=rng.standard_normal(mesh.nnodesP),
-                      tau_old=[rng.standard_normal(mesh.nq * mesh.nels) * 0.3 for _ in range(nt)],
-                      gammaP=rng.uniform(1, 5, mesh.nnodesP), M_P=rng.uniform(0.01, 0.1, mesh.nnodesP),
-                      Pnum=rng.standard_normal(mesh.nnodesP) * 0.1,
-                      bc=[(mesh.boundary_nodes, np.zeros(len(mesh.boundary_nodes)))] * dim)
-    return case
+StokesCase = fem.configs.StokesCase
+vep_layers_case = fem.configs.vep_layers_case
+inclusion_2d_case = fem.configs.inclusion_2d_case
+random_state_case = fem.configs.random_state_case
