@@ -145,7 +145,9 @@ SIGNATURES = {
                                         _P(StokesStatsC)]),
     "femb200_profile": (C.c_int, [_vp, C.c_int32]),
     "femb200_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_int64)]),
+    "femb200_solve_thermal_noalloc": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
 }
+NOALLOC_MAX_NODES = 8388608   # FEMB200_NOALLOC_MAX_NODES
 PROF_RESIDUAL, PROF_JACOBIAN, PROF_NODE, PROF_ALL, PROF_COUNT = range(5)
 
 _lib = None

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.cuh"
 
@@ -1064,6 +1065,178 @@ int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t, const f
     Coupled cp{t, Tref, shear_heating ? phi_scratch : nullptr};
     RC(dispatch<DoSolve>(p, h, p, c, st, &cp));
     return finish_solve(h, c, st);
+}
+
+}  // extern "C"
+
+// ---- allocation-free thermal solve (femb200_solve_thermal_noalloc) ----------
+//
+// For hosts that own all device memory through their own pool, or that cannot
+// take the device-wide synchronisation of cudaFree / cudaMallocHost, this solve
+// keeps its Dirichlet mask and reduction partials in one fixed array of the
+// library's device image instead of handle buffers grown with cudaMalloc. The
+// final reduction over blocks runs on the device (one thread per slot, blocks in
+// order, the same summation order as fetch_sums), so the host reads back a few
+// doubles into a stack buffer and needs no pinned memory.
+namespace {
+
+constexpr int64_t NA_MAX_NODES = FEMB200_NOALLOC_MAX_NODES;
+constexpr int NA_MAX_BLOCKS = 1024;
+constexpr size_t NA_PARTIALS = (size_t)NA_MAX_BLOCKS * RED_SLOTS;   // doubles
+constexpr size_t NA_RESULT = 16;                                     // doubles
+constexpr size_t NA_BYTES = (NA_PARTIALS + NA_RESULT) * sizeof(double) + (size_t)NA_MAX_NODES;
+constexpr int NA_MAX_DEVICES = 64;
+
+}  // namespace
+
+// Layout: [block partials | reduced slots | one mask byte per node]. In host code
+// the name is only a handle for cudaGetSymbolAddress, never a device address.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_base[NA_MAX_DEVICES] = {};
+
+struct NoallocScratch {
+    double* partials;
+    double* result;
+    uint8_t* mask;
+};
+
+// Device address of the scratch array on the handle's device, looked up once per
+// device (the first call on a device does it; it must not fall inside a capture).
+int noalloc_scratch(femb200_handle* h, NoallocScratch& s) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev != h->device) {
+        h->err = "femb200_solve_thermal_noalloc: the current device (" + std::to_string(dev) +
+                 ") is not the handle's device (" + std::to_string(h->device) + ")";
+        return FEMB200_EINVAL;
+    }
+    if (dev < 0 || dev >= NA_MAX_DEVICES) { h->err = "femb200_solve_thermal_noalloc: device ordinal out of range"; return FEMB200_EINVAL; }
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void* p = nullptr;
+            CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_base[dev] = static_cast<unsigned char*>(p);
+        }
+        base = g_noalloc_base[dev];
+    }
+    s.partials = reinterpret_cast<double*>(base);
+    s.result = s.partials + NA_PARTIALS;
+    s.mask = reinterpret_cast<uint8_t*>(s.result + NA_RESULT);
+    return FEMB200_OK;
+}
+
+// result[s] = Σ_b partials[b][s] (mode 0, s < nslots) or, for the λmax check
+// (mode 1), result[0] = max_b partials[b][0] and result[1] = 1 if any block
+// flagged a NaN. One thread per slot, blocks in ascending order.
+__global__ void noalloc_finalize_kernel(const double* partials, int blocks, int nslots, int mode, double* result) {
+    const int s = threadIdx.x;
+    if (s >= nslots) return;
+    if (mode == 0) {
+        double t = 0;
+        for (int b = 0; b < blocks; ++b) t += partials[(size_t)b * RED_SLOTS + s];
+        result[s] = t;
+    } else if (s == 0) {
+        double m = -INFINITY, f = 0;
+        for (int b = 0; b < blocks; ++b) {
+            m = fmax(m, partials[(size_t)b * RED_SLOTS]);
+            if (partials[(size_t)b * RED_SLOTS + 1] != 0) f = 1;
+        }
+        result[0] = m;
+        result[1] = f;
+    }
+}
+
+int noalloc_read(femb200_handle* h, const NoallocScratch& s, int blocks, int nslots, int mode, double* out) {
+    count_launch();
+    noalloc_finalize_kernel<<<1, 32, 0, h->stream>>>(s.partials, blocks, nslots, mode, s.result);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, s.result, sizeof(double) * nslots, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FEMB200_OK;
+}
+
+// _checked_λmax (src/utils.jl:152-158) on the scratch partials.
+int noalloc_lmax(femb200_handle* h, const NoallocScratch& s, const double* J, const double* PC, int64_t n, int blocks,
+                 double& out) {
+    CK(launch_ratio_max<double>(J, PC, n, s.partials, blocks, h->stream));
+    double r[2];
+    RC(noalloc_read(h, s, blocks, 2, 1, r));
+    double m = r[1] != 0 ? NAN : r[0];
+    if (!(std::isfinite(m) && m > 0)) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "thermal diffusion preconditioner produced invalid λmax = %g; check for zero or non-finite preconditioner entries", m);
+        h->err = buf;
+        return FEMB200_ELAMBDA;
+    }
+    out = m;
+    return FEMB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// solve_dynamic_relaxation! for the thermal DR (src/dynamic_relaxation/solver.jl:61-122),
+// step for step as femb200_solve_thermal, with all scratch in g_noalloc_scratch.
+int femb200_solve_thermal_noalloc(femb200_handle* h, const femb200_thermal_problem* t, const femb200_thermal_controls* c,
+                                  femb200_thermal_stats* st) {
+    if (!h || !t || !c || !st) return FEMB200_EINVAL;
+    if (t->dtype != FEMB200_F64 || t->geo_dtype != FEMB200_F64) { h->err = "the thermal solver runs in FP64"; return FEMB200_EUNSUPPORTED; }
+    if (t->nnodes < 1 || t->nnodes > NA_MAX_NODES) {
+        h->err = "femb200_solve_thermal_noalloc: nnodes = " + std::to_string((long long)t->nnodes) +
+                 " is outside 1:" + std::to_string((long long)NA_MAX_NODES) +
+                 " (the fixed scratch size; use femb200_solve_thermal for larger meshes)";
+        return FEMB200_EINVAL;
+    }
+    if (c->check_interval < 1) { h->err = "check_interval must be positive"; return FEMB200_EINVAL; }
+    using T = double;
+    NoallocScratch s;
+    RC(noalloc_scratch(h, s));
+    RC(upload_thermal_material(h, t));
+    const int64_t n = t->nnodes;
+    // the mask region keeps the previous call's bits: clear it before setting this call's
+    CK(cudaMemsetAsync(s.mask, 0, (size_t)n, h->stream));
+    if (t->bc_n > 0) CK(launch_build_mask(s.mask, t->bc_dofs, t->bc_n, 0, h->stream));
+    const int nbk = std::min(red_blocks(h, n), NA_MAX_BLOCKS);
+    double a = 0, b = 0, nr0 = 0, last = NAN, lmax = 0;
+    for (int64_t it = 1; it <= c->max_iterations; ++it) {
+        const bool dj = (it % c->check_interval == 0) || it == 1;
+        if (dj) CK(launch_copy<T>(static_cast<T*>(t->R0), static_cast<const T*>(t->R), n, h->stream));
+        RC((thermal_assemble<T, T>(h, t, c->dt, c->Tref, dj, t->source_ip)));
+        if (dj) RC(noalloc_lmax(h, s, static_cast<const T*>(t->dRdT), static_cast<const T*>(t->PC), n, nbk, lmax));
+        CK(launch_thermal_update<T>(static_cast<T*>(t->T), static_cast<T*>(t->rate), static_cast<T*>(t->R),
+                                    static_cast<const T*>(t->PC), s.mask, n, a, b, h->stream));
+        if (t->bc_n > 0) CK(launch_dirichlet<T>(static_cast<T*>(t->T), t->bc_dofs, static_cast<const T*>(t->bc_vals), t->bc_n, h->stream));
+        if (dj) {
+            const double dtau = 2 / std::sqrt(lmax) * t->cfl;
+            CK(launch_lmin_sums<T>(static_cast<const T*>(t->rate), static_cast<const T*>(t->R), static_cast<const T*>(t->R0),
+                                   static_cast<const T*>(t->PC), n, dtau, s.partials, nbk, h->stream));
+            double r[3];
+            RC(noalloc_read(h, s, nbk, 3, 0, r));
+            const double nr = std::sqrt(r[2]);
+            if (it == 1) nr0 = std::max(nr, julia_eps(nr));
+            if (std::isnan(nr / nr0)) { char bb[64]; std::snprintf(bb, sizeof bb, "NaNs at PT iter %lld", (long long)it); h->err = bb; return FEMB200_ENAN; }
+            const double lmin = (it == 1 || r[0] == 0) ? 0.0 : std::fabs(r[1]) / r[0];
+            cheb(dtau, lmin, t->c_fact, a, b);
+            last = nr / nr0;
+            if (last < c->tolerance) { st->converged = 1; st->iterations = it; st->residual = last; return FEMB200_OK; }
+        }
+    }
+    st->converged = 0; st->iterations = c->max_iterations; st->residual = last;
+    if (c->throw_on_failure) {
+        char bb[256];
+        std::snprintf(bb, sizeof bb, "Thermal diffusion DR solver did not converge after %lld pseudo-transient iterations (relative residual = %g)",
+                      (long long)c->max_iterations, last);
+        h->err = bb;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
 }
 
 }  // extern "C"

@@ -342,6 +342,38 @@ int femb200_profile(femb200_handle* h, int32_t enable);
  * kernel class (arrays of FEMB200_PROF_COUNT). Synchronises the handle's stream. */
 int femb200_profile_read(femb200_handle* h, double* ms, int64_t* launches);
 
+/* ---- allocation-free thermal solve ---------------------------------------- */
+
+/* Largest thermal mesh (velocity-node count) femb200_solve_thermal_noalloc accepts. */
+#define FEMB200_NOALLOC_MAX_NODES 8388608
+
+/* No counterpart in the reference. The same thermal DR solve as
+ * femb200_solve_thermal, for callers that must not have the library allocate GPU
+ * or pinned host memory: a host that hands all device memory to its own pool
+ * (Julia's CUDA.jl pool, PyTorch's caching allocator, an arena sized to the GPU)
+ * and runs close to the limit, where a cudaMalloc from the library fails or forces
+ * the pool to release memory; or a host that cannot afford the implicit device-wide
+ * synchronisation of cudaFree and cudaMallocHost while other streams are busy.
+ * femb200_solve_thermal grows its Dirichlet mask and reduction buffers with those
+ * calls; this entry point uses instead one fixed scratch array in the library's
+ * device image (FEMB200_NOALLOC_MAX_NODES bytes of mask plus about 100 KB of
+ * reduction space, 8.5 MB in all), which every GPU that loads the library holds
+ * until the process exits. It calls no cudaMalloc, cudaFree, cudaMallocHost or
+ * other allocating routine.
+ *
+ * - Inputs, outputs and status are those of femb200_solve_thermal (FP64 only).
+ * - t->nnodes above FEMB200_NOALLOC_MAX_NODES is rejected with FEMB200_EINVAL
+ *   before any work is queued.
+ * - The first call on a device looks up the scratch array's device address
+ *   (cudaGetSymbolAddress, with that device current; it must be the handle's
+ *   device). Make that first call before any stream capture begins.
+ * - Every call, on every stream and handle of the process, shares the one array,
+ *   and the array keeps the last call's contents; each call clears the part that
+ *   must start at zero. Calls that overlap on the GPU (other streams, other host
+ *   threads) race on it and give wrong results: serialise them. */
+int femb200_solve_thermal_noalloc(femb200_handle* h, const femb200_thermal_problem* t,
+                                  const femb200_thermal_controls* c, femb200_thermal_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif
