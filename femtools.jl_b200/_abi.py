@@ -71,7 +71,6 @@ class StokesControlsC(C.Structure):
         ("precision", C.c_int32),
         ("cfl_v", C.c_double), ("c_fact", C.c_double),
         ("history", C.POINTER(C.c_double)), ("history_capacity", C.c_int64),
-        ("mixed_inner_drop", C.c_double),
     ]
 
 

@@ -13,6 +13,7 @@
 #include <vector>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -52,6 +53,15 @@ struct femb200_handle {
     int* h_flag = nullptr;
     bool geo_c_valid = false;
     int use_pipe = 1;   // the pipelined sweep on affine meshes (0 forces the general sweep)
+    // FP32 arrays of the mixed-precision solve, carved from one allocation
+    struct Mixed {
+        void* mem = nullptr;
+        size_t cap = 0;
+        float *dv[3], *rate[3], *R[3], *R0[3], *Rk[3], *dRdv[3], *PC[3], *v32[3];
+        float *dP, *RP, *RPk, *gP, *MP, *P32, *P0, *T, *T0, *Pf;
+        float *base[7], *told[6], *eta;
+        float* geo;
+    } mixed;
 };
 
 namespace {
@@ -751,6 +761,274 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
     return FEMB200_OK;
 }
 
+// ---- mixed precision: FP32 Chebyshev iterations on increments, FP64 outer steps ----
+//
+// The solve runs the DR iteration of solve_dyrel with one change in how the
+// residual is evaluated. At every Powell–Hestenes step the FP32 increments
+// (δv, δP) are folded into the caller's FP64 state and an FP64 sweep gives the
+// outer convergence test exactly as the plain solve computes it; a second FP64
+// sweep (with Pnum) gives the base residual R_k and stores the trial stress and
+// yield value of every integration point in FP32. The Chebyshev iterations then
+// update δ in FP32 against R_k + [R(x_k + δ) − R(x_k)], whose bracket the
+// incremental sweep forms from δ alone, so that FP32 rounding scales with the
+// increment (and, late in the solve, with the small residual) rather than with
+// the state. The Jacobian diagnostics (λmax and the preconditioner) run in FP32 on
+// the FP32 image of x_k + δ. FP64 is used for every norm and convergence test,
+// the outer residual, and the return map of points near the yield-surface apex.
+
+int ensure_mixed(femb200_handle* h, const femb200_stokes_problem* p) {
+    auto& m = h->mixed;
+    const size_t nn = p->nnodes, nP = p->nnodesP, nip = (size_t)p->nq * p->nels;
+    const bool ip = p->tau_old_layout == FEMB200_FIELD_IP;
+    std::vector<std::pair<float**, size_t>> parts;
+    for (int c = 0; c < 3; ++c)
+        for (float** a : {&m.dv[c], &m.rate[c], &m.R[c], &m.R0[c], &m.Rk[c], &m.dRdv[c], &m.PC[c], &m.v32[c]})
+            parts.push_back({a, c < p->dim ? nn : 0});
+    for (float** a : {&m.dP, &m.RP, &m.RPk, &m.gP, &m.MP, &m.P32}) parts.push_back({a, nP});
+    parts.push_back({&m.P0, p->P0 ? nP : 0});
+    parts.push_back({&m.T, p->T ? nP : 0});
+    parts.push_back({&m.T0, p->T0 ? nP : 0});
+    parts.push_back({&m.Pf, p->Pf ? nP : 0});
+    for (int c = 0; c < 7; ++c) parts.push_back({&m.base[c], nip});
+    for (int c = 0; c < 6; ++c) parts.push_back({&m.told[c], ip && p->tau_old[c] ? nip : 0});
+    parts.push_back({&m.eta, p->viscosity_ip ? nip : 0});
+    parts.push_back({&m.geo, (size_t)p->nels * 10});
+    auto al = [](size_t n) { return (n * sizeof(float) + 255) / 256 * 256; };
+    size_t total = 0;
+    for (auto& pr : parts) total += al(pr.second);
+    if (total > m.cap) {
+        if (m.mem) cudaFree(m.mem);
+        m.mem = nullptr; m.cap = 0;
+        CK(cudaMalloc(&m.mem, total));
+        m.cap = total;
+    }
+    char* b = static_cast<char*>(m.mem);
+    size_t off = 0;
+    for (auto& pr : parts) {
+        *pr.first = pr.second ? reinterpret_cast<float*>(b + off) : nullptr;
+        off += al(pr.second);
+    }
+    return FEMB200_OK;
+}
+
+template <class TG>
+int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
+                      femb200_stokes_stats* st) {
+    using T = double;
+    const int D = p->dim;
+    const int64_t nn = p->nnodes, nP = p->nnodesP;
+    const double dt = c->dt;
+    const int finite_K = c->finite_K;
+    const bool freeze = c->freeze_jacobian < 0 ? (p->mat.plastic == 0) : (c->freeze_jacobian != 0);
+    const int64_t nout = c->check_interval > 0 ? c->check_interval : 50;
+    const double cfl = c->cfl_v > 0 ? c->cfl_v : 0.98, cf = c->c_fact > 0 ? c->c_fact : 0.9;
+    static const char* labels[3] = {"stokes vx", "stokes vy", "stokes vz"};
+    std::memset(st, 0, sizeof(*st));
+    if (D != 3) { h->err = "the mixed-precision solve needs a 3-D Hex27 mesh"; return FEMB200_EUNSUPPORTED; }
+    if (!p->RP || !p->M_P || !p->gammaP || !p->Pnum) { h->err = "RP, M_P, γP and Pnum are required"; return FEMB200_EINVAL; }
+    if (p->P_old && p->P_old_layout == FEMB200_FIELD_IP) { h->err = "the mixed-precision solve takes P_old on pressure DoFs"; return FEMB200_EUNSUPPORTED; }
+
+    RC(upload_material(h, p->mat, finite_K, dt));
+    RC((prepare_geometry<T, TG>(h, p)));
+    if (!h->geo_c_valid) { h->err = "the mixed-precision solve needs affine (parallelepiped) Hex27 elements"; return FEMB200_EUNSUPPORTED; }
+    RC(build_mask(h, p));
+    RC(ensure_mixed(h, p));
+    auto& m = h->mixed;
+    cudaStream_t s = h->stream;
+    const size_t nip = (size_t)p->nq * p->nels;
+    CK(launch_compress_geometry<TG, float>(static_cast<const TG*>(p->geo_v), static_cast<const TG*>(p->geo_P), p->nels,
+                                           m.geo, h->d_flag, s));
+    CK(launch_round(m.gP, static_cast<const T*>(p->gammaP), nullptr, nP, s));
+    CK(launch_round(m.MP, static_cast<const T*>(p->M_P), nullptr, nP, s));
+    if (m.P0) CK(launch_round(m.P0, static_cast<const T*>(p->P0), nullptr, nP, s));
+    if (m.T) CK(launch_round(m.T, static_cast<const T*>(p->T), nullptr, nP, s));
+    if (m.T0) CK(launch_round(m.T0, static_cast<const T*>(p->T0), nullptr, nP, s));
+    if (m.Pf) CK(launch_round(m.Pf, static_cast<const T*>(p->Pf), nullptr, nP, s));
+    for (int k = 0; k < 6; ++k)
+        if (m.told[k]) CK(launch_round(m.told[k], static_cast<const T*>(p->tau_old[k]), nullptr, (int64_t)nip, s));
+    if (m.eta) CK(launch_round(m.eta, static_cast<const T*>(p->viscosity_ip), nullptr, (int64_t)nip, s));
+    for (int k = 0; k < D; ++k) {
+        CK(cudaMemsetAsync(m.dv[k], 0, sizeof(float) * nn, s));
+        CK(cudaMemsetAsync(m.rate[k], 0, sizeof(float) * nn, s));
+        CK(cudaMemsetAsync(m.R0[k], 0, sizeof(float) * nn, s));
+    }
+    CK(cudaMemsetAsync(m.dP, 0, sizeof(float) * nP, s));
+
+    // FP32 image of x_k + δ for the Jacobian diagnostics
+    femb200_stokes_problem pj = *p;
+    pj.dtype = FEMB200_F32;
+    for (int k = 0; k < 3; ++k) { pj.v[k] = m.v32[k]; pj.dRdv[k] = m.dRdv[k]; pj.PC[k] = m.PC[k]; }
+    pj.P = m.P32; pj.P0 = m.P0; pj.T = m.T; pj.T0 = m.T0; pj.Pf = m.Pf; pj.gammaP = m.gP; pj.M_P = m.MP;
+    for (int k = 0; k < 6; ++k) pj.tau_old[k] = m.told[k];
+    pj.viscosity_ip = m.eta;
+    double lmax[3] = {0, 0, 0};
+    int64_t jac_assemblies = 0;
+    auto jacobian32 = [&]() -> int {
+        for (int k = 0; k < D; ++k) CK(launch_round(m.v32[k], static_cast<const T*>(p->v[k]), m.dv[k], nn, s));
+        CK(launch_round(m.P32, static_cast<const T*>(p->P), m.dP, nP, s));
+        RC((jacobian_sweep<float, TG>(h, &pj, dt)));
+        ++jac_assemblies;
+        for (int k = 0; k < D; ++k) RC(checked_lmax<float>(h, m.dRdv[k], m.PC[k], nn, labels[k], lmax[k]));
+        return FEMB200_OK;
+    };
+
+    // incremental FP32 sweep: v, P are δv, δP; Rv starts from R_k
+    femb200_stokes_problem pi = *p;
+    pi.dtype = FEMB200_F32; pi.geo_dtype = FEMB200_F32; pi.geo_v = nullptr; pi.geo_P = nullptr;
+    for (int k = 0; k < 3; ++k) { pi.v[k] = m.dv[k]; pi.Rv[k] = m.R[k]; pi.tau_old[k] = nullptr; pi.tau_old[k + 3] = nullptr; }
+    pi.P = m.dP; pi.P0 = nullptr; pi.P_old = nullptr; pi.T = nullptr; pi.T0 = nullptr; pi.Q = nullptr; pi.Pf = nullptr;
+    pi.gammaP = m.gP; pi.M_P = m.MP; pi.RP = m.RP; pi.viscosity_ip = m.eta;
+    H27Args<float, float> ai = residual_args<float, float>(&pi, dt);
+    ai.with_pnum = 1; ai.do_momentum = 1; ai.write_RP = 1; ai.Pnum_out = nullptr;
+    for (int k = 0; k < 7; ++k) ai.base_in[k] = m.base[k];
+    ai.RP_base = m.RPk;
+    auto incr_sweep = [&]() -> int {
+        for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
+        RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
+        CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
+        RC(prof_end(h, FEMB200_PROF_RESIDUAL));
+        return FEMB200_OK;
+    };
+    auto apply_bc_R = [&]() -> int {
+        for (int k = 0; k < D; ++k) {
+            if (p->body_force[k]) CK(launch_sub<T>(static_cast<T*>(p->Rv[k]), static_cast<const T*>(p->body_force[k]), nn, s));
+            if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(static_cast<T*>(p->Rv[k]), p->bc_dofs[k], nullptr, p->bc_n[k], s));
+        }
+        return FEMB200_OK;
+    };
+    // FP64 base sweep at x_k (with Pnum): R_k, RP_k and the per-point base data
+    int64_t base_sweeps = 0;
+    auto base_sweep = [&]() -> int {
+        H27Args<T, TG> a = residual_args<T, TG>(p, dt);
+        a.with_pnum = 1; a.do_momentum = 1; a.write_RP = 1;
+        a.Pnum_out = static_cast<T*>(p->Pnum);
+        for (int k = 0; k < 7; ++k) a.base_out[k] = m.base[k];
+        RC((launch_residual<T, TG>(h, p, a)));
+        RC(apply_bc_R());
+        for (int k = 0; k < D; ++k) CK(launch_round(m.Rk[k], static_cast<const T*>(p->Rv[k]), nullptr, nn, s));
+        CK(launch_round(m.RPk, static_cast<const T*>(p->RP), nullptr, nP, s));
+        ++base_sweeps;
+        return FEMB200_OK;
+    };
+    auto fold = [&]() -> int {
+        for (int k = 0; k < D; ++k) CK(launch_fold(static_cast<T*>(p->v[k]), m.dv[k], nn, s));
+        CK(launch_fold(static_cast<T*>(p->P), m.dP, nP, s));
+        return FEMB200_OK;
+    };
+
+    RC(jacobian32());
+    double lmax_g = *std::max_element(lmax, lmax + D);
+    double alpha[3] = {0, 0, 0}, beta[3] = {0, 0, 0}, dtau[3];
+    for (int k = 0; k < D; ++k) { dtau[k] = 2 / std::sqrt(lmax[k]) * cfl; cheb(dtau[k], 0.0, cf, alpha[k], beta[k]); }
+
+    double err_min = INFINITY, eps = c->tolerance;
+    double err = 2 * eps, err_abs = INFINITY, err_rel = INFINITY;
+    double err_v0 = 1.0, err_P0 = 1.0, err_v00 = 1.0, err_v = INFINITY, err_P = INFINITY;
+    int64_t iter = 0, itPH_done = 0, hist = 0;
+    bool converged = false;
+    double rel_drop = c->rel_drop0;
+    const double sq_nn = std::sqrt((double)nn), sq_nP = std::sqrt((double)nP);
+    auto push_hist = [&](double it, double ev, double eP, const double* comps) {
+        if (c->history && hist < c->history_capacity) {
+            double* hh = c->history + hist * (4 + D);
+            hh[0] = it; hh[1] = ev; hh[2] = eP; hh[3] = 0;
+            for (int k = 0; k < D; ++k) hh[4 + k] = comps[k];
+        }
+        ++hist;
+    };
+    const int nb = red_blocks(h, nn);
+    RC(ensure_partials(h, std::max(nb, red_blocks(h, nP))));
+
+    for (int64_t itPH = 1; itPH <= c->max_ph_iterations; ++itPH) {
+        itPH_done = itPH;
+        RC(fold());
+        RC((residual_sweep<T, TG>(h, p, dt, 0, 1, 1)));
+        RC(apply_bc_R());
+        double sP;
+        RC(sumsq<T>(h, static_cast<const T*>(p->RP), static_cast<const T*>(p->M_P), nP, sP));
+        err_P = std::sqrt(sP) / sq_nP;
+        double comps[3] = {0, 0, 0};
+        err_v = 0;
+        for (int k = 0; k < D; ++k) {
+            double sv;
+            RC(sumsq<T>(h, static_cast<const T*>(p->Rv[k]), (const T*)nullptr, nn, sv));
+            comps[k] = std::sqrt(sv) / (2 * sq_nn);
+            err_v = std::max(err_v, std::sqrt(sv));
+        }
+        err_v /= 2 * sq_nn;
+        push_hist((double)iter, err_v, err_P, comps);
+        if (itPH == 1) { err_P0 = err_P + julia_eps(err_P); err_v0 = err_v + julia_eps(err_v); }
+        else if (itPH == 2) err_P0 = err_P + julia_eps(err_P);
+        err_abs = std::max(err_v, err_P);
+        err_rel = std::max(err_v / err_v0, err_P / err_P0);
+        err = std::min(err_abs, err_rel);
+        if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_ENAN; }
+        if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_EKABOOM; }
+        if (err < eps) { converged = true; break; }
+        if (err > err_min * 1.05) rel_drop = std::max(rel_drop * 0.1, 1.0e-3);
+        err_min = std::min(err_min, err);
+        const double eps_vel = err * rel_drop;
+        RC(base_sweep());
+        int64_t itPT = 0;
+        while (err > eps_vel && itPT <= c->iter_max) {
+            ++itPT; ++iter;
+            const bool do_check = iter % nout == 0;
+            if (do_check)
+                for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R0[k], m.R[k], nn, s));
+            RC(incr_sweep());
+            NodeArgs<float> na;
+            std::memset(&na, 0, sizeof(na));
+            for (int k = 0; k < 3; ++k) {
+                na.v[k] = m.dv[k]; na.rate[k] = m.rate[k]; na.Rv[k] = m.R[k]; na.Rv0[k] = m.R0[k]; na.PC[k] = m.PC[k];
+                na.alpha[k] = -alpha[k]; na.beta[k] = beta[k]; na.lam_step[k] = alpha[k];
+            }
+            na.mask = h->d_mask; na.n = nn; na.dim = D;
+            na.reduce = do_check ? 1 : 0;
+            na.partials = h->d_partials;
+            RC(prof_begin(h, FEMB200_PROF_NODE));
+            CK(launch_node_update<float>(na, nb, s));
+            RC(prof_end(h, FEMB200_PROF_NODE));
+            if (do_check) {
+                double sr[RED_SLOTS];
+                RC(fetch_sums(h, nb, RED_SLOTS, sr));
+                double ev = 0, cmp[3] = {0, 0, 0};
+                for (int k = 0; k < D; ++k) { ev = std::max(ev, std::sqrt(sr[3 * k])); cmp[k] = std::sqrt(sr[3 * k]) / (2 * sq_nn); }
+                ev /= 2 * sq_nn;
+                if (iter == nout) err_v00 = ev + julia_eps(ev);
+                err = ev <= eps ? ev : std::max(ev / err_v00, ev);
+                if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_ENAN; }
+                if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_EKABOOM; }
+                if (c->history) {
+                    double sPc;
+                    RC(sumsq<float>(h, m.RP, m.MP, nP, sPc));
+                    push_hist((double)iter, ev, std::sqrt(sPc) / sq_nP, cmp);
+                } else {
+                    ++hist;
+                }
+                double lmin[3];
+                for (int k = 0; k < D; ++k) lmin[k] = sr[3 * k + 1] == 0 ? 0.0 : std::fabs(sr[3 * k + 2]) / sr[3 * k + 1];
+                if (!freeze) {
+                    RC(jacobian32());
+                    lmax_g = *std::max_element(lmax, lmax + D);
+                }
+                for (int k = 0; k < D; ++k) { dtau[k] = 2 / std::sqrt(lmax[k]) * cfl; cheb(dtau[k], lmin[k], cf, alpha[k], beta[k]); }
+            }
+            if (iter > c->max_iterations) break;
+        }
+        CK(launch_pressure_update<float>(m.dP, m.gP, m.RP, m.MP, nP, s));
+        if (iter > c->max_iterations) break;
+    }
+    RC(fold());
+    CK(cudaStreamSynchronize(s));
+    st->itPH = itPH_done; st->iter = iter; st->err = err; st->err_abs = err_abs; st->err_rel = err_rel;
+    st->err_v = err_v; st->err_P = err_P; st->converged = converged; st->reached_total_iter = iter > c->max_iterations;
+    st->lambda_max = *std::max_element(lmax, lmax + D); st->lambda_max_gershgorin = lmax_g;
+    st->jacobian_assemblies = jac_assemblies;
+    st->defect_corrections = base_sweeps;
+    st->history_len = c->history ? std::min<int64_t>(hist, c->history_capacity) : 0;
+    return FEMB200_OK;
+}
+
 int finish_solve(femb200_handle* h, const femb200_stokes_controls* c, femb200_stokes_stats* st) {
     if (!st->converged && c->throw_on_failure) {
         char b[256];
@@ -819,6 +1097,11 @@ template <class T, class TG> struct DoSolve {
             RC(upload_material(h, p->mat, c->finite_K, c->dt));
             RC((pressure_scaling_impl<T, TG>(h, p, c->pressure_factor, c->dt)));
         }
+        if (c->precision == FEMB200_PRECISION_MIXED) {
+            if (!std::is_same<T, double>::value) { h->err = "the mixed-precision solve takes an FP64 state"; return FEMB200_EUNSUPPORTED; }
+            if (cp) { h->err = "the coupled solve runs in FP64 only"; return FEMB200_EUNSUPPORTED; }
+            return solve_dyrel_mixed<TG>(h, p, c, st);
+        }
         RC((solve_dyrel<T, TG>(h, p, c, st, cp)));
         return FEMB200_OK;
     }
@@ -828,7 +1111,7 @@ int check_controls(femb200_handle* h, const femb200_stokes_controls* c) {
     if (!c) { h->err = "null controls"; return FEMB200_EINVAL; }
     if (!(c->dt > 0)) { h->err = "dt must be positive"; return FEMB200_EINVAL; }
     if (c->check_interval <= 0) { h->err = "check_interval must be positive"; return FEMB200_EINVAL; }
-    if (c->precision != FEMB200_PRECISION_FP64) { h->err = "this build runs the FP64 DR path only"; return FEMB200_EUNSUPPORTED; }
+    if (c->precision != FEMB200_PRECISION_FP64 && c->precision != FEMB200_PRECISION_MIXED) { h->err = "unknown precision"; return FEMB200_EINVAL; }
     return FEMB200_OK;
 }
 
@@ -887,6 +1170,7 @@ int femb200_destroy(femb200_handle* h) {
     if (h->d_geo_c) cudaFree(h->d_geo_c);
     if (h->d_flag) cudaFree(h->d_flag);
     if (h->h_flag) cudaFreeHost(h->h_flag);
+    if (h->mixed.mem) cudaFree(h->mixed.mem);
     delete h;
     return FEMB200_OK;
 }

@@ -181,4 +181,5 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
     __syncwarp();
 }
 
+
 }  // namespace femb

@@ -43,6 +43,14 @@ struct H27Args {
     int with_pnum;
     int do_momentum;
     int write_RP;
+    // Mixed precision (FP32 increments about an FP64 base state, pipelined sweep only):
+    // the base sweep writes the trial stress (6) and yield value (1) of every
+    // integration point as FP32 into base_out; the incremental sweep reads them
+    // from base_in, takes v and P as the increments δv, δP and adds its
+    // increments to Rv (pre-filled with the base residual) and to RP_base.
+    float* base_out[7];
+    const float* base_in[7];
+    const T* RP_base;
 };
 
 template <class T, class TG>
@@ -51,6 +59,8 @@ cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaS
 // Pipelined sweep over affine Hex27 elements with one J⁻¹, |det J| per element.
 template <class T>
 cudaError_t launch_hex27_residual_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, cudaStream_t st);
+// FP32 incremental sweep of the mixed-precision solve (args.base_in, args.RP_base set).
+cudaError_t launch_hex27_residual_incr(const H27Args<float, float>& args, const float* geo_c, int num_sms, cudaStream_t st);
 template <class TG, class TC>
 cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t nels, TC* out, int* not_affine,
                                      cudaStream_t st);
@@ -152,6 +162,9 @@ template <class T>
 cudaError_t launch_sub(T* x, const T* y, int64_t n, cudaStream_t st);
 template <class T>
 cudaError_t launch_copy(T* dst, const T* src, int64_t n, cudaStream_t st);
+// Mixed precision: x += δ and δ = 0 (FP64 state, FP32 increment); y = (float)(x [+ δ]).
+cudaError_t launch_fold(double* x, float* d, int64_t n, cudaStream_t st);
+cudaError_t launch_round(float* y, const double* x, const float* d, int64_t n, cudaStream_t st);
 
 template <class T>
 cudaError_t launch_transfer_temperature(T* TP, const T* Tn, const int32_t* dofsP, const int32_t* el2nP, int64_t n,

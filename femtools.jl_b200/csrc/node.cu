@@ -292,4 +292,29 @@ FEMB_INST(double)
 FEMB_INST(float)
 #undef FEMB_INST
 
+
+// Mixed precision: fold the FP32 increment into the FP64 state (x += δ, δ = 0),
+// and FP32 images of FP64 arrays (y = x, or y = x + δ).
+__global__ void fold_kernel(double* x, float* d, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { x[i] += (double)d[i]; d[i] = 0.0f; }
+}
+__global__ void round_kernel(float* y, const double* x, const float* d, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = d ? (float)(x[i] + (double)d[i]) : (float)x[i];
+}
+
+cudaError_t launch_fold(double* x, float* d, int64_t n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    count_launch();
+    fold_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, d, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_round(float* y, const double* x, const float* d, int64_t n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    count_launch();
+    round_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(y, x, d, n);
+    return cudaGetLastError();
+}
+
 }  // namespace femb

@@ -6,11 +6,13 @@
 //     boxes and any parallelepiped cells) the per-point J⁻¹ and |det J|·ω of the
 //     reference layout collapse to one J⁻¹ and |det J| per element, built once per
 //     solve by compress_geometry (80 B per element instead of 2376 B);
-//   * each warp keeps three elements in flight and prefetches the next group's
-//     stress history, geometry and pressure-DoF data with cp.async into a second
-//     shared-memory buffer (and its velocity gather into registers) while it
-//     computes the current group, so one memory round trip overlaps one group of
-//     sum-factorised element work;
+//   * each warp keeps three elements in flight; as soon as the quadrature loop
+//     of the current group has consumed its shared-memory buffer, the warp issues
+//     the next group's stress history, geometry and pressure-DoF loads (cp.async)
+//     into that buffer and its velocity gather into registers, so the loads
+//     overlap the transposed contraction, the scatter and the next gradient;
+//   * one buffer per element slot (not two) keeps shared memory at 17 KB per warp
+//     (FP64) and 8.5 KB (FP32), so FP32 runs 16 resident warps per SM;
 //   * elements whose 27 nodes share a phase use per-phase constants prepared on
 //     the host (ηve, 2ηve, C·cosϕ, the reciprocal plastic denominator).
 #include "kernels.cuh"
@@ -18,10 +20,20 @@
 
 namespace femb {
 
-constexpr int PL_THREADS = 256;     // 8 warps, one block per SM
+// Threads per block (one block per SM): 8 warps in FP64 (more would spill the
+// 27-value gradient/flux lines of each thread), 16 in FP32.
+template <class T> struct PipeThreads { static constexpr int value = 256; };
+template <> struct PipeThreads<float> { static constexpr int value = 512; };
 constexpr int PL_STAGE = 500;       // stage scratch per element slot (≥ 496)
-constexpr int PL_BUF = 208;         // prefetch buffer per element (τ_old 162, geo 10, DoF data 32)
-constexpr int BUF_TOLD = 0, BUF_GEO = 162, BUF_DOF = 172;
+// Load buffer of one element slot: per-point fields (τ_old, 6 × 27; or, in the
+// incremental sweep, the base trial stress and yield value, 7 × 27), the affine
+// geometry (10) and the pressure-DoF data (32).
+template <bool INCR> struct PipeLayout {
+    static constexpr int NT = INCR ? 7 : 6;
+    static constexpr int GEO = NT * 27;
+    static constexpr int DOF = GEO + 10;
+    static constexpr int BUF = INCR ? 232 : 208;
+};
 enum { PT_TWOE, PT_TWOE_EL, PT_RHO0, PT_ALPHA, PT_BETA, PT_CC, PT_SPHI, PT_INVDEN, PT_INVBULKDT, PT_BULK, PT_FIELDS };
 
 namespace {
@@ -60,30 +72,40 @@ FEMB_D GroupIds load_ids(const H27Args<T, T>& a, int64_t base, int s, int m, con
 
 // Issue the prefetch of one group: velocity gather into registers, stress history,
 // geometry and pressure-DoF data into the shared-memory buffer.
-template <class T>
+template <class T, bool INCR>
 FEMB_D void issue_prefetch(const H27Args<T, T>& a, const T* geo_c, const GroupIds& id, int64_t base, int s, int m,
                            int m1, int m2, T* buf, T vn[3][3]) {
+    using L = PipeLayout<INCR>;
     if (!id.act) return;
     const int64_t e = base + s;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) vn[c][i] = ld(a.v[c] + id.node[i]);
-    T* B = buf + s * PL_BUF;
-    if (a.told[0]) {
+    T* B = buf + s * L::BUF;
+    if constexpr (INCR) {
+#pragma unroll
+        for (int c = 0; c < 7; ++c)
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) {
+                const int q = tidx(m1, m2, qz);
+                cp_async(B + c * 27 + q, a.base_in[c] + e * 27 + q);
+            }
+    } else if (a.told[0]) {
 #pragma unroll
         for (int c = 0; c < 6; ++c)
 #pragma unroll
             for (int qz = 0; qz < 3; ++qz) {
                 const int q = tidx(m1, m2, qz);
-                cp_async(B + BUF_TOLD + c * 27 + q, a.told[c] + e * 27 + q);
+                cp_async(B + c * 27 + q, a.told[c] + e * 27 + q);
             }
     }
-    cp_async(B + BUF_GEO + m, geo_c + e * 10 + m);
-    if (m == 0) cp_async(B + BUF_GEO + 9, geo_c + e * 10 + 9);
+    cp_async(B + L::GEO + m, geo_c + e * 10 + m);
+    if (m == 0) cp_async(B + L::GEO + 9, geo_c + e * 10 + 9);
     if (m < 4) {
-        T* D = B + BUF_DOF;
+        T* D = B + L::DOF;
         cp_async(D + 0 * 4 + m, a.P + id.dof);
+        if constexpr (INCR) cp_async(D + 1 * 4 + m, a.RP_base + id.dof);
         if (a.P0) cp_async(D + 1 * 4 + m, a.P0 + id.dof);
         if (a.gammaP) cp_async(D + 2 * 4 + m, a.gammaP + id.dof);
         if (a.MP) cp_async(D + 3 * 4 + m, a.MP + id.dof);
@@ -94,21 +116,54 @@ FEMB_D void issue_prefetch(const H27Args<T, T>& a, const T* geo_c, const GroupId
     }
 }
 
+// Stress increment of the Drucker–Prager radial return (rheology.jl:441-472)
+// between the base trial stress tb (yield value Fk) and the trial stress tb + dtt,
+// with pressure increment dPeq. Written in increments (J2 difference through the
+// cross term, f' − f through δλ and δτII), so that no two nearly equal stresses
+// are subtracted and the FP32 error scales with the increment, not the stress.
+// The return is τ = τtr − f·M·τtr with M = ½ on the normal and 1 on the shear
+// components and f = 2ηve·λ/(τII + ε²), λ = F/den.
+template <class U>
+FEMB_D void dp_increment(const U tb[6], U Fk, const U dtt[6], U dPeq, U twoe, U sphi, U inv_den, U eps2, U out[6]) {
+    const U Jk = U(0.5) * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] + tb[4] * tb[4] + tb[5] * tb[5];
+    const U cross = tb[0] * dtt[0] + tb[1] * dtt[1] + tb[2] * dtt[2] + U(2) * (tb[3] * dtt[3] + tb[4] * dtt[4] + tb[5] * dtt[5]);
+    const U dd = U(0.5) * (dtt[0] * dtt[0] + dtt[1] * dtt[1] + dtt[2] * dtt[2]) + dtt[3] * dtt[3] + dtt[4] * dtt[4] + dtt[5] * dtt[5];
+    const U tIIk = sqrt(Jk + eps2);
+    const U tIIn = sqrt(Jk + eps2 + (cross + dd));
+    const U dtII = (cross + dd) / (tIIn + tIIk);
+    const U dF = dtII - sphi * dPeq;
+    const U Fn = Fk + dF;
+    const bool pk = Fk > U(0), pn = Fn > U(0);
+    const U lamk = pk ? Fk * inv_den : U(0);
+    U fn = U(0), df = U(0);
+    if (pn) {
+        fn = twoe * (Fn * inv_den) / (tIIn + eps2);
+        df = pk ? twoe * (dF * inv_den * (tIIk + eps2) - lamk * dtII) / ((tIIn + eps2) * (tIIk + eps2)) : fn;
+    } else if (pk) {
+        df = -(twoe * lamk / (tIIk + eps2));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = dtt[c] - U(0.5) * (fn * dtt[c] + df * tb[c]);
+#pragma unroll
+    for (int c = 3; c < 6; ++c) out[c] = dtt[c] - (fn * dtt[c] + df * tb[c]);
+}
+
 }  // namespace
 
-template <class T>
-__global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27Args<T, T> a, const T* __restrict__ geo_c) {
+template <class T, bool INCR>
+__global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_kernel(H27Args<T, T> a, const T* __restrict__ geo_c) {
+    static_assert(!INCR || sizeof(T) == 4, "the incremental sweep runs in FP32");
+    using L = PipeLayout<INCR>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
     // lanes 27..31 carry no element: they follow slot 0's reads but never write
     const int s = lane_ok ? lane / 9 : 0, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* base_w = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (3 * PL_STAGE + 2 * 3 * PL_BUF);
+    T* base_w = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (3 * PL_STAGE + 3 * L::BUF);
     T* E = base_w + s * PL_STAGE;
-    T* BUF0 = base_w + 3 * PL_STAGE;
-    T* BUF1 = BUF0 + 3 * PL_BUF;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * (3 * PL_STAGE + 2 * 3 * PL_BUF)) +
+    T* BUF = base_w + 3 * PL_STAGE;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * (3 * PL_STAGE + 3 * L::BUF)) +
               (warp * 3 + s) * 28;
     const int sl = s;
 
@@ -146,13 +201,14 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
     }
     __syncthreads();
     const bool bulk_inf = c_mat.all_bulk_inf != 0;
-    const T EPS2 = eps2<T>();
+    // the incremental sweep models the FP64 problem: its ε² is FP64's
+    const T EPS2 = INCR ? (T)eps2<double>() : eps2<T>();
     const bool nodal_phases = a.phv && a.phv_layout != FEMB200_PHASE_CELL;
 
     const int64_t stride = (int64_t)gridDim.x * wpb * 3;
     int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3;
 
-    // prologue: ids of the first two groups, prefetch of the first
+    // prologue: ids of the first two groups, loads of the first
     GroupIds id_cur = load_ids(a, base, s, m, tn_own, lane_ok);
     GroupIds id_next = load_ids(a, base + stride, s, m, tn_own, lane_ok);
     T vn[3][3];
@@ -160,13 +216,11 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int i = 0; i < 3; ++i) vn[c][i] = T(0);
-    issue_prefetch(a, geo_c, id_cur, base, s, m, m1, m2, BUF0, vn);
+    issue_prefetch<T, INCR>(a, geo_c, id_cur, base, s, m, m1, m2, BUF, vn);
     cp_commit();
+    const bool do_qp = a.do_momentum || a.phi;
 
-    int it = 0;
-    for (; base < a.nels; base += stride, ++it) {
-        T* cur = (it & 1) ? BUF1 : BUF0;
-        T* nxt = (it & 1) ? BUF0 : BUF1;
+    for (; base < a.nels; base += stride) {
         cp_wait_all();
         __syncwarp();
         T v[3][3];
@@ -177,13 +231,8 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
         const GroupIds id = id_cur;
         const bool act = id.act;
         const int64_t ec = act ? base + s : 0;
-        // prefetch the next group and the ids of the one after
-        issue_prefetch(a, geo_c, id_next, base + stride, s, m, m1, m2, nxt, vn);
-        cp_commit();
-        id_cur = id_next;
-        id_next = load_ids(a, base + 2 * stride, s, m, tn_own, lane_ok);
 
-        const T* B = cur + sl * PL_BUF;
+        const T* B = BUF + sl * L::BUF;
         // ---- phases ----
         int p0 = id.phase;
         bool uniform = true;
@@ -216,9 +265,9 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
         // ---- geometry of the element (affine: constant J⁻¹ and |det J|) ----
         T Ji[9];
 #pragma unroll
-        for (int r = 0; r < 9; ++r) Ji[r] = B[BUF_GEO + r];
-        const T detJ = B[BUF_GEO + 9];
-        const T* D = B + BUF_DOF;
+        for (int r = 0; r < 9; ++r) Ji[r] = B[L::GEO + r];
+        const T detJ = B[L::GEO + 9];
+        const T* D = B + L::DOF;
 
         T g[3][3][3];
         h27_gradient(tb, v, E, m1, m2, g, lane_ok);
@@ -231,9 +280,14 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
             const T dO = act ? detJ * w_own[qz] : T(0);
             const T ze = (T)c_tab.qx[qz];
             const T NP[4] = {T(1) - xi - et - ze, xi, et, ze};
-            T div = T(0);
+            // physical gradient ∂v_c/∂x_k, kept in g for the momentum loop
 #pragma unroll
-            for (int c = 0; c < 3; ++c) div += g[c][0][qz] * Ji[0 + 3 * c] + g[c][1][qz] * Ji[1 + 3 * c] + g[c][2][qz] * Ji[2 + 3 * c];
+            for (int c = 0; c < 3; ++c) {
+                const T r0 = g[c][0][qz], r1 = g[c][1][qz], r2 = g[c][2][qz];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) g[c][k][qz] = r0 * Ji[0 + 3 * k] + r1 * Ji[1 + 3 * k] + r2 * Ji[2 + 3 * k];
+            }
+            const T div = g[0][0][qz] + g[1][1][qz] + g[2][2][qz];
             T dPdt = T(0);
             if (!bulk_inf) {
                 T dPinc = T(0);
@@ -269,129 +323,168 @@ __global__ void __launch_bounds__(PL_THREADS, 1) hex27_residual_pipe_kernel(H27A
 #pragma unroll
             for (int p = 0; p < 4; ++p) rp[p] += NP[p] * f;
         }
+        // element sums of RP: lane m < 4 of each element sums component m, computes
+        // its Pnum = γP·RP/M_P and shares it with the element's other lanes
         T* RPs = E + 460;
         if (lane_ok) {
 #pragma unroll
             for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = rp[p];
         }
         __syncwarp();
-        T RPe[4];
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
+        T pn_own = T(0);
+        if (m < 4) {
             T acc = T(0);
 #pragma unroll
-            for (int t = 0; t < 9; ++t) acc += RPs[t * 4 + p];
-            RPe[p] = acc;
+            for (int t = 0; t < 9; ++t) acc += RPs[t * 4 + m];
+            if (act && a.write_RP) a.RP[id.dof] = INCR ? D[4 + m] + acc : acc;
+            const T gam = a.gammaP ? D[8 + m] : T(0);
+            const T mp = a.MP ? D[12 + m] : T(1);
+            pn_own = a.with_pnum ? gam * acc / mp : T(0);
+            if (act && a.Pnum_out && a.with_pnum) a.Pnum_out[id.dof] = pn_own;
         }
-        __syncwarp();
-        if (act && a.write_RP && m < 4) a.RP[id.dof] = RPe[m];
         T Pn[4];
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            const T gam = a.gammaP ? D[8 + p] : T(0);
-            const T mp = a.MP ? D[12 + p] : T(1);
-            Pn[p] = a.with_pnum ? gam * RPe[p] / mp : T(0);
-        }
-        if (act && a.Pnum_out && a.with_pnum && m < 4) a.Pnum_out[id.dof] = Pn[m];
-        if (!a.do_momentum && !a.phi) continue;
+        for (int p = 0; p < 4; ++p) Pn[p] = __shfl_sync(0xffffffffu, pn_own, (lane_ok ? s * 9 : 0) + p);
 
-        // ---- stress and reference-frame fluxes; F overwrites g point by point ----
-        T beta_q[3];
+        T beta_q[3] = {T(0), T(0), T(0)};
+        if (do_qp) {
+            // ---- stress and reference-frame fluxes; F overwrites g point by point ----
 #pragma unroll
-        for (int qz = 0; qz < 3; ++qz) {
-            const int q = tidx(m1, m2, qz);
-            const T dO = act ? detJ * w_own[qz] : T(0);
-            const T ze = (T)c_tab.qx[qz];
-            const T NP[4] = {T(1) - xi - et - ze, xi, et, ze};
-            T gq[3][3];
+            for (int qz = 0; qz < 3; ++qz) {
+                const int q = tidx(m1, m2, qz);
+                const T dO = act ? detJ * w_own[qz] : T(0);
+                const T ze = (T)c_tab.qx[qz];
+                const T NP[4] = {T(1) - xi - et - ze, xi, et, ze};
+                T gq[3][3];
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) gq[c][k] = g[c][0][qz] * Ji[0 + 3 * k] + g[c][1][qz] * Ji[1 + 3 * k] + g[c][2][qz] * Ji[2 + 3 * k];
-            T Pq = T(0), Pfq = T(0), Pnq = T(0), Tq = T(0);
+                    for (int k = 0; k < 3; ++k) gq[c][k] = g[c][k][qz];
+                T Pq = T(0), Pfq = T(0), Pnq = T(0), Tq = T(0);
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                Pq += NP[p] * D[p];
-                Pnq += NP[p] * Pn[p];
-                if (a.Pf) Pfq += NP[p] * D[28 + p];
-                if (a.temp) Tq += NP[p] * D[16 + p];
-            }
-            const T Peq = a.Pf ? Pq - Pfq : Pq;
-            T twoe, twoe_el, rho0, alpha, beta, cC = T(0), sphi = T(0), inv_den = T(0), etave;
-            const bool fast = uniform && consts_ok && !a.eta_ip;
-            if (fast) {
-                twoe = PT[PT_TWOE][p0];
-                twoe_el = PT[PT_TWOE_EL][p0];
-                etave = T(0.5) * twoe;
-                rho0 = PT[PT_RHO0][p0]; alpha = PT[PT_ALPHA][p0]; beta = PT[PT_BETA][p0];
-                if (plastic) { cC = PT[PT_CC][p0]; sphi = PT[PT_SPHI][p0]; inv_den = PT[PT_INVDEN][p0]; }
-            } else {
-                T eta = T(0), invG = T(0), cphi = T(0), C = T(0), spsi = T(0), ereg = T(0), Kb = T(0);
-                rho0 = alpha = beta = T(0);
-                for (int k = 0; k < 3; ++k)
-                    for (int j = 0; j < 3; ++j)
-                        for (int i = 0; i < 3; ++i) {
-                            const T N = tb.B[m1][i] * tb.B[m2][j] * tb.B[qz][k];
-                            const int p = uniform ? p0 : PH[tidx(i, j, k)];
-                            eta += N * (T)c_mat.eta[p]; invG += N * (T)c_mat.invG[p];
-                            rho0 += N * (T)c_mat.rho0[p]; alpha += N * (T)c_mat.alpha[p]; beta += N * (T)c_mat.beta[p];
-                            if (plastic) {
-                                cphi += N * (T)c_mat.cos_phi[p]; sphi += N * (T)c_mat.sin_phi[p];
-                                spsi += N * (T)c_mat.sin_psi[p]; C += N * (T)c_mat.C[p];
-                                ereg += N * (T)c_mat.eta_reg[p]; Kb += N * (T)c_mat.Kb[p];
+                for (int p = 0; p < 4; ++p) {
+                    Pq += NP[p] * D[p];
+                    Pnq += NP[p] * Pn[p];
+                    if (a.Pf) Pfq += NP[p] * D[28 + p];
+                    if (a.temp) Tq += NP[p] * D[16 + p];
+                }
+                const T Peq = a.Pf ? Pq - Pfq : Pq;
+                T twoe, twoe_el, rho0, alpha, beta, cC = T(0), sphi = T(0), inv_den = T(0), etave;
+                const bool fast = uniform && consts_ok && !a.eta_ip;
+                if (fast) {
+                    twoe = PT[PT_TWOE][p0];
+                    twoe_el = PT[PT_TWOE_EL][p0];
+                    etave = T(0.5) * twoe;
+                    rho0 = PT[PT_RHO0][p0]; alpha = PT[PT_ALPHA][p0]; beta = PT[PT_BETA][p0];
+                    if (plastic) { cC = PT[PT_CC][p0]; sphi = PT[PT_SPHI][p0]; inv_den = PT[PT_INVDEN][p0]; }
+                } else {
+                    T eta = T(0), invG = T(0), cphi = T(0), C = T(0), spsi = T(0), ereg = T(0), Kb = T(0);
+                    rho0 = alpha = beta = T(0);
+                    for (int k = 0; k < 3; ++k)
+                        for (int j = 0; j < 3; ++j)
+                            for (int i = 0; i < 3; ++i) {
+                                const T N = tb.B[m1][i] * tb.B[m2][j] * tb.B[qz][k];
+                                const int p = uniform ? p0 : PH[tidx(i, j, k)];
+                                eta += N * (T)c_mat.eta[p]; invG += N * (T)c_mat.invG[p];
+                                rho0 += N * (T)c_mat.rho0[p]; alpha += N * (T)c_mat.alpha[p]; beta += N * (T)c_mat.beta[p];
+                                if (plastic) {
+                                    cphi += N * (T)c_mat.cos_phi[p]; sphi += N * (T)c_mat.sin_phi[p];
+                                    spsi += N * (T)c_mat.sin_psi[p]; C += N * (T)c_mat.C[p];
+                                    ereg += N * (T)c_mat.eta_reg[p]; Kb += N * (T)c_mat.Kb[p];
+                                }
                             }
-                        }
-                if (a.eta_ip) eta = act ? ld(a.eta_ip + ec * 27 + q) : T(1);
-                if (!act) eta = T(1);
-                etave = T(1) / (T(1) / eta + invG / dt);
-                twoe = T(2) * etave;
-                twoe_el = twoe * (invG / (T(2) * dt));
-                cC = cphi * C;
-                inv_den = T(1) / (etave + ereg + Kb * dt * (-spsi) * (-sphi));
-            }
-            const T tr = (gq[0][0] + gq[1][1] + gq[2][2]) * T(1.0 / 3.0);
-            const T eps_[6] = {gq[0][0] - tr, gq[1][1] - tr, gq[2][2] - tr, T(0.5) * (gq[0][1] + gq[1][0]),
-                               T(0.5) * (gq[0][2] + gq[2][0]), T(0.5) * (gq[1][2] + gq[2][1])};
-            T tau[6], told[6];
+                    if (a.eta_ip) eta = act ? ld(a.eta_ip + ec * 27 + q) : T(1);
+                    if (!act) eta = T(1);
+                    etave = T(1) / (T(1) / eta + invG / dt);
+                    twoe = T(2) * etave;
+                    twoe_el = twoe * (invG / (T(2) * dt));
+                    cC = cphi * C;
+                    inv_den = T(1) / (etave + ereg + Kb * dt * (-spsi) * (-sphi));
+                }
+                const T tr = (gq[0][0] + gq[1][1] + gq[2][2]) * T(1.0 / 3.0);
+                const T eps_[6] = {gq[0][0] - tr, gq[1][1] - tr, gq[2][2] - tr, T(0.5) * (gq[0][1] + gq[1][0]),
+                                   T(0.5) * (gq[0][2] + gq[2][0]), T(0.5) * (gq[1][2] + gq[2][1])};
+                T tau[6];
+            if constexpr (INCR) {
+                // τ(base + δ) − τ(base): the trial stress is affine in the strain rate
+                T tb[6], dtt[6];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                told[c] = a.told[0] ? B[BUF_TOLD + c * 27 + q] : T(0);
-                tau[c] = twoe * eps_[c] + twoe_el * told[c];
-            }
-            if (plastic) {
-                const T tII = sqrt(T(0.5) * (tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) + tau[3] * tau[3] +
-                                   tau[4] * tau[4] + tau[5] * tau[5] + EPS2);
-                const T Fy = tII - cC - sphi * Peq;
-                if (Fy > T(0)) {
-                    const T lam = Fy * inv_den;
-                    const T f = twoe * lam / (tII + EPS2);
-                    tau[0] -= T(0.5) * f * tau[0]; tau[1] -= T(0.5) * f * tau[1]; tau[2] -= T(0.5) * f * tau[2];
-                    tau[3] -= f * tau[3]; tau[4] -= f * tau[4]; tau[5] -= f * tau[5];
+                for (int c = 0; c < 6; ++c) { tb[c] = B[c * 27 + q]; dtt[c] = twoe * eps_[c]; }
+                if (plastic) {
+                    const T Fk = B[6 * 27 + q];
+                    const T Jk = T(0.5) * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] + tb[4] * tb[4] + tb[5] * tb[5];
+                    if (Jk < T(1e-6) * cC * cC) {
+                        // within 1e-3·C·cosϕ of the yield-surface apex: the return direction
+                        // is ill-conditioned, so this point's increment is formed in FP64
+                        double tbd[6], dtd[6], outd[6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) { tbd[c] = tb[c]; dtd[c] = dtt[c]; }
+                        dp_increment<double>(tbd, (double)Fk, dtd, (double)Peq, (double)twoe, (double)sphi, (double)inv_den,
+                                             eps2<double>(), outd);
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) tau[c] = (T)outd[c];
+                    } else {
+                        dp_increment<T>(tb, Fk, dtt, Peq, twoe, sphi, inv_den, EPS2, tau);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
+                }
+            } else {
+                T told[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    told[c] = a.told[0] ? B[c * 27 + q] : T(0);
+                    tau[c] = twoe * eps_[c] + twoe_el * told[c];
+                }
+                if (act && a.base_out[0]) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) a.base_out[c][ec * 27 + q] = (float)tau[c];
+                }
+                if (plastic) {
+                    const T tII = sqrt(T(0.5) * (tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) + tau[3] * tau[3] +
+                                       tau[4] * tau[4] + tau[5] * tau[5] + EPS2);
+                    const T Fy = tII - cC - sphi * Peq;
+                    if (act && a.base_out[6]) a.base_out[6][ec * 27 + q] = (float)Fy;
+                    if (Fy > T(0)) {
+                        const T lam = Fy * inv_den;
+                        const T f = twoe * lam / (tII + EPS2);
+                        tau[0] -= T(0.5) * f * tau[0]; tau[1] -= T(0.5) * f * tau[1]; tau[2] -= T(0.5) * f * tau[2];
+                        tau[3] -= f * tau[3]; tau[4] -= f * tau[4]; tau[5] -= f * tau[5];
+                    }
+                }
+                if (act && a.tau_store[0]) {
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) a.tau_store[c][ec * 27 + q] = tau[c];
+                }
+                if (act && a.phi) {
+                    const T inv2Gdt = twoe_el / twoe;
+                    const T power = tau[0] * gq[0][0] + tau[1] * gq[1][1] + tau[2] * gq[2][2] + tau[3] * (gq[0][1] + gq[1][0]) +
+                                    tau[4] * (gq[0][2] + gq[2][0]) + tau[5] * (gq[1][2] + gq[2][1]);
+                    const T el = (tau[0] * (tau[0] - told[0]) + tau[1] * (tau[1] - told[1]) + tau[2] * (tau[2] - told[2]) +
+                                  T(2) * (tau[3] * (tau[3] - told[3]) + tau[4] * (tau[4] - told[4]) + tau[5] * (tau[5] - told[5]))) *
+                                 inv2Gdt;
+                    a.phi[ec * 27 + q] = power - el;
                 }
             }
-            if (act && a.tau_store[0]) {
-#pragma unroll
-                for (int c = 0; c < 6; ++c) a.tau_store[c][ec * 27 + q] = tau[c];
-            }
-            if (act && a.phi) {
-                const T inv2Gdt = twoe_el / twoe;
-                const T power = tau[0] * gq[0][0] + tau[1] * gq[1][1] + tau[2] * gq[2][2] + tau[3] * (gq[0][1] + gq[1][0]) +
-                                tau[4] * (gq[0][2] + gq[2][0]) + tau[5] * (gq[1][2] + gq[2][1]);
-                const T el = (tau[0] * (tau[0] - told[0]) + tau[1] * (tau[1] - told[1]) + tau[2] * (tau[2] - told[2]) +
-                              T(2) * (tau[3] * (tau[3] - told[3]) + tau[4] * (tau[4] - told[4]) + tau[5] * (tau[5] - told[5]))) *
-                             inv2Gdt;
-                a.phi[ec * 27 + q] = power - el;
-            }
             const T Ptot = (a.Pf ? Peq + Pfq : Pq) + Pnq;
-            const T rhoq = rho0 * (T(1) - alpha * (Tq - (T)c_mat.Tref) + beta * Pq);
-            beta_q[qz] = act ? rhoq * dO : T(0);
-            const T sg[3][3] = {{tau[0] - Ptot, tau[3], tau[4]}, {tau[3], tau[1] - Ptot, tau[5]}, {tau[4], tau[5], tau[2] - Ptot}};
+                // EOS density (momentum_residuals.jl:11-16); its increment is ρ0·β·δP
+            const T rhoq = INCR ? rho0 * beta * Pq : rho0 * (T(1) - alpha * (Tq - (T)c_mat.Tref) + beta * Pq);
+                beta_q[qz] = act ? rhoq * dO : T(0);
+                const T sg[3][3] = {{tau[0] - Ptot, tau[3], tau[4]}, {tau[3], tau[1] - Ptot, tau[5]}, {tau[4], tau[5], tau[2] - Ptot}};
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    g[c][d][qz] = dO * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
+                    for (int d = 0; d < 3; ++d)
+                        g[c][d][qz] = dO * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
+            }
         }
+        // every lane is done with this group's buffer: load the next group into it
+        __syncwarp();
+        issue_prefetch<T, INCR>(a, geo_c, id_next, base + stride, s, m, m1, m2, BUF, vn);
+        cp_commit();
+        id_cur = id_next;
+        id_next = load_ids(a, base + 2 * stride, s, m, tn_own, lane_ok);
         if (!a.do_momentum) continue;
         T R[3][3];
         h27_transpose(tb, g, beta_q, gvec, E, m1, m2, R, lane_ok);
@@ -438,32 +531,43 @@ cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t n
     return cudaGetLastError();
 }
 
-template <class T>
+template <class T, bool INCR>
 size_t pipe_smem_bytes() {
-    const int wpb = PL_THREADS / 32;
-    return (size_t)wpb * (3 * PL_STAGE + 2 * 3 * PL_BUF) * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
+    const int wpb = PipeThreads<T>::value / 32;
+    return (size_t)wpb * (3 * PL_STAGE + 3 * PipeLayout<INCR>::BUF) * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
 }
 
-template <class T>
-cudaError_t launch_hex27_residual_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, cudaStream_t st) {
-    const size_t smem = pipe_smem_bytes<T>();
+template <class T, bool INCR>
+cudaError_t launch_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, cudaStream_t st) {
+    const size_t smem = pipe_smem_bytes<T, INCR>();
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(hex27_residual_pipe_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(hex27_residual_pipe_kernel<T, INCR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_residual_pipe_kernel<T>, PL_THREADS, smem);
+    constexpr int threads = PipeThreads<T>::value;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_residual_pipe_kernel<T, INCR>, threads, smem);
     if (per_sm < 1) per_sm = 1;
     const int64_t groups = (args.nels + 2) / 3;
-    int64_t blocks = (groups + PL_THREADS / 32 - 1) / (PL_THREADS / 32);
+    int64_t blocks = (groups + threads / 32 - 1) / (threads / 32);
     const int64_t cap = (int64_t)num_sms * per_sm;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     count_launch();
-    hex27_residual_pipe_kernel<T><<<(unsigned)blocks, PL_THREADS, smem, st>>>(args, geo_c);
+    hex27_residual_pipe_kernel<T, INCR><<<(unsigned)blocks, threads, smem, st>>>(args, geo_c);
     return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_hex27_residual_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, cudaStream_t st) {
+    return launch_pipe<T, false>(args, geo_c, num_sms, st);
+}
+
+cudaError_t launch_hex27_residual_incr(const H27Args<float, float>& args, const float* geo_c, int num_sms, cudaStream_t st) {
+    return launch_pipe<float, true>(args, geo_c, num_sms, st);
 }
 
 template cudaError_t launch_hex27_residual_pipe<double>(const H27Args<double, double>&, const double*, int, cudaStream_t);

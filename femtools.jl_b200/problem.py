@@ -173,8 +173,7 @@ def fill_stokes_problem(s: abi.StokesProblemC, mesh: dict, state: dict, mat: abi
 def controls_struct(dt, pressure_factor=50.0, tolerance=1e-6, max_iterations=50_000, check_interval=50,
                     iter_max=50_000, max_ph_iterations=1000, rel_drop0=1e-2, freeze_jacobian=None,
                     finite_K=False, assemble_scaling=True, throw_on_failure=True,
-                    precision=abi.PRECISION_FP64, cfl_v=0.98, c_fact=0.9, history=None,
-                    mixed_inner_drop=1e-3) -> abi.StokesControlsC:
+                    precision=abi.PRECISION_FP64, cfl_v=0.98, c_fact=0.9, history=None) -> abi.StokesControlsC:
     c = abi.StokesControlsC()
     c.dt, c.pressure_factor, c.tolerance = float(dt), float(pressure_factor), float(tolerance)
     c.max_iterations, c.check_interval, c.iter_max = int(max_iterations), int(check_interval), int(iter_max)
@@ -183,7 +182,6 @@ def controls_struct(dt, pressure_factor=50.0, tolerance=1e-6, max_iterations=50_
     c.finite_K, c.assemble_scaling = int(bool(finite_K)), int(bool(assemble_scaling))
     c.throw_on_failure, c.precision = int(bool(throw_on_failure)), int(precision)
     c.cfl_v, c.c_fact = float(cfl_v), float(c_fact)
-    c.mixed_inner_drop = float(mixed_inner_drop)
     if history is not None:
         import ctypes
         c.history = history.ctypes.data_as(ctypes.POINTER(ctypes.c_double))

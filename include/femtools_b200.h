@@ -59,8 +59,13 @@ enum { FEMB200_PHASE_NODAL = 0, FEMB200_PHASE_CELL = 1, FEMB200_PHASE_ELEMENT_NO
  * nodal (interpolated with the shape functions). */
 enum { FEMB200_FIELD_NONE = 0, FEMB200_FIELD_IP = 1, FEMB200_FIELD_NODAL = 2 };
 
-/* Arithmetic of the DR sweeps. FP64 is the reference algorithm; MIXED runs the
- * residual and update sweeps in FP32 inside an FP64 defect-correction loop. */
+/* Arithmetic of the DR sweeps. FP64 is the reference algorithm. MIXED (3-D
+ * affine Hex27, FP64 state) keeps the state in FP64 and runs the Chebyshev
+ * iterations in FP32 on increments δv, δP: at every Powell–Hestenes step the
+ * increments are folded into the state, the outer residual and convergence test
+ * are evaluated in FP64 (as in FP64 mode), and the FP32 residual sweeps evaluate
+ * R(x) + [R(x + δ) − R(x)] with the bracket formed from the increments, so FP32
+ * rounding scales with δ. Norms are accumulated in FP64. */
 enum { FEMB200_PRECISION_FP64 = 0, FEMB200_PRECISION_MIXED = 1 };
 
 #define FEMB200_MAX_PHASES 16
@@ -176,9 +181,6 @@ typedef struct femb200_stokes_controls {
      * (iter, err_v, err_P, unused, err_v_components[dim]). */
     double* history;
     int64_t history_capacity;
-    /* Mixed precision: FP32 inner sweeps run until their residual drops by
-     * this factor before each FP64 defect-correction step (default 1e-3). */
-    double mixed_inner_drop;
 } femb200_stokes_controls;
 
 typedef struct femb200_stokes_stats {
@@ -193,7 +195,7 @@ typedef struct femb200_stokes_stats {
     int64_t history_len;
     double err_T;
     int64_t thermal_iterations;
-    int64_t defect_corrections;   /* mixed precision: outer FP64 corrections */
+    int64_t defect_corrections;   /* mixed precision: FP64 base sweeps (one per Powell–Hestenes step) */
 } femb200_stokes_stats;
 
 /* Thermal diffusion (ThermalDiffusionDR, src/heat_diffusion/types/heat_diffusion_types.jl:90). */
