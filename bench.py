@@ -65,6 +65,24 @@ def mesh_is_affine(mesh, tol=1e-12):
     return bool(ok)
 
 
+def incremental_kernel_bytes(case):
+    """Algorithmic bytes of one FP32 incremental sweep of the mixed-precision solve:
+    δv, connectivity, the FP32 affine geometry, δP with the base RP, γP and M_P,
+    the cell phase, the base trial stress and yield value of every integration
+    point (7 × 27 FP32), RP written and the Rv read-modify-write (FP32)."""
+    m = case.mesh
+    nels, nn, nP = m.nels, m.nnodes, m.nnodesP
+    b = 3 * nn * 4                         # δv
+    b += 27 * 4 * nels + 4 * 4 * nels      # el2n, dofsP
+    b += 10 * 4 * nels                     # J⁻¹ and |det J| per element
+    b += 4 * nP * 4                        # δP, RP_base, γP, M_P
+    b += 4 * nels                          # cell phase
+    b += 7 * 27 * 4 * nels                 # base trial stress and yield value
+    b += nP * 4                            # RP written
+    b += 2 * 3 * nn * 4                    # Rv atomic read-modify-write
+    return b
+
+
 def residual_kernel_bytes(case, itemsize=8, geo_itemsize=8, affine=None):
     """Algorithmic bytes of one fused residual-sweep launch: every array the sweep
     must touch, once, at its stored precision (Rv read-modify-write counted twice).
@@ -184,8 +202,8 @@ def sweep_mode(args, fem, case, dr, lib, h):
         fem.assemble_stokes_residuals(dr, case.dt)
     for _ in range(max(1, args.steps // 10)):
         fem.assemble_augmented_momentum_jacobian(dr, case.dt)
-    prof_ms = (C.c_double * 4)()
-    prof_n = (C.c_int64 * 4)()
+    prof_ms = (C.c_double * fem._abi.PROF_COUNT)()
+    prof_n = (C.c_int64 * fem._abi.PROF_COUNT)()
     lib.femb200_profile_read(h, prof_ms, prof_n)
     lib.femb200_profile(h, 0)
     nbytes = residual_kernel_bytes(case)
@@ -231,7 +249,9 @@ def main():
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="the chosen method (mixed: FP32 increments inside FP64 outer steps)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--check-interval", type=int, default=100)
     ap.add_argument("--tolerance", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -311,8 +331,8 @@ def main():
     ev1.record(stream)
     barrier()
     ms_total = ev0.elapsed_time(ev1)
-    prof_ms = (C.c_double * 4)()
-    prof_n = (C.c_int64 * 4)()
+    prof_ms = (C.c_double * fem._abi.PROF_COUNT)()
+    prof_n = (C.c_int64 * fem._abi.PROF_COUNT)()
     lib.femb200_profile_read(h, prof_ms, prof_n)
     lib.femb200_profile(h, 0)
     clocks = sampler.stop()
@@ -354,9 +374,48 @@ def main():
     st = step_stats[-1]
     iters = st["iter"]
     jacs = st["jacobian_assemblies"]
+
+    def snapshot():
+        fem.update_stokes_current_stress(dr, case.dt)
+        return {"v": torch.cat([x.clone() for x in dr.v]), "P": dr.P.clone(),
+                "tau": torch.cat([x.clone() for x in dr.tau])}
+
+    # ---- the plain FP64 DR solve of the same workload, and the chosen method's field error ----
+    plain = None
+    if args.precision == "mixed" and not args.no_plain:
+        chosen_fields = snapshot()
+        kw64 = dict(kw, precision="fp64")
+        reset()
+        fem.solve(dr, bc, **kw64)
+        barrier()
+        lib.femb200_profile(h, 1)
+        reset()
+        ev0.record(stream)
+        st64 = fem.solve(dr, bc, **kw64)
+        ev1.record(stream)
+        barrier()
+        t64 = ev0.elapsed_time(ev1) / 1e3
+        pm = (C.c_double * fem._abi.PROF_COUNT)()
+        pn = (C.c_int64 * fem._abi.PROF_COUNT)()
+        lib.femb200_profile_read(h, pm, pn)
+        lib.femb200_profile(h, 0)
+        if world > 1:
+            tt = torch.tensor([t64], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t64 = tt.item()
+        f64 = snapshot()
+        err = {k: float(torch.linalg.norm(chosen_fields[k] - f64[k]) / torch.linalg.norm(f64[k])) for k in f64}
+        plain = {"value": t64, "unit": "s", "iterations": st64["iter"], "itPH": st64["itPH"],
+                 "jacobian_assemblies": st64["jacobian_assemblies"], "converged": bool(st64["converged"]),
+                 "err": st64["err"],
+                 "kernel_ms": {"residual": pm[0], "jacobian": pm[1], "node_update": pm[2]},
+                 "residual_avg_ms": pm[0] / max(pn[0], 1),
+                 "field_rel_err_chosen_vs_fp64": err}
+    path_iters, path_jacs = (plain["iterations"], plain["jacobian_assemblies"]) if plain else (iters, jacs)
+
     peak, peak_kind = measured_peaks()
-    itemsize = 8 if args.precision == "fp64" else 4
-    nbytes = residual_kernel_bytes(case, itemsize=8, geo_itemsize=8)
+    mixed = args.precision == "mixed"
+    nbytes = incremental_kernel_bytes(case) if mixed else residual_kernel_bytes(case, itemsize=8, geo_itemsize=8)
     res_avg_ms = prof_ms[0] / max(prof_n[0], 1)
     achieved = nbytes / (res_avg_ms / 1e3) / 1e9
     traffic = None
@@ -368,14 +427,21 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        est, cores, sample = cpu_baseline_estimate(case, iters, jacs)
+        est, cores, sample = cpu_baseline_estimate(case, path_iters, path_jacs)
         cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
 
     if rank == 0:
         os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
-        if args.n == 64 and args.precision == "fp64":
-            json.dump({"iterations": iters, "jacobian_assemblies": jacs, "itPH": st["itPH"]},
+        if args.n == 64 and (plain or args.precision == "fp64"):
+            json.dump({"iterations": path_iters, "jacobian_assemblies": path_jacs,
+                       "itPH": plain["itPH"] if plain else st["itPH"]},
                       open(os.path.join(ROOT, "profiles", "bench_path.json"), "w"))
+        if mixed:
+            kernel = "hex27_residual_pipe_kernel<float, incremental> (FP32 incremental sweep: RP, Pnum, Rv increments)"
+        elif mesh_is_affine(case.mesh):
+            kernel = "hex27_residual_pipe_kernel<double> (fused RP + Pnum + Rv sweep, affine geometry)"
+        else:
+            kernel = "hex27_residual_kernel (fused RP + Pnum + Rv sweep)"
         line = {
             "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
@@ -383,21 +449,23 @@ def main():
             "data": "synthetic",
             "config": {
                 "workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
+                "method": "mixed precision (FP32 increments, FP64 outer steps)" if mixed else "plain FP64 DR",
                 "precision": args.precision, "tolerance": args.tolerance, "check_interval": args.check_interval,
                 "dt": case.dt, "iterations": iters, "itPH": st["itPH"], "jacobian_assemblies": jacs,
+                "fp64_outer_sweeps": st.get("defect_corrections", 0),
                 "converged": bool(st["converged"]), "err": st["err"],
                 "nels": case.mesh.nels, "nnodes": case.mesh.nnodes, "nnodesP": case.mesh.nnodesP,
                 "l2": "inputs larger than L2 (geometry alone %.0f MB)" % (case.mesh.geo_v.nbytes / 1e6),
                 "parallelism": f"replicas{world}",
             },
+            "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (plain["value"] / t_step) if plain else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "hex27_residual_pipe_kernel (fused RP + Pnum + Rv sweep, affine geometry)"
-                                   if mesh_is_affine(case.mesh) else "hex27_residual_kernel (fused RP + Pnum + Rv sweep)",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": res_avg_ms,
                          "launches": int(prof_n[0]), "peak_kind": peak_kind},
             "kernel_ms": {"residual": prof_ms[0], "jacobian": prof_ms[1], "node_update": prof_ms[2],
-                          "total_timed": ms_total},
+                          "outer_fp64_sweeps": prof_ms[4], "total_timed": ms_total},
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(prof_n[3]),
             "cpu_baseline": cpu,

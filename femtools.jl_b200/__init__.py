@@ -9,15 +9,17 @@ from . import _abi  # noqa: F401
 from . import mesh  # noqa: F401
 from . import problem  # noqa: F401
 from . import configs  # noqa: F401
+from . import coloring  # noqa: F401
+from .coloring import color_mesh, generate_element_groups  # noqa: F401
 from .mesh import structured_mixed_mesh, element_tables, MixedMesh  # noqa: F401
 from .problem import StokesMaterial, DruckerPrager, DirichletBoundaryCondition  # noqa: F401
 
 __all__ = ["structured_mixed_mesh", "element_tables", "MixedMesh", "StokesMaterial", "DruckerPrager",
-           "DirichletBoundaryCondition"]
+           "DirichletBoundaryCondition", "color_mesh", "generate_element_groups"]
 
 from . import solver  # noqa: E402,F401
 from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, solve_coupled,  # noqa: E402,F401
                      solve_thermal, assemble_pressure_residual, assemble_momentum_residual,
                      assemble_stokes_residuals, assemble_augmented_momentum_jacobian,
                      assemble_viscosity_weighted_pressure_scaling, update_stokes_current_stress,
-                     assemble_shear_heating, assemble_thermal_residual)
+                     assemble_shear_heating, assemble_thermal_residual, assemble_diffusion_matrices_colored)

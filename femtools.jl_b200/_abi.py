@@ -144,10 +144,14 @@ SIGNATURES = {
                                         _P(StokesStatsC)]),
     "femb200_profile": (C.c_int, [_vp, C.c_int32]),
     "femb200_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_int64)]),
+    "femb200_color_mesh": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _P(C.c_int32)]),
+    "femb200_color_groups": (C.c_int, [_vp, C.c_int64, C.c_int32, _vp, _vp]),
+    "femb200_thermal_residual_colored": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32,
+                                                   _vp, _vp, C.c_int32]),
     "femb200_solve_thermal_noalloc": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
 }
 NOALLOC_MAX_NODES = 8388608   # FEMB200_NOALLOC_MAX_NODES
-PROF_RESIDUAL, PROF_JACOBIAN, PROF_NODE, PROF_ALL, PROF_COUNT = range(5)
+PROF_RESIDUAL, PROF_JACOBIAN, PROF_NODE, PROF_ALL, PROF_OUTER, PROF_COUNT = range(6)
 
 _lib = None
 

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfemtools_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["api.cu", "stokes3d.cu", "stokes3d_pipe.cu", "jacobian3d.cu", "simple.cu", "node.cu"]
+SOURCES = ["api.cu", "stokes3d.cu", "stokes3d_pipe.cu", "jacobian3d.cu", "simple.cu", "node.cu", "coloring.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-rdc=true"]
@@ -33,7 +33,7 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or verbose_ptxas or _stale(o, [s] + headers):
             cmd = [NVCC, *FLAGS, *extra, "-c", s, "-o", o]

@@ -42,9 +42,10 @@ struct femb200_handle {
     // profiling: event pairs per kernel class, folded into totals when the pool fills
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool[FEMB200_PROF_COUNT];
-    size_t ev_used[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
-    double prof_ms[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
-    int64_t prof_n[FEMB200_PROF_COUNT] = {0, 0, 0, 0};
+    size_t ev_used[FEMB200_PROF_COUNT] = {};
+    double prof_ms[FEMB200_PROF_COUNT] = {};
+    int64_t prof_n[FEMB200_PROF_COUNT] = {};
+    int prof_sweep = FEMB200_PROF_RESIDUAL;   // class of launch_residual's sweeps
     unsigned long long launches_at_reset = 0;
     // compressed affine geometry (one J⁻¹, |det J| per element), rebuilt per call
     void* d_geo_c = nullptr;
@@ -371,10 +372,11 @@ int prepare_geometry(femb200_handle* h, const femb200_stokes_problem* p) {
 }
 
 template <class T, class TG>
-int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H27Args<T, TG>& a) {
-    if (a.do_momentum)
+int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H27Args<T, TG>& a,
+                    bool rv_zeroed = false) {
+    if (a.do_momentum && !rv_zeroed)
         for (int c = 0; c < p->dim; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(T) * p->nnodes, h->stream));
-    RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
+    RC(prof_begin(h, h->prof_sweep));
     if (p->dim == 3 && h->geo_c_valid) {
         H27Args<T, T> b;
         std::memcpy(&b, &a, sizeof(b));   // identical layout; the pipelined sweep reads geometry from d_geo_c
@@ -385,14 +387,14 @@ int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H2
     } else {
         CK(launch_q9_residual<T, TG>(a, h->stream));
     }
-    RC(prof_end(h, FEMB200_PROF_RESIDUAL));
+    RC(prof_end(h, h->prof_sweep));
     return FEMB200_OK;
 }
 
 // Residual sweep: RP (+ Pnum) and, optionally, Rv.
 template <class T, class TG>
 int residual_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt, int with_pnum, int do_momentum,
-                   int write_RP) {
+                   int write_RP, bool rv_zeroed = false) {
     H27Args<T, TG> a = residual_args<T, TG>(p, dt);
     a.with_pnum = with_pnum;
     a.do_momentum = do_momentum;
@@ -404,7 +406,7 @@ int residual_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
     if (do_momentum)
         for (int c = 0; c < p->dim; ++c)
             if (!p->Rv[c]) { h->err = "Rv is required"; return FEMB200_EINVAL; }
-    return launch_residual<T, TG>(h, p, a);
+    return launch_residual<T, TG>(h, p, a, rv_zeroed);
 }
 
 template <class T, class TG>
@@ -501,6 +503,32 @@ int thermal_assemble(femb200_handle* h, const femb200_thermal_problem* t, double
         CK(cudaMemsetAsync(t->PC, 0, sizeof(T) * t->nnodes, h->stream));
     }
     CK(launch_thermal<T, TG>(a, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+// assemble_dr_matrices_colored! (src/dynamic_relaxation/assembly.jl:71-92): the
+// colour groups one launch after another, each scattering with plain adds.
+template <class T, class TG>
+int thermal_assemble_colored(femb200_handle* h, const femb200_thermal_problem* t, double dt, double Tref, bool jac,
+                             const int32_t* groups, const int64_t* offsets, int32_t ngroups) {
+    ThermalArgs<T, TG> a;
+    std::memset(&a, 0, sizeof(a));
+    a.dim = t->dim; a.el2n = t->el2n; a.geo = static_cast<const TG*>(t->geo);
+    a.Tn = static_cast<const T*>(t->T); a.T0 = static_cast<const T*>(t->T0); a.P = static_cast<const T*>(t->P);
+    a.src = static_cast<const T*>(t->source); a.src_ip = static_cast<const T*>(t->source_ip);
+    a.ph = t->phases; a.ph_layout = t->phases_layout;
+    a.R = static_cast<T*>(t->R); a.dRdT = static_cast<T*>(t->dRdT); a.PC = static_cast<T*>(t->PC);
+    a.nels = t->nels; a.dt = (T)dt; a.Tref = (T)Tref; a.jac = jac ? 1 : 0;
+    CK(cudaMemsetAsync(t->R, 0, sizeof(T) * t->nnodes, h->stream));
+    if (jac) {
+        CK(cudaMemsetAsync(t->dRdT, 0, sizeof(T) * t->nnodes, h->stream));
+        CK(cudaMemsetAsync(t->PC, 0, sizeof(T) * t->nnodes, h->stream));
+    }
+    for (int32_t g = 0; g < ngroups; ++g) {
+        a.group = groups + offsets[g];
+        a.ngroup = offsets[g + 1] - offsets[g];
+        CK(launch_thermal<T, TG>(a, h->num_sms, h->stream));
+    }
     return FEMB200_OK;
 }
 
@@ -693,13 +721,16 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
         while ((err > eps_vel || !thermal_converged) && itPT <= c->iter_max) {
             ++itPT; ++iter;
             const bool do_check = iter % nout == 0;
-            if (do_check)
+            // After the first iteration of a Powell–Hestenes step the previous node
+            // update has zeroed Rv for this sweep and, before a check, saved R0.
+            const bool fused = itPT > 1 && nout > 1;
+            if (do_check && !fused)
                 for (int k = 0; k < D; ++k) CK(launch_copy<T>(static_cast<T*>(p->Rv0[k]), static_cast<const T*>(p->Rv[k]), nn, h->stream));
             if (cp) {
                 RC((thermal_coupled_step<T, TG>(h, *cp, ti, p, nout, dt)));
                 thermal_converged = ti.converged;
             }
-            RC((residual_sweep<T, TG>(h, p, dt, 1, 1, 1)));
+            RC((residual_sweep<T, TG>(h, p, dt, 1, 1, 1, fused)));
             RC(apply_bc_R());
             NodeArgs<T> na;
             std::memset(&na, 0, sizeof(na));
@@ -712,6 +743,8 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
             na.mask = h->d_mask; na.n = nn; na.dim = D;
             na.reduce = do_check ? 1 : 0;
             na.partials = h->d_partials;
+            na.save_R0 = nout > 1 && (iter + 1) % nout == 0;
+            na.fill = nout > 1;
             RC(prof_begin(h, FEMB200_PROF_NODE));
             CK(launch_node_update<T>(na, nb, h->stream));
             RC(prof_end(h, FEMB200_PROF_NODE));
@@ -831,6 +864,12 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     RC(upload_material(h, p->mat, finite_K, dt));
     RC((prepare_geometry<T, TG>(h, p)));
     if (!h->geo_c_valid) { h->err = "the mixed-precision solve needs affine (parallelepiped) Hex27 elements"; return FEMB200_EUNSUPPORTED; }
+    // the FP64 outer sweeps are timed apart from the FP32 incremental sweeps
+    struct SweepClass {
+        femb200_handle* h;
+        ~SweepClass() { h->prof_sweep = FEMB200_PROF_RESIDUAL; }
+    } restore{h};
+    h->prof_sweep = FEMB200_PROF_OUTER;
     RC(build_mask(h, p));
     RC(ensure_mixed(h, p));
     auto& m = h->mixed;
@@ -882,8 +921,9 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     ai.with_pnum = 1; ai.do_momentum = 1; ai.write_RP = 1; ai.Pnum_out = nullptr;
     for (int k = 0; k < 7; ++k) ai.base_in[k] = m.base[k];
     ai.RP_base = m.RPk;
-    auto incr_sweep = [&]() -> int {
-        for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
+    auto incr_sweep = [&](bool prefilled) -> int {
+        if (!prefilled)
+            for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
         RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
         CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
         RC(prof_end(h, FEMB200_PROF_RESIDUAL));
@@ -973,9 +1013,12 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
         while (err > eps_vel && itPT <= c->iter_max) {
             ++itPT; ++iter;
             const bool do_check = iter % nout == 0;
-            if (do_check)
+            // after the first iteration of the step the previous node update has set
+            // R = R_k for this sweep and, before a check, saved R0
+            const bool fused = itPT > 1 && nout > 1;
+            if (do_check && !fused)
                 for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R0[k], m.R[k], nn, s));
-            RC(incr_sweep());
+            RC(incr_sweep(fused));
             NodeArgs<float> na;
             std::memset(&na, 0, sizeof(na));
             for (int k = 0; k < 3; ++k) {
@@ -985,6 +1028,9 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             na.mask = h->d_mask; na.n = nn; na.dim = D;
             na.reduce = do_check ? 1 : 0;
             na.partials = h->d_partials;
+            na.save_R0 = nout > 1 && (iter + 1) % nout == 0;
+            na.fill = nout > 1;
+            for (int k = 0; k < 3; ++k) na.Rfill[k] = m.Rk[k];
             RC(prof_begin(h, FEMB200_PROF_NODE));
             CK(launch_node_update<float>(na, nb, s));
             RC(prof_end(h, FEMB200_PROF_NODE));
@@ -1280,6 +1326,19 @@ int femb200_thermal_residual(femb200_handle* h, const femb200_thermal_problem* t
     RC(upload_thermal_material(h, t));
     if (t->dtype == FEMB200_F64) return thermal_assemble<double, double>(h, t, dt, Tref, jac != 0, t->source_ip);
     return thermal_assemble<float, float>(h, t, dt, Tref, jac != 0, t->source_ip);
+}
+
+int femb200_thermal_residual_colored(femb200_handle* h, const femb200_thermal_problem* t, double dt, double Tref,
+                                     int32_t jac, const int32_t* groups, const int64_t* offsets, int32_t ngroups) {
+    if (!h || !t) return FEMB200_EINVAL;
+    if (!groups || !offsets || ngroups < 1) { h->err = "colour groups are required"; return FEMB200_EINVAL; }
+    if (offsets[0] != 0 || offsets[ngroups] != t->nels) { h->err = "colour groups must cover every element once"; return FEMB200_EINVAL; }
+    for (int32_t g = 0; g < ngroups; ++g)
+        if (offsets[g + 1] < offsets[g]) { h->err = "colour group offsets must not decrease"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    RC(upload_thermal_material(h, t));
+    if (t->dtype == FEMB200_F64) return thermal_assemble_colored<double, double>(h, t, dt, Tref, jac != 0, groups, offsets, ngroups);
+    return thermal_assemble_colored<float, float>(h, t, dt, Tref, jac != 0, groups, offsets, ngroups);
 }
 
 int femb200_solve_thermal(femb200_handle* h, const femb200_thermal_problem* t, const femb200_thermal_controls* c,

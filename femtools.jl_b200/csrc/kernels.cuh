@@ -130,7 +130,9 @@ struct NodeArgs {
     int dim;
     double alpha[3];       // negated Chebyshev step (v += alpha·rate)
     double beta[3];
-    int save_R0;           // copy (masked) R into Rv0 after the update
+    int save_R0;           // copy (masked) R into Rv0 after the update (the next iteration checks)
+    int fill;              // then set Rv to the next sweep's starting value: Rfill, or 0
+    const T* Rfill[3];
     int reduce;            // write block partials of the norms and λmin sums
     double lam_step[3];    // α used in the λmin sums (DR.jl:722-724)
     double* partials;      // gridDim.x × RED_SLOTS
@@ -182,6 +184,10 @@ struct ThermalArgs {
     int64_t nels;
     T dt, Tref;
     int jac;
+    // colour group (1-based element indices, elements sharing no node) or null: with
+    // a group the launch covers only its elements and scatters with plain adds
+    const int32_t* group;
+    int64_t ngroup;
 };
 template <class T, class TG>
 cudaError_t launch_thermal(const ThermalArgs<T, TG>& a, int num_sms, cudaStream_t st);

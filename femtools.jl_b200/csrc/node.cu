@@ -43,27 +43,39 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_kernel(NodeArgs<T> a
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         const unsigned msk = a.mask ? a.mask[i] : 0u;
+        // all loads of the node first: the stores below may alias them as far as the
+        // compiler knows, and would otherwise serialise the components' round trips
+        T R[3], rt[3], pc[3], vv[3], r0[3], rf[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (c < a.dim) {
+                R[c] = a.Rv[c][i]; rt[c] = a.rate[c][i]; pc[c] = a.PC[c][i]; vv[c] = a.v[c][i];
+                r0[c] = a.reduce ? a.Rv0[c][i] : T(0);
+                rf[c] = (a.fill && a.Rfill[c]) ? a.Rfill[c][i] : T(0);
+            }
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (c >= a.dim) break;
-            T R = a.Rv[c][i];
             T r;
             if ((msk >> c) & 1u) {
-                R = T(0);
-                a.Rv[c][i] = T(0);
+                R[c] = T(0);
+                if (!a.fill) a.Rv[c][i] = T(0);
                 r = T(0);
                 a.rate[c][i] = T(0);
             } else {
-                r = (T)a.beta[c] * a.rate[c][i] + R / a.PC[c][i];
+                r = (T)a.beta[c] * rt[c] + R[c] / pc[c];
                 a.rate[c][i] = r;
-                a.v[c][i] += (T)a.alpha[c] * r;
+                a.v[c][i] = vv[c] + (T)a.alpha[c] * r;
             }
+            if (a.save_R0) a.Rv0[c][i] = R[c];
+            if (a.fill) a.Rv[c][i] = rf[c];
             if (a.reduce) {
-                const double Rd = (double)R;
+                const double Rd = (double)R[c];
                 const double sr = a.lam_step[c] * (double)r;
                 acc[c * 3 + 0] += Rd * Rd;
                 acc[c * 3 + 1] += sr * sr;
-                acc[c * 3 + 2] += sr * ((Rd - (double)a.Rv0[c][i]) / (double)a.PC[c][i]);
+                acc[c * 3 + 2] += sr * ((Rd - (double)r0[c]) / (double)pc[c]);
             }
         }
     }

@@ -368,8 +368,9 @@ template <int DIM, class T, class TG>
 __global__ void thermal_kernel(ThermalArgs<T, TG> a) {
     using TB = Tabs<DIM>;
     constexpr int NV = TB::NV, NQ = TB::NQ, S = DIM * DIM + 1;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.nels) return;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (a.group ? a.ngroup : a.nels)) return;
+    const int64_t e = a.group ? (int64_t)__ldg(a.group + t) - 1 : t;
     int node[NV], ph[NV];
     T Tl[NV];
     for (int i = 0; i < NV; ++i) {
@@ -419,7 +420,10 @@ __global__ void thermal_kernel(ThermalArgs<T, TG> a) {
             R[i] += rate * (T)TB::N(q, i) * dO - dtrc * KT * dO;
         }
     }
-    for (int i = 0; i < NV; ++i) atomic_add(a.R + node[i], R[i]);
+    for (int i = 0; i < NV; ++i) {
+        if (a.group) a.R[node[i]] += R[i];
+        else atomic_add(a.R + node[i], R[i]);
+    }
     if (!a.jac) return;
     // Jacobian rows: J[i][b] = Σ_q dΩ [ (−N_b + ∂dtrc_b (s_q + Φ_q)) N_i − ∂dtrc_b KT_i − dtrc k ∇N_i·∇N_b ]
     // with ∂dtrc/∂T_b = dtrc·αq·ρ0q·N_b/ρq (EOS dependence of the density).
@@ -471,8 +475,13 @@ __global__ void thermal_kernel(ThermalArgs<T, TG> a) {
         }
         T row = T(0);
         for (int b = 0; b < NV; ++b) row += fabs(Jrow[b]);
-        atomic_add(a.dRdT + node[i], row);
-        atomic_add(a.PC + node[i], fabs(Jrow[i]));
+        if (a.group) {
+            a.dRdT[node[i]] += row;
+            a.PC[node[i]] += fabs(Jrow[i]);
+        } else {
+            atomic_add(a.dRdT + node[i], row);
+            atomic_add(a.PC + node[i], fabs(Jrow[i]));
+        }
     }
 }
 
@@ -513,9 +522,11 @@ cudaError_t launch_q9_jacobian(const H27JacArgs<T, TG>& args, cudaStream_t st) {
 template <class T, class TG>
 cudaError_t launch_thermal(const ThermalArgs<T, TG>& a, int num_sms, cudaStream_t st) {
     (void)num_sms;
+    const int64_t n = a.group ? a.ngroup : a.nels;
+    if (n <= 0) return cudaSuccess;
     count_launch();
-    if (a.dim == 3) thermal_kernel<3, T, TG><<<nb(a.nels, 64), 64, 0, st>>>(a);
-    else thermal_kernel<2, T, TG><<<nb(a.nels, 128), 128, 0, st>>>(a);
+    if (a.dim == 3) thermal_kernel<3, T, TG><<<nb(n, 64), 64, 0, st>>>(a);
+    else thermal_kernel<2, T, TG><<<nb(n, 128), 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

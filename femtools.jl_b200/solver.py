@@ -312,6 +312,19 @@ def assemble_thermal_residual(th: ThermalDiffusionDR, dt, Tref=273.0, compute_ja
     _check(lib, h, lib.femb200_thermal_residual(h, C.byref(th.problem()), float(dt), float(Tref), int(compute_jacobian)))
 
 
+def assemble_diffusion_matrices_colored(th: ThermalDiffusionDR, groups, dt, Tref=273.0, compute_jacobian=False):
+    """assemble_diffusion_matrices_colored! (heat_diffusion/assembly/residual_colored.jl:10):
+    one launch per colour group of `groups` (coloring.ElementGroups), plain adds."""
+    lib, h = _Handle.get()
+    dev = getattr(groups, "_device", None)
+    if dev is None:
+        dev = torch.as_tensor(groups.elements, device=th.device)
+        groups._device = dev
+    _check(lib, h, lib.femb200_thermal_residual_colored(h, C.byref(th.problem()), float(dt), float(Tref),
+                                                        int(compute_jacobian), C.c_void_p(_ptr(dev)),
+                                                        groups.offsets.ctypes.data, groups.ncolors))
+
+
 def solve_thermal(th: ThermalDiffusionDR, bc, dt, Tref=273.0, tolerance=None, max_iterations=10_000,
                   check_interval=100, throw_on_failure=True):
     """solve!(dr::ThermalDiffusionDR, mesh, bc; dt) (heat_diffusion/solvers/DR.jl:50)."""

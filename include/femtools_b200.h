@@ -306,6 +306,28 @@ int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p,
 int femb200_thermal_residual(femb200_handle* h, const femb200_thermal_problem* t,
                              double dt, double Tref, int32_t compute_jacobian);
 
+/* ---- element colouring (host code) -------------------------------------- */
+
+/* color_mesh_greedy / color_mesh (src/mesh/coloring.jl:26-64): elements are
+ * visited in order and each takes the smallest positive colour not used by an
+ * element sharing a node with it. Host arrays: el2n is nv × nels (1-based),
+ * colors receives nels colours in 1..ncolors. Needs no GPU. */
+int femb200_color_mesh(const int32_t* el2n, int32_t nv, int64_t nels, int64_t nnodes,
+                       int32_t* colors, int32_t* ncolors);
+/* generate_element_groups (src/mesh/coloring.jl:77-81): the 1-based element
+ * indices of each colour, ascending, as CSR — group c is
+ * elements[offsets[c-1] .. offsets[c]-1]; offsets has ncolors + 1 entries. Host
+ * arrays; needs no GPU. */
+int femb200_color_groups(const int32_t* colors, int64_t nels, int32_t ncolors,
+                         int64_t* offsets, int32_t* elements);
+/* assemble_diffusion_matrices_colored! (src/heat_diffusion/assembly/residual_colored.jl:10):
+ * the thermal residual (and with jac the Jacobian row sums and |diagonal|) by one
+ * launch per colour group, scattering with plain adds. groups: device array of
+ * the CSR elements above; offsets: host array of ncolors + 1 entries. */
+int femb200_thermal_residual_colored(femb200_handle* h, const femb200_thermal_problem* t,
+                                     double dt, double Tref, int32_t jac,
+                                     const int32_t* groups, const int64_t* offsets, int32_t ngroups);
+
 /* solve!(::ThermalDiffusionDR, …) (src/heat_diffusion/solvers/DR.jl:50 →
  * src/dynamic_relaxation/solver.jl:61). */
 int femb200_solve_thermal(femb200_handle* h, const femb200_thermal_problem* t,
@@ -332,9 +354,11 @@ int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t,
 /* ---- measurement (no counterpart in the reference, which has no timers) ---- */
 
 /* Kernel classes timed when profiling is on; slot FEMB200_PROF_ALL counts every
- * kernel the library launched (its milliseconds are not measured). */
+ * kernel the library launched (its milliseconds are not measured). In a
+ * mixed-precision solve RESIDUAL holds the FP32 incremental sweeps and OUTER the
+ * FP64 sweeps of the Powell–Hestenes steps. */
 enum { FEMB200_PROF_RESIDUAL = 0, FEMB200_PROF_JACOBIAN = 1, FEMB200_PROF_NODE = 2, FEMB200_PROF_ALL = 3,
-       FEMB200_PROF_COUNT = 4 };
+       FEMB200_PROF_OUTER = 4, FEMB200_PROF_COUNT = 5 };
 
 /* Turn per-launch CUDA-event timing of the residual sweep, the Jacobian
  * diagnostics and the node update on (1) or off (0), and reset the totals. The

@@ -263,3 +263,27 @@ def test_fp32_state_tracks_fp64_oracle():
     for c in range(3):
         close(dr.Rv[c].double(), hs.Rv[c], rtol=5e-4, atol_rel=5e-5, what=f"FP32 Rv[{c}]")
     close(dr.RP.double(), hs.RP, rtol=5e-4, atol_rel=5e-5, what="FP32 RP")
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_colored_thermal_assembly_matches_atomic(dim):
+    # assemble_diffusion_matrices_colored! vs the atomic assembler (test/test_assembler_api.jl:8-60),
+    # on a mesh with mixed phases, and against the oracle.
+    mesh = fem.structured_mixed_mesh(dim, (4,) * dim)
+    rng = np.random.default_rng(9)
+    kw = dict(k=(1.0, 2.5), Cp=(1.0, 1.3), rho0=(1.0, 1.2), alpha=(0.05, 0.02), K=(50.0, 80.0))
+    ph = rng.integers(1, 3, mesh.nnodes).astype(np.int32)
+    th = fem.ThermalDiffusionDR(mesh, phases=ph, **kw)
+    ht = oh.HostThermal(mesh, phases=ph, **kw)
+    for name in ("T", "T0", "source"):
+        x = rng.uniform(0, 1, mesh.nnodes)
+        getattr(th, name).copy_(torch.as_tensor(x))
+        getattr(ht, name)[:] = x
+    groups = fem.generate_element_groups(fem.color_mesh(mesh))
+    fem.assemble_thermal_residual(th, 0.1, 0.3, compute_jacobian=True)
+    atomic = [x.clone() for x in (th.R, th.dRdT, th.PC)]
+    fem.assemble_diffusion_matrices_colored(th, groups, 0.1, 0.3, compute_jacobian=True)
+    ht.residual(0.1, 0.3, jac=True)
+    for got, ref, host, what in zip((th.R, th.dRdT, th.PC), atomic, (ht.R, ht.dRdT, ht.PC), ("R", "∂R∂T", "PC")):
+        close(got, ref.cpu().numpy(), rtol=1e-12, atol_rel=1e-14, what=what + " colored vs atomic")
+        close(got, host, rtol=1e-9, what=what + " colored vs oracle")
