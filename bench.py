@@ -258,6 +258,8 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="iteration count of the GPU run used to scale the reference sample")
     ap.add_argument("--ref-jacobians", type=int, default=0)
+    ap.add_argument("--max-iterations", type=int, default=2_000_000,
+                    help="cap on DR iterations per solve (profiling runs of a few sweeps)")
     ap.add_argument("--mode", default="solve", choices=["solve", "sweep"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
@@ -309,7 +311,7 @@ def main():
             dr.tau_old[c].copy_(init["tau_old"][c])
 
     kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
-              max_iterations=2_000_000, iter_max=2_000_000, precision=args.precision)
+              max_iterations=args.max_iterations, iter_max=args.max_iterations, precision=args.precision)
     stats = None
     for _ in range(args.warmup):
         reset()

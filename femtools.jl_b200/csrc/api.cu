@@ -8,6 +8,7 @@
 // host norms do) and the iteration scalars α, β are passed by value.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -16,6 +17,7 @@
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "rheology.cuh"
 
 namespace femb {
 __constant__ DevStokesMaterial c_mat;
@@ -54,14 +56,18 @@ struct femb200_handle {
     int* h_flag = nullptr;
     bool geo_c_valid = false;
     int use_pipe = 1;   // the pipelined sweep on affine meshes (0 forces the general sweep)
+    int use_incr_thread = 1;   // the thread-per-element incremental sweep where it applies (0: warp-cooperative)
     // FP32 arrays of the mixed-precision solve, carved from one allocation
     struct Mixed {
         void* mem = nullptr;
         size_t cap = 0;
         float *dv[3], *rate[3], *R[3], *R0[3], *Rk[3], *dRdv[3], *PC[3], *v32[3];
         float *dP, *RP, *RPk, *gP, *MP, *P32, *P0, *T, *T0, *Pf;
-        float *base[7], *told[6], *eta;
+        float *base, *told[6], *eta;
         float* geo;
+        // tiled inputs of the thread-per-element incremental sweep
+        int32_t *el2n_t, *dofs_t, *phase_t;
+        float *geo_t, *eta_t, *pscale_t, *RPinc;
     } mixed;
 };
 
@@ -822,7 +828,15 @@ int ensure_mixed(femb200_handle* h, const femb200_stokes_problem* p) {
     parts.push_back({&m.T, p->T ? nP : 0});
     parts.push_back({&m.T0, p->T0 ? nP : 0});
     parts.push_back({&m.Pf, p->Pf ? nP : 0});
-    for (int c = 0; c < 7; ++c) parts.push_back({&m.base[c], nip});
+    const size_t nslots = ((size_t)p->nels + 31) / 32 * 32;
+    parts.push_back({&m.base, nslots * 27 * BASE_FIELDS});
+    parts.push_back({reinterpret_cast<float**>(&m.el2n_t), nslots * 27});
+    parts.push_back({reinterpret_cast<float**>(&m.dofs_t), nslots * 4});
+    parts.push_back({reinterpret_cast<float**>(&m.phase_t), nslots * 2});
+    parts.push_back({&m.geo_t, nslots * 10});
+    parts.push_back({&m.eta_t, p->viscosity_ip ? nslots * 27 : 0});
+    parts.push_back({&m.pscale_t, nslots * 4});
+    parts.push_back({&m.RPinc, nP});
     for (int c = 0; c < 6; ++c) parts.push_back({&m.told[c], ip && p->tau_old[c] ? nip : 0});
     parts.push_back({&m.eta, p->viscosity_ip ? nip : 0});
     parts.push_back({&m.geo, (size_t)p->nels * 10});
@@ -919,13 +933,63 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     pi.gammaP = m.gP; pi.M_P = m.MP; pi.RP = m.RP; pi.viscosity_ip = m.eta;
     H27Args<float, float> ai = residual_args<float, float>(&pi, dt);
     ai.with_pnum = 1; ai.do_momentum = 1; ai.write_RP = 1; ai.Pnum_out = nullptr;
-    for (int k = 0; k < 7; ++k) ai.base_in[k] = m.base[k];
+    ai.base_in = m.base;
     ai.RP_base = m.RPk;
+    // the thread-per-element sweep, on meshes whose elements each carry one phase
+    IncrArgs at;
+    std::memset(&at, 0, sizeof(at));
+    at.el2n_t = m.el2n_t; at.dofs_t = m.dofs_t; at.geo_t = m.geo_t; at.phase_t = m.phase_t; at.base_t = m.base;
+    at.eta_t = m.eta ? m.eta_t : nullptr;
+    at.pscale_t = m.pscale_t;
+    for (int k = 0; k < 3; ++k) { at.dv[k] = m.dv[k]; at.R[k] = m.R[k]; at.g[k] = (float)p->mat.g[k]; }
+    at.dP = m.dP; at.RPinc = m.RPinc;
+    at.nels = p->nels;
+    at.plastic = p->mat.plastic;
+    {
+        bool all_inf = true;
+        for (int i = 0; i < p->mat.nphases; ++i) all_inf = all_inf && std::isinf(finite_K ? p->mat.K[i] : p->mat.eta_b[i]);
+        for (int i = 0; i < FEMB200_MAX_PHASES; ++i) {
+            const femb200_stokes_material& mt = p->mat;
+            const double invG = 1.0 / mt.G[i];
+            const double etave = 1.0 / (1.0 / mt.eta[i] + invG / dt);
+            const double rest = mt.eta_reg[i] + mt.Kb[i] * dt * (-mt.sin_psi[i]) * (-mt.sin_phi[i]);
+            IncrPhase& q = at.ph[i];
+            q.twoe = (float)(2 * etave);
+            q.rho0beta = (float)(mt.rho0[i] / mt.K[i]);
+            q.cC = (float)(mt.cos_phi[i] * mt.C[i]);
+            q.sphi = (float)mt.sin_phi[i];
+            q.inv_den = (float)(1.0 / (etave + rest));
+            q.invbulkdt = all_inf ? 0.0f : (float)(1.0 / ((finite_K ? mt.K[i] : mt.eta_b[i]) * dt));
+            q.invG_dt = (float)(invG / dt);
+            q.den_rest = (float)rest;
+        }
+    }
+    {
+        IncrTileSrc ts;
+        ts.el2n = p->el2n; ts.dofsP = p->dofsP; ts.geo_c = m.geo; ts.eta = m.eta; ts.gP = m.gP; ts.MP = m.MP;
+        ts.phv = p->phases_v; ts.phv_layout = p->phases_v_layout;
+        ts.php = p->phases_P; ts.php_layout = p->phases_P_layout;
+        ts.nphases = p->mat.nphases;
+        CK(cudaMemsetAsync(m.base, 0, sizeof(float) * ((size_t)p->nels + 31) / 32 * 32 * 27 * BASE_FIELDS, s));
+        CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+        CK(launch_incr_tiles(ts, p->nels, at, h->d_flag, s));
+        CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    const bool thread_sweep = (*h->h_flag & INCR_MIXED_PHASES) == 0 && h->use_incr_thread;
+    at.dofs_linear = (*h->h_flag & INCR_DOFS_GENERAL) == 0;
+    // the thread-per-element sweep writes the increment of RP; RP itself is formed
+    // where it is read (checks and the Powell–Hestenes pressure update)
+    auto form_RP = [&]() -> int {
+        if (thread_sweep) CK(launch_add_f32(m.RP, m.RPk, m.RPinc, nP, s));
+        return FEMB200_OK;
+    };
     auto incr_sweep = [&](bool prefilled) -> int {
         if (!prefilled)
             for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
         RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
-        CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
+        if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s));
+        else CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
         RC(prof_end(h, FEMB200_PROF_RESIDUAL));
         return FEMB200_OK;
     };
@@ -942,7 +1006,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
         H27Args<T, TG> a = residual_args<T, TG>(p, dt);
         a.with_pnum = 1; a.do_momentum = 1; a.write_RP = 1;
         a.Pnum_out = static_cast<T*>(p->Pnum);
-        for (int k = 0; k < 7; ++k) a.base_out[k] = m.base[k];
+        a.base_out = m.base;
         RC((launch_residual<T, TG>(h, p, a)));
         RC(apply_bc_R());
         for (int k = 0; k < D; ++k) CK(launch_round(m.Rk[k], static_cast<const T*>(p->Rv[k]), nullptr, nn, s));
@@ -1046,6 +1110,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
                 if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_EKABOOM; }
                 if (c->history) {
                     double sPc;
+                    RC(form_RP());
                     RC(sumsq<float>(h, m.RP, m.MP, nP, sPc));
                     push_hist((double)iter, ev, std::sqrt(sPc) / sq_nP, cmp);
                 } else {
@@ -1061,6 +1126,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             }
             if (iter > c->max_iterations) break;
         }
+        RC(form_RP());
         CK(launch_pressure_update<float>(m.dP, m.gP, m.RP, m.MP, nP, s));
         if (iter > c->max_iterations) break;
     }
@@ -1177,6 +1243,9 @@ int femb200_create(femb200_handle** out) {
     }
     int rc = ensure_tables(h);
     if (rc) { delete h; *out = nullptr; return rc; }
+    // FEMB200_INCR_SWEEP=warp selects the warp-cooperative incremental sweep of the
+    // mixed-precision solve (for comparisons); the default is thread-per-element
+    if (const char* v = std::getenv("FEMB200_INCR_SWEEP")) h->use_incr_thread = std::strcmp(v, "warp") != 0;
     *out = h;
     return FEMB200_OK;
 }

@@ -45,11 +45,12 @@ struct H27Args {
     int write_RP;
     // Mixed precision (FP32 increments about an FP64 base state, pipelined sweep only):
     // the base sweep writes the trial stress (6) and yield value (1) of every
-    // integration point as FP32 into base_out; the incremental sweep reads them
-    // from base_in, takes v and P as the increments δv, δP and adds its
-    // increments to Rv (pre-filled with the base residual) and to RP_base.
-    float* base_out[7];
-    const float* base_in[7];
+    // integration point as FP32 into base_out (tiled, rheology.cuh base_index);
+    // the incremental sweep reads them from base_in, takes v and P as the
+    // increments δv, δP and adds its increments to Rv (pre-filled with the base
+    // residual) and to RP_base.
+    float* base_out;
+    const float* base_in;
     const T* RP_base;
 };
 
@@ -64,6 +65,61 @@ cudaError_t launch_hex27_residual_incr(const H27Args<float, float>& args, const 
 template <class TG, class TC>
 cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t nels, TC* out, int* not_affine,
                                      cudaStream_t st);
+
+// Thread-per-element FP32 incremental sweep (stokes3d_incr.cu) on meshes whose
+// elements each carry one phase (any layout). Its per-element inputs are re-laid in tiles of 32 elements
+// (element e at tile e/32, lane e%32) once per solve, so every per-element read of
+// a warp is one coalesced line.
+struct IncrPhase {
+    float twoe;        // 2ηve at the solve's Δt
+    float rho0beta;    // ρ0/K: EOS density increment per unit pressure increment
+    float cC;          // C·cosϕ
+    float sphi;        // sinϕ
+    float inv_den;     // 1/(ηve + η_reg + Kb·Δt·sinΨ·sinϕ)
+    float invbulkdt;   // 1/(bulk·Δt), 0 when every phase is incompressible
+    float invG_dt;     // 1/(GΔt), for viscosities given per integration point
+    float den_rest;    // η_reg + Kb·Δt·sinΨ·sinϕ, likewise
+};
+struct IncrArgs {
+    const int32_t* el2n_t;   // [tiles][27][32] 0-based nodes in tensor order i + 3j + 9k
+    const int32_t* dofs_t;   // [tiles][4][32]  0-based pressure DoFs
+    const float* geo_t;      // [tiles][10][32] J⁻¹ (column-major) and |det J|
+    const int32_t* phase_t;  // [2][tiles·32] 0-based phase of the element's velocity nodes, then of its pressure DoFs
+    const float* base_t;     // tiled base data (rheology.cuh base_index)
+    const float* eta_t;      // [tiles][27][32] viscosity per integration point, or null
+    const float* pscale_t;   // [tiles][4][32] γP/M_P of the element's pressure DoFs
+    const float* dv[3];
+    const float* dP;
+    float* R[3];             // pre-filled with the base residual; increments added
+    float* RPinc;            // increment of the pressure residual at the DoFs
+    int64_t nels;
+    int dofs_linear;         // the pressure DoFs of element e are 4e … 4e+3 (dofs_t not read)
+    int plastic;
+    float g[3];
+    IncrPhase ph[MAXPH];
+};
+// Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
+// copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.
+// Sets bit INCR_MIXED_PHASES of *flags when some element's nodes or DoFs carry
+// more than one phase (the thread-per-element sweep then does not apply) and
+// INCR_DOFS_GENERAL when the pressure DoFs are not numbered 4e + p.
+enum { INCR_MIXED_PHASES = 1, INCR_DOFS_GENERAL = 2 };
+struct IncrTileSrc {
+    const int32_t* el2n;
+    const int32_t* dofsP;
+    const float* geo_c;
+    const float* eta;
+    const float* gP;
+    const float* MP;
+    const int32_t* phv; int phv_layout;
+    const int32_t* php; int php_layout;
+    int nphases;
+};
+cudaError_t launch_incr_tiles(const IncrTileSrc& src, int64_t nels, const IncrArgs& dst, int32_t* flags,
+                              cudaStream_t st);
+cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st);
+// out = x + y (FP32)
+cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n, cudaStream_t st);
 
 // Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
 template <class T, class TG>

@@ -1,0 +1,535 @@
+// stokes3d_incr.cu — thread-per-element FP32 incremental sweep of the mixed-precision solve.
+//
+// The sweep computes, for every Hex27/P1-disc element, the increments of the
+// pressure residual, of the element-local Pnum and of the visco-elasto-plastic
+// momentum residual between the FP64 base state x_k and x_k + δ
+// (pressure_residual.jl:132-158, momentum_residuals.jl:209-258, rheology.jl:413-472),
+// with the base trial stress and yield value of every integration point read
+// from the tiled FP32 base data written by the FP64 base sweep.
+//
+// Mapping: one thread owns one element. Its 81 velocity increments and its 81
+// residual accumulators live in thread-private shared-memory slots (bank = lane,
+// conflict-free); the quadrature runs plane by plane (ζ): per plane the thread
+// contracts the ζ-direction into 2 × 27 more private slots (W0, W1), per row (η)
+// into 27 registers, evaluates the 3 points of the row with fully unrolled 1-D
+// contractions whose Gauss-rule coefficients are compile-time constants (zero
+// coefficients of the middle point drop out), and accumulates the transposed
+// contraction of the fluxes into 2 × 27 + 9 registers that are expanded into the
+// residual slots once per plane.
+// No shared-memory exchange between threads and no idle lanes: the per-element
+// instruction count is about a third of the warp-cooperative sweep's.
+//
+// Pnum enters the momentum residual only through −Pnum·I in the stress, which is
+// linear in the four element-local Pnum values, so its contribution is added in
+// the scatter from the constant table K[p][d][a] = Σ_q w_q N^P_p(q) ∂_d N_a(q):
+// the element's pressure residual (which Pnum needs) and its momentum residual
+// come out of one pass over the quadrature points.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include "kernels.cuh"
+#include "rheology.cuh"
+
+namespace femb {
+namespace {
+
+constexpr int IN_THREADS = 128;     // 4 warps; two blocks per SM
+constexpr int IN_WARPS = IN_THREADS / 32;
+constexpr int IN_SLOTS = 216;       // thread-private shared words: δv (81), residual (81), plane (54)
+
+// 1-D quadratic Lagrange basis on (−1, 0, 1) at the 3-point Gauss rule ±√(3/5), 0
+// (Hex27: src/elements/shape_functions.jl:404-446, Gauss rule integration_points.jl:321).
+constexpr float GA = 0.774596669241483377f;
+FEMB_HD constexpr float gx(int q) { return q == 0 ? -GA : (q == 1 ? 0.0f : GA); }
+FEMB_HD constexpr float gw(int q) { return q == 1 ? 8.0f / 9.0f : 5.0f / 9.0f; }
+FEMB_HD constexpr float Lb(int q, int i) {
+    return i == 0 ? gx(q) * (gx(q) - 1.0f) * 0.5f : (i == 1 ? 1.0f - gx(q) * gx(q) : gx(q) * (gx(q) + 1.0f) * 0.5f);
+}
+FEMB_HD constexpr float Ld(int q, int i) { return i == 0 ? gx(q) - 0.5f : (i == 1 ? -2.0f * gx(q) : gx(q) + 0.5f); }
+
+// fma with a coefficient that is a compile-time constant after unrolling: zero
+// coefficients (middle Gauss point) fold away
+FEMB_D float cfma(float c, float x, float acc) { return c != 0.0f ? fmaf(c, x, acc) : acc; }
+
+}  // namespace
+
+// K[p][d][a] = Σ_q w_q N^P_p(q) ∂N_a/∂ξ_d(q), a in tensor order.
+__constant__ float c_inc_K[4][3][27];
+
+namespace {
+
+void host_pnum_table(float K[4][3][27]) {
+    const double ga = std::sqrt(3.0 / 5.0);
+    const double x[3] = {-ga, 0.0, ga}, w[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    auto l = [&](int q, int i) { return i == 0 ? x[q] * (x[q] - 1) * 0.5 : (i == 1 ? 1 - x[q] * x[q] : x[q] * (x[q] + 1) * 0.5); };
+    auto dl = [&](int q, int i) { return i == 0 ? x[q] - 0.5 : (i == 1 ? -2 * x[q] : x[q] + 0.5); };
+    for (int p = 0; p < 4; ++p)
+        for (int d = 0; d < 3; ++d)
+            for (int a = 0; a < 27; ++a) {
+                const int ia[3] = {a % 3, (a / 3) % 3, a / 9};
+                double s = 0;
+                for (int q = 0; q < 27; ++q) {
+                    const int iq[3] = {q % 3, (q / 3) % 3, q / 9};
+                    const double np = p == 0 ? 1 - x[iq[0]] - x[iq[1]] - x[iq[2]] : x[iq[p - 1]];
+                    double dn = 1;
+                    for (int r = 0; r < 3; ++r) dn *= r == d ? dl(iq[r], ia[r]) : l(iq[r], ia[r]);
+                    s += w[iq[0]] * w[iq[1]] * w[iq[2]] * np * dn;
+                }
+                K[p][d][a] = (float)s;
+            }
+}
+
+// Phase of an element for the sweep: the common phase of its nodes (or DoFs) in
+// any of the three layouts (src/utils.jl:70-74), 0-based; -1 when they differ.
+__device__ int uniform_phase(const int32_t* ph, int layout, const int32_t* ids, int n, int64_t e) {
+    if (!ph) return 0;
+    if (layout == FEMB200_PHASE_CELL) return ph[e] - 1;
+    int p0 = -2;
+    for (int i = 0; i < n; ++i) {
+        const int p = (layout == FEMB200_PHASE_ELEMENT_NODE ? ph[(int64_t)n * e + i] : ph[ids[(int64_t)n * e + i] - 1]) - 1;
+        if (p0 == -2) p0 = p;
+        else if (p != p0) return -1;
+    }
+    return p0;
+}
+
+__global__ void incr_tiles_kernel(const IncrTileSrc src, int64_t nels, int64_t nslots, IncrArgs dst, int* flags) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nslots) return;
+    const int64_t tile = e >> 5;
+    const int lane = (int)(e & 31);
+    const bool act = e < nels;
+    int32_t* el2n_t = const_cast<int32_t*>(dst.el2n_t);
+    int32_t* dofs_t = const_cast<int32_t*>(dst.dofs_t);
+    float* geo_t = const_cast<float*>(dst.geo_t);
+    float* pscale_t = const_cast<float*>(dst.pscale_t);
+    for (int t = 0; t < 27; ++t) el2n_t[(tile * 27 + t) * 32 + lane] = act ? src.el2n[27 * e + c_tab.tn3[t]] - 1 : 0;
+    bool linear = true;
+    for (int p = 0; p < 4; ++p) {
+        const int32_t d = act ? src.dofsP[4 * e + p] - 1 : 0;
+        linear = linear && (!act || d == 4 * e + p);
+        dofs_t[(tile * 4 + p) * 32 + lane] = d;
+        pscale_t[(tile * 4 + p) * 32 + lane] = act ? src.gP[d] / src.MP[d] : 0.0f;
+    }
+    if (!linear) atomicOr(flags, INCR_DOFS_GENERAL);
+    for (int r = 0; r < 10; ++r) geo_t[(tile * 10 + r) * 32 + lane] = act ? src.geo_c[10 * e + r] : 0.0f;
+    if (src.eta) {
+        float* eta_t = const_cast<float*>(dst.eta_t);
+        for (int q = 0; q < 27; ++q) eta_t[(tile * 27 + q) * 32 + lane] = act ? src.eta[27 * e + q] : 1.0f;
+    }
+    int pv = 0, pp = 0;
+    if (act) {
+        pv = uniform_phase(src.phv, src.phv_layout, src.el2n, 27, e);
+        pp = uniform_phase(src.php, src.php_layout, src.dofsP, 4, e);
+        if (pv < 0 || pp < 0 || pv >= src.nphases || pp >= src.nphases) {
+            atomicOr(flags, INCR_MIXED_PHASES);
+            pv = pp = 0;
+        }
+    }
+    int32_t* phase_t = const_cast<int32_t*>(dst.phase_t);
+    phase_t[e] = pv;
+    phase_t[nslots + e] = pp;
+}
+
+FEMB_D void cp_async4(float* dst, const float* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+FEMB_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+FEMB_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Inputs and output of the FP64 return near the yield-surface apex, passed by value
+// so that the caller's arrays stay in registers on the common (FP32) path.
+struct ApexIn {
+    float tb[6], dtt[6], Fk, Pq, twoe, sphi, inv_den;
+};
+struct ApexOut {
+    float tau[6];
+};
+__device__ __noinline__ ApexOut apex_increment_f64(const ApexIn in) {
+    double tbd[6], dtd[6], outd[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) { tbd[c] = in.tb[c]; dtd[c] = in.dtt[c]; }
+    dp_increment<double>(tbd, (double)in.Fk, dtd, (double)in.Pq, (double)in.twoe, (double)in.sphi, (double)in.inv_den,
+                         eps2<double>(), outd);
+    ApexOut o;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) o.tau[c] = (float)outd[c];
+    return o;
+}
+
+// Base data of one quadrature row (3 points × 7 fields, contiguous in the tiled
+// layout) into registers.
+FEMB_D void load_row(float (&r)[3 * BASE_FIELDS], const float* row) {
+#pragma unroll
+    for (int j = 0; j < 3 * BASE_FIELDS; ++j) r[j] = __ldg(row + j * 32);
+}
+
+// Per-element data of a tile, loaded one tile ahead (during the previous tile's
+// scatter) so that its latency is hidden.
+struct ElemData {
+    float Ji[9];
+    float detJ;
+    float dP[4];
+    int ph, phP;
+};
+
+FEMB_D int elem_dof(const IncrArgs& a, int64_t tile, int lane, int p) {
+    return a.dofs_linear ? (int)(4 * (tile * 32 + lane) + p) : __ldg(a.dofs_t + (tile * 4 + p) * 32 + lane);
+}
+
+FEMB_D void load_elem(const IncrArgs& a, int64_t tile, int lane, int64_t nslots, ElemData& d) {
+    const int64_t e = tile * 32 + lane;
+    const float* gt = a.geo_t + tile * 10 * 32 + lane;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) d.Ji[r] = __ldg(gt + r * 32);
+    d.detJ = __ldg(gt + 9 * 32);   // 0 on padding lanes
+#pragma unroll
+    for (int p = 0; p < 4; ++p) d.dP[p] = __ldg(a.dP + elem_dof(a, tile, lane, p));
+    d.ph = __ldg(a.phase_t + e);
+    d.phP = __ldg(a.phase_t + nslots + e);
+}
+
+__global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArgs a) {
+    extern __shared__ float in_smem[];
+    __shared__ IncrPhase PT[MAXPH];
+    for (int t = threadIdx.x; t < MAXPH; t += blockDim.x) PT[t] = a.ph[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* V = in_smem + (size_t)warp * IN_SLOTS * 32 + lane;   // slot s at V[s * 32]
+    int* Vi = reinterpret_cast<int*>(V);
+    float* RS = V + 81 * 32;
+    float* WS = V + 162 * 32;
+    // the incremental sweep models the FP64 problem: its ε² is FP64's
+    const float EPS2 = (float)eps2<double>();
+    const int64_t ntiles = (a.nels + 31) >> 5;
+    const int64_t nslots = ntiles * 32;
+    const int64_t tstride = (int64_t)gridDim.x * IN_WARPS;
+    const bool plastic = a.plastic != 0;
+    int64_t tile = (int64_t)blockIdx.x * IN_WARPS + warp;
+    if (tile >= ntiles) return;
+
+    // Software pipeline across tiles: the next tile's connectivity (cp.async) and
+    // δv gather (cp.async, indexed by it) run during the last quadrature plane, its
+    // per-element data loads during this tile's scatter, and the base data of the
+    // next quadrature row is loaded into registers while the current row computes.
+    {
+        const int32_t* nd = a.el2n_t + tile * 27 * 32 + lane;
+#pragma unroll 9
+        for (int k = 0; k < 27; ++k) {
+            const int n = __ldg(nd + k * 32);
+            cp_async4(V + (0 * 27 + k) * 32, a.dv[0] + n);
+            cp_async4(V + (1 * 27 + k) * 32, a.dv[1] + n);
+            cp_async4(V + (2 * 27 + k) * 32, a.dv[2] + n);
+        }
+        cp_async_commit();
+    }
+    float pre[3 * BASE_FIELDS];
+    if (plastic) load_row(pre, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane);
+    ElemData cur;
+    load_elem(a, tile, lane, nslots, cur);
+
+    for (; tile < ntiles; tile += tstride) {
+        const int64_t e = tile * 32 + lane;
+        const bool act = e < a.nels;
+        const int64_t tnext = tile + tstride;
+        const bool has_next = tnext < ntiles;
+        const IncrPhase M = PT[cur.ph];
+        // storage term of the continuity residual: the phase of the pressure DoFs
+        const float invbulkdt = PT[cur.phP].invbulkdt;
+        const float* etq = a.eta_t ? a.eta_t + tile * 27 * 32 + lane : nullptr;
+        float rp[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        cp_async_wait_all();
+
+#pragma unroll 1
+        for (int qz = 0; qz < 3; ++qz) {
+            const float bz[3] = {Lb(qz, 0), Lb(qz, 1), Lb(qz, 2)};
+            const float dz[3] = {Ld(qz, 0), Ld(qz, 1), Ld(qz, 2)};
+            const float ze = gx(qz), wz = gw(qz);
+            // ζ-contraction of the plane into the thread's W slots:
+            // W0 = Σ_k L_k(ζ) v_ijk, W1 = Σ_k L'_k(ζ) v_ijk
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int ij = 0; ij < 9; ++ij) {
+                    const float v0 = V[(c * 27 + ij) * 32], v1 = V[(c * 27 + ij + 9) * 32], v2 = V[(c * 27 + ij + 18) * 32];
+                    WS[(c * 9 + ij) * 32] = fmaf(bz[0], v0, fmaf(bz[1], v1, bz[2] * v2));
+                    WS[(27 + c * 9 + ij) * 32] = fmaf(dz[0], v0, fmaf(dz[1], v1, dz[2] * v2));
+                }
+            // the δv slots are free from here on: the next tile's connectivity goes
+            // into the first 27 of them
+            if (qz == 2 && has_next) {
+                const int32_t* nd = a.el2n_t + tnext * 27 * 32 + lane;
+#pragma unroll
+                for (int k = 0; k < 27; ++k) cp_async4(reinterpret_cast<float*>(Vi + k * 32), reinterpret_cast<const float*>(nd + k * 32));
+                cp_async_commit();
+            }
+            // plane accumulators; the body-force term −g_c β carries the same L_k(ζ)
+            // factor as the ξ/η fluxes and is folded into U0
+            float U0[3][9], U1[3][9];
+#pragma unroll
+            for (int ij = 0; ij < 9; ++ij)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { U0[c][ij] = 0.0f; U1[c][ij] = 0.0f; }
+#pragma unroll 1
+            for (int qy = 0; qy < 3; ++qy) {
+                if (qz == 2 && qy == 1 && has_next) {
+                    // the connectivity has landed: gather the next tile's δv (slot k is
+                    // read before the copy that overwrites it is issued)
+                    cp_async_wait_all();
+#pragma unroll 9
+                    for (int k = 0; k < 27; ++k) {
+                        const int n = Vi[k * 32];
+                        cp_async4(V + (2 * 27 + k) * 32, a.dv[2] + n);
+                        cp_async4(V + (1 * 27 + k) * 32, a.dv[1] + n);
+                        cp_async4(V + (0 * 27 + k) * 32, a.dv[0] + n);
+                    }
+                    cp_async_commit();
+                }
+                const float by[3] = {Lb(qy, 0), Lb(qy, 1), Lb(qy, 2)};
+                const float dy[3] = {Ld(qy, 0), Ld(qy, 1), Ld(qy, 2)};
+                const float et = gx(qy), wyz = gw(qy) * wz;
+                // base data of the next row (rows in (qz, qy) order, then the next tile's
+                // first row): each point's 7 registers are refilled as soon as the
+                // point has read them
+                const int rnext = 3 * qz + qy + 1;
+                const float* next_row = rnext < 9 ? a.base_t + (tile * 27 + 3 * rnext) * BASE_FIELDS * 32 + lane
+                                                  : (has_next ? a.base_t + tnext * 27 * BASE_FIELDS * 32 + lane : nullptr);
+                // η-contraction of the row: X = Σ_j L_j(η) W0, Y = Σ_j L'_j(η) W0, Z = Σ_j L_j(η) W1
+                float X[3][3], Y[3][3], Z[3][3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        float x = 0.0f, y = 0.0f, z = 0.0f;
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            const float w0 = WS[(c * 9 + i + 3 * j) * 32], w1 = WS[(27 + c * 9 + i + 3 * j) * 32];
+                            x = fmaf(by[j], w0, x);
+                            y = fmaf(dy[j], w0, y);
+                            z = fmaf(by[j], w1, z);
+                        }
+                        X[c][i] = x; Y[c][i] = y; Z[c][i] = z;
+                    }
+                // the row's fluxes, contracted over ξ: A = Σ_qx L'_i F_ξ, B = Σ_qx L_i F_η,
+                // C = Σ_qx L_i F_ζ, Ab = Σ_qx L_i β
+                float A[3][3], Bf[3][3], Cf[3][3], Ab[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    Ab[i] = 0.0f;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) { A[c][i] = 0.0f; Bf[c][i] = 0.0f; Cf[c][i] = 0.0f; }
+                }
+#pragma unroll
+                for (int qx = 0; qx < 3; ++qx) {
+                    const int q = qx + 3 * qy + 9 * qz;
+                    // reference gradient gr[c][d] = ∂δv_c/∂ξ_d at the point
+                    float gr[3][3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            s0 = cfma(Ld(qx, i), X[c][i], s0);
+                            s1 = cfma(Lb(qx, i), Y[c][i], s1);
+                            s2 = cfma(Lb(qx, i), Z[c][i], s2);
+                        }
+                        gr[c][0] = s0; gr[c][1] = s1; gr[c][2] = s2;
+                    }
+                    // physical gradient ∂δv_c/∂x_k = Σ_d gr[c][d] ∂ξ_d/∂x_k
+                    float gq[3][3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            gq[c][k] = fmaf(gr[c][0], cur.Ji[3 * k], fmaf(gr[c][1], cur.Ji[1 + 3 * k], gr[c][2] * cur.Ji[2 + 3 * k]));
+                    const float div = gq[0][0] + gq[1][1] + gq[2][2];
+                    const float xi = gx(qx);
+                    const float NP0 = 1.0f - xi - et - ze;
+                    const float dO = cur.detJ * gw(qx) * wyz;
+                    const float Pq = fmaf(NP0, cur.dP[0], cfma(xi, cur.dP[1], fmaf(et, cur.dP[2], ze * cur.dP[3])));
+                    // continuity: −∇·δv − δP/(bulk·Δt) (pressure_residual.jl:132-158)
+                    const float f = (-div - Pq * invbulkdt) * dO;
+                    rp[0] = fmaf(NP0, f, rp[0]);
+                    rp[1] = cfma(xi, f, rp[1]);
+                    rp[2] = fmaf(et, f, rp[2]);
+                    rp[3] = fmaf(ze, f, rp[3]);
+                    // deviatoric strain-rate increment and the stress increment
+                    const float tr = div * (1.0f / 3.0f);
+                    const float ed[6] = {gq[0][0] - tr, gq[1][1] - tr, gq[2][2] - tr, 0.5f * (gq[0][1] + gq[1][0]),
+                                         0.5f * (gq[0][2] + gq[2][0]), 0.5f * (gq[1][2] + gq[2][1])};
+                    float twoe = M.twoe, inv_den = M.inv_den;
+                    if (etq) {
+                        const float eq = act ? __ldg(etq + q * 32) : 1.0f;
+                        const float etave = 1.0f / (1.0f / eq + M.invG_dt);
+                        twoe = 2.0f * etave;
+                        inv_den = 1.0f / (etave + M.den_rest);
+                    }
+                    float dtt[6], tau[6];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) dtt[c] = twoe * ed[c];
+                    if (plastic) {
+                        float tb[6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) tb[c] = pre[qx * BASE_FIELDS + c];
+                        const float Fk = pre[qx * BASE_FIELDS + 6];
+                        if (next_row) {
+#pragma unroll
+                            for (int c = 0; c < BASE_FIELDS; ++c)
+                                pre[qx * BASE_FIELDS + c] = __ldg(next_row + (qx * BASE_FIELDS + c) * 32);
+                        }
+                        const float Jk = 0.5f * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] +
+                                         tb[4] * tb[4] + tb[5] * tb[5];
+                        if (Jk < 1e-6f * M.cC * M.cC) {
+                            // within 1e-3·C·cosϕ of the yield-surface apex the return direction
+                            // is ill-conditioned: this point's increment is formed in FP64 (out of
+                            // line, so that the rare branch does not raise the register count)
+                            ApexIn in;
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) { in.tb[c] = tb[c]; in.dtt[c] = dtt[c]; }
+                            in.Fk = Fk; in.Pq = Pq; in.twoe = twoe; in.sphi = M.sphi; in.inv_den = inv_den;
+                            const ApexOut o = apex_increment_f64(in);
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) tau[c] = o.tau[c];
+                        } else {
+                            dp_increment<float, true>(tb, Fk, dtt, Pq, twoe, M.sphi, inv_den, EPS2, tau);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
+                    }
+                    // reference-frame fluxes F[c][d] = dΩ Σ_k ∂ξ_d/∂x_k σ_kc, σ = δτ − δP·I
+                    const float sg[3][3] = {{tau[0] - Pq, tau[3], tau[4]}, {tau[3], tau[1] - Pq, tau[5]}, {tau[4], tau[5], tau[2] - Pq}};
+                    // EOS density increment ρ0·δP/K (momentum_residuals.jl:11-16)
+                    const float bq = M.rho0beta * Pq * dO;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        float F[3];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                            F[d] = dO * fmaf(cur.Ji[d], sg[0][c], fmaf(cur.Ji[d + 3], sg[1][c], cur.Ji[d + 6] * sg[2][c]));
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            A[c][i] = cfma(Ld(qx, i), F[0], A[c][i]);
+                            Bf[c][i] = cfma(Lb(qx, i), F[1], Bf[c][i]);
+                            Cf[c][i] = cfma(Lb(qx, i), F[2], Cf[c][i]);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) Ab[i] = cfma(Lb(qx, i), bq, Ab[i]);
+                }
+                // contract the row over η: U0 += L_j(η) (A − g_c Ab) + L'_j(η) B, U1 += L_j(η) C
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const float ag = fmaf(-a.g[c], Ab[i], A[c][i]);
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            U0[c][i + 3 * j] = fmaf(by[j], ag, fmaf(dy[j], Bf[c][i], U0[c][i + 3 * j]));
+                            U1[c][i + 3 * j] = fmaf(by[j], Cf[c][i], U1[c][i + 3 * j]);
+                        }
+                    }
+            }
+            // expand the plane: R_c(ijk) += L_k(ζ) U0 + L'_k(ζ) U1
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int ij = 0; ij < 9; ++ij) {
+                        const float r = fmaf(bz[k], U0[c][ij], dz[k] * U1[c][ij]);
+                        float* slot = RS + (c * 27 + ij + 9 * k) * 32;
+                        *slot = qz == 0 ? r : *slot + r;
+                    }
+        }
+        // ---- pressure residual and Pnum increments (element-local) ----
+        float Pn[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            Pn[p] = __ldg(a.pscale_t + (tile * 4 + p) * 32 + lane) * rp[p];
+            if (act) a.RPinc[elem_dof(a, tile, lane, p)] = rp[p];
+        }
+        const float Ji[9] = {cur.Ji[0], cur.Ji[1], cur.Ji[2], cur.Ji[3], cur.Ji[4], cur.Ji[5], cur.Ji[6], cur.Ji[7], cur.Ji[8]};
+        const float detJ = cur.detJ;
+        // the next tile's element data, in flight during the scatter
+        if (has_next) load_elem(a, tnext, lane, nslots, cur);
+        // ---- scatter, with the Pnum term −|det J| Σ_d ∂ξ_d/∂x_c Σ_p Pn_p K[p][d][a] ----
+        const int32_t* nd = a.el2n_t + tile * 27 * 32 + lane;
+#pragma unroll 3
+        for (int t = 0; t < 27; ++t) {
+            float S[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                S[d] = fmaf(Pn[0], c_inc_K[0][d][t], fmaf(Pn[1], c_inc_K[1][d][t], fmaf(Pn[2], c_inc_K[2][d][t], Pn[3] * c_inc_K[3][d][t])));
+            const int n = __ldg(nd + t * 32);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float val = RS[(c * 27 + t) * 32] - detJ * fmaf(Ji[3 * c], S[0], fmaf(Ji[3 * c + 1], S[1], Ji[3 * c + 2] * S[2]));
+                if (act) atomicAdd(a.R[c] + n, val);
+            }
+        }
+    }
+    cp_async_wait_all();
+}
+
+std::mutex g_inc_mutex;
+bool g_inc_ready[64] = {};
+
+}  // namespace
+
+cudaError_t launch_incr_tiles(const IncrTileSrc& src, int64_t nels, const IncrArgs& dst, int32_t* flags,
+                              cudaStream_t st) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    {
+        // the Pnum table and the kernel's shared-memory limit, once per device
+        std::lock_guard<std::mutex> lk(g_inc_mutex);
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        if (!g_inc_ready[dev]) {
+            static float K[4][3][27];
+            host_pnum_table(K);
+            err = cudaMemcpyToSymbol(c_inc_K, K, sizeof(K));
+            if (err != cudaSuccess) return err;
+            err = cudaFuncSetAttribute(hex27_incr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
+            if (err != cudaSuccess) return err;
+            g_inc_ready[dev] = true;
+        }
+    }
+    const int64_t nslots = (nels + 31) / 32 * 32;
+    count_launch();
+    incr_tiles_kernel<<<(unsigned)((nslots + 255) / 256), 256, 0, st>>>(src, nels, nslots, dst, flags);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void add_f32_kernel(float* out, const float* x, const float* y, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = x[i] + y[i];
+}
+}  // namespace
+
+cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n, cudaStream_t st) {
+    count_launch();
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 8);
+    add_f32_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(out, x, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
+    const size_t smem = (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float);
+    const int64_t ntiles = (a.nels + 31) / 32;
+    int per_sm = 2;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel, IN_THREADS, smem);
+    if (per_sm < 1) per_sm = 1;
+    int64_t blocks = (ntiles + IN_WARPS - 1) / IN_WARPS;
+    blocks = std::min<int64_t>(blocks, (int64_t)num_sms * per_sm);
+    if (blocks < 1) blocks = 1;
+    count_launch();
+    hex27_incr_kernel<<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace femb

@@ -17,6 +17,7 @@
 //     the host (ηve, 2ηve, C·cosϕ, the reciprocal plastic denominator).
 #include "kernels.cuh"
 #include "hex27.cuh"
+#include "rheology.cuh"
 
 namespace femb {
 
@@ -89,7 +90,7 @@ FEMB_D void issue_prefetch(const H27Args<T, T>& a, const T* geo_c, const GroupId
 #pragma unroll
             for (int qz = 0; qz < 3; ++qz) {
                 const int q = tidx(m1, m2, qz);
-                cp_async(B + c * 27 + q, a.base_in[c] + e * 27 + q);
+                cp_async(B + c * 27 + q, a.base_in + base_index(e, q, c));
             }
     } else if (a.told[0]) {
 #pragma unroll
@@ -114,38 +115,6 @@ FEMB_D void issue_prefetch(const H27Args<T, T>& a, const T* geo_c, const GroupId
         if (a.Q) cp_async(D + 6 * 4 + m, a.Q + id.dof);
         if (a.Pf) cp_async(D + 7 * 4 + m, a.Pf + id.dof);
     }
-}
-
-// Stress increment of the Drucker–Prager radial return (rheology.jl:441-472)
-// between the base trial stress tb (yield value Fk) and the trial stress tb + dtt,
-// with pressure increment dPeq. Written in increments (J2 difference through the
-// cross term, f' − f through δλ and δτII), so that no two nearly equal stresses
-// are subtracted and the FP32 error scales with the increment, not the stress.
-// The return is τ = τtr − f·M·τtr with M = ½ on the normal and 1 on the shear
-// components and f = 2ηve·λ/(τII + ε²), λ = F/den.
-template <class U>
-FEMB_D void dp_increment(const U tb[6], U Fk, const U dtt[6], U dPeq, U twoe, U sphi, U inv_den, U eps2, U out[6]) {
-    const U Jk = U(0.5) * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] + tb[4] * tb[4] + tb[5] * tb[5];
-    const U cross = tb[0] * dtt[0] + tb[1] * dtt[1] + tb[2] * dtt[2] + U(2) * (tb[3] * dtt[3] + tb[4] * dtt[4] + tb[5] * dtt[5]);
-    const U dd = U(0.5) * (dtt[0] * dtt[0] + dtt[1] * dtt[1] + dtt[2] * dtt[2]) + dtt[3] * dtt[3] + dtt[4] * dtt[4] + dtt[5] * dtt[5];
-    const U tIIk = sqrt(Jk + eps2);
-    const U tIIn = sqrt(Jk + eps2 + (cross + dd));
-    const U dtII = (cross + dd) / (tIIn + tIIk);
-    const U dF = dtII - sphi * dPeq;
-    const U Fn = Fk + dF;
-    const bool pk = Fk > U(0), pn = Fn > U(0);
-    const U lamk = pk ? Fk * inv_den : U(0);
-    U fn = U(0), df = U(0);
-    if (pn) {
-        fn = twoe * (Fn * inv_den) / (tIIn + eps2);
-        df = pk ? twoe * (dF * inv_den * (tIIk + eps2) - lamk * dtII) / ((tIIn + eps2) * (tIIk + eps2)) : fn;
-    } else if (pk) {
-        df = -(twoe * lamk / (tIIk + eps2));
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) out[c] = dtt[c] - U(0.5) * (fn * dtt[c] + df * tb[c]);
-#pragma unroll
-    for (int c = 3; c < 6; ++c) out[c] = dtt[c] - (fn * dtt[c] + df * tb[c]);
 }
 
 }  // namespace
@@ -437,15 +406,15 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
                     told[c] = a.told[0] ? B[c * 27 + q] : T(0);
                     tau[c] = twoe * eps_[c] + twoe_el * told[c];
                 }
-                if (act && a.base_out[0]) {
+                if (act && a.base_out) {
 #pragma unroll
-                    for (int c = 0; c < 6; ++c) a.base_out[c][ec * 27 + q] = (float)tau[c];
+                    for (int c = 0; c < 6; ++c) a.base_out[base_index(ec, q, c)] = (float)tau[c];
                 }
                 if (plastic) {
                     const T tII = sqrt(T(0.5) * (tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) + tau[3] * tau[3] +
                                        tau[4] * tau[4] + tau[5] * tau[5] + EPS2);
                     const T Fy = tII - cC - sphi * Peq;
-                    if (act && a.base_out[6]) a.base_out[6][ec * 27 + q] = (float)Fy;
+                    if (act && a.base_out) a.base_out[base_index(ec, q, 6)] = (float)Fy;
                     if (Fy > T(0)) {
                         const T lam = Fy * inv_den;
                         const T f = twoe * lam / (tII + EPS2);

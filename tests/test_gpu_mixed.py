@@ -75,3 +75,29 @@ def test_mixed_rejects_unsupported_meshes():
     dr2 = case2.device_state(fem)
     with pytest.raises(abi.FemB200Error, match="3-D"):
         fem.solve(dr2, case2.bc_device(), dt=case2.dt, precision="mixed")
+
+
+@pytest.mark.parametrize("layout", ["element_node", "nodal"])
+def test_mixed_solve_phase_layouts(layout):
+    # Element-node phases that repeat the cell phase keep every element in one phase
+    # (the thread-per-element incremental sweep); nodal phases put the nodes of the
+    # layer interfaces in one phase or the other, so interface elements mix phases
+    # (the warp-cooperative sweep). Both must agree with the FP64 solve.
+    case = vep_layers_case(n=3, seed=6)
+    cell = case.phases_v
+    if layout == "element_node":
+        case.phases_v = np.repeat(cell[:, None], case.mesh.nv, axis=1).astype(np.int32)
+        case.phases_v_layout = abi.PHASE_ELEMENT_NODE
+        case.phases_P = np.repeat(cell[:, None], case.mesh.np_, axis=1).astype(np.int32)
+        case.phases_P_layout = abi.PHASE_ELEMENT_NODE
+    else:
+        nodal = np.ones(case.mesh.nnodes, dtype=np.int32)
+        nodal[case.mesh.el2n.reshape(-1) - 1] = np.repeat(cell, case.mesh.nv)
+        case.phases_v, case.phases_v_layout = nodal, abi.PHASE_NODAL
+        case.phases_P = np.repeat(cell, case.mesh.np_).astype(np.int32)
+        case.phases_P_layout = abi.PHASE_NODAL
+    st64, f64 = solve_fields(case, 1e-8, "fp64")
+    stm, fm = solve_fields(case, 1e-8, "mixed")
+    assert st64["converged"] and stm["converged"] and stm["err"] < 1e-8
+    for k in ("v", "P", "tau"):
+        assert rel_l2(fm[k], f64[k]) < 1e-6, (layout, k, rel_l2(fm[k], f64[k]))
