@@ -22,4 +22,5 @@ from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, so
                      solve_thermal, assemble_pressure_residual, assemble_momentum_residual,
                      assemble_stokes_residuals, assemble_augmented_momentum_jacobian,
                      assemble_viscosity_weighted_pressure_scaling, update_stokes_current_stress,
-                     assemble_shear_heating, assemble_thermal_residual, assemble_diffusion_matrices_colored)
+                     assemble_shear_heating, assemble_thermal_residual, assemble_diffusion_matrices_colored,
+                     assemble_adjoint_residual, viscosity_sensitivity, solve_adjoint)

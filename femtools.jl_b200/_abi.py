@@ -135,6 +135,12 @@ SIGNATURES = {
     "femb200_pressure_scaling": (C.c_int, [_vp, _P(StokesProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_store_stress": (C.c_int, [_vp, _P(StokesProblemC), C.c_double]),
     "femb200_solve_stokes": (C.c_int, [_vp, _P(StokesProblemC), _P(StokesControlsC), _P(StokesStatsC)]),
+    "femb200_stokes_adjoint_residual": (C.c_int, [_vp, _P(StokesProblemC), C.c_double, C.c_int32, C.c_int32,
+                                                  _vp * 3, _vp, _vp * 3, _vp]),
+    "femb200_stokes_viscosity_sensitivity": (C.c_int, [_vp, _P(StokesProblemC), C.c_double, C.c_int32, C.c_int32,
+                                                       _vp * 3, _vp, _vp]),
+    "femb200_solve_stokes_adjoint": (C.c_int, [_vp, _P(StokesProblemC), _P(StokesControlsC), _vp * 3, _vp * 3, _vp,
+                                               _P(StokesStatsC)]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

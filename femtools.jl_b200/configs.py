@@ -191,3 +191,76 @@ def random_state_case(dim=3, n=3, seed=0, phases="nodal", plastic=True, nphases=
                       Pnum=rng.standard_normal(mesh.nnodesP) * 0.1,
                       bc=[(mesh.boundary_nodes, np.zeros(len(mesh.boundary_nodes)))] * dim)
     return case
+
+
+@dataclass
+class AdjointCase:
+    """Stokes part of the adjoint workload: a forward StokesCase with the viscosity
+    given per integration point as η_q = exp(−0.1·T_q)·exp(δ_e) (δ_e one log-viscosity
+    per element), an objective J = Σ_top |v − v_target|² over the top-surface nodes,
+    and the temperature frozen on the pressure DoFs."""
+    case: StokesCase
+    T_ip: np.ndarray        # temperature at the integration points (nq × nels)
+    delta: np.ndarray       # per-element log-viscosity perturbation
+    top: np.ndarray         # 1-based top-surface nodes
+    v_target: list          # target velocity per component on all nodes (zero off the top)
+
+    def eta_ip(self, delta=None):
+        d = self.delta if delta is None else delta
+        nq = self.case.mesh.nq
+        return np.exp(-0.1 * self.T_ip) * np.repeat(np.exp(d), nq)
+
+    def objective(self, v):
+        """J and ∂J/∂v (numpy or torch velocity components)."""
+        top = self.top - 1
+        J = 0.0
+        grad = []
+        for c in range(3):
+            x = v[c].detach().double().cpu().numpy() if hasattr(v[c], "detach") else np.asarray(v[c])
+            diff = np.zeros_like(x)
+            diff[top] = x[top] - self.v_target[c][top]
+            J += float(np.sum(diff[top] ** 2))
+            grad.append(2.0 * diff)
+        return J, grad
+
+
+def adjoint_case(n=4, seed=0, eta_b=10.0, alpha=0.1):
+    """3-D Hex27/P1-disc viscous Stokes on the unit cube for the adjoint gradient:
+    temperature linear from 1 at the bottom to 0 at the top plus N(0, 0.01²) noise on
+    the pressure DoFs (frozen), ρ = ρ0(1 − α(T − 0)), g = (0, 0, −1), viscosity
+    η = exp(−0.1·T)·exp(δ_e) with δ_e ~ N(0, 0.1²) per element; free slip on the
+    sides and the bottom, a free top surface; J = Σ_top |v − v_target|² with a seeded
+    target. Fixed here (the configuration leaves them open): ηb = 10, α = 0.1, Δt = 1."""
+    rng = np.random.default_rng(seed)
+    mesh = fem.structured_mixed_mesh(3, (n, n, n))
+    nels, nq = mesh.nels, mesh.nq
+    zc = fem.mesh.cell_centroids(mesh)[:, 2]
+    h = 1.0 / n
+    # P1-disc DoFs of T = 1 − z: the centre value and the centre plus one half-cell slope
+    Tdof = np.zeros((nels, 4))
+    Tc = 1.0 - zc
+    Tdof[:, 0] = Tc
+    Tdof[:, 1] = Tc
+    Tdof[:, 2] = Tc
+    Tdof[:, 3] = Tc - 0.5 * h
+    Tdof += rng.normal(0.0, 0.01, size=Tdof.shape)
+    T = np.zeros(mesh.nnodesP)
+    T[mesh.dofsP.reshape(-1) - 1] = Tdof.reshape(-1)
+    tabs = fem.element_tables(3)
+    T_ip = (Tdof @ tabs.NP.T).reshape(-1)          # nels × nq, element-major
+    delta = rng.normal(0.0, 0.1, size=nels)
+    mat = fem.StokesMaterial(eta=(1.0,), eta_b=(eta_b,), G=(math.inf,), alpha=(alpha,), rho0=(1.0,), K=(math.inf,),
+                             g=(0.0, 0.0, -1.0), Tref=0.0)
+    bx = fem.mesh.wall_nodes(mesh, 0)
+    by = fem.mesh.wall_nodes(mesh, 1)
+    bz = fem.mesh.wall_nodes(mesh, 2, hi=-1.0)   # bottom only
+    bc = [(bx, np.zeros(len(bx))), (by, np.zeros(len(by))), (bz, np.zeros(len(bz)))]
+    z = mesh.coords[:, 2]
+    top = (np.nonzero(np.abs(z - 1.0) < 1e-12)[0] + 1).astype(np.int32)
+    v_target = [np.zeros(mesh.nnodes) for _ in range(3)]
+    for c in range(3):
+        v_target[c][top - 1] = rng.normal(0.0, 0.01, size=len(top))
+    case = StokesCase(mesh, mat, None, 1.0, v=[np.zeros(mesh.nnodes) for _ in range(3)], P=np.zeros(mesh.nnodesP),
+                      P0=np.zeros(mesh.nnodesP), T=T, T0=T.copy(), tau_old=[np.zeros(nq * nels) for _ in range(6)],
+                      bc=bc)
+    return AdjointCase(case, T_ip, delta, top, v_target)

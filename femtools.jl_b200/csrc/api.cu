@@ -56,6 +56,8 @@ struct femb200_handle {
     int* h_flag = nullptr;
     bool geo_c_valid = false;
     int use_pipe = 1;   // the pipelined sweep on affine meshes (0 forces the general sweep)
+    void* adj_mem = nullptr;   // adjoint workspace: λrate, Resλv, Resλv0, ResλP
+    size_t adj_cap = 0;
     int use_incr_thread = 1;   // the thread-per-element incremental sweep where it applies (0: warp-cooperative)
     // FP32 arrays of the mixed-precision solve, carved from one allocation
     struct Mixed {
@@ -1219,6 +1221,191 @@ template <class T, class TG> struct DoSolve {
     }
 };
 
+// ---- adjoint ------------------------------------------------------------------
+
+int check_adjoint_problem(femb200_handle* h, const femb200_stokes_problem* p) {
+    RC(check_problem(h, p));
+    if (p->dim != 3) { h->err = "the adjoint is implemented for 3-D Hex27/P1-disc meshes"; return FEMB200_EUNSUPPORTED; }
+    if (p->dtype != FEMB200_F64 || p->geo_dtype != FEMB200_F64) { h->err = "the adjoint runs in FP64"; return FEMB200_EUNSUPPORTED; }
+    if (p->tau_old_layout == FEMB200_FIELD_NODAL) { h->err = "the adjoint takes τ_old at integration points"; return FEMB200_EUNSUPPORTED; }
+    if (p->P_old && p->P_old_layout == FEMB200_FIELD_IP) {
+        // P_old enters only the storage term's constant part; its layout does not matter
+    }
+    return FEMB200_OK;
+}
+
+AdjArgs<double> adjoint_args(const femb200_stokes_problem* p, double dt, int with_pnum, const void* const lam_v[3],
+                             const void* lam_P) {
+    AdjArgs<double> a;
+    std::memset(&a, 0, sizeof(a));
+    a.el2n = p->el2n; a.dofsP = p->dofsP;
+    a.geo_v = static_cast<const double*>(p->geo_v); a.geo_P = static_cast<const double*>(p->geo_P);
+    for (int c = 0; c < 3; ++c) { a.v[c] = static_cast<const double*>(p->v[c]); a.lam_v[c] = static_cast<const double*>(lam_v[c]); }
+    a.P = static_cast<const double*>(p->P);
+    a.Pf = static_cast<const double*>(p->Pf);
+    a.gammaP = static_cast<const double*>(p->gammaP);
+    a.MP = static_cast<const double*>(p->M_P);
+    a.phv = p->phases_v; a.phv_layout = p->phases_v_layout;
+    a.php = p->phases_P; a.php_layout = p->phases_P_layout;
+    for (int c = 0; c < 6; ++c)
+        a.told[c] = p->tau_old_layout == FEMB200_FIELD_IP ? static_cast<const double*>(p->tau_old[c]) : nullptr;
+    a.eta_ip = static_cast<const double*>(p->viscosity_ip);
+    a.lam_P = static_cast<const double*>(lam_P);
+    a.nels = p->nels;
+    a.dt = dt;
+    a.with_pnum = with_pnum && p->gammaP && p->M_P;
+    return a;
+}
+
+// Adjoint PH/DYREL solve with the frozen operator (_solve_stokes_adjoint_dyrel!,
+// src/stokes/solvers/DR_adjoint.jl:3-325): the velocity adjoint advances by the
+// Chebyshev-accelerated damped iteration, the pressure adjoint by the
+// Arrow–Hurwicz update λP += γP·ResλP/M_P, with the Gershgorin λmax of the
+// augmented Jacobian diagnostics (the :matrix_free/:enzyme paths' λmax, :94-116).
+struct AdjWork {
+    void* mem = nullptr;
+    size_t cap = 0;
+};
+
+int solve_adjoint_impl(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
+                       const void* const objective_v[3], void* const lam_v[3], void* lam_P, femb200_stokes_stats* st) {
+    using T = double;
+    const int64_t nn = p->nnodes, nP = p->nnodesP;
+    const double dt = c->dt;
+    const int64_t ncheck = c->check_interval > 0 ? c->check_interval : 50;
+    const double cfl = c->cfl_v > 0 ? c->cfl_v : 0.98, cf = c->c_fact > 0 ? c->c_fact : 0.9;
+    const double tol = c->tolerance > 0 ? c->tolerance : 1e-6;
+    const double rel_drop = c->rel_drop0 > 0 ? c->rel_drop0 : 0.1;
+    const int64_t iter_max = c->iter_max > 0 ? c->iter_max : 50000;
+    const int64_t total_max = c->max_iterations > 0 ? c->max_iterations : 50000;
+    const int64_t max_ph = c->max_ph_iterations > 0 ? c->max_ph_iterations : 100;
+    static const char* labels[3] = {"adjoint vx", "adjoint vy", "adjoint vz"};
+    std::memset(st, 0, sizeof(*st));
+    if (!p->dRdv[0] || !p->PC[0] || !p->gammaP || !p->M_P) { h->err = "dRdv, PC, γP and M_P are required"; return FEMB200_EINVAL; }
+    cudaStream_t s = h->stream;
+    RC(upload_material(h, p->mat, c->finite_K, dt));
+    RC(build_mask(h, p));
+    // workspace: λrate, Resλv, Resλv0 (3 each) and ResλP
+    const size_t need = (9 * (size_t)nn + (size_t)nP) * sizeof(T);
+    if (need > h->adj_cap) {
+        if (h->adj_mem) cudaFree(h->adj_mem);
+        h->adj_mem = nullptr; h->adj_cap = 0;
+        CK(cudaMalloc(&h->adj_mem, need));
+        h->adj_cap = need;
+    }
+    T* w = static_cast<T*>(h->adj_mem);
+    T *rate[3], *Res[3], *Res0[3];
+    for (int k = 0; k < 3; ++k) { rate[k] = w + k * nn; Res[k] = w + (3 + k) * nn; Res0[k] = w + (6 + k) * nn; }
+    T* ResP = w + 9 * nn;
+    for (int k = 0; k < 3; ++k) CK(cudaMemsetAsync(rate[k], 0, sizeof(T) * nn, s));
+    // λ on the constrained velocity DoFs is zero
+    for (int k = 0; k < 3; ++k)
+        if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(static_cast<T*>(lam_v[k]), p->bc_dofs[k], nullptr, p->bc_n[k], s));
+
+    // Jacobi diagonal and Gershgorin row sums of the augmented Jacobian at the forward state
+    RC((jacobian_sweep<T, T>(h, p, dt)));
+    double lmax[3];
+    for (int k = 0; k < 3; ++k) RC(checked_lmax<T>(h, static_cast<const T*>(p->dRdv[k]), static_cast<const T*>(p->PC[k]), nn, labels[k], lmax[k]));
+    double dtau[3], alpha[3], beta[3];
+    for (int k = 0; k < 3; ++k) { dtau[k] = 2 / std::sqrt(lmax[k]) * cfl; cheb(dtau[k], 0.0, cf, alpha[k], beta[k]); }
+
+    const void* lv[3] = {lam_v[0], lam_v[1], lam_v[2]};
+    AdjArgs<T> a = adjoint_args(p, dt, 1, lv, lam_P);
+    for (int k = 0; k < 3; ++k) a.out_dv[k] = Res[k];
+    a.out_dP = ResP;
+    auto assemble = [&]() -> int {
+        for (int k = 0; k < 3; ++k) CK(launch_copy<T>(Res[k], static_cast<const T*>(objective_v[k]), nn, s));
+        RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
+        CK(launch_hex27_adjoint<T>(a, h->num_sms, s));
+        RC(prof_end(h, FEMB200_PROF_RESIDUAL));
+        for (int k = 0; k < 3; ++k)
+            if (p->bc_n[k] > 0) CK(launch_dirichlet<T>(Res[k], p->bc_dofs[k], nullptr, p->bc_n[k], s));
+        return FEMB200_OK;
+    };
+    const double sq_nn = std::sqrt((double)nn), sq_nP = std::sqrt((double)nP);
+    auto velocity_error = [&](double& ev) -> int {
+        ev = 0;
+        for (int k = 0; k < 3; ++k) {
+            double sv;
+            RC(sumsq<T>(h, Res[k], (const T*)nullptr, nn, sv));
+            ev = std::max(ev, std::sqrt(sv));
+        }
+        ev /= sq_nn;
+        return FEMB200_OK;
+    };
+    auto pressure_error = [&](double& ep) -> int {
+        double sp;
+        RC(sumsq<T>(h, ResP, (const T*)nullptr, nP, sp));
+        ep = std::sqrt(sp) / sq_nP;
+        return FEMB200_OK;
+    };
+    const int nb = red_blocks(h, nn);
+    RC(ensure_partials(h, nb));
+
+    int64_t iter = 0, itPH_done = 0;
+    double err = INFINITY, err_v0 = 1.0, err_P0 = 1.0, err_v = INFINITY, err_P = INFINITY;
+    bool converged = false;
+    for (int64_t itPH = 1; itPH <= max_ph; ++itPH) {
+        itPH_done = itPH;
+        RC(assemble());
+        RC(velocity_error(err_v));
+        RC(pressure_error(err_P));
+        if (itPH == 1) { err_v0 = err_v + julia_eps(err_v); err_P0 = err_P + julia_eps(err_P); }
+        err = std::max(std::min(err_v, err_v / err_v0), std::min(err_P, err_P / err_P0));
+        if (std::isnan(err)) { h->err = "NaN detected in the adjoint solve"; return FEMB200_ENAN; }
+        if (err < tol) { converged = true; break; }
+        const double target_v = std::max(err_v * rel_drop, tol);
+        int64_t inner = 0;
+        while (err_v > target_v && inner < iter_max && iter < total_max) {
+            ++inner; ++iter;
+            NodeArgs<T> na;
+            std::memset(&na, 0, sizeof(na));
+            for (int k = 0; k < 3; ++k) {
+                na.v[k] = static_cast<T*>(lam_v[k]); na.rate[k] = rate[k]; na.Rv[k] = Res[k]; na.Rv0[k] = Res0[k];
+                na.PC[k] = static_cast<const T*>(p->PC[k]);
+                na.alpha[k] = -alpha[k]; na.beta[k] = beta[k];
+            }
+            na.mask = h->d_mask; na.n = nn; na.dim = 3;
+            na.save_R0 = 1;
+            RC(prof_begin(h, FEMB200_PROF_NODE));
+            CK(launch_node_update<T>(na, nb, s));
+            RC(prof_end(h, FEMB200_PROF_NODE));
+            RC(assemble());
+            if (iter % ncheck == 0) {
+                RC(velocity_error(err_v));
+                if (std::isnan(err_v)) { h->err = "NaN detected in the adjoint solve"; return FEMB200_ENAN; }
+                // λmin from the change of the residual over the last step (_stokes_λmin, DR.jl:32-37)
+                for (int k = 0; k < 3; ++k) {
+                    CK(launch_lmin_sums<T>(rate[k], Res[k], Res0[k], static_cast<const T*>(p->PC[k]), nn, alpha[k],
+                                           h->d_partials, nb, s));
+                    double r[3];
+                    RC(fetch_sums(h, nb, 3, r));
+                    const double lmin = r[0] == 0 ? 0.0 : std::fabs(r[1]) / r[0];
+                    cheb(dtau[k], lmin, cf, alpha[k], beta[k]);
+                }
+            }
+        }
+        // Arrow–Hurwicz update of the pressure adjoint (DR_adjoint.jl:296)
+        CK(launch_pressure_update<T>(static_cast<T*>(lam_P), static_cast<const T*>(p->gammaP), ResP,
+                                     static_cast<const T*>(p->M_P), nP, s));
+        if (iter >= total_max) break;
+    }
+    if (!converged) {
+        RC(assemble());
+        RC(velocity_error(err_v));
+        RC(pressure_error(err_P));
+        err = std::max(std::min(err_v, err_v / err_v0), std::min(err_P, err_P / err_P0));
+    }
+    CK(cudaStreamSynchronize(s));
+    st->itPH = itPH_done; st->iter = iter; st->err = err; st->err_v = err_v; st->err_P = err_P;
+    st->converged = converged || err < tol;
+    st->reached_total_iter = iter >= total_max;
+    st->lambda_max = *std::max_element(lmax, lmax + 3);
+    st->lambda_max_gershgorin = st->lambda_max;
+    st->jacobian_assemblies = 1;
+    return FEMB200_OK;
+}
+
 int check_controls(femb200_handle* h, const femb200_stokes_controls* c) {
     if (!c) { h->err = "null controls"; return FEMB200_EINVAL; }
     if (!(c->dt > 0)) { h->err = "dt must be positive"; return FEMB200_EINVAL; }
@@ -1286,6 +1473,7 @@ int femb200_destroy(femb200_handle* h) {
     if (h->d_flag) cudaFree(h->d_flag);
     if (h->h_flag) cudaFreeHost(h->h_flag);
     if (h->mixed.mem) cudaFree(h->mixed.mem);
+    if (h->adj_mem) cudaFree(h->adj_mem);
     delete h;
     return FEMB200_OK;
 }
@@ -1379,6 +1567,50 @@ int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p, con
     if (!st) { h->err = "null stats"; return FEMB200_EINVAL; }
     RC(dispatch<DoSolve>(p, h, p, c, st, (Coupled*)nullptr));
     return finish_solve(h, c, st);
+}
+
+int femb200_stokes_adjoint_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K,
+                                    int32_t with_pnum, const void* const lam_v[3], const void* lam_P,
+                                    void* const out_dv[3], void* out_dP) {
+    RC(check_adjoint_problem(h, p));
+    if (!lam_v || !lam_P || !out_dv || !out_dP) { h->err = "λ and the outputs are required"; return FEMB200_EINVAL; }
+    RC(upload_material(h, p->mat, finite_K, dt));
+    AdjArgs<double> a = adjoint_args(p, dt, with_pnum, lam_v, lam_P);
+    for (int k = 0; k < 3; ++k) {
+        a.out_dv[k] = static_cast<double*>(out_dv[k]);
+        CK(cudaMemsetAsync(out_dv[k], 0, sizeof(double) * p->nnodes, h->stream));
+    }
+    a.out_dP = static_cast<double*>(out_dP);
+    CK(launch_hex27_adjoint<double>(a, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_stokes_viscosity_sensitivity(femb200_handle* h, const femb200_stokes_problem* p, double dt,
+                                         int32_t finite_K, int32_t with_pnum, const void* const lam_v[3],
+                                         const void* lam_P, void* out_eta_ip) {
+    RC(check_adjoint_problem(h, p));
+    if (!lam_v || !lam_P || !out_eta_ip) { h->err = "λ and the output are required"; return FEMB200_EINVAL; }
+    RC(upload_material(h, p->mat, finite_K, dt));
+    AdjArgs<double> a = adjoint_args(p, dt, with_pnum, lam_v, lam_P);
+    a.out_eta = static_cast<double*>(out_eta_ip);
+    CK(launch_hex27_adjoint<double>(a, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_solve_stokes_adjoint(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
+                                 const void* const objective_v[3], void* const lam_v[3], void* lam_P,
+                                 femb200_stokes_stats* st) {
+    RC(check_adjoint_problem(h, p));
+    RC(check_controls(h, c));
+    if (!st || !objective_v || !lam_v || !lam_P) { h->err = "objective, λ and stats are required"; return FEMB200_EINVAL; }
+    RC(solve_adjoint_impl(h, p, c, objective_v, lam_v, lam_P, st));
+    if (c->throw_on_failure && !st->converged) {
+        char b[160];
+        std::snprintf(b, sizeof b, "Adjoint solve did not converge: err=%.3e after %lld iterations", st->err, (long long)st->iter);
+        h->err = b;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
 }
 
 int femb200_transfer_temperature(femb200_handle* h, void* TP, const void* Tn, const int32_t* dofsP, const int32_t* el2nP,

@@ -121,6 +121,36 @@ cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st);
 // out = x + y (FP32)
 cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n, cudaStream_t st);
 
+// Adjoint (transposed-Jacobian) residual of the Hex27/P1-disc element at the forward
+// state (adjoint3d.cu): out_dv += (dR/dv)ᵀλ (atomics), out_dP = (dR/dP)ᵀλ (element-
+// private stores), optionally out_eta = λ·∂R/∂η per integration point.
+template <class T>
+struct AdjArgs {
+    const int32_t* el2n;
+    const int32_t* dofsP;
+    const T* geo_v;
+    const T* geo_P;
+    const T* v[3];
+    const T* P;
+    const T* Pf;
+    const T* gammaP;
+    const T* MP;
+    const int32_t* phv; int phv_layout;
+    const int32_t* php; int php_layout;
+    const T* told[6];
+    const T* eta_ip;
+    const T* lam_v[3];
+    const T* lam_P;
+    T* out_dv[3];
+    T* out_dP;
+    T* out_eta;
+    int64_t nels;
+    T dt;
+    int with_pnum;
+};
+template <class T>
+cudaError_t launch_hex27_adjoint(const AdjArgs<T>& args, int num_sms, cudaStream_t st);
+
 // Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
 template <class T, class TG>
 struct H27JacArgs {

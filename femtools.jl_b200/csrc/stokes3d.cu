@@ -14,55 +14,6 @@
 
 namespace femb {
 
-namespace {
-
-// Per-element material at one quadrature point, interpolated with the velocity
-// shape functions over the element's node phases (interp2ip_phase, utils.jl:37).
-template <class T>
-struct QpMat {
-    T eta, invG, alpha, rho0, beta;
-    T cphi, sphi, spsi, C, ereg, Kb;
-};
-
-template <class T>
-FEMB_D void interp_material(QpMat<T>& m, bool uniform, int p0, const int* PH, int qx, int qy, int qz,
-                            bool plastic, const T* eta_override) {
-    if (uniform) {
-        const T s = (T)c_tab.sumN3[tidx(qx, qy, qz)];
-        m.eta = (T)c_mat.eta[p0] * s;
-        m.invG = (T)c_mat.invG[p0] * s;
-        m.alpha = (T)c_mat.alpha[p0] * s;
-        m.rho0 = (T)c_mat.rho0[p0] * s;
-        m.beta = (T)c_mat.beta[p0] * s;
-        if (plastic) {
-            m.cphi = (T)c_mat.cos_phi[p0] * s; m.sphi = (T)c_mat.sin_phi[p0] * s; m.spsi = (T)c_mat.sin_psi[p0] * s;
-            m.C = (T)c_mat.C[p0] * s; m.ereg = (T)c_mat.eta_reg[p0] * s; m.Kb = (T)c_mat.Kb[p0] * s;
-        }
-    } else {
-        m.eta = m.invG = m.alpha = m.rho0 = m.beta = T(0);
-        m.cphi = m.sphi = m.spsi = m.C = m.ereg = m.Kb = T(0);
-        for (int k = 0; k < 3; ++k)
-            for (int j = 0; j < 3; ++j)
-                for (int i = 0; i < 3; ++i) {
-                    const T N = (T)c_tab.B[qx][i] * (T)c_tab.B[qy][j] * (T)c_tab.B[qz][k];
-                    const int p = PH[tidx(i, j, k)];
-                    m.eta += N * (T)c_mat.eta[p];
-                    m.invG += N * (T)c_mat.invG[p];
-                    m.alpha += N * (T)c_mat.alpha[p];
-                    m.rho0 += N * (T)c_mat.rho0[p];
-                    m.beta += N * (T)c_mat.beta[p];
-                    if (plastic) {
-                        m.cphi += N * (T)c_mat.cos_phi[p]; m.sphi += N * (T)c_mat.sin_phi[p];
-                        m.spsi += N * (T)c_mat.sin_psi[p]; m.C += N * (T)c_mat.C[p];
-                        m.ereg += N * (T)c_mat.eta_reg[p]; m.Kb += N * (T)c_mat.Kb[p];
-                    }
-                }
-    }
-    if (eta_override) m.eta = *eta_override;
-}
-
-}  // namespace
-
 template <class T, class TG>
 __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, TG> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -258,6 +258,61 @@ def _solve(dr, bc_v, dt, assemble_scaling, scaling_viscosity=None, history_capac
     return out
 
 
+# ---- adjoint (src/stokes/solvers/DR_adjoint.jl) ----------------------------------
+
+def _vec3(ts):
+    return (C.c_void_p * 3)(*[C.c_void_p(_ptr(t)) for t in ts])
+
+
+def assemble_adjoint_residual(dr: StokesDR, dt, lam_v, lam_P, finite_K=False, with_pnum=True):
+    """(dR/du)ᵀλ at dr's state for the augmented residual (Pnum = γP·RP/M_P inline):
+    returns (dv components, dP). The matrix-free apply of the reference's frozen
+    adjoint operator (apply_adjoint_operator!, adjoint_operator.jl:640-660)."""
+    lib, h = _Handle.get()
+    z = lambda n: torch.zeros(n, dtype=dr.dtype, device=dr.device)
+    dv = [z(dr.mesh.nnodes) for _ in range(3)]
+    dP = z(dr.mesh.nnodesP)
+    _check(lib, h, lib.femb200_stokes_adjoint_residual(h, C.byref(dr.problem()), float(dt), int(finite_K),
+                                                        int(with_pnum), _vec3(lam_v), C.c_void_p(_ptr(lam_P)),
+                                                        _vec3(dv), C.c_void_p(_ptr(dP))))
+    return dv, dP
+
+
+def viscosity_sensitivity(dr: StokesDR, dt, lam_v, lam_P, finite_K=False, with_pnum=True):
+    """λ·∂R/∂η at every integration point (nq × nels): the gradient of λᵀR(u, η) in the
+    viscosity field; per-element or per-phase gradients follow by the chain rule."""
+    lib, h = _Handle.get()
+    out = torch.zeros(dr.mesh.nq * dr.mesh.nels, dtype=dr.dtype, device=dr.device)
+    _check(lib, h, lib.femb200_stokes_viscosity_sensitivity(h, C.byref(dr.problem()), float(dt), int(finite_K),
+                                                             int(with_pnum), _vec3(lam_v), C.c_void_p(_ptr(lam_P)),
+                                                             C.c_void_p(_ptr(out))))
+    return out
+
+
+def solve_adjoint(dr: StokesDR, bc_v, dt, objective_v, lam_v=None, lam_P=None, tolerance=1e-6,
+                  max_iterations=50_000, check_interval=50, iter_max=50_000, max_ph_iterations=100, rel_drop=0.1,
+                  throw_on_failure=True, finite_K=False):
+    """solve_adjoint!(dr, mesh, bc_v; dt, objective_v, λv, λP, …) (DR_adjoint.jl:396-433).
+
+    Solves (dR/du)ᵀλ = −objective_v at the converged forward state in `dr` (dr.gammaP
+    and dr.M_P as in the forward solve) with the frozen-operator PH/DYREL iteration.
+    Returns (λv, λP, stats). With J(u(m)) and R(u, m) = 0, dJ/dm = λᵀ ∂R/∂m.
+    """
+    lib, h = _Handle.get()
+    z = lambda n: torch.zeros(n, dtype=dr.dtype, device=dr.device)
+    lam_v = [z(dr.mesh.nnodes) for _ in range(3)] if lam_v is None else lam_v
+    lam_P = z(dr.mesh.nnodesP) if lam_P is None else lam_P
+    obj = [o.contiguous() for o in objective_v]
+    c, _ = _controls(dt, tolerance=tolerance, max_iterations=max_iterations, check_interval=check_interval,
+                     iter_max=iter_max, max_ph_iterations=max_ph_iterations, rel_drop0=rel_drop,
+                     throw_on_failure=throw_on_failure, finite_K=finite_K, cfl_v=dr.CFL_v, c_fact=dr.c_fact)
+    st = abi.StokesStatsC()
+    rc = lib.femb200_solve_stokes_adjoint(h, C.byref(dr.problem(bc_v)), C.byref(c), _vec3(obj), _vec3(lam_v),
+                                          C.c_void_p(_ptr(lam_P)), C.byref(st))
+    _check(lib, h, rc)
+    return lam_v, lam_P, prob.stats_dict(st)
+
+
 class ThermalDiffusionDR:
     """Thermal DR state on the device (heat_diffusion_types.jl:90-132)."""
 

@@ -299,6 +299,41 @@ int femb200_store_stress(femb200_handle* h, const femb200_stokes_problem* p, dou
 int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p,
                          const femb200_stokes_controls* c, femb200_stokes_stats* stats);
 
+/* ---- adjoint (3-D Hex27/P1-disc, FP64) ------------------------------------ */
+
+/* Transposed Jacobian of the augmented residual (Rv with Pnum = γP·RP/M_P formed
+ * inline when with_pnum, and RP) at the problem's forward state, applied to
+ * λ = (lam_v, lam_P): out_dv = (dR/dv)ᵀλ, out_dP = (dR/dP)ᵀλ. Replaces the
+ * reference's frozen element-block apply apply_adjoint_operator!
+ * (src/stokes/assemblers/adjoint_operator.jl:640-660; the operator of :3-73) and
+ * its Enzyme residual (src/stokes/solvers/DR_adjoint.jl:156-205), matrix-free.
+ * Device pointers, nnodes and nnodesP entries. No Dirichlet rows are applied. */
+int femb200_stokes_adjoint_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt,
+                                    int32_t finite_K, int32_t with_pnum, const void* const lam_v[3],
+                                    const void* lam_P, void* const out_dv[3], void* out_dP);
+
+/* λ·∂R/∂η at every integration point (nq × nels, the viscosity_ip layout): the
+ * sensitivity of λᵀR to the viscosity field, from which a gradient with respect to
+ * any viscosity parameterisation follows by the chain rule (the reference forms
+ * per-element material gradients this way, examples/.../sinking_block_adj.jl:117-239,
+ * and per phase in src/stokes/solvers/DR_adjoint.jl:495-531). */
+int femb200_stokes_viscosity_sensitivity(femb200_handle* h, const femb200_stokes_problem* p, double dt,
+                                         int32_t finite_K, int32_t with_pnum, const void* const lam_v[3],
+                                         const void* lam_P, void* out_eta_ip);
+
+/* solve_adjoint! (src/stokes/solvers/DR_adjoint.jl:396-433, core :3-325): solves
+ * (dR/du)ᵀλ = −objective (objective = ∂J/∂v on the velocity DoFs, zero on the
+ * constrained ones) by the Powell–Hestenes/DYREL iteration with the frozen operator
+ * at the problem's forward state. The Gershgorin λmax of the Jacobian diagnostics
+ * sets the pseudo-time step (the reference's measure_λmax = false). Uses
+ * controls: dt, tolerance (adjoint_tol), check_interval (ncheck), rel_drop0
+ * (rel_drop, default 0.1), iter_max (iterMax), max_iterations (total_iterMax),
+ * max_ph_iterations, finite_K, cfl_v, c_fact, throw_on_failure. Writes the
+ * problem's dRdv and PC. lam_v, lam_P: initial guess in, adjoint out. */
+int femb200_solve_stokes_adjoint(femb200_handle* h, const femb200_stokes_problem* p,
+                                 const femb200_stokes_controls* c, const void* const objective_v[3],
+                                 void* const lam_v[3], void* lam_P, femb200_stokes_stats* stats);
+
 /* ---- thermal diffusion ---------------------------------------------------- */
 
 /* assemble_diffusion_matrices_atomix! (src/heat_diffusion/assembly/residual_atomics.jl:10)

@@ -141,13 +141,15 @@ inline void ve_coeffs(const double* N, double etaq, const double* G, const int* 
 
 // 3-D stress with optional Drucker–Prager return (rheology.jl:413-472).
 // grad[i][k] = ∂v_i/∂x_k. Returns λ through lam_out.
-template <class S>
-void stress3d(const S grad[3][3], double etave, double inv2Gdt, const double told[6], const Plastic* pl,
-              double Pq, S tau[6], double* lam_out) {
+// SE (the Maxwell viscosity) and SP (the pressure) may be dual numbers as well,
+// for the adjoint checks that differentiate with respect to them.
+template <class S, class SE = double, class SP = double>
+void stress3d(const S grad[3][3], SE etave, double inv2Gdt, const double told[6], const Plastic* pl,
+              SP Pq, S tau[6], double* lam_out) {
     S tr = (grad[0][0] + grad[1][1] + grad[2][2]) / 3.0;
     S eps[6] = {grad[0][0] - tr, grad[1][1] - tr, grad[2][2] - tr,
                 (grad[0][1] + grad[1][0]) / 2.0, (grad[0][2] + grad[2][0]) / 2.0, (grad[1][2] + grad[2][1]) / 2.0};
-    for (int c = 0; c < 6; ++c) tau[c] = (2 * etave) * (eps[c] + told[c] * inv2Gdt);
+    for (int c = 0; c < 6; ++c) tau[c] = (2.0 * etave) * (eps[c] + told[c] * inv2Gdt);
     double lam_v = 0;
     if (pl) {
         S tII = sqrt((tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]) / 2.0 + tau[3] * tau[3] + tau[4] * tau[4] +
@@ -160,7 +162,7 @@ void stress3d(const S grad[3][3], double etave, double inv2Gdt, const double tol
         S lam = val(F) > 0 ? F / (etave + pl->ereg + pl->Kb * 1.0 * dQdP * dFdP) : S(0.0);
         lam_v = val(lam);
         if (val(lam) > 0)
-            for (int c = 0; c < 6; ++c) tau[c] = tau[c] - (2 * etave) * lam * dQ[c];
+            for (int c = 0; c < 6; ++c) tau[c] = tau[c] - (2.0 * etave) * lam * dQ[c];
     }
     if (lam_out) *lam_out = lam_v;
 }
@@ -435,6 +437,183 @@ void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K) {
 void jacobian_impl(const femb200_stokes_problem* p, double dt, int finite_K) {
     if (p->dim == 3) jacobian_impl_t<27>(p, dt, finite_K);
     else jacobian_impl_t<9>(p, dt, finite_K);
+}
+
+// ---- adjoint checks -----------------------------------------------------------
+// The whole Hex27 Stokes element residual with every input a scalar of type S: the
+// velocities, the element's pressure DoFs and the viscosity at each quadrature
+// point. Rv carries Pnum = γP·RP/M_P formed inline from the element's own RP (the
+// augmented residual the DR loop drives to zero, DR.jl:674-676), RP is the
+// continuity residual. It restates pressure_element and momentum_element with
+// those inputs typed S so that forward-mode duals can seed any of them; the
+// reference's adjoint operator (FrozenAdjointOperator,
+// src/stokes/assemblers/adjoint_operator.jl:3-73, applied at :640-660) is the
+// transpose of this function's Jacobian.
+template <class S>
+void stokes_element_all(const Tables& t, const Elem& el, const femb200_stokes_material& m, const S v[3][27],
+                        const S Pe[4], const S etaq[27], const double* bulk, double dt, bool with_pnum, S Rv[3][27],
+                        S RP[4]) {
+    const int D = 3, NV = 27, NP = 4, NQ = 27;
+    bool all_inf = true;
+    for (int ph = 0; ph < FEMB200_MAX_PHASES; ++ph) if (!std::isinf(bulk[ph])) { all_inf = false; break; }
+    double beta[FEMB200_MAX_PHASES];
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) beta[i] = 1.0 / m.K[i];
+    double dNdx[27][3];
+    // pressure residual (pressure_residual.jl:132-158)
+    for (int i = 0; i < NP; ++i) RP[i] = S(0.0);
+    for (int q = 0; q < NQ; ++q) {
+        dNdx_at(t, el.geo, D, q, dNdx);
+        const double dO = el.geoP[q];
+        const double* Nv = t.NP[q];
+        const double ebq = all_inf ? INFINITY : interp_phase(Nv, bulk, el.php, NP);
+        const double aq = interp_phase(Nv, m.alpha, el.php, NP);
+        S dPinc(0.0);
+        if (el.P0_ip) { for (int i = 0; i < NP; ++i) dPinc = dPinc + Nv[i] * Pe[i]; dPinc = dPinc - el.P0q[q]; }
+        else for (int i = 0; i < NP; ++i) dPinc = dPinc + Nv[i] * (Pe[i] - el.P0[i]);
+        const S dPdt = all_inf ? S(0.0) : dPinc / (ebq * dt);
+        double dT = 0;
+        for (int i = 0; i < NP; ++i) dT += Nv[i] * (el.T[i] - el.T0[i]);
+        const double dTdt = aq * dT / dt;
+        S div(0.0);
+        for (int j = 0; j < D; ++j)
+            for (int a = 0; a < NV; ++a) div = div + dNdx[a][j] * v[j][a];
+        for (int i = 0; i < NP; ++i) RP[i] = RP[i] + Nv[i] * ((S(0.0) - div - dPdt + dTdt) * dO);
+    }
+    S pn[4];
+    for (int i = 0; i < NP; ++i) pn[i] = with_pnum ? (el.gam[i] * RP[i]) / el.MP[i] : S(0.0);
+    // momentum residual (momentum_residuals.jl:209-258)
+    for (int c = 0; c < D; ++c) for (int a = 0; a < NV; ++a) Rv[c][a] = S(0.0);
+    double invG[FEMB200_MAX_PHASES];
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) invG[i] = 1.0 / m.G[i];
+    for (int q = 0; q < NQ; ++q) {
+        dNdx_at(t, el.geo, D, q, dNdx);
+        const double dO = el.geo[q * (D * D + 1) + D * D];
+        const double* Nv = t.N[q];
+        const double* NPq = t.NP[q];
+        S Pq(0.0); for (int i = 0; i < NP; ++i) Pq = Pq + NPq[i] * Pe[i];
+        double Pfq = 0; if (el.hasPf) for (int i = 0; i < NP; ++i) Pfq += NPq[i] * el.Pf[i];
+        const S Peq = el.hasPf ? Pq - Pfq : Pq;
+        const double invGq = interp_phase(Nv, invG, el.phv, NV);
+        const S etave = 1.0 / (1.0 / etaq[q] + invGq / dt);
+        const double inv2Gdt = invGq / (2 * dt);
+        Plastic pl; const Plastic* plp = nullptr;
+        if (m.plastic) { pl = plastic_at(m, Nv, el.phv, NV, dt); plp = &pl; }
+        S grad[3][3];
+        for (int i = 0; i < D; ++i)
+            for (int k = 0; k < D; ++k) {
+                S g(0.0);
+                for (int a = 0; a < NV; ++a) g = g + dNdx[a][k] * v[i][a];
+                grad[i][k] = g;
+            }
+        S tau[6];
+        stress3d<S, S, S>(grad, etave, inv2Gdt, el.told[q], plp, Peq, tau, nullptr);
+        const S sig[3][3] = {{tau[0], tau[3], tau[4]}, {tau[3], tau[1], tau[5]}, {tau[4], tau[5], tau[2]}};
+        S Ptot = el.hasPf ? Peq + Pfq : Pq;
+        S pq(0.0); for (int i = 0; i < NP; ++i) pq = pq + NPq[i] * pn[i];
+        Ptot = Ptot + pq;
+        double Tq = 0; for (int i = 0; i < NP; ++i) Tq += NPq[i] * el.T[i];
+        const S rhoq = interp_phase(Nv, m.rho0, el.phv, NV) *
+                       (1.0 - interp_phase(Nv, m.alpha, el.phv, NV) * (Tq - m.Tref) + interp_phase(Nv, beta, el.phv, NV) * Pq);
+        for (int i = 0; i < D; ++i) {
+            const S bg = rhoq * m.g[i];
+            for (int a = 0; a < NV; ++a) {
+                S sa(0.0);
+                for (int j = 0; j < D; ++j) sa = sa + dNdx[a][j] * (j == i ? sig[j][i] - Ptot : sig[j][i]);
+                Rv[i][a] = Rv[i][a] + (sa - Nv[a] * bg) * dO;
+            }
+        }
+    }
+}
+
+// Viscosity at each quadrature point: the given per-point field, or the phase
+// interpolation of the material's (interp2ip_phase, src/utils.jl:37-44).
+void element_viscosity(const Tables& t, const Elem& el, const femb200_stokes_material& m, double eta[27]) {
+    for (int q = 0; q < el.NQ; ++q) eta[q] = el.eta_ip ? el.etaq_ip[q] : interp_phase(t.N[q], m.eta, el.phv, el.NV);
+}
+
+// (∂R/∂u)ᵀλ over the mesh: dv = (dRv/dv)ᵀλv + (dRP/dv)ᵀλP, dP = (dRv/dP)ᵀλv +
+// (dRP/dP)ᵀλP, from the element Jacobians by forward-mode duals (27 partials per
+// velocity component, 4 for the pressure DoFs).
+void adjoint_residual_impl(const femb200_stokes_problem* p, double dt, int finite_K, bool with_pnum,
+                           const double* const lam_v[3], const double* lam_P, double* const out_dv[3], double* out_dP) {
+    const Tables& t = tables_for(3);
+    const double* bulk = bulk_table(p, finite_K);
+    std::vector<double> buf((size_t)p->nels * 85);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t e = 0; e < p->nels; ++e) {
+        Elem el; gather(p, e, el);
+        double vd[3][27]; load_v(p, el, vd);
+        double eta[27]; element_viscosity(t, el, p->mat, eta);
+        double lv[3][27], lp[4];
+        for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) lv[c][a] = lam_v[c][el.nodes[a] - 1];
+        for (int i = 0; i < 4; ++i) lp[i] = lam_P[el.dofs[i] - 1];
+        double* o = &buf[(size_t)e * 85];
+        {
+            using DU = Dual<27>;
+            for (int j = 0; j < 3; ++j) {
+                DU v[3][27], Pe[4], et[27], Rv[3][27], RP[4];
+                for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) v[c][a] = DU(vd[c][a]);
+                for (int b = 0; b < 27; ++b) v[j][b].d[b] = 1.0;
+                for (int i = 0; i < 4; ++i) Pe[i] = DU(el.P[i]);
+                for (int q = 0; q < 27; ++q) et[q] = DU(eta[q]);
+                stokes_element_all<DU>(t, el, p->mat, v, Pe, et, bulk, dt, with_pnum, Rv, RP);
+                for (int b = 0; b < 27; ++b) {
+                    double s = 0;
+                    for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) s += lv[c][a] * Rv[c][a].d[b];
+                    for (int i = 0; i < 4; ++i) s += lp[i] * RP[i].d[b];
+                    o[j * 27 + b] = s;
+                }
+            }
+        }
+        {
+            using DU = Dual<4>;
+            DU v[3][27], Pe[4], et[27], Rv[3][27], RP[4];
+            for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) v[c][a] = DU(vd[c][a]);
+            for (int i = 0; i < 4; ++i) { Pe[i] = DU(el.P[i]); Pe[i].d[i] = 1.0; }
+            for (int q = 0; q < 27; ++q) et[q] = DU(eta[q]);
+            stokes_element_all<DU>(t, el, p->mat, v, Pe, et, bulk, dt, with_pnum, Rv, RP);
+            for (int k = 0; k < 4; ++k) {
+                double s = 0;
+                for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) s += lv[c][a] * Rv[c][a].d[k];
+                for (int i = 0; i < 4; ++i) s += lp[i] * RP[i].d[k];
+                o[81 + k] = s;
+            }
+        }
+    }
+    for (int c = 0; c < 3; ++c) std::fill(out_dv[c], out_dv[c] + p->nnodes, 0.0);
+    std::fill(out_dP, out_dP + p->nnodesP, 0.0);
+    for (int64_t e = 0; e < p->nels; ++e) {
+        const double* o = &buf[(size_t)e * 85];
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 27; ++a) out_dv[c][p->el2n[27 * e + a] - 1] += o[c * 27 + a];
+        for (int i = 0; i < 4; ++i) out_dP[p->dofsP[4 * e + i] - 1] += o[81 + i];
+    }
+}
+
+// λ·∂R/∂η_q for the viscosity at every quadrature point (the per-point field
+// p->viscosity_ip, or the phase-interpolated viscosity), nq × nels.
+void viscosity_sensitivity_impl(const femb200_stokes_problem* p, double dt, int finite_K, bool with_pnum,
+                                const double* const lam_v[3], const double* lam_P, double* out) {
+    const Tables& t = tables_for(3);
+    const double* bulk = bulk_table(p, finite_K);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t e = 0; e < p->nels; ++e) {
+        Elem el; gather(p, e, el);
+        double vd[3][27]; load_v(p, el, vd);
+        double eta[27]; element_viscosity(t, el, p->mat, eta);
+        using DU = Dual<27>;
+        DU v[3][27], Pe[4], et[27], Rv[3][27], RP[4];
+        for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) v[c][a] = DU(vd[c][a]);
+        for (int i = 0; i < 4; ++i) Pe[i] = DU(el.P[i]);
+        for (int q = 0; q < 27; ++q) { et[q] = DU(eta[q]); et[q].d[q] = 1.0; }
+        stokes_element_all<DU>(t, el, p->mat, v, Pe, et, bulk, dt, with_pnum, Rv, RP);
+        for (int q = 0; q < 27; ++q) {
+            double s = 0;
+            for (int c = 0; c < 3; ++c) for (int a = 0; a < 27; ++a) s += lam_v[c][el.nodes[a] - 1] * Rv[c][a].d[q];
+            for (int i = 0; i < 4; ++i) s += lam_P[el.dofs[i] - 1] * RP[i].d[q];
+            out[27 * e + q] = s;
+        }
+    }
 }
 
 // Pressure mass and scale (pressure_scaling.jl:118-216).
@@ -1038,6 +1217,25 @@ int orc_solve_thermal(const femb200_thermal_problem* tp, const femb200_thermal_c
 int orc_transfer_temperature(double* TP, const double* T, const int32_t* dofsP, const int32_t* el2nP, int64_t n) {
     transfer_T(TP, T, dofsP, el2nP, n);
     return 0;
+}
+
+int orc_stokes_adjoint_residual(const femb200_stokes_problem* p, double dt, int32_t finite_K, int32_t with_pnum,
+                                const double* const lam_v[3], const double* lam_P, double* const out_dv[3],
+                                double* out_dP) {
+    int rc = check_problem(p);
+    if (rc) return rc;
+    if (p->dim != 3) { g_last_error = "the adjoint oracle is 3-D (Hex27) only"; return FEMB200_EUNSUPPORTED; }
+    adjoint_residual_impl(p, dt, finite_K, with_pnum != 0, lam_v, lam_P, out_dv, out_dP);
+    return FEMB200_OK;
+}
+
+int orc_stokes_viscosity_sensitivity(const femb200_stokes_problem* p, double dt, int32_t finite_K, int32_t with_pnum,
+                                     const double* const lam_v[3], const double* lam_P, double* out_eta_ip) {
+    int rc = check_problem(p);
+    if (rc) return rc;
+    if (p->dim != 3) { g_last_error = "the adjoint oracle is 3-D (Hex27) only"; return FEMB200_EUNSUPPORTED; }
+    viscosity_sensitivity_impl(p, dt, finite_K, with_pnum != 0, lam_v, lam_P, out_eta_ip);
+    return FEMB200_OK;
 }
 
 int orc_shear_heating(const femb200_stokes_problem* p, double dt, double* phi) {

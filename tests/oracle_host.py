@@ -49,6 +49,10 @@ def lib():
             "orc_solve_thermal": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.ThermalControlsC), _P(abi.ThermalStatsC)]),
             "orc_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64]),
             "orc_shear_heating": (C.c_int, [_P(abi.StokesProblemC), C.c_double, _vp]),
+            "orc_stokes_adjoint_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
+                                                      _vp * 3, _vp, _vp * 3, _vp]),
+            "orc_stokes_viscosity_sensitivity": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
+                                                           _vp * 3, _vp, _vp]),
             "orc_solve_coupled": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.StokesProblemC), _P(abi.StokesControlsC),
                                             C.c_double, C.c_int32, _vp, _P(abi.StokesStatsC)]),
             "orc_element_custom": (C.c_int, [C.c_int] * 4 + [_vp] * 15 + [_P(abi.StokesMaterialC), C.c_double,
@@ -161,6 +165,29 @@ class HostStokes:
         phi = np.zeros(self.mesh.nq * self.mesh.nels)
         check(lib().orc_shear_heating(C.byref(self.struct()), dt, ptr(phi)))
         return phi
+
+    def adjoint_residual(self, dt, lam_v, lam_P, finite_K=False, with_pnum=True):
+        """(dR/du)ᵀλ at the current state (R the augmented residual: Pnum = γP·RP/M_P
+        inline): returns (dv per component, dP)."""
+        lam_v = [np.ascontiguousarray(x, dtype=np.float64) for x in lam_v]
+        lam_P = np.ascontiguousarray(lam_P, dtype=np.float64)
+        dv = [np.zeros(self.mesh.nnodes) for _ in range(3)]
+        dP = np.zeros(self.mesh.nnodesP)
+        lv = (_vp * 3)(*[ptr(x) for x in lam_v])
+        ov = (_vp * 3)(*[ptr(x) for x in dv])
+        check(lib().orc_stokes_adjoint_residual(C.byref(self.struct()), dt, int(finite_K), int(with_pnum), lv,
+                                                 ptr(lam_P), ov, ptr(dP)))
+        return dv, dP
+
+    def viscosity_sensitivity(self, dt, lam_v, lam_P, finite_K=False, with_pnum=True):
+        """λ·∂R/∂η at every integration point (nq × nels)."""
+        lam_v = [np.ascontiguousarray(x, dtype=np.float64) for x in lam_v]
+        lam_P = np.ascontiguousarray(lam_P, dtype=np.float64)
+        out = np.zeros(self.mesh.nq * self.mesh.nels)
+        lv = (_vp * 3)(*[ptr(x) for x in lam_v])
+        check(lib().orc_stokes_viscosity_sensitivity(C.byref(self.struct()), dt, int(finite_K), int(with_pnum), lv,
+                                                      ptr(lam_P), ptr(out)))
+        return out
 
     def solve(self, history_capacity=0, **kw):
         hist = np.zeros((history_capacity, 4 + self.mesh.dim)) if history_capacity else None

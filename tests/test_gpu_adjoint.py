@@ -1,0 +1,121 @@
+"""GPU adjoint (the hand-written reverse-mode element kernel and the frozen-operator
+PH/DYREL adjoint solve) against the oracle and against central finite differences.
+
+The oracle's transposed Jacobian is itself pinned by finite differences of its
+forward residual (test_adjoint_oracle.py)."""
+import numpy as np
+import pytest
+
+import oracle_host as oh
+from cases import random_state_case
+from conftest import fem
+from test_adjoint_oracle import dense_adjoint
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.concatenate([np.ravel(x.detach().cpu().numpy() if hasattr(x, "detach") else x) for x in a])
+    b = np.concatenate([np.ravel(x) for x in b])
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def device_and_host(case, gammaP=True):
+    dr = case.device_state(fem)
+    hs = case.host_state(oh)
+    if gammaP and case.gammaP is None:
+        rng = np.random.default_rng(3)
+        g, m = rng.uniform(1, 5, case.mesh.nnodesP), rng.uniform(0.01, 0.1, case.mesh.nnodesP)
+        hs.gammaP[:], hs.M_P[:] = g, m
+        dr.gammaP.copy_(dr.tensor(g)); dr.M_P.copy_(dr.tensor(m))
+    return dr, hs
+
+
+@pytest.mark.parametrize("phases,plastic,finite_K,with_pnum", [
+    ("nodal", True, False, True), ("cell", True, True, True), ("element", False, False, True),
+    ("nodal", True, True, False)])
+def test_adjoint_residual_matches_oracle(phases, plastic, finite_K, with_pnum):
+    case = random_state_case(dim=3, n=3, seed=31, phases=phases, plastic=plastic, distort=True)
+    dr, hs = device_and_host(case)
+    rng = np.random.default_rng(7)
+    lv = [rng.standard_normal(case.mesh.nnodes) for _ in range(3)]
+    lP = rng.standard_normal(case.mesh.nnodesP)
+    dv, dP = fem.assemble_adjoint_residual(dr, case.dt, [dr.tensor(x) for x in lv], dr.tensor(lP), finite_K=finite_K,
+                                           with_pnum=with_pnum)
+    torch.cuda.synchronize()
+    rv, rP = hs.adjoint_residual(case.dt, lv, lP, finite_K=finite_K, with_pnum=with_pnum)
+    assert rel(dv, rv) < 1e-11, rel(dv, rv)
+    assert rel([dP], [rP]) < 1e-11, rel([dP], [rP])
+
+
+def test_viscosity_sensitivity_matches_oracle():
+    case = random_state_case(dim=3, n=3, seed=32, phases="nodal", plastic=True, distort=True)
+    dr, hs = device_and_host(case)
+    rng = np.random.default_rng(8)
+    eta = 10 ** rng.uniform(0, 1, case.mesh.nq * case.mesh.nels)
+    hs.viscosity_ip = eta
+    dr.viscosity_ip = dr.tensor(eta)
+    lv = [rng.standard_normal(case.mesh.nnodes) for _ in range(3)]
+    lP = rng.standard_normal(case.mesh.nnodesP)
+    s = fem.viscosity_sensitivity(dr, case.dt, [dr.tensor(x) for x in lv], dr.tensor(lP))
+    ref = hs.viscosity_sensitivity(case.dt, lv, lP)
+    assert rel([s], [ref]) < 1e-11
+
+
+def forward(ac, delta, tol=1e-13):
+    dr = ac.case.device_state(fem)
+    dr.viscosity_ip = dr.tensor(ac.eta_ip(delta))
+    st = fem.solve(dr, ac.case.bc_device(), dt=ac.case.dt, tolerance=tol, check_interval=50,
+                   max_iterations=400_000, iter_max=400_000, throw_on_failure=False)
+    assert st["converged"]
+    return dr
+
+
+def adjoint_gradient(ac, dr, tol=1e-12):
+    J, obj = ac.objective(dr.v)
+    lam_v, lam_P, st = fem.solve_adjoint(dr, ac.case.bc_device(), ac.case.dt, [dr.tensor(o) for o in obj],
+                                         tolerance=tol, max_iterations=400_000, iter_max=400_000,
+                                         max_ph_iterations=400)
+    sens = fem.viscosity_sensitivity(dr, ac.case.dt, lam_v, lam_P)
+    eta = dr.viscosity_ip
+    grad = (eta * sens).reshape(dr.mesh.nels, dr.mesh.nq).sum(dim=1)
+    return J, obj, lam_v, lam_P, grad, st
+
+
+def test_adjoint_solve_matches_dense_oracle_adjoint():
+    ac = fem.configs.adjoint_case(n=2, seed=1)
+    dr = forward(ac, ac.delta)
+    J, obj, lam_v, lam_P, grad, st = adjoint_gradient(ac, dr)
+    assert st["converged"], st
+    # the oracle's dense transposed Jacobian at the GPU forward state
+    hs = ac.case.host_state(oh)
+    hs.viscosity_ip = ac.eta_ip()
+    for c in range(3):
+        hs.v[c][:] = dr.v[c].cpu().numpy()
+    hs.P[:] = dr.P.cpu().numpy()
+    hs.gammaP[:] = dr.gammaP.cpu().numpy()
+    hs.M_P[:] = dr.M_P.cpu().numpy()
+    rl_v, rl_P = dense_adjoint(hs, ac.case.dt, obj, ac.case.bc)
+    assert rel(lam_v, rl_v) < 1e-6, rel(lam_v, rl_v)
+    assert rel([lam_P], [rl_P]) < 1e-6, rel([lam_P], [rl_P])
+    sens = hs.viscosity_sensitivity(ac.case.dt, rl_v, rl_P)
+    rgrad = (ac.eta_ip() * sens).reshape(hs.mesh.nels, hs.mesh.nq).sum(axis=1)
+    assert rel([grad], [rgrad]) < 1e-6
+
+
+def test_adjoint_gradient_matches_central_differences():
+    # central differences of J(δ) with the forward solve converged far below h²
+    ac = fem.configs.adjoint_case(n=3, seed=2)
+    dr = forward(ac, ac.delta)
+    J, obj, lam_v, lam_P, grad, st = adjoint_gradient(ac, dr)
+    grad = grad.cpu().numpy()
+    rng = np.random.default_rng(9)
+    h = 1e-4
+    for k in rng.choice(dr.mesh.nels, size=6, replace=False):
+        d = ac.delta.copy(); d[k] += h
+        Jp = ac.objective(forward(ac, d).v)[0]
+        d[k] -= 2 * h
+        Jm = ac.objective(forward(ac, d).v)[0]
+        fd = (Jp - Jm) / (2 * h)
+        assert abs(fd - grad[k]) <= 1e-5 * np.abs(grad).max() + 1e-6 * abs(fd), (k, fd, grad[k])
