@@ -216,6 +216,95 @@ def sweep_mode(args, fem, case, dr, lib, h):
     return 0
 
 
+def adjoint_mode(args, fem):
+    """Adjoint workload (coupled thermal–Stokes forward with shear heating on a Hex27 n³
+    mesh, T-dependent viscosity η = exp(−0.1·T)·exp(δ_e)): the coupled forward solve,
+    then with the temperature frozen at its converged value the device adjoint solve
+    and the per-element log-viscosity gradient, checked against central differences
+    of Stokes solves on `--fd-elements` random elements. Prints one JSON line."""
+    import torch
+    n = args.n
+    ac = fem.configs.adjoint_case(n=n, seed=args.seed)
+    case = ac.case
+    mesh = case.mesh
+    dt = args.adjoint_dt
+    rng = np.random.default_rng(args.seed + 100)
+    # thermal state on the Hex27 nodes: T linear from 1 at the bottom to 0 at the top, plus noise
+    z = mesh.coords[:, 2]
+    T0n = 1.0 - z + rng.normal(0.0, 0.01, size=mesh.nnodes)
+    bot = (np.nonzero(np.abs(z) < 1e-12)[0] + 1).astype(np.int32)
+    topn = (np.nonzero(np.abs(z - 1.0) < 1e-12)[0] + 1).astype(np.int32)
+    T0n[bot - 1] = 1.0
+    T0n[topn - 1] = 0.0
+    bcT = fem.DirichletBoundaryCondition(np.concatenate([bot, topn]),
+                                         np.concatenate([np.ones(len(bot)), np.zeros(len(topn))]))
+    th = fem.ThermalDiffusionDR(mesh, k=(1.0,), Cp=(1.0,), rho0=(1.0,), alpha=(case.material.alpha[0],), eps=1e-8)
+    th.T.copy_(torch.as_tensor(T0n, device="cuda"))
+    th.T0.copy_(th.T)
+    dr = case.device_state(fem)
+    Tq = (T0n[mesh.el2n - 1] @ fem.element_tables(3).N.T).reshape(-1)   # initial T at the integration points
+    eta0 = dr.tensor(np.exp(-0.1 * Tq))
+    dr.viscosity_ip = (eta0 * torch.repeat_interleave(dr.tensor(np.exp(ac.delta)), mesh.nq)).contiguous()
+    bc = case.bc_device()
+    lib, h = fem.solver._Handle.get()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    e0, e1, e2, e3, e4 = ev(), ev(), ev(), ev(), ev()
+    e0.record()
+    stf, _phi = fem.solve_coupled(th, dr, bcT, bc, dt, Tref=0.0, shear_heating=True, tolerance=args.tolerance,
+                                  max_iterations=2_000_000, iter_max=2_000_000, throw_on_failure=False)
+    e1.record()
+    J, obj = ac.objective(dr.v)
+    lam_v, lam_P, sta = fem.solve_adjoint(dr, bc, dt, [dr.tensor(o) for o in obj], tolerance=args.tolerance,
+                                          max_iterations=2_000_000, iter_max=2_000_000, max_ph_iterations=1000,
+                                          throw_on_failure=False)
+    e2.record()
+    sens = fem.viscosity_sensitivity(dr, dt, lam_v, lam_P)
+    grad = (dr.viscosity_ip * sens).reshape(mesh.nels, mesh.nq).sum(dim=1)
+    e3.record()
+    torch.cuda.synchronize()
+    grad = grad.cpu().numpy()
+    # central differences with T frozen at the converged coupled state
+    ck = fem.DRCheckpoint(dr)
+    kfd = min(args.fd_elements, mesh.nels)
+    els = rng.choice(mesh.nels, size=kfd, replace=False)
+    scale = float(np.abs(grad).max())
+    fd_out = []
+    fd_iters = 0
+    for hh in [float(x) for x in str(args.fd_h).split(",")]:
+        errs, fds = [], []
+        for k in els:
+            vals = []
+            for sgn in (1.0, -1.0):
+                ck.restore(dr)
+                d = ac.delta.copy()
+                d[k] += sgn * hh
+                dr.viscosity_ip = (eta0 * torch.repeat_interleave(dr.tensor(np.exp(d)), mesh.nq)).contiguous()
+                st = fem.solve(dr, bc, dt, tolerance=args.fd_tolerance, max_iterations=2_000_000,
+                               iter_max=2_000_000, throw_on_failure=False)
+                fd_iters += st["iter"]
+                vals.append(ac.objective(dr.v)[0])
+            fd = (vals[0] - vals[1]) / (2 * hh)
+            fds.append(fd)
+            errs.append(abs(fd - grad[k]) / max(abs(fd), 1e-300))
+        fd_out.append({"h": hh, "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+                       "max_abs_err_over_max_grad": float(max(abs(f - grad[k]) for f, k in zip(fds, els)) / scale)})
+    e4.record()
+    torch.cuda.synchronize()
+    line = {
+        "mode": "adjoint", "workload": f"coupled-thermal-stokes-adjoint-hex27-{n}^3", "n": n, "dt": dt,
+        "forward": {"ms": e0.elapsed_time(e1), "iterations": stf["iter"], "itPH": stf["itPH"],
+                    "converged": bool(stf["converged"]), "thermal_iterations": stf["thermal_iterations"]},
+        "adjoint": {"ms": e1.elapsed_time(e2), "iterations": sta["iter"], "itPH": sta["itPH"],
+                    "converged": bool(sta["converged"]), "err": sta["err"]},
+        "gradient_ms": e2.elapsed_time(e3), "J": J,
+        "fd": {"elements": int(kfd), "tolerance": args.fd_tolerance, "ms": e3.elapsed_time(e4),
+               "iterations": fd_iters, "per_h": fd_out},
+        "scope": "T frozen at the converged coupled state in the adjoint and the differences",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -260,7 +349,11 @@ def main():
     ap.add_argument("--ref-jacobians", type=int, default=0)
     ap.add_argument("--max-iterations", type=int, default=2_000_000,
                     help="cap on DR iterations per solve (profiling runs of a few sweeps)")
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep"],
+    ap.add_argument("--adjoint-dt", type=float, default=1e-2)
+    ap.add_argument("--fd-elements", type=int, default=20)
+    ap.add_argument("--fd-h", default="1e-6,1e-4", help="central-difference steps, comma-separated")
+    ap.add_argument("--fd-tolerance", type=float, default=1e-13)
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -292,6 +385,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    if args.mode == "adjoint":
+        return adjoint_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()

@@ -24,3 +24,5 @@ from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, so
                      assemble_viscosity_weighted_pressure_scaling, update_stokes_current_stress,
                      assemble_shear_heating, assemble_thermal_residual, assemble_diffusion_matrices_colored,
                      assemble_adjoint_residual, viscosity_sensitivity, solve_adjoint)
+from . import autodiff  # noqa: E402,F401
+from .autodiff import DRCheckpoint, solve_log_viscosity  # noqa: E402,F401

@@ -119,3 +119,53 @@ def test_adjoint_gradient_matches_central_differences():
         Jm = ac.objective(forward(ac, d).v)[0]
         fd = (Jp - Jm) / (2 * h)
         assert abs(fd - grad[k]) <= 1e-5 * np.abs(grad).max() + 1e-6 * abs(fd), (k, fd, grad[k])
+
+
+def test_autograd_rule_matches_central_differences_and_reuses_checkpoint():
+    # the rrule analogue: torch autograd through the solve, backward by the device adjoint
+    ac = fem.configs.adjoint_case(n=2, seed=4)
+    dr = ac.case.device_state(fem)
+    bc = ac.case.bc_device()
+    eta0 = dr.tensor(ac.eta_ip(np.zeros_like(ac.delta)))
+    vt = torch.cat([dr.tensor(x) for x in ac.v_target])
+    top = torch.zeros(3 * dr.mesh.nnodes, dtype=torch.bool, device=dr.device)
+    for c in range(3):
+        top[c * dr.mesh.nnodes + torch.as_tensor(ac.top - 1, device=dr.device).long()] = True
+    kw = dict(tolerance=1e-13, max_iterations=400_000, iter_max=400_000, throw_on_failure=False, check_interval=50)
+
+    def loss_of(delta):
+        v = fem.solve_log_viscosity(delta, dr, bc, ac.case.dt, eta0, solve_kw=kw,
+                                    adjoint_kw=dict(tolerance=1e-12, max_iterations=400_000, iter_max=400_000,
+                                                    max_ph_iterations=400))
+        return (((v - vt) * top) ** 2).sum()
+
+    delta = dr.tensor(ac.delta).requires_grad_(True)
+    L = loss_of(delta)
+    # clobber the state between forward and backward: the checkpoint must restore it
+    for x in dr.v:
+        x.zero_()
+    L.backward()
+    g = delta.grad.cpu().numpy()
+    h = 1e-4
+    for k in (0, 3, 6):
+        d = ac.delta.copy(); d[k] += h
+        Lp = float(loss_of(dr.tensor(d)))
+        d[k] -= 2 * h
+        Lm = float(loss_of(dr.tensor(d)))
+        fd = (Lp - Lm) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-5 * np.abs(g).max() + 1e-6 * abs(fd), (k, fd, g[k])
+
+
+def test_checkpoint_host_spill_round_trip():
+    case = random_state_case(dim=3, n=2, seed=33, phases="cell", plastic=False, distort=False)
+    dr = case.device_state(fem)
+    ck = fem.DRCheckpoint(dr, host=True)
+    torch.cuda.synchronize()
+    ref = [x.clone() for x in dr.v] + [dr.P.clone()]
+    for x in dr.v:
+        x.add_(1.0)
+    dr.P.mul_(3.0)
+    ck.restore(dr)
+    torch.cuda.synchronize()
+    for a, b in zip([*dr.v, dr.P], ref):
+        assert torch.equal(a, b)
