@@ -26,3 +26,4 @@ from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, so
                      assemble_adjoint_residual, viscosity_sensitivity, solve_adjoint)
 from . import autodiff  # noqa: E402,F401
 from .autodiff import DRCheckpoint, solve_log_viscosity  # noqa: E402,F401
+from . import warmstart  # noqa: E402,F401

@@ -141,6 +141,22 @@ SIGNATURES = {
                                                        _vp * 3, _vp, _vp]),
     "femb200_solve_stokes_adjoint": (C.c_int, [_vp, _P(StokesProblemC), _P(StokesControlsC), _vp * 3, _vp * 3, _vp,
                                                _P(StokesStatsC)]),
+    "femb200_conv3x3_forward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_int32, C.c_int32]),
+    "femb200_conv3x3_weight_grad": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                              C.c_int32]),
+    "femb200_conv3x3_flip_weights": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_int32]),
+    "femb200_mse_loss_grad": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_double, _vp, C.c_int64,
+                                        _P(C.c_double)]),
+    "femb200_adam_step": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_int64]),
+    "femb200_f32_to_bf16": (C.c_int, [_vp, _vp, _vp, C.c_int64]),
+    "femb200_q9_grid_fields": (C.c_int, [_vp, _P(StokesProblemC), _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_double,
+                                         C.c_double, _vp]),
+    "femb200_net_input": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64]),
+    "femb200_net_target": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64]),
+    "femb200_apply_warm_start": (C.c_int, [_vp, _P(StokesProblemC), _vp * 2, _vp * 2, _vp, _vp, _vp, C.c_int32,
+                                           _P(C.c_float)]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

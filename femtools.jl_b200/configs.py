@@ -264,3 +264,34 @@ def adjoint_case(n=4, seed=0, eta_b=10.0, alpha=0.1):
                       P0=np.zeros(mesh.nnodesP), T=T, T0=T.copy(), tau_old=[np.zeros(nq * nels) for _ in range(6)],
                       bc=bc)
     return AdjointCase(case, T_ip, delta, top, v_target)
+
+
+def shear_band_2d_case(n=256, seed=0, dt=0.1, eta_reg=1.0, Kb=10.0, bulk=10.0):
+    """2-D plane-strain Q9/P1-disc visco-elasto-plastic shear-band experiment on the unit
+    square, n² cells: matrix η = 1e2 with a seeded weak inclusion of radius 0.02 and
+    η = 1 (position uniform in [0.4, 0.6]²), G = 1, cohesion 0.5, ϕ = 30°, ψ = 0,
+    simple-shear boundary velocities vx = y − ½, vy = 0 on all walls.
+
+    Fixed here (the configuration leaves them open): Δt = 0.1, Kb = ηb = K = 10 (the
+    3-D layered case's values) and the Perzyna viscosity η_reg = 1: the reference's
+    shear-band example notes that values well below it diverge the DR iteration on
+    fine meshes (examples/miniapps/stokes/vevp/stokes_2D_shear_bands_triangle.jl:42-44),
+    and 1e-2 does so here once the first points yield."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0.4, 0.6, size=2)
+    mesh = fem.structured_mixed_mesh(2, (n, n))
+    c = fem.mesh.cell_centroids(mesh)
+    phase = np.where(np.hypot(c[:, 0] - cx, c[:, 1] - cy) < 0.02, 2, 1).astype(np.int32)
+    mat = fem.StokesMaterial(eta=(1e2, 1.0), eta_b=(bulk, bulk), G=(1.0, 1.0), alpha=(0.0, 0.0), rho0=(1.0, 1.0),
+                             K=(bulk, bulk), g=(0.0, 0.0), Tref=0.0)
+    pl = fem.DruckerPrager.from_angles((math.radians(30),) * 2, (0.0,) * 2, (0.5, 0.5), (eta_reg,) * 2, (Kb,) * 2)
+    x, y = mesh.coords.T
+    b = mesh.boundary_nodes
+    fields = [y - 0.5, np.zeros_like(y)]
+    bc = [(b, f[b - 1].copy()) for f in fields]
+    case = StokesCase(mesh, mat, pl, dt, phases_v=phase, phases_v_layout=abi.PHASE_CELL, phases_P=phase,
+                      phases_P_layout=abi.PHASE_CELL, v=[f.copy() for f in fields], P=np.zeros(mesh.nnodesP),
+                      P0=np.zeros(mesh.nnodesP), T=np.zeros(mesh.nnodesP), T0=np.zeros(mesh.nnodesP),
+                      tau_old=[np.zeros(mesh.nq * mesh.nels) for _ in range(3)], bc=bc)
+    case.meta = dict(center=(cx, cy))
+    return case

@@ -1569,6 +1569,109 @@ int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p, con
     return finish_solve(h, c, st);
 }
 
+int femb200_conv3x3_forward(femb200_handle* h, const void* in, const void* wt, const float* bias, const void* mask,
+                            void* out, int32_t batch, int32_t height, int32_t width, int32_t ci, int32_t co,
+                            int32_t mode) {
+    if (!h) return FEMB200_EINVAL;
+    if ((ci != 16 && ci != 32) || (co != 16 && co != 32) || mode < 0 || mode > 2) {
+        h->err = "conv3x3: ci and co must be 16 or 32, mode 0, 1 or 2"; return FEMB200_EUNSUPPORTED;
+    }
+    if (!in || !wt || !out || (mode != 2 && !bias) || (mode == 2 && !mask) || batch < 1 || height < 1 || width < 1) {
+        h->err = "conv3x3: missing array or empty grid"; return FEMB200_EINVAL;
+    }
+    CK(launch_conv3x3(ci, co, mode, in, wt, bias, mask, out, batch, height, width, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_conv3x3_weight_grad(femb200_handle* h, const void* in, const void* dy, float* dw, float* db, int32_t batch,
+                                int32_t height, int32_t width, int32_t ci, int32_t co) {
+    if (!h) return FEMB200_EINVAL;
+    if ((ci != 16 && ci != 32) || (co != 16 && co != 32)) { h->err = "conv3x3: ci and co must be 16 or 32"; return FEMB200_EUNSUPPORTED; }
+    if (!in || !dy || !dw || batch < 1 || height < 1 || width < 1) { h->err = "conv3x3: missing array or empty grid"; return FEMB200_EINVAL; }
+    CK(launch_conv3x3_wgrad(ci, co, in, dy, dw, db, batch, height, width, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_conv3x3_flip_weights(femb200_handle* h, const void* w, void* wT, int32_t ci, int32_t co) {
+    if (!h) return FEMB200_EINVAL;
+    if ((ci != 16 && ci != 32) || (co != 16 && co != 32) || !w || !wT) { h->err = "conv3x3: bad flip arguments"; return FEMB200_EINVAL; }
+    CK(launch_flip_weights(w, wT, ci, co, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_mse_loss_grad(femb200_handle* h, const float* out, const float* target, int32_t nt, int32_t co, double scale,
+                          void* dy, int64_t npix, double* loss) {
+    if (!h) return FEMB200_EINVAL;
+    if (!out || !target || !dy || nt < 1 || nt > co || npix < 1) { h->err = "mse: bad arguments"; return FEMB200_EINVAL; }
+    const int blocks = red_blocks(h, npix * co);
+    RC(ensure_partials(h, blocks));
+    CK(launch_mse(out, target, nt, co, (float)scale, dy, npix, h->d_partials, blocks, h->stream));
+    if (loss) {
+        double s;
+        RC(fetch_sums(h, blocks, 1, &s));
+        *loss = scale * s;
+    }
+    return FEMB200_OK;
+}
+
+int femb200_adam_step(femb200_handle* h, float* w, float* m, float* v, const float* g, void* w_bf16, int64_t n, double lr,
+                      double beta1, double beta2, double eps, int64_t step) {
+    if (!h) return FEMB200_EINVAL;
+    if (!w || !m || !v || !g || n < 1 || step < 1) { h->err = "adam: bad arguments"; return FEMB200_EINVAL; }
+    CK(launch_adam(w, m, v, g, w_bf16, n, (float)lr, (float)beta1, (float)beta2, (float)eps, step, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_f32_to_bf16(femb200_handle* h, const float* x, void* y, int64_t n) {
+    if (!h) return FEMB200_EINVAL;
+    if (!x || !y || n < 0) { h->err = "f32_to_bf16: bad arguments"; return FEMB200_EINVAL; }
+    if (n) CK(launch_f32_to_bf16(x, y, n, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_q9_grid_fields(femb200_handle* h, const femb200_stokes_problem* p, const int32_t* node_elem,
+                           const int8_t* node_xi, const int8_t* node_eta, int32_t nx, int32_t ny, double dx, double dy,
+                           float* out) {
+    RC(check_problem(h, p));
+    if (p->dim != 2 || p->dtype != FEMB200_F64) { h->err = "grid fields: 2-D Q9 FP64 states only"; return FEMB200_EUNSUPPORTED; }
+    if ((int64_t)nx * ny != p->nnodes || !node_elem || !node_xi || !node_eta || !out) { h->err = "grid fields: the grid must cover the nodes"; return FEMB200_EINVAL; }
+    CK(launch_grid_fields<double>(static_cast<const double*>(p->v[0]), static_cast<const double*>(p->v[1]),
+                                  static_cast<const double*>(p->P), p->dofsP, node_elem, node_xi, node_eta, nx, ny,
+                                  (float)dx, (float)dy, out, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_net_input(femb200_handle* h, const float* Fprev, const float* Fcur, const float* scale, void* X, int64_t npix) {
+    if (!h) return FEMB200_EINVAL;
+    if (!Fprev || !Fcur || !scale || !X || npix < 1) { h->err = "net input: bad arguments"; return FEMB200_EINVAL; }
+    CK(launch_net_input(Fprev, Fcur, scale, X, npix, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_net_target(femb200_handle* h, const float* Fprev, const float* Fcur, const float* Fnext, const float* scale,
+                       float* target, int64_t npix) {
+    if (!h) return FEMB200_EINVAL;
+    if (!Fprev || !Fcur || !Fnext || !scale || !target || npix < 1) { h->err = "net target: bad arguments"; return FEMB200_EINVAL; }
+    CK(launch_net_target(Fprev, Fcur, Fnext, scale, target, npix, h->stream));
+    return FEMB200_OK;
+}
+
+int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[2],
+                             const void* const vcur[2], const void* Pprev, const void* Pcur, const float* out,
+                             int32_t co, const float scale[3]) {
+    RC(check_problem(h, p));
+    if (p->dim != 2 || p->dtype != FEMB200_F64 || p->np != 3) { h->err = "warm start: 2-D Q9/P1-disc FP64 states only"; return FEMB200_EUNSUPPORTED; }
+    if (!vprev || !vcur || !Pprev || !Pcur || (out && (!scale || co < 3))) { h->err = "warm start: bad arguments"; return FEMB200_EINVAL; }
+    RC(build_mask(h, p));
+    const double* vp[2] = {static_cast<const double*>(vprev[0]), static_cast<const double*>(vprev[1])};
+    const double* vc[2] = {static_cast<const double*>(vcur[0]), static_cast<const double*>(vcur[1])};
+    double* v[2] = {static_cast<double*>(p->v[0]), static_cast<double*>(p->v[1])};
+    CK(launch_apply_guess<double>(vp, vc, static_cast<const double*>(Pprev), static_cast<const double*>(Pcur), out, co,
+                                  scale, h->d_mask, v, static_cast<double*>(p->P), p->dofsP, p->el2n, p->nnodes, p->nels,
+                                  h->stream));
+    return FEMB200_OK;
+}
+
 int femb200_stokes_adjoint_residual(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K,
                                     int32_t with_pnum, const void* const lam_v[3], const void* lam_P,
                                     void* const out_dv[3], void* out_dP) {

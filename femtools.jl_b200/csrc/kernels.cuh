@@ -151,6 +151,29 @@ struct AdjArgs {
 template <class T>
 cudaError_t launch_hex27_adjoint(const AdjArgs<T>& args, int num_sms, cudaStream_t st);
 
+// ---- learned warm start (conv_bf16.cu, warmstart_fields.cu) ----
+cudaError_t launch_conv3x3(int ci, int co, int mode, const void* in, const void* wt, const float* bias,
+                           const void* mask, void* out, int B, int H, int W, cudaStream_t st);
+cudaError_t launch_conv3x3_wgrad(int ci, int co, const void* x, const void* dy, float* dw, float* db, int B, int H, int W,
+                                 int num_sms, cudaStream_t st);
+cudaError_t launch_flip_weights(const void* w, void* wT, int ci, int co, cudaStream_t st);
+cudaError_t launch_mse(const float* out, const float* target, int nt, int co, float scale, void* dy, int64_t npix,
+                       double* partials, int blocks, cudaStream_t st);
+cudaError_t launch_adam(float* w, float* m, float* v, const float* g, void* wb, int64_t n, float lr, float b1, float b2,
+                        float eps, int64_t step, cudaStream_t st);
+cudaError_t launch_f32_to_bf16(const float* x, void* y, int64_t n, cudaStream_t st);
+template <class T>
+cudaError_t launch_grid_fields(const T* vx, const T* vy, const T* P, const int32_t* dofsP, const int32_t* node_elem,
+                               const int8_t* node_xi, const int8_t* node_eta, int nx, int ny, float dx, float dy,
+                               float* out, cudaStream_t st);
+cudaError_t launch_net_input(const float* Fp, const float* Fc, const float* s, void* X, int64_t npix, cudaStream_t st);
+cudaError_t launch_net_target(const float* Fp, const float* Fc, const float* Fn, const float* s, float* tgt, int64_t npix,
+                              cudaStream_t st);
+template <class T>
+cudaError_t launch_apply_guess(const T* vprev[2], const T* vcur[2], const T* Pprev, const T* Pcur, const float* out, int co,
+                               const float* s, const uint8_t* mask, T* v[2], T* P, const int32_t* dofsP,
+                               const int32_t* el2n, int64_t nnodes, int64_t nels, cudaStream_t st);
+
 // Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
 template <class T, class TG>
 struct H27JacArgs {

@@ -334,6 +334,56 @@ int femb200_solve_stokes_adjoint(femb200_handle* h, const femb200_stokes_problem
                                  const femb200_stokes_controls* c, const void* const objective_v[3],
                                  void* const lam_v[3], void* lam_P, femb200_stokes_stats* stats);
 
+/* ---- learned warm start (no reference counterpart: FEMTools.jl has no learned
+ * component) --------------------------------------------------------------------
+ * A convolutional network over the node grid of a structured 2-D Q9/P1-disc mesh
+ * predicts the next time step's correction to linear extrapolation of (vx, vy, P);
+ * its BF16 tensor-core kernels (FP32 accumulation) and the field transfers are
+ * below. Activations are NHWC BF16 with 16 or 32 channels; weights are
+ * [co][9·ci + 8] (k = (3·ky + kx)·ci + c, eight padding entries per row). */
+
+/* 3×3 same-padded convolution (zero outside the grid), ci, co ∈ {16, 32}.
+ * mode 0: out = ReLU(conv + bias) as BF16; 1: out = conv + bias as FP32;
+ * 2: out = conv where mask > 0, else 0, as BF16 (the data gradient through a ReLU:
+ *    in = the output gradient, wt = the flipped weights, mask = the layer input). */
+int femb200_conv3x3_forward(femb200_handle* h, const void* in, const void* wt, const float* bias,
+                            const void* mask, void* out, int32_t batch, int32_t height, int32_t width,
+                            int32_t ci, int32_t co, int32_t mode);
+/* dw[co][k] += Σ_pixels patch(in)[k]·dy[co] (FP32), db[co] += Σ dy[co] (db may be NULL). */
+int femb200_conv3x3_weight_grad(femb200_handle* h, const void* in, const void* dy, float* dw, float* db,
+                                int32_t batch, int32_t height, int32_t width, int32_t ci, int32_t co);
+/* The data-gradient weights: wT[c][(8 − tap)·co + o] = w[o][tap·ci + c], [ci][9·co + 8]. */
+int femb200_conv3x3_flip_weights(femb200_handle* h, const void* w, void* wT, int32_t ci, int32_t co);
+/* loss = scale·Σ (out[:, :nt] − target)² (out FP32 with co channels, target FP32 with nt);
+ * dy = its gradient in out as BF16 (co channels). loss: host pointer or NULL. */
+int femb200_mse_loss_grad(femb200_handle* h, const float* out, const float* target, int32_t nt, int32_t co,
+                          double scale, void* dy, int64_t npix, double* loss);
+/* One Adam step (Kingma & Ba, 2015) on FP32 parameters, writing a BF16 copy when
+ * w_bf16 is not NULL; step counts from 1. */
+int femb200_adam_step(femb200_handle* h, float* w, float* m, float* v, const float* g, void* w_bf16,
+                      int64_t n, double lr, double beta1, double beta2, double eps, int64_t step);
+int femb200_f32_to_bf16(femb200_handle* h, const float* x, void* y, int64_t n);
+/* (vx, vy, P, ε̇II) of a 2-D Q9 FP64 state on its (2n+1)² node grid, FP32 (npix × 4):
+ * P from the owning element's linear pressure at the node's (ξ, η), ε̇II of the
+ * plane-strain deviatoric strain rate by central differences. */
+int femb200_q9_grid_fields(femb200_handle* h, const femb200_stokes_problem* p, const int32_t* node_elem,
+                           const int8_t* node_xi, const int8_t* node_eta, int32_t nx, int32_t ny, double dx,
+                           double dy, float* out);
+/* Network input of two consecutive grid states (BF16, 16 channels: F_cur and
+ * F_cur − F_prev, divided by the 8 device-side scales; 8 unused) and the training target (F_next − (2 F_cur − F_prev))
+ * of vx, vy, P divided by 3 device-side scales. */
+int femb200_net_input(femb200_handle* h, const float* Fprev, const float* Fcur, const float* scale, void* X,
+                      int64_t npix);
+int femb200_net_target(femb200_handle* h, const float* Fprev, const float* Fcur, const float* Fnext,
+                       const float* scale, float* target, int64_t npix);
+/* Initial guess of the next step: v = 2 v_cur − v_prev (+ scale·out) on the nodes that
+ * p's Dirichlet sets leave free, P = 2 P_cur − P_prev (+ scale·out at the node of each
+ * P1-disc DoF). out: the network's FP32 output (co channels) or NULL; scale: 3 host
+ * floats. Writes p->v and p->P. */
+int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[2],
+                             const void* const vcur[2], const void* Pprev, const void* Pcur, const float* out,
+                             int32_t co, const float scale[3]);
+
 /* ---- thermal diffusion ---------------------------------------------------- */
 
 /* assemble_diffusion_matrices_atomix! (src/heat_diffusion/assembly/residual_atomics.jl:10)
