@@ -66,19 +66,22 @@ def mesh_is_affine(mesh, tol=1e-12):
 
 
 def incremental_kernel_bytes(case):
-    """Algorithmic bytes of one FP32 incremental sweep of the mixed-precision solve:
-    δv, connectivity, the FP32 affine geometry, δP with the base RP, γP and M_P,
-    the cell phase, the base trial stress and yield value of every integration
-    point (7 × 27 FP32), RP written and the Rv read-modify-write (FP32)."""
+    """Algorithmic bytes of one FP32 incremental sweep of the mixed-precision solve
+    (hex27_incr_kernel): δv, the tiled connectivity, FP32 affine geometry, the two
+    element phases, δP, the Pnum scale γP/M_P of the element's DoFs, the base trial
+    stress and yield value of every integration point (7 × 27 FP32), the RP increment
+    written and the Rv read-modify-write (FP32). The pressure DoFs are numbered 4e + p
+    on the structured mesh, so no DoF table is read."""
     m = case.mesh
     nels, nn, nP = m.nels, m.nnodes, m.nnodesP
     b = 3 * nn * 4                         # δv
-    b += 27 * 4 * nels + 4 * 4 * nels      # el2n, dofsP
+    b += 27 * 4 * nels                     # el2n (tiled)
     b += 10 * 4 * nels                     # J⁻¹ and |det J| per element
-    b += 4 * nP * 4                        # δP, RP_base, γP, M_P
-    b += 4 * nels                          # cell phase
+    b += 2 * 4 * nels                      # phases of the velocity nodes and of the pressure DoFs
+    b += nP * 4                            # δP
+    b += 4 * 4 * nels                      # γP/M_P
     b += 7 * 27 * 4 * nels                 # base trial stress and yield value
-    b += nP * 4                            # RP written
+    b += nP * 4                            # RP increment written
     b += 2 * 3 * nn * 4                    # Rv atomic read-modify-write
     return b
 
@@ -534,7 +537,7 @@ def main():
                        "itPH": plain["itPH"] if plain else st["itPH"]},
                       open(os.path.join(ROOT, "profiles", "bench_path.json"), "w"))
         if mixed:
-            kernel = "hex27_residual_pipe_kernel<float, incremental> (FP32 incremental sweep: RP, Pnum, Rv increments)"
+            kernel = "hex27_incr_kernel (thread-per-element FP32 incremental sweep: RP, Pnum, Rv increments)"
         elif mesh_is_affine(case.mesh):
             kernel = "hex27_residual_pipe_kernel<double> (fused RP + Pnum + Rv sweep, affine geometry)"
         else:
