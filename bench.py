@@ -308,6 +308,36 @@ def adjoint_mode(args, fem):
     return 0
 
 
+def warmstart_mode(args, fem):
+    """Learned-warm-start workload (2-D Q9/P1-disc shear band, n², `--ws-steps` steps,
+    trained on the first `--ws-train`): DR iterations and time to the tolerance per step
+    from the plain start, from linear extrapolation and from extrapolation + the network,
+    each over the same states. Prints one JSON line."""
+    import torch
+    rows_out = []
+    res = fem.warmstart.shear_band_warm_start(n=args.n, nsteps=args.ws_steps, ntrain=args.ws_train,
+                                              epochs=args.ws_epochs, seed=args.seed, tolerance=args.tolerance,
+                                              log=(lambda r: rows_out.append(r)))
+    test = [r for r in res["rows"] if "learned_iter" in r]
+    mean = lambda k: float(np.mean([r[k] for r in test])) if test else None
+    tot = lambda k: float(np.sum([r[k] for r in test])) if test else None
+    line = {
+        "mode": "warmstart", "workload": f"shear-band-q9-{args.n}^2", "n": args.n, "steps": args.ws_steps,
+        "train_steps": args.ws_train, "epochs": args.ws_epochs, "train_ms": res["train_ms"],
+        "train_loss_first_last": [res["train_loss"][0], res["train_loss"][-1]] if res["train_loss"] else None,
+        "gain": res["gain"], "test_steps": len(test),
+        "iterations_mean": {"plain": mean("plain_iter"), "extrapolation": mean("extrap_iter"),
+                            "learned": mean("learned_iter")},
+        "time_ms_total": {"plain": tot("plain_ms"), "extrapolation": tot("extrap_ms"), "learned": tot("learned_ms")},
+        "inference_ms_mean": mean("infer_ms"),
+        "learned_vs_plain_max_rel": max(r["learned_vs_plain_rel"] for r in test) if test else None,
+        "all_converged": all(r["plain_converged"] for r in res["rows"]) and all(r["learned_converged"] for r in test),
+        "per_step": [{k: r.get(k) for k in ("step", "plain_iter", "extrap_iter", "learned_iter")} for r in test],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -356,7 +386,10 @@ def main():
     ap.add_argument("--fd-elements", type=int, default=20)
     ap.add_argument("--fd-h", default="1e-6,1e-4", help="central-difference steps, comma-separated")
     ap.add_argument("--fd-tolerance", type=float, default=1e-13)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint"],
+    ap.add_argument("--ws-steps", type=int, default=200)
+    ap.add_argument("--ws-train", type=int, default=50)
+    ap.add_argument("--ws-epochs", type=int, default=300)
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -390,6 +423,8 @@ def main():
 
     if args.mode == "adjoint":
         return adjoint_mode(args, fem)
+    if args.mode == "warmstart":
+        return warmstart_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()
