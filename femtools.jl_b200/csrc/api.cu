@@ -980,6 +980,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     }
     const bool thread_sweep = (*h->h_flag & INCR_MIXED_PHASES) == 0 && h->use_incr_thread;
     at.dofs_linear = (*h->h_flag & INCR_DOFS_GENERAL) == 0;
+    at.diag_geometry = (*h->h_flag & INCR_GEOMETRY_FULL) == 0;
     // the thread-per-element sweep writes the increment of RP; RP itself is formed
     // where it is read (checks and the Powell–Hestenes pressure update)
     auto form_RP = [&]() -> int {
@@ -1016,8 +1017,15 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
         ++base_sweeps;
         return FEMB200_OK;
     };
+    // x_k += δ, then the Dirichlet values on v (DR.jl:697): δ is pinned to zero on the
+    // constrained DoFs, so the base state carries the boundary values from here on
     auto fold = [&]() -> int {
-        for (int k = 0; k < D; ++k) CK(launch_fold(static_cast<T*>(p->v[k]), m.dv[k], nn, s));
+        for (int k = 0; k < D; ++k) {
+            CK(launch_fold(static_cast<T*>(p->v[k]), m.dv[k], nn, s));
+            if (p->bc_n[k] > 0)
+                CK(launch_dirichlet<T>(static_cast<T*>(p->v[k]), p->bc_dofs[k], static_cast<const T*>(p->bc_vals[k]),
+                                       p->bc_n[k], s));
+        }
         CK(launch_fold(static_cast<T*>(p->P), m.dP, nP, s));
         return FEMB200_OK;
     };

@@ -94,6 +94,7 @@ struct IncrArgs {
     float* RPinc;            // increment of the pressure residual at the DoFs
     int64_t nels;
     int dofs_linear;         // the pressure DoFs of element e are 4e … 4e+3 (dofs_t not read)
+    int diag_geometry;       // every element's J⁻¹ is diagonal
     int plastic;
     float g[3];
     IncrPhase ph[MAXPH];
@@ -101,9 +102,10 @@ struct IncrArgs {
 // Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
 // copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.
 // Sets bit INCR_MIXED_PHASES of *flags when some element's nodes or DoFs carry
-// more than one phase (the thread-per-element sweep then does not apply) and
-// INCR_DOFS_GENERAL when the pressure DoFs are not numbered 4e + p.
-enum { INCR_MIXED_PHASES = 1, INCR_DOFS_GENERAL = 2 };
+// more than one phase (the thread-per-element sweep then does not apply),
+// INCR_DOFS_GENERAL when the pressure DoFs are not numbered 4e + p and
+// INCR_GEOMETRY_FULL when some element's J⁻¹ has an off-diagonal entry.
+enum { INCR_MIXED_PHASES = 1, INCR_DOFS_GENERAL = 2, INCR_GEOMETRY_FULL = 4 };
 struct IncrTileSrc {
     const int32_t* el2n;
     const int32_t* dofsP;

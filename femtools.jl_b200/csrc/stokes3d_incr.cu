@@ -112,7 +112,13 @@ __global__ void incr_tiles_kernel(const IncrTileSrc src, int64_t nels, int64_t n
         pscale_t[(tile * 4 + p) * 32 + lane] = act ? src.gP[d] / src.MP[d] : 0.0f;
     }
     if (!linear) atomicOr(flags, INCR_DOFS_GENERAL);
-    for (int r = 0; r < 10; ++r) geo_t[(tile * 10 + r) * 32 + lane] = act ? src.geo_c[10 * e + r] : 0.0f;
+    bool offdiag = false;
+    for (int r = 0; r < 10; ++r) {
+        const float gv = act ? src.geo_c[10 * e + r] : 0.0f;
+        offdiag = offdiag || (r < 9 && r % 4 != 0 && gv != 0.0f);
+        geo_t[(tile * 10 + r) * 32 + lane] = gv;
+    }
+    if (offdiag) atomicOr(flags, INCR_GEOMETRY_FULL);
     if (src.eta) {
         float* eta_t = const_cast<float*>(dst.eta_t);
         for (int q = 0; q < 27; ++q) eta_t[(tile * 27 + q) * 32 + lane] = act ? src.eta[27 * e + q] : 1.0f;
@@ -178,11 +184,12 @@ FEMB_D int elem_dof(const IncrArgs& a, int64_t tile, int lane, int p) {
     return a.dofs_linear ? (int)(4 * (tile * 32 + lane) + p) : __ldg(a.dofs_t + (tile * 4 + p) * 32 + lane);
 }
 
+template <bool DIAG>
 FEMB_D void load_elem(const IncrArgs& a, int64_t tile, int lane, int64_t nslots, ElemData& d) {
     const int64_t e = tile * 32 + lane;
     const float* gt = a.geo_t + tile * 10 * 32 + lane;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) d.Ji[r] = __ldg(gt + r * 32);
+    for (int r = 0; r < 9; ++r) d.Ji[r] = (!DIAG || r % 4 == 0) ? __ldg(gt + r * 32) : 0.0f;
     d.detJ = __ldg(gt + 9 * 32);   // 0 on padding lanes
 #pragma unroll
     for (int p = 0; p < 4; ++p) d.dP[p] = __ldg(a.dP + elem_dof(a, tile, lane, p));
@@ -190,6 +197,9 @@ FEMB_D void load_elem(const IncrArgs& a, int64_t tile, int lane, int64_t nslots,
     d.phP = __ldg(a.phase_t + nslots + e);
 }
 
+// DIAG: every element's J⁻¹ is diagonal (axis-aligned boxes, the structured
+// generators' meshes), so the gradient and flux transforms are one product per entry.
+template <bool DIAG>
 __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArgs a) {
     extern __shared__ float in_smem[];
     __shared__ IncrPhase PT[MAXPH];
@@ -227,7 +237,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     float pre[3 * BASE_FIELDS];
     if (plastic) load_row(pre, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane);
     ElemData cur;
-    load_elem(a, tile, lane, nslots, cur);
+    load_elem<DIAG>(a, tile, lane, nslots, cur);
 
     for (; tile < ntiles; tile += tstride) {
         const int64_t e = tile * 32 + lane;
@@ -342,7 +352,8 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                     for (int c = 0; c < 3; ++c)
 #pragma unroll
                         for (int k = 0; k < 3; ++k)
-                            gq[c][k] = fmaf(gr[c][0], cur.Ji[3 * k], fmaf(gr[c][1], cur.Ji[1 + 3 * k], gr[c][2] * cur.Ji[2 + 3 * k]));
+                            gq[c][k] = DIAG ? gr[c][k] * cur.Ji[4 * k]
+                                            : fmaf(gr[c][0], cur.Ji[3 * k], fmaf(gr[c][1], cur.Ji[1 + 3 * k], gr[c][2] * cur.Ji[2 + 3 * k]));
                     const float div = gq[0][0] + gq[1][1] + gq[2][2];
                     const float xi = gx(qx);
                     const float NP0 = 1.0f - xi - et - ze;
@@ -407,7 +418,8 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                         float F[3];
 #pragma unroll
                         for (int d = 0; d < 3; ++d)
-                            F[d] = dO * fmaf(cur.Ji[d], sg[0][c], fmaf(cur.Ji[d + 3], sg[1][c], cur.Ji[d + 6] * sg[2][c]));
+                            F[d] = DIAG ? dO * cur.Ji[4 * d] * sg[d][c]
+                                        : dO * fmaf(cur.Ji[d], sg[0][c], fmaf(cur.Ji[d + 3], sg[1][c], cur.Ji[d + 6] * sg[2][c]));
 #pragma unroll
                         for (int i = 0; i < 3; ++i) {
                             A[c][i] = cfma(Ld(qx, i), F[0], A[c][i]);
@@ -453,7 +465,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         const float Ji[9] = {cur.Ji[0], cur.Ji[1], cur.Ji[2], cur.Ji[3], cur.Ji[4], cur.Ji[5], cur.Ji[6], cur.Ji[7], cur.Ji[8]};
         const float detJ = cur.detJ;
         // the next tile's element data, in flight during the scatter
-        if (has_next) load_elem(a, tnext, lane, nslots, cur);
+        if (has_next) load_elem<DIAG>(a, tnext, lane, nslots, cur);
         // ---- scatter, with the Pnum term −|det J| Σ_d ∂ξ_d/∂x_c Σ_p Pn_p K[p][d][a] ----
         const int32_t* nd = a.el2n_t + tile * 27 * 32 + lane;
 #pragma unroll 3
@@ -465,7 +477,8 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
             const int n = __ldg(nd + t * 32);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const float val = RS[(c * 27 + t) * 32] - detJ * fmaf(Ji[3 * c], S[0], fmaf(Ji[3 * c + 1], S[1], Ji[3 * c + 2] * S[2]));
+                const float val = RS[(c * 27 + t) * 32] -
+                                  detJ * (DIAG ? Ji[4 * c] * S[c] : fmaf(Ji[3 * c], S[0], fmaf(Ji[3 * c + 1], S[1], Ji[3 * c + 2] * S[2])));
                 if (act) atomicAdd(a.R[c] + n, val);
             }
         }
@@ -492,7 +505,10 @@ cudaError_t launch_incr_tiles(const IncrTileSrc& src, int64_t nels, const IncrAr
             host_pnum_table(K);
             err = cudaMemcpyToSymbol(c_inc_K, K, sizeof(K));
             if (err != cudaSuccess) return err;
-            err = cudaFuncSetAttribute(hex27_incr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            err = cudaFuncSetAttribute(hex27_incr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
+            if (err != cudaSuccess) return err;
+            err = cudaFuncSetAttribute(hex27_incr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
             if (err != cudaSuccess) return err;
             g_inc_ready[dev] = true;
@@ -522,13 +538,15 @@ cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
     const size_t smem = (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float);
     const int64_t ntiles = (a.nels + 31) / 32;
     int per_sm = 2;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel, IN_THREADS, smem);
+    if (a.diag_geometry) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel<true>, IN_THREADS, smem);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel<false>, IN_THREADS, smem);
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (ntiles + IN_WARPS - 1) / IN_WARPS;
     blocks = std::min<int64_t>(blocks, (int64_t)num_sms * per_sm);
     if (blocks < 1) blocks = 1;
     count_launch();
-    hex27_incr_kernel<<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
+    if (a.diag_geometry) hex27_incr_kernel<true><<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
+    else hex27_incr_kernel<false><<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -105,8 +105,7 @@ class WarmStartNet:
             self.layers.append(L)
         self.lr = lr
         self.step = 0
-        self.in_scale = torch.ones(8, device=dev)
-        self.out_scale = torch.ones(3, device=dev)
+        self.field_scale = torch.ones(4, device=dev)
         self.gain = 1.0
         self._sync_bf16()
 
@@ -177,29 +176,38 @@ class WarmStartNet:
         return loss.value, dy
 
     # ---- data of the time loop ----
+    # The fields are scaled by their spread over the training history; the step change
+    # F_t − F_{t−1} and the target (the next step's correction to linear
+    # extrapolation) by the RMS of the current step change, per field, so that the
+    # network predicts a dimensionless correction and its output shrinks with the
+    # dynamics of the step it is applied to.
+    @staticmethod
+    def step_rms(Fp, Fc):
+        return (Fc - Fp).pow(2).mean(dim=0).sqrt().clamp_min(1e-30).float()
+
     def make_input(self, Fp, Fc):
         lib, h = _lib()
         npix = Fp.shape[0]
         X = torch.empty(npix * IN_CH, dtype=torch.bfloat16, device=Fp.device)
-        _check(lib.femb200_net_input(h, _p(Fp), _p(Fc), _p(self.in_scale), _p(X), npix))
+        scale = torch.cat([self.field_scale, self.step_rms(Fp, Fc)]).contiguous()
+        _check(lib.femb200_net_input(h, _p(Fp), _p(Fc), _p(scale), _p(X), npix))
         return X
 
     def make_target(self, Fp, Fc, Fn):
         lib, h = _lib()
         npix = Fp.shape[0]
         T = torch.empty(npix * N_TARGET, dtype=torch.float32, device=Fp.device)
-        _check(lib.femb200_net_target(h, _p(Fp), _p(Fc), _p(Fn), _p(self.out_scale), _p(T), npix))
+        scale = self.step_rms(Fp, Fc)[:N_TARGET].contiguous()
+        _check(lib.femb200_net_target(h, _p(Fp), _p(Fc), _p(Fn), _p(scale), _p(T), npix))
         return T
 
+    def output_scale(self, Fp, Fc):
+        """Host scales of the network's output channels for the step (Fp, Fc), gain included."""
+        return [self.gain * float(x) for x in self.step_rms(Fp, Fc)[:N_TARGET].cpu()]
+
     def fit_scales(self, F):
-        """Input scales: the spread of each field and of its step-to-step change over
-        the history; output scales: the spread of the extrapolation corrections."""
         stack = torch.stack(F)                            # steps × npix × 4
-        s = stack.std(dim=(0, 1)).clamp_min(1e-12)
-        d = (stack[1:] - stack[:-1]).std(dim=(0, 1)).clamp_min(1e-12)
-        self.in_scale = torch.cat([s, d]).float().contiguous()
-        corr = torch.stack([F[t + 1][:, :3] - (2 * F[t][:, :3] - F[t - 1][:, :3]) for t in range(1, len(F) - 1)])
-        self.out_scale = corr.std(dim=(0, 1)).clamp_min(1e-12).float().contiguous()
+        self.field_scale = stack.std(dim=(0, 1)).clamp_min(1e-12).float().contiguous()
 
     def train(self, F, H, W, epochs=200, batch=8, seed=0):
         """Fit on the history F[0..n−1] of grid fields: inputs (F[t−1], F[t]), targets the
@@ -308,8 +316,7 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record()
             out = net.predict(F[-2], F[-1], H, W)
-            apply_guess(dr, bc, hist_v[-2], hist_v[-1], hist_P[-2], hist_P[-1], out,
-                        [net.gain * x for x in net.out_scale.cpu().tolist()])
+            apply_guess(dr, bc, hist_v[-2], hist_v[-1], hist_P[-2], hist_P[-1], out, net.output_scale(F[-2], F[-1]))
             e1 = torch.cuda.Event(enable_timing=True)
             e1.record()
             st, ms = timed_solve()

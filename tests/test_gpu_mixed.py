@@ -101,3 +101,13 @@ def test_mixed_solve_phase_layouts(layout):
     assert st64["converged"] and stm["converged"] and stm["err"] < 1e-8
     for k in ("v", "P", "tau"):
         assert rel_l2(fm[k], f64[k]) < 1e-6, (layout, k, rel_l2(fm[k], f64[k]))
+
+
+def test_mixed_solve_on_sheared_affine_cells():
+    # parallelepiped cells (a full J⁻¹): the general-geometry form of the FP32 sweep
+    case = random_state_case(dim=3, n=3, seed=8, phases="cell", plastic=False, distort=False)
+    st64, f64 = solve_fields(case, 1e-8, "fp64")
+    stm, fm = solve_fields(case, 1e-8, "mixed")
+    assert st64["converged"] and stm["converged"] and stm["err"] < 1e-8
+    for k in ("v", "P"):
+        assert rel_l2(fm[k], f64[k]) < 1e-6, (k, rel_l2(fm[k], f64[k]))
