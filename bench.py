@@ -326,6 +326,7 @@ def warmstart_mode(args, fem):
         "train_steps": args.ws_train, "epochs": args.ws_epochs, "train_ms": res["train_ms"],
         "train_loss_first_last": [res["train_loss"][0], res["train_loss"][-1]] if res["train_loss"] else None,
         "gain": res["gain"], "test_steps": len(test),
+        "gain_trace": [r.get("gain") for r in test][::10],
         "iterations_mean": {"plain": mean("plain_iter"), "extrapolation": mean("extrap_iter"),
                             "learned": mean("learned_iter")},
         "time_ms_total": {"plain": tot("plain_ms"), "extrapolation": tot("extrap_ms"), "learned": tot("learned_ms")},

@@ -105,7 +105,7 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
 // Transposed contraction: nodal residual R[c][ix] on the owned x-line from the
 // reference-frame fluxes F[c][d][qz] and the body-force density beta[qz]
 // (R_c(a) = Σ_q Σ_d ∂_d N_a(q) F_cd(q) − g_c Σ_q N_a(q) β(q)).
-template <class T>
+template <class T, bool BODY = true>
 FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3], const T gvec[3], T* E,
                           int m1, int m2, T R[3][3], bool wr = true) {
     // Z^T: thread owns z-line (qx = m1, qy = m2)
@@ -122,10 +122,12 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
                 E[(c * 3 + 2) * 27 + tidx(m1, m2, iz)] = z2;
             }
         }
+    if constexpr (BODY) {
 #pragma unroll
-    for (int iz = 0; iz < 3; ++iz) {
-        const T zb = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
-        if (wr) E[9 * 27 + tidx(m1, m2, iz)] = zb;
+        for (int iz = 0; iz < 3; ++iz) {
+            const T zb = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
+            if (wr) E[9 * 27 + tidx(m1, m2, iz)] = zb;
+        }
     }
     __syncwarp();
     // Y^T: thread owns y-line (qx = m1, ·, iz = m2)
@@ -150,7 +152,7 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
             }
         }
     }
-    {
+    if constexpr (BODY) {
         T TD[3];
 #pragma unroll
         for (int qy = 0; qy < 3; ++qy) TD[qy] = E[9 * 27 + tidx(m1, qy, m2)];
@@ -162,12 +164,14 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
     }
     __syncwarp();
     // X^T: thread owns x-line (·, iy = m1, iz = m2)
-    T UD[3];
+    T body[3] = {T(0), T(0), T(0)};
+    if constexpr (BODY) {
+        T UD[3];
 #pragma unroll
-    for (int qx = 0; qx < 3; ++qx) UD[qx] = E1[6 * 27 + tidx(qx, m1, m2)];
-    T body[3];
+        for (int qx = 0; qx < 3; ++qx) UD[qx] = E1[6 * 27 + tidx(qx, m1, m2)];
 #pragma unroll
-    for (int ix = 0; ix < 3; ++ix) body[ix] = t.B[0][ix] * UD[0] + t.B[1][ix] * UD[1] + t.B[2][ix] * UD[2];
+        for (int ix = 0; ix < 3; ++ix) body[ix] = t.B[0][ix] * UD[0] + t.B[1][ix] * UD[1] + t.B[2][ix] * UD[2];
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         T UA[3], UB[3];
@@ -176,7 +180,7 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
 #pragma unroll
         for (int ix = 0; ix < 3; ++ix)
             R[c][ix] = (t.Dd[0][ix] * UA[0] + t.Dd[1][ix] * UA[1] + t.Dd[2][ix] * UA[2]) +
-                       (t.B[0][ix] * UB[0] + t.B[1][ix] * UB[1] + t.B[2][ix] * UB[2]) - gvec[c] * body[ix];
+                       (t.B[0][ix] * UB[0] + t.B[1][ix] * UB[1] + t.B[2][ix] * UB[2]) - (BODY ? gvec[c] * body[ix] : T(0));
     }
     __syncwarp();
 }

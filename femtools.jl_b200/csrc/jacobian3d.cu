@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
         h27_gradient(tb, v, E, m1, m2, g);
 
         // primal state at the owned points with η_pc
-        T pe[3], plam[3], ptt[3][6], ptII[3], ptIIs[3], pden[3];
+        // per point: ηve, λ, the trial stress and the reciprocals the 81 columns use
+        T pe[3], plam[3], ptt[3][6], pitII[3], pitIIs[3], piden[3];
 #pragma unroll
         for (int qz = 0; qz < 3; ++qz) {
             const int q = tidx(m1, m2, qz);
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
             }
             pe[qz] = etave;
             plam[qz] = T(0);
-            ptII[qz] = T(1); ptIIs[qz] = T(1); pden[qz] = T(1);
+            pitII[qz] = T(1); pitIIs[qz] = T(1); piden[qz] = T(1);
             if (plastic) {
                 T Pq = T(0), Pfq = T(0);
 #pragma unroll
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 const T Fy = tII - cphi * C - sphi * Peq;
                 const T den = etave + ereg + Kb * dt * (-spsi) * (-sphi);
                 const T lam = Fy > T(0) ? Fy / den : T(0);
-                plam[qz] = lam; ptII[qz] = tII; ptIIs[qz] = tII + EPS2; pden[qz] = den;
+                plam[qz] = lam; pitII[qz] = T(1) / tII; pitIIs[qz] = T(1) / (tII + EPS2); piden[qz] = T(1) / den;
             }
         }
 
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                     for (int d = 0; d < 3; ++d) Fp[c][d][qz] = w * Ji[d + 3 * c];
             }
             T Rp[3][3];
-            h27_transpose(tb, Fp, zero3, zero3, E, m1, m2, Rp);
+            h27_transpose<T, false>(tb, Fp, zero3, zero3, E, m1, m2, Rp);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -217,6 +218,17 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 #pragma unroll 1
         for (int b = 0; b < 27; ++b) {
             const int bx = b % 3, by = (b / 3) % 3, bz = b / 9;
+            // physical gradient of N_b at the owned points, shared by the three columns of node b
+            T dnb[3][3];
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) {
+                const T* Ji = GEO + tidx(m1, m2, qz) * 11;
+                const T rx = tb.Dd[m1][bx] * tb.B[m2][by] * tb.B[qz][bz];
+                const T ry = tb.B[m1][bx] * tb.Dd[m2][by] * tb.B[qz][bz];
+                const T rz = tb.B[m1][bx] * tb.B[m2][by] * tb.Dd[qz][bz];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) dnb[qz][k] = rx * Ji[0 + 3 * k] + ry * Ji[1 + 3 * k] + rz * Ji[2 + 3 * k];
+            }
 #pragma unroll 1
             for (int j = 0; j < 3; ++j) {
                 const int col = b * 3 + j;
@@ -226,38 +238,35 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 for (int qz = 0; qz < 3; ++qz) {
                     const int q = tidx(m1, m2, qz);
                     const T* Ji = GEO + q * 11;
-                    const T rx = tb.Dd[m1][bx] * tb.B[m2][by] * tb.B[qz][bz];
-                    const T ry = tb.B[m1][bx] * tb.Dd[m2][by] * tb.B[qz][bz];
-                    const T rz = tb.B[m1][bx] * tb.B[m2][by] * tb.Dd[qz][bz];
-                    T dn[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) dn[k] = rx * Ji[0 + 3 * k] + ry * Ji[1 + 3 * k] + rz * Ji[2 + 3 * k];
+                    const T (&dn)[3] = dnb[qz];
                     // δg[i][k] = δ_ij dn[k]
                     T dg[3][3];
 #pragma unroll
                     for (int i = 0; i < 3; ++i)
 #pragma unroll
                         for (int k = 0; k < 3; ++k) dg[i][k] = (i == j) ? dn[k] : T(0);
-                    const T tr = (dg[0][0] + dg[1][1] + dg[2][2]) / T(3);
-                    const T de[6] = {dg[0][0] - tr, dg[1][1] - tr, dg[2][2] - tr, (dg[0][1] + dg[1][0]) / T(2),
-                                     (dg[0][2] + dg[2][0]) / T(2), (dg[1][2] + dg[2][1]) / T(2)};
+                    const T tr = (dg[0][0] + dg[1][1] + dg[2][2]) * T(1.0 / 3.0);
+                    const T de[6] = {dg[0][0] - tr, dg[1][1] - tr, dg[2][2] - tr, (dg[0][1] + dg[1][0]) * T(0.5),
+                                     (dg[0][2] + dg[2][0]) * T(0.5), (dg[1][2] + dg[2][1]) * T(0.5)};
                     const T two_e = T(2) * pe[qz];
                     T dt_[6];
 #pragma unroll
                     for (int c = 0; c < 6; ++c) dt_[c] = two_e * de[c];
                     T dtau[6];
                     if (plam[qz] > T(0)) {
+                        // linearised radial return (rheology.jl:441-472) with the reciprocals
+                        // of τII, τII + ε² and the plastic denominator formed once per point
                         const T* t = ptt[qz];
-                        const T tII = ptII[qz], tIIs = ptIIs[qz];
-                        const T dtII = (t[0] * dt_[0] + t[1] * dt_[1] + t[2] * dt_[2]) / (T(2) * tII) +
-                                       (t[3] * dt_[3] + t[4] * dt_[4] + t[5] * dt_[5]) / tII;
-                        const T dlam = dtII / pden[qz];
+                        const T itII = pitII[qz], itIIs = pitIIs[qz];
+                        const T dtII = ((t[0] * dt_[0] + t[1] * dt_[1] + t[2] * dt_[2]) * T(0.5) +
+                                        (t[3] * dt_[3] + t[4] * dt_[4] + t[5] * dt_[5])) * itII;
+                        const T dlam = dtII * piden[qz];
                         const T lam = plam[qz];
 #pragma unroll
                         for (int c = 0; c < 6; ++c) {
-                            const T fac = c < 3 ? T(2) * tIIs : tIIs;
-                            const T mq = t[c] / fac;
-                            const T dm = dt_[c] / fac - t[c] * dtII / (fac * tIIs);
+                            const T ifac = c < 3 ? T(0.5) * itIIs : itIIs;
+                            const T mq = t[c] * ifac;
+                            const T dm = (dt_[c] - t[c] * dtII * itIIs) * ifac;
                             dtau[c] = dt_[c] - two_e * (dlam * mq + lam * dm);
                         }
                     } else {
@@ -276,7 +285,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                             Fd[c][d][qz] = dOq * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
                 }
                 T dR[3][3];
-                h27_transpose(tb, Fd, zero3, zero3, E, m1, m2, dR);
+                h27_transpose<T, false>(tb, Fd, zero3, zero3, E, m1, m2, dR);
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll

@@ -10,6 +10,12 @@ DR solve of each step starts from extrapolation + prediction instead of the prev
 step's solution. The plain DR iteration still runs to the same tolerance from that
 start, so the network can only change how many iterations a step takes, never the
 answer it converges to.
+
+The network's output is multiplied by a gain g ∈ [0, 1]: fitted on held-out training
+pairs, then (by default) recalibrated after every solved step by least squares of the
+network's predictions against the corrections the solver actually produced over the
+last few steps, so that a network that stops matching the dynamics fades to plain
+extrapolation instead of adding error.
 """
 from __future__ import annotations
 
@@ -266,7 +272,7 @@ def apply_guess(dr, bc_v, vprev, vcur, Pprev, Pcur, out=None, scale=None):
 
 
 def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tolerance=1e-8, check_interval=100,
-                          log=None):
+                          log=None, online_gain=True, gain_window=5):
     """The learned-warm-start experiment on the 2-D shear-band time loop.
 
     Steps 1..ntrain run plain DR (each from the previous step's solution) and record
@@ -287,6 +293,8 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
     F = []
     hist_v, hist_P = [], []
     rows = []
+    cal = []          # (⟨prediction, realised correction⟩, ⟨prediction, prediction⟩) per solved step
+    pending = None
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     train_loss, train_ms = None, 0.0
 
@@ -316,7 +324,10 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record()
             out = net.predict(F[-2], F[-1], H, W)
-            apply_guess(dr, bc, hist_v[-2], hist_v[-1], hist_P[-2], hist_P[-1], out, net.output_scale(F[-2], F[-1]))
+            scale = net.output_scale(F[-2], F[-1])
+            pending = (out.view(-1, OUT_CH)[:, :N_TARGET] * net.step_rms(F[-2], F[-1])[:N_TARGET]).clone() \
+                if online_gain else None
+            apply_guess(dr, bc, hist_v[-2], hist_v[-1], hist_P[-2], hist_P[-1], out, scale)
             e1 = torch.cuda.Event(enable_timing=True)
             e1.record()
             st, ms = timed_solve()
@@ -333,6 +344,17 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
         for c in range(3):
             dr.tau_old[c].copy_(dr.tau[c])
         F.append(gm.fields(dr).clone())
+        if online_gain and pending is not None and len(F) >= 3:
+            # calibrate the gain on the step just solved: the realised correction to
+            # linear extrapolation against the network's (unit-gain) prediction for it
+            real = F[-1][:, :N_TARGET] - (2 * F[-2][:, :N_TARGET] - F[-3][:, :N_TARGET])
+            cal.append((float((pending * real).sum()), float((pending * pending).sum())))
+            num = sum(a for a, _ in cal[-gain_window:])
+            den = sum(b for _, b in cal[-gain_window:])
+            if den > 0:
+                net.gain = min(max(num / den, 0.0), 1.0)
+            row["gain"] = net.gain
+            pending = None
         hist_v.append([x.clone() for x in dr.v])
         hist_P.append(dr.P.clone())
         if len(hist_v) > 2:
@@ -343,9 +365,9 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
             train_loss = net.train(F, H, W, epochs=epochs, seed=seed)
             torch.cuda.synchronize()
             train_ms = (time.perf_counter() - t0) * 1e3
-            F = F[-2:]
+            F = F[-3:]
         elif step > ntrain:
-            F = F[-2:]
+            F = F[-3:]
         rows.append(row)
         if log:
             log(row)
