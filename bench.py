@@ -339,6 +339,54 @@ def warmstart_mode(args, fem):
     return 0
 
 
+def timeloop_mode(args, fem):
+    """Time loop of the layered visco-elasto-plastic case (BASELINE config 2 shape): each
+    step P0 ← P, solve to the tolerance, τ_old ← τ. Arms, each on its own trajectory:
+    plain FP64 DR from the previous step's solution; mixed precision from the previous
+    solution; mixed precision from the linearly extrapolated state 2x_t − x_{t−1}
+    (steps ≥ 3). Prints one JSON line with per-step iterations and times."""
+    import torch
+    case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(precision, extrapolate):
+        dr = case.device_state()
+        bc = case.bc_device()
+        hist, rows = [], []
+        for step in range(1, args.tl_steps + 1):
+            dr.P0.copy_(dr.P)
+            torch.cuda.synchronize()
+            ev0.record()
+            if extrapolate and len(hist) == 2:
+                fem.warmstart.extrapolate_state(dr, bc, hist[0][0], hist[1][0], hist[0][1], hist[1][1])
+            st = fem.solve(dr, bc, dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval,
+                           throw_on_failure=False, max_iterations=2_000_000, iter_max=2_000_000, precision=precision)
+            ev1.record()
+            torch.cuda.synchronize()
+            rows.append({"step": step, "iter": st["iter"], "ms": ev0.elapsed_time(ev1), "converged": bool(st["converged"])})
+            fem.update_stokes_current_stress(dr, case.dt)
+            for c in range(6):
+                dr.tau_old[c].copy_(dr.tau[c])
+            hist.append(([x.clone() for x in dr.v], dr.P.clone()))
+            hist = hist[-2:]
+        return rows, torch.cat(list(dr.v)), dr.P.clone()
+
+    arms = {"plain_fp64": run("fp64", False), "mixed": run("mixed", False), "mixed_extrapolated": run("mixed", True)}
+    ref_v, ref_P = arms["plain_fp64"][1], arms["plain_fp64"][2]
+    out = {"mode": "timeloop", "workload": f"vep-layers-hex27-{args.n}^3 x {args.tl_steps} steps", "n": args.n,
+           "steps": args.tl_steps, "tolerance": args.tolerance, "arms": {}}
+    for name, (rows, v, P) in arms.items():
+        out["arms"][name] = {
+            "total_s": sum(r["ms"] for r in rows) / 1e3, "iterations": [r["iter"] for r in rows],
+            "all_converged": all(r["converged"] for r in rows),
+            "final_rel_err_vs_plain": {"v": float(torch.linalg.norm(v - ref_v) / torch.linalg.norm(ref_v)),
+                                       "P": float(torch.linalg.norm(P - ref_P) / torch.linalg.norm(ref_P))}}
+    tp = out["arms"]["plain_fp64"]["total_s"]
+    out["speedup_vs_plain_fp64"] = {k: tp / a["total_s"] for k, a in out["arms"].items()}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -390,7 +438,8 @@ def main():
     ap.add_argument("--ws-steps", type=int, default=200)
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart"],
+    ap.add_argument("--tl-steps", type=int, default=10)
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -426,6 +475,8 @@ def main():
         return adjoint_mode(args, fem)
     if args.mode == "warmstart":
         return warmstart_mode(args, fem)
+    if args.mode == "timeloop":
+        return timeloop_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()

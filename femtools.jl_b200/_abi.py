@@ -157,6 +157,7 @@ SIGNATURES = {
     "femb200_net_target": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64]),
     "femb200_apply_warm_start": (C.c_int, [_vp, _P(StokesProblemC), _vp * 2, _vp * 2, _vp, _vp, _vp, C.c_int32,
                                            _P(C.c_float)]),
+    "femb200_extrapolate_state": (C.c_int, [_vp, _P(StokesProblemC), _vp * 3, _vp * 3, _vp, _vp]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

@@ -1664,6 +1664,24 @@ int femb200_net_target(femb200_handle* h, const float* Fprev, const float* Fcur,
     return FEMB200_OK;
 }
 
+int femb200_extrapolate_state(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[3],
+                              const void* const vcur[3], const void* Pprev, const void* Pcur) {
+    RC(check_problem(h, p));
+    if (p->dtype != FEMB200_F64) { h->err = "extrapolation: FP64 states only"; return FEMB200_EUNSUPPORTED; }
+    if (!vprev || !vcur || !Pprev || !Pcur) { h->err = "extrapolation: bad arguments"; return FEMB200_EINVAL; }
+    RC(build_mask(h, p));
+    const double* vp[3];
+    const double* vc[3];
+    double* v[3];
+    for (int k = 0; k < p->dim; ++k) {
+        vp[k] = static_cast<const double*>(vprev[k]); vc[k] = static_cast<const double*>(vcur[k]);
+        v[k] = static_cast<double*>(p->v[k]);
+    }
+    CK(launch_extrapolate_guess<double>(p->dim, vp, vc, static_cast<const double*>(Pprev), static_cast<const double*>(Pcur),
+                                        h->d_mask, v, static_cast<double*>(p->P), p->nnodes, p->nnodesP, h->stream));
+    return FEMB200_OK;
+}
+
 int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[2],
                              const void* const vcur[2], const void* Pprev, const void* Pcur, const float* out,
                              int32_t co, const float scale[3]) {

@@ -172,6 +172,10 @@ cudaError_t launch_net_input(const float* Fp, const float* Fc, const float* s, v
 cudaError_t launch_net_target(const float* Fp, const float* Fc, const float* Fn, const float* s, float* tgt, int64_t npix,
                               cudaStream_t st);
 template <class T>
+cudaError_t launch_extrapolate_guess(int dim, const T* const* vprev, const T* const* vcur, const T* Pprev,
+                                     const T* Pcur, const uint8_t* mask, T* const* v, T* P, int64_t nnodes,
+                                     int64_t nP, cudaStream_t st);
+template <class T>
 cudaError_t launch_apply_guess(const T* vprev[2], const T* vcur[2], const T* Pprev, const T* Pcur, const float* out, int co,
                                const float* s, const uint8_t* mask, T* v[2], T* P, const int32_t* dofsP,
                                const int32_t* el2n, int64_t nnodes, int64_t nels, cudaStream_t st);

@@ -126,6 +126,30 @@ cudaError_t launch_net_target(const float* Fp, const float* Fc, const float* Fn,
 }
 
 template <class T>
+__global__ void extrapolate_kernel(const T* __restrict__ prev, const T* __restrict__ cur, T* x, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = (T)(2.0 * (double)cur[i] - (double)prev[i]);
+}
+
+template <class T>
+cudaError_t launch_extrapolate_guess(int dim, const T* const* vprev, const T* const* vcur, const T* Pprev,
+                                     const T* Pcur, const uint8_t* mask, T* const* v, T* P, int64_t nnodes,
+                                     int64_t nP, cudaStream_t st) {
+    for (int c = 0; c < dim; ++c) {
+        count_launch();
+        apply_guess_v_kernel<T><<<blk(nnodes), 256, 0, st>>>(vprev[c], vcur[c], nullptr, 0, c, 0.0f, mask, v[c], nnodes);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    count_launch();
+    extrapolate_kernel<T><<<blk(nP), 256, 0, st>>>(Pprev, Pcur, P, nP);
+    return cudaGetLastError();
+}
+template cudaError_t launch_extrapolate_guess<double>(int, const double* const*, const double* const*, const double*,
+                                                      const double*, const uint8_t*, double* const*, double*, int64_t,
+                                                      int64_t, cudaStream_t);
+
+template <class T>
 cudaError_t launch_apply_guess(const T* vprev[2], const T* vcur[2], const T* Pprev, const T* Pcur, const float* out, int co,
                                const float* s, const uint8_t* mask, T* v[2], T* P, const int32_t* dofsP,
                                const int32_t* el2n, int64_t nnodes, int64_t nels, cudaStream_t st) {

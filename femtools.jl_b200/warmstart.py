@@ -271,6 +271,15 @@ def apply_guess(dr, bc_v, vprev, vcur, Pprev, Pcur, out=None, scale=None):
                                         sc))
 
 
+def extrapolate_state(dr, bc_v, vprev, vcur, Pprev, Pcur):
+    """v, P of dr ← 2·cur − prev (2-D or 3-D); Dirichlet DoFs keep their values."""
+    lib, h = _lib()
+    z = vcur[0]
+    vp = (C.c_void_p * 3)(*[C.c_void_p(x.data_ptr()) for x in (list(vprev) + [z] * 3)[:3]])
+    vc = (C.c_void_p * 3)(*[C.c_void_p(x.data_ptr()) for x in (list(vcur) + [z] * 3)[:3]])
+    _check(lib.femb200_extrapolate_state(h, C.byref(dr.problem(bc_v)), vp, vc, _p(Pprev), _p(Pcur)))
+
+
 def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tolerance=1e-8, check_interval=100,
                           log=None, online_gain=True, gain_window=5):
     """The learned-warm-start experiment on the 2-D shear-band time loop.

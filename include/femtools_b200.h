@@ -384,6 +384,12 @@ int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p,
                              const void* const vcur[2], const void* Pprev, const void* Pcur, const float* out,
                              int32_t co, const float scale[3]);
 
+/* Initial guess of the next time step by linear extrapolation of a 2-D or 3-D FP64
+ * state: v = 2 v_cur − v_prev on the DoFs p's Dirichlet sets leave free, P = 2 P_cur −
+ * P_prev on every pressure DoF. Writes p->v and p->P. */
+int femb200_extrapolate_state(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[3],
+                              const void* const vcur[3], const void* Pprev, const void* Pcur);
+
 /* ---- thermal diffusion ---------------------------------------------------- */
 
 /* assemble_diffusion_matrices_atomix! (src/heat_diffusion/assembly/residual_atomics.jl:10)
