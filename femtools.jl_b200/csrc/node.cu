@@ -1,6 +1,7 @@
 // node.cu — node-wise DR kernels: the fused Chebyshev velocity update with its
 // check-iteration reductions, Dirichlet pins, the Powell–Hestenes pressure
 // update, spectral-bound reductions and the temperature transfer.
+#include <type_traits>
 #include "kernels.cuh"
 
 namespace femb {
@@ -77,6 +78,96 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_kernel(NodeArgs<T> a
                 acc[c * 3 + 1] += sr * sr;
                 acc[c * 3 + 2] += sr * ((Rd - (double)r0[c]) / (double)pc[c]);
             }
+        }
+    }
+    if (a.reduce) block_reduce_store<RED_SLOTS>(acc, a.partials);
+}
+
+// One component of one node of node_update_kernel, on values already loaded:
+// returns the new rate and velocity and the values Rv0 and Rv take.
+struct NodeOut {
+    float rate, v, R0, Rv;
+};
+FEMB_D NodeOut node_comp(const NodeArgs<float>& a, int c, bool masked, float R, float rt, float pc, float vv, float r0,
+                         float rf, double* acc) {
+    NodeOut o;
+    float r;
+    if (masked) {
+        R = 0.0f;
+        r = 0.0f;
+        o.v = vv;
+    } else {
+        r = (float)a.beta[c] * rt + R / pc;
+        o.v = vv + (float)a.alpha[c] * r;
+    }
+    o.rate = r;
+    o.R0 = R;
+    o.Rv = a.fill ? rf : R;
+    if (a.reduce) {
+        const double Rd = (double)R;
+        const double sr = a.lam_step[c] * (double)r;
+        acc[c * 3 + 0] += Rd * Rd;
+        acc[c * 3 + 1] += sr * sr;
+        acc[c * 3 + 2] += sr * ((Rd - (double)r0) / (double)pc);
+    }
+    return o;
+}
+
+// node_update_kernel for FP32 state, four nodes per thread with 128-bit accesses
+// (every array 16-byte aligned); the n mod 4 last nodes go one per thread.
+__global__ void __launch_bounds__(NODE_THREADS) node_update_f32x4_kernel(NodeArgs<float> a) {
+    double acc[RED_SLOTS];
+#pragma unroll
+    for (int s = 0; s < RED_SLOTS; ++s) acc[s] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n4 = a.n >> 2;
+    for (int64_t g = tid; g < n4; g += stride) {
+        const uint32_t m4 = a.mask ? __ldg(reinterpret_cast<const uint32_t*>(a.mask) + g) : 0u;
+        float4 R[3], rt[3], pc[3], vv[3], r0[3], rf[3];
+        const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (c < a.dim) {
+                R[c] = reinterpret_cast<const float4*>(a.Rv[c])[g];
+                rt[c] = reinterpret_cast<const float4*>(a.rate[c])[g];
+                pc[c] = __ldg(reinterpret_cast<const float4*>(a.PC[c]) + g);
+                vv[c] = reinterpret_cast<const float4*>(a.v[c])[g];
+                r0[c] = a.reduce ? reinterpret_cast<const float4*>(a.Rv0[c])[g] : z4;
+                rf[c] = (a.fill && a.Rfill[c]) ? __ldg(reinterpret_cast<const float4*>(a.Rfill[c]) + g) : z4;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (c >= a.dim) break;
+            const float* Rj = &R[c].x; const float* tj = &rt[c].x; const float* pj = &pc[c].x;
+            const float* vj = &vv[c].x; const float* r0j = &r0[c].x; const float* rfj = &rf[c].x;
+            float4 orate, ov, oR0, oRv;
+            float* pr = &orate.x; float* pv = &ov.x; float* p0 = &oR0.x; float* pR = &oRv.x;
+            bool any_masked = false;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const bool masked = (m4 >> (8 * j + c)) & 1u;
+                any_masked |= masked;
+                const NodeOut o = node_comp(a, c, masked, Rj[j], tj[j], pj[j], vj[j], r0j[j], rfj[j], acc);
+                pr[j] = o.rate; pv[j] = o.v; p0[j] = o.R0; pR[j] = o.Rv;
+            }
+            reinterpret_cast<float4*>(a.rate[c])[g] = orate;
+            reinterpret_cast<float4*>(a.v[c])[g] = ov;
+            if (a.save_R0) reinterpret_cast<float4*>(a.Rv0[c])[g] = oR0;
+            if (a.fill || any_masked) reinterpret_cast<float4*>(a.Rv[c])[g] = oRv;
+        }
+    }
+    for (int64_t i = 4 * n4 + tid; i < a.n; i += stride) {
+        const unsigned msk = a.mask ? a.mask[i] : 0u;
+        for (int c = 0; c < a.dim; ++c) {
+            const bool masked = (msk >> c) & 1u;
+            const NodeOut o = node_comp(a, c, masked, a.Rv[c][i], a.rate[c][i], a.PC[c][i], a.v[c][i],
+                                        a.reduce ? a.Rv0[c][i] : 0.0f, (a.fill && a.Rfill[c]) ? a.Rfill[c][i] : 0.0f, acc);
+            a.rate[c][i] = o.rate;
+            a.v[c][i] = o.v;
+            if (a.save_R0) a.Rv0[c][i] = o.R0;
+            if (a.fill || masked) a.Rv[c][i] = o.Rv;
         }
     }
     if (a.reduce) block_reduce_store<RED_SLOTS>(acc, a.partials);
@@ -197,9 +288,23 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t
 
 }  // namespace
 
+namespace {
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+}  // namespace
+
 template <class T>
 cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st) {
     count_launch();
+    if constexpr (std::is_same<T, float>::value) {
+        bool ok = aligned16(a.mask);
+        for (int c = 0; c < a.dim; ++c)
+            ok = ok && aligned16(a.v[c]) && aligned16(a.rate[c]) && aligned16(a.Rv[c]) && aligned16(a.PC[c]) &&
+                 aligned16(a.Rv0[c]) && aligned16(a.Rfill[c]);
+        if (ok) {
+            node_update_f32x4_kernel<<<blocks, NODE_THREADS, 0, st>>>(a);
+            return cudaGetLastError();
+        }
+    }
     node_update_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }

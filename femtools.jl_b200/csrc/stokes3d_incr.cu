@@ -164,11 +164,25 @@ __device__ __noinline__ ApexOut apex_increment_f64(const ApexIn in) {
     return o;
 }
 
+// The base data is read once per sweep and is larger than L2: it is loaded with an
+// evict-first L2 policy so that the node arrays (δv gathers, residual atomics, the node
+// update) stay resident across sweeps.
+FEMB_D uint64_t l2_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+FEMB_D float ldg_stream(const float* ptr, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(ptr), "l"(pol));
+    return v;
+}
+
 // Base data of one quadrature row (3 points × 7 fields, contiguous in the tiled
 // layout) into registers.
-FEMB_D void load_row(float (&r)[3 * BASE_FIELDS], const float* row) {
+FEMB_D void load_row(float (&r)[3 * BASE_FIELDS], const float* row, uint64_t pol) {
 #pragma unroll
-    for (int j = 0; j < 3 * BASE_FIELDS; ++j) r[j] = __ldg(row + j * 32);
+    for (int j = 0; j < 3 * BASE_FIELDS; ++j) r[j] = ldg_stream(row + j * 32, pol);
 }
 
 // Per-element data of a tile, loaded one tile ahead (during the previous tile's
@@ -181,7 +195,9 @@ struct ElemData {
 };
 
 FEMB_D int elem_dof(const IncrArgs& a, int64_t tile, int lane, int p) {
-    return a.dofs_linear ? (int)(4 * (tile * 32 + lane) + p) : __ldg(a.dofs_t + (tile * 4 + p) * 32 + lane);
+    // padding lanes (past the last element) read the first element's DoFs
+    const int64_t e = tile * 32 + lane;
+    return a.dofs_linear ? (int)(4 * (e < a.nels ? e : 0) + p) : __ldg(a.dofs_t + (tile * 4 + p) * 32 + lane);
 }
 
 template <bool DIAG>
@@ -195,6 +211,38 @@ FEMB_D void load_elem(const IncrArgs& a, int64_t tile, int lane, int64_t nslots,
     for (int p = 0; p < 4; ++p) d.dP[p] = __ldg(a.dP + elem_dof(a, tile, lane, p));
     d.ph = __ldg(a.phase_t + e);
     d.phP = __ldg(a.phase_t + nslots + e);
+}
+
+// The next tile's per-element data into a thread's slots 31.. (slot s at S[s * 32]):
+// J⁻¹ (its diagonal when DIAG), det J, the two phase indices and, for linear pressure
+// numbering, δP at the element's four pressure DoFs.
+template <bool DIAG>
+FEMB_D void load_elem_async(const IncrArgs& a, int64_t tile, int lane, int64_t nslots, float* S) {
+    const int64_t e = tile * 32 + lane;
+    const float* gt = a.geo_t + tile * 10 * 32 + lane;
+    int s = 31;
+#pragma unroll
+    for (int r = 0; r < 9; ++r)
+        if (!DIAG || r % 4 == 0) cp_async4(S + (s++) * 32, gt + r * 32);
+    cp_async4(S + (s++) * 32, gt + 9 * 32);
+    cp_async4(S + (s++) * 32, reinterpret_cast<const float*>(a.phase_t + e));
+    cp_async4(S + (s++) * 32, reinterpret_cast<const float*>(a.phase_t + nslots + e));
+    if (a.dofs_linear) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) cp_async4(S + (s + p) * 32, a.dP + elem_dof(a, tile, lane, p));
+    }
+}
+
+template <bool DIAG>
+FEMB_D void read_elem(const IncrArgs& a, int64_t tile, int lane, const float* S, ElemData& d) {
+    int s = 31;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) d.Ji[r] = (!DIAG || r % 4 == 0) ? S[(s++) * 32] : 0.0f;
+    d.detJ = S[(s++) * 32];
+    d.ph = __float_as_int(S[(s++) * 32]);
+    d.phP = __float_as_int(S[(s++) * 32]);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) d.dP[p] = a.dofs_linear ? S[(s + p) * 32] : __ldg(a.dP + elem_dof(a, tile, lane, p));
 }
 
 // DIAG: every element's J⁻¹ is diagonal (axis-aligned boxes, the structured
@@ -235,7 +283,8 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         cp_async_commit();
     }
     float pre[3 * BASE_FIELDS];
-    if (plastic) load_row(pre, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane);
+    const uint64_t pol = l2_evict_first();
+    if (plastic) load_row(pre, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane, pol);
     ElemData cur;
     load_elem<DIAG>(a, tile, lane, nslots, cur);
 
@@ -346,6 +395,18 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                         }
                         gr[c][0] = s0; gr[c][1] = s1; gr[c][2] = s2;
                     }
+                    if (qz == 2 && qy == 2 && qx == 1) {
+                        // the plane slots were last read by this row's η-contraction, whose
+                        // values the first point consumed: the scatter's node indices and
+                        // pressure scales go there, in flight during the last two points
+                        const int32_t* ndc = a.el2n_t + tile * 27 * 32 + lane;
+#pragma unroll
+                        for (int k = 0; k < 27; ++k) cp_async4(WS + k * 32, reinterpret_cast<const float*>(ndc + k * 32));
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) cp_async4(WS + (27 + p) * 32, a.pscale_t + (tile * 4 + p) * 32 + lane);
+                        if (has_next) load_elem_async<DIAG>(a, tnext, lane, nslots, WS);
+                        cp_async_commit();
+                    }
                     // physical gradient ∂δv_c/∂x_k = Σ_d gr[c][d] ∂ξ_d/∂x_k
                     float gq[3][3];
 #pragma unroll
@@ -387,7 +448,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                         if (next_row) {
 #pragma unroll
                             for (int c = 0; c < BASE_FIELDS; ++c)
-                                pre[qx * BASE_FIELDS + c] = __ldg(next_row + (qx * BASE_FIELDS + c) * 32);
+                                pre[qx * BASE_FIELDS + c] = ldg_stream(next_row + (qx * BASE_FIELDS + c) * 32, pol);
                         }
                         const float Jk = 0.5f * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] +
                                          tb[4] * tb[4] + tb[5] * tb[5];
@@ -456,32 +517,56 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                     }
         }
         // ---- pressure residual and Pnum increments (element-local) ----
+        cp_async_wait_all();
         float Pn[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            Pn[p] = __ldg(a.pscale_t + (tile * 4 + p) * 32 + lane) * rp[p];
+            Pn[p] = WS[(27 + p) * 32] * rp[p];
             if (act) a.RPinc[elem_dof(a, tile, lane, p)] = rp[p];
         }
-        const float Ji[9] = {cur.Ji[0], cur.Ji[1], cur.Ji[2], cur.Ji[3], cur.Ji[4], cur.Ji[5], cur.Ji[6], cur.Ji[7], cur.Ji[8]};
+        const float* Ji = cur.Ji;
         const float detJ = cur.detJ;
-        // the next tile's element data, in flight during the scatter
-        if (has_next) load_elem<DIAG>(a, tnext, lane, nslots, cur);
         // ---- scatter, with the Pnum term −|det J| Σ_d ∂ξ_d/∂x_c Σ_p Pn_p K[p][d][a] ----
-        const int32_t* nd = a.el2n_t + tile * 27 * 32 + lane;
-#pragma unroll 3
-        for (int t = 0; t < 27; ++t) {
-            float S[3];
+        // nodes (ξ, η, ζ) = (i, j, k) in groups of one (j, k) line
+#pragma unroll 1
+        for (int jk = 0; jk < 9; ++jk) {
+            float val[3][3];
+            int n[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d)
-                S[d] = fmaf(Pn[0], c_inc_K[0][d][t], fmaf(Pn[1], c_inc_K[1][d][t], fmaf(Pn[2], c_inc_K[2][d][t], Pn[3] * c_inc_K[3][d][t])));
-            const int n = __ldg(nd + t * 32);
+            for (int i = 0; i < 3; ++i) {
+                const int t = 3 * jk + i;
+                float S[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    S[d] = fmaf(Pn[0], c_inc_K[0][d][t], fmaf(Pn[1], c_inc_K[1][d][t], fmaf(Pn[2], c_inc_K[2][d][t], Pn[3] * c_inc_K[3][d][t])));
+                n[i] = __float_as_int(WS[t * 32]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    val[i][c] = RS[(c * 27 + t) * 32] -
+                                detJ * (DIAG ? Ji[4 * c] * S[c] : fmaf(Ji[3 * c], S[0], fmaf(Ji[3 * c + 1], S[1], Ji[3 * c + 2] * S[2])));
+            }
+            // when the next lane's element shares this line's ξ = +1 node as its ξ = −1
+            // node (tiles that run along ξ), its contribution is added here and one
+            // atomic per component is saved; any shared node folds correctly
+            const int n0n = __shfl_down_sync(0xffffffffu, n[0], 1);
+            const int actn = __shfl_down_sync(0xffffffffu, (int)act, 1);
+            const bool fold = lane < 31 && actn && n0n == n[2];
+            const bool folded = __shfl_up_sync(0xffffffffu, (int)fold, 1) && lane > 0;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const float val = RS[(c * 27 + t) * 32] -
-                                  detJ * (DIAG ? Ji[4 * c] * S[c] : fmaf(Ji[3 * c], S[0], fmaf(Ji[3 * c + 1], S[1], Ji[3 * c + 2] * S[2])));
-                if (act) atomicAdd(a.R[c] + n, val);
+                const float v0n = __shfl_down_sync(0xffffffffu, val[0][c], 1);
+                if (fold) val[2][c] += v0n;
+            }
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (!folded) atomicAdd(a.R[c] + n[0], val[0][c]);
+                    atomicAdd(a.R[c] + n[1], val[1][c]);
+                    atomicAdd(a.R[c] + n[2], val[2][c]);
+                }
             }
         }
+        if (has_next) read_elem<DIAG>(a, tnext, lane, WS, cur);
     }
     cp_async_wait_all();
 }
