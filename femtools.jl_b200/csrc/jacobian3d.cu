@@ -18,7 +18,72 @@ namespace femb {
 constexpr int JAC_THREADS = 64;                // 2 warps, 6 elements per block
 constexpr int JAC_GEO = 27 * 11;               // J⁻¹ (9), dΩ, dΩ_P per point
 constexpr int JAC_BP = 4 * 81;                 // ∂RP_p/∂v_(b,j)
-constexpr int JAC_ELEM = H27_ELEM_SMEM + JAC_GEO + JAC_BP;
+// Shared memory per element slot (3 elements and an idle-lane slot per warp). The
+// column loop's transposed contraction stores its two intermediate stages with the
+// strided layouts LA(i,j,k) = 3i + 9j + 10k and LB(i,j,k) = 9i + 10j + 3k (45 words
+// per component block); with slots 1025 ≡ 1 (mod 32) words apart and the idle lanes
+// on m = 8, every stage access of the warp hits 28 distinct banks. The geometry
+// slots, 306 ≡ 18 (mod 32) words apart, are conflict-free for the same lane map.
+// FP64 keeps the compact h27 stage layout (its slots already fill three blocks per SM).
+constexpr int JAC_LA = 9 * 45;                 // stage-1 scratch: 9 blocks
+template <class T>
+struct JacSmem {
+    static constexpr bool strided = sizeof(T) == 4;
+    static constexpr int stage = strided ? JAC_LA + 6 * 45 : H27_ELEM_SMEM;   // BP follows the stage scratch
+    static constexpr int e_stride = strided ? 1025 : H27_ELEM_SMEM + JAC_BP;
+    static constexpr int g_stride = strided ? 306 : JAC_GEO;
+    static_assert(stage + JAC_BP <= e_stride && stage >= H27_ELEM_SMEM && g_stride >= JAC_GEO, "slot layout");
+    static_assert(!strided || (e_stride % 32 == 1 && g_stride % 32 == 18), "bank layout");
+};
+
+FEMB_D int jla(int i, int j, int k) { return 3 * i + 9 * j + 10 * k; }
+FEMB_D int jlb(int i, int j, int k) { return 9 * i + 10 * j + 3 * k; }
+
+// h27_transpose without body force, with the conflict-free stage layouts above.
+template <class T>
+FEMB_D void jac_transpose(const Tab1D<T>& t, const T F[3][3][3], T* E, int m1, int m2, T R[3][3]) {
+    // Z^T: thread owns z-line (qx = m1, qy = m2)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            E[(c * 3 + 0) * 45 + jla(m1, m2, iz)] = t.B[0][iz] * F[c][0][0] + t.B[1][iz] * F[c][0][1] + t.B[2][iz] * F[c][0][2];
+            E[(c * 3 + 1) * 45 + jla(m1, m2, iz)] = t.B[0][iz] * F[c][1][0] + t.B[1][iz] * F[c][1][1] + t.B[2][iz] * F[c][1][2];
+            E[(c * 3 + 2) * 45 + jla(m1, m2, iz)] = t.Dd[0][iz] * F[c][2][0] + t.Dd[1][iz] * F[c][2][1] + t.Dd[2][iz] * F[c][2][2];
+        }
+    __syncwarp();
+    // Y^T: thread owns y-line (qx = m1, ·, iz = m2)
+    T* E1 = E + JAC_LA;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T TA[3], TB[3], TC[3];
+#pragma unroll
+        for (int qy = 0; qy < 3; ++qy) {
+            TA[qy] = E[(c * 3 + 0) * 45 + jla(m1, qy, m2)];
+            TB[qy] = E[(c * 3 + 1) * 45 + jla(m1, qy, m2)];
+            TC[qy] = E[(c * 3 + 2) * 45 + jla(m1, qy, m2)];
+        }
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            E1[(c * 2 + 0) * 45 + jlb(m1, iy, m2)] = t.B[0][iy] * TA[0] + t.B[1][iy] * TA[1] + t.B[2][iy] * TA[2];
+            E1[(c * 2 + 1) * 45 + jlb(m1, iy, m2)] = (t.Dd[0][iy] * TB[0] + t.Dd[1][iy] * TB[1] + t.Dd[2][iy] * TB[2]) +
+                                                      (t.B[0][iy] * TC[0] + t.B[1][iy] * TC[1] + t.B[2][iy] * TC[2]);
+        }
+    }
+    __syncwarp();
+    // X^T: thread owns x-line (·, iy = m1, iz = m2)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T UA[3], UB[3];
+#pragma unroll
+        for (int qx = 0; qx < 3; ++qx) { UA[qx] = E1[(c * 2 + 0) * 45 + jlb(qx, m1, m2)]; UB[qx] = E1[(c * 2 + 1) * 45 + jlb(qx, m1, m2)]; }
+#pragma unroll
+        for (int ix = 0; ix < 3; ++ix)
+            R[c][ix] = (t.Dd[0][ix] * UA[0] + t.Dd[1][ix] * UA[1] + t.Dd[2][ix] * UA[2]) +
+                       (t.B[0][ix] * UB[0] + t.B[1][ix] * UB[1] + t.B[2][ix] * UB[2]);
+    }
+    __syncwarp();
+}
 
 template <class T, class TG>
 __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<T, TG> a) {
@@ -28,11 +93,13 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     const bool lane_ok = lane < 27;
     // lanes 27..31 carry no element; they work in a private scratch slot (3) so
     // their (discarded) stage writes never touch an element's shared memory.
-    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * JAC_ELEM;
-    T* GEO = E + H27_ELEM_SMEM;
-    T* BP = GEO + JAC_GEO;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * JAC_ELEM) + (warp * 4 + s) * 28;
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 8, m1 = m % 3, m2 = m / 3;
+    using L = JacSmem<T>;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * L::e_stride;
+    T* GEO = reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * L::e_stride + ((size_t)warp * 4 + s) * L::g_stride;
+    T* BP = E + L::stage;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * (L::e_stride + L::g_stride)) +
+              (warp * 4 + s) * 28;
 
     Tab1D<T> tb; tb.load();
     const T dt = a.dt;
@@ -201,7 +268,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                     for (int d = 0; d < 3; ++d) Fp[c][d][qz] = w * Ji[d + 3 * c];
             }
             T Rp[3][3];
-            h27_transpose<T, false>(tb, Fp, zero3, zero3, E, m1, m2, Rp);
+            if constexpr (L::strided) jac_transpose<T>(tb, Fp, E, m1, m2, Rp);
+            else h27_transpose<T, false>(tb, Fp, zero3, zero3, E, m1, m2, Rp);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -285,7 +353,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                             Fd[c][d][qz] = dOq * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
                 }
                 T dR[3][3];
-                h27_transpose<T, false>(tb, Fd, zero3, zero3, E, m1, m2, dR);
+                if constexpr (L::strided) jac_transpose<T>(tb, Fd, E, m1, m2, dR);
+                else h27_transpose<T, false>(tb, Fd, zero3, zero3, E, m1, m2, dR);
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -311,7 +380,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 template <class T, class TG>
 cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st) {
     const int wpb = JAC_THREADS / 32;
-    const size_t smem = (size_t)wpb * 4 * JAC_ELEM * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
+    const size_t smem = (size_t)wpb * 4 * (JacSmem<T>::e_stride + JacSmem<T>::g_stride) * sizeof(T) +
+                        (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

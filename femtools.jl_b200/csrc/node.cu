@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_kernel(NodeArgs<T> a
 struct NodeOut {
     float rate, v, R0, Rv;
 };
+template <bool REDUCE>
 FEMB_D NodeOut node_comp(const NodeArgs<float>& a, int c, bool masked, float R, float rt, float pc, float vv, float r0,
                          float rf, double* acc) {
     NodeOut o;
@@ -103,7 +104,7 @@ FEMB_D NodeOut node_comp(const NodeArgs<float>& a, int c, bool masked, float R, 
     o.rate = r;
     o.R0 = R;
     o.Rv = a.fill ? rf : R;
-    if (a.reduce) {
+    if (REDUCE) {
         const double Rd = (double)R;
         const double sr = a.lam_step[c] * (double)r;
         acc[c * 3 + 0] += Rd * Rd;
@@ -115,7 +116,10 @@ FEMB_D NodeOut node_comp(const NodeArgs<float>& a, int c, bool masked, float R, 
 
 // node_update_kernel for FP32 state, four nodes per thread with 128-bit accesses
 // (every array 16-byte aligned); the n mod 4 last nodes go one per thread.
-__global__ void __launch_bounds__(NODE_THREADS) node_update_f32x4_kernel(NodeArgs<float> a) {
+// REDUCE (check iterations only) carries the FP64 partial sums; without it the
+// kernel needs no FP64 registers.
+template <bool REDUCE>
+__global__ void __launch_bounds__(NODE_THREADS, 2) node_update_f32x4_kernel(NodeArgs<float> a) {
     double acc[RED_SLOTS];
 #pragma unroll
     for (int s = 0; s < RED_SLOTS; ++s) acc[s] = 0.0;
@@ -133,7 +137,7 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_f32x4_kernel(NodeArg
                 rt[c] = reinterpret_cast<const float4*>(a.rate[c])[g];
                 pc[c] = __ldg(reinterpret_cast<const float4*>(a.PC[c]) + g);
                 vv[c] = reinterpret_cast<const float4*>(a.v[c])[g];
-                r0[c] = a.reduce ? reinterpret_cast<const float4*>(a.Rv0[c])[g] : z4;
+                r0[c] = REDUCE ? reinterpret_cast<const float4*>(a.Rv0[c])[g] : z4;
                 rf[c] = (a.fill && a.Rfill[c]) ? __ldg(reinterpret_cast<const float4*>(a.Rfill[c]) + g) : z4;
             }
         }
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_f32x4_kernel(NodeArg
             for (int j = 0; j < 4; ++j) {
                 const bool masked = (m4 >> (8 * j + c)) & 1u;
                 any_masked |= masked;
-                const NodeOut o = node_comp(a, c, masked, Rj[j], tj[j], pj[j], vj[j], r0j[j], rfj[j], acc);
+                const NodeOut o = node_comp<REDUCE>(a, c, masked, Rj[j], tj[j], pj[j], vj[j], r0j[j], rfj[j], acc);
                 pr[j] = o.rate; pv[j] = o.v; p0[j] = o.R0; pR[j] = o.Rv;
             }
             reinterpret_cast<float4*>(a.rate[c])[g] = orate;
@@ -162,15 +166,15 @@ __global__ void __launch_bounds__(NODE_THREADS) node_update_f32x4_kernel(NodeArg
         const unsigned msk = a.mask ? a.mask[i] : 0u;
         for (int c = 0; c < a.dim; ++c) {
             const bool masked = (msk >> c) & 1u;
-            const NodeOut o = node_comp(a, c, masked, a.Rv[c][i], a.rate[c][i], a.PC[c][i], a.v[c][i],
-                                        a.reduce ? a.Rv0[c][i] : 0.0f, (a.fill && a.Rfill[c]) ? a.Rfill[c][i] : 0.0f, acc);
+            const NodeOut o = node_comp<REDUCE>(a, c, masked, a.Rv[c][i], a.rate[c][i], a.PC[c][i], a.v[c][i],
+                                        REDUCE ? a.Rv0[c][i] : 0.0f, (a.fill && a.Rfill[c]) ? a.Rfill[c][i] : 0.0f, acc);
             a.rate[c][i] = o.rate;
             a.v[c][i] = o.v;
             if (a.save_R0) a.Rv0[c][i] = o.R0;
             if (a.fill || masked) a.Rv[c][i] = o.Rv;
         }
     }
-    if (a.reduce) block_reduce_store<RED_SLOTS>(acc, a.partials);
+    if (REDUCE) block_reduce_store<RED_SLOTS>(acc, a.partials);
 }
 
 template <class T>
@@ -301,7 +305,8 @@ cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st
             ok = ok && aligned16(a.v[c]) && aligned16(a.rate[c]) && aligned16(a.Rv[c]) && aligned16(a.PC[c]) &&
                  aligned16(a.Rv0[c]) && aligned16(a.Rfill[c]);
         if (ok) {
-            node_update_f32x4_kernel<<<blocks, NODE_THREADS, 0, st>>>(a);
+            if (a.reduce) node_update_f32x4_kernel<true><<<blocks, NODE_THREADS, 0, st>>>(a);
+            else node_update_f32x4_kernel<false><<<blocks, NODE_THREADS, 0, st>>>(a);
             return cudaGetLastError();
         }
     }
