@@ -23,7 +23,11 @@ from .solver import (StokesDR, ThermalDiffusionDR, solve, solve_stokes_dyrel, so
                      assemble_stokes_residuals, assemble_augmented_momentum_jacobian,
                      assemble_viscosity_weighted_pressure_scaling, update_stokes_current_stress,
                      assemble_shear_heating, assemble_thermal_residual, assemble_diffusion_matrices_colored,
-                     assemble_adjoint_residual, viscosity_sensitivity, solve_adjoint)
+                     assemble_adjoint_residual, viscosity_sensitivity, solve_adjoint, precompute_geometry,
+                     update_geometry)
 from . import autodiff  # noqa: E402,F401
 from .autodiff import DRCheckpoint, solve_log_viscosity  # noqa: E402,F401
 from . import warmstart  # noqa: E402,F401
+from . import postprocess  # noqa: E402,F401
+from .postprocess import (compute_strain_rate_stress_postprocess, update_old_stress_from_cells,  # noqa: E402,F401
+                          write_vtk, write_stokes_vtk, VtkMesh)

@@ -158,6 +158,8 @@ SIGNATURES = {
     "femb200_apply_warm_start": (C.c_int, [_vp, _P(StokesProblemC), _vp * 2, _vp * 2, _vp, _vp, _vp, C.c_int32,
                                            _P(C.c_float)]),
     "femb200_extrapolate_state": (C.c_int, [_vp, _P(StokesProblemC), _vp * 3, _vp * 3, _vp, _vp]),
+    "femb200_precompute_geometry": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int32]),
+    "femb200_strain_rate_stress": (C.c_int, [_vp, _P(StokesProblemC), _vp * 6, _vp * 14]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

@@ -1424,6 +1424,24 @@ int check_controls(femb200_handle* h, const femb200_stokes_controls* c) {
 
 }  // namespace
 
+namespace {
+template <class T, class TG>
+int strain_rate_stress_impl(femb200_handle* h, const femb200_stokes_problem* p, const void* const tau_ip[6],
+                            void* const out[14]) {
+    PostArgs<T, TG> a;
+    std::memset(&a, 0, sizeof(a));
+    a.el2n = p->el2n;
+    a.geo_v = static_cast<const TG*>(p->geo_v);
+    a.nels = p->nels;
+    const int nt = p->dim == 3 ? 6 : 3, nf = p->dim == 3 ? 14 : 10;
+    for (int c = 0; c < p->dim; ++c) a.v[c] = static_cast<const T*>(p->v[c]);
+    for (int c = 0; c < nt; ++c) a.tau[c] = static_cast<const T*>(tau_ip[c]);
+    for (int k = 0; k < nf; ++k) a.out[k] = static_cast<T*>(out[k]);
+    CK(launch_strain_rate_stress<T, TG>(p->dim, a, h->stream));
+    return FEMB200_OK;
+}
+}  // namespace
+
 extern "C" {
 
 int femb200_create(femb200_handle** out) {
@@ -1662,6 +1680,51 @@ int femb200_net_target(femb200_handle* h, const float* Fprev, const float* Fcur,
     if (!Fprev || !Fcur || !Fnext || !scale || !target || npix < 1) { h->err = "net target: bad arguments"; return FEMB200_EINVAL; }
     CK(launch_net_target(Fprev, Fcur, Fnext, scale, target, npix, h->stream));
     return FEMB200_OK;
+}
+
+int femb200_precompute_geometry(femb200_handle* h, int32_t dim, int64_t nels, int64_t nnodes, const double* coords,
+                                const int32_t* el2n, void* geo_v, void* geo_P, int32_t geo_dtype) {
+    if (!h) return FEMB200_EINVAL;
+    if ((dim != 2 && dim != 3) || nels < 0 || (geo_dtype != FEMB200_F64 && geo_dtype != FEMB200_F32)) {
+        h->err = "precompute_geometry: bad arguments";
+        return FEMB200_EINVAL;
+    }
+    if (nels == 0) return FEMB200_OK;
+    if (nnodes < 1 || !coords || !el2n || !geo_v) { h->err = "precompute_geometry: bad arguments"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    if (!h->d_flag) {
+        CK(cudaMalloc(&h->d_flag, sizeof(int)));
+        CK(cudaMallocHost(&h->h_flag, sizeof(int)));
+    }
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    if (geo_dtype == FEMB200_F64)
+        CK(launch_geometry<double>(dim, coords, el2n, nels, nnodes, static_cast<double*>(geo_v), static_cast<double*>(geo_P),
+                                   h->d_flag, h->stream));
+    else
+        CK(launch_geometry<float>(dim, coords, el2n, nels, nnodes, static_cast<float*>(geo_v), static_cast<float*>(geo_P),
+                                  h->d_flag, h->stream));
+    CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (*h->h_flag) { h->err = "precompute_geometry: a connectivity entry lies outside 1:nnodes"; return FEMB200_EINVAL; }
+    return FEMB200_OK;
+}
+
+
+int femb200_strain_rate_stress(femb200_handle* h, const femb200_stokes_problem* p, const void* const tau_ip[6],
+                               void* const out[14]) {
+    RC(check_problem(h, p));
+    const int nt = p->dim == 3 ? 6 : 3, nf = p->dim == 3 ? 14 : 10;
+    if (!tau_ip || !out) { h->err = "strain_rate_stress: stresses and outputs are required"; return FEMB200_EINVAL; }
+    for (int c = 0; c < nt; ++c)
+        if (!tau_ip[c]) { h->err = "strain_rate_stress: stresses and outputs are required"; return FEMB200_EINVAL; }
+    for (int k = 0; k < nf; ++k)
+        if (!out[k]) { h->err = "strain_rate_stress: stresses and outputs are required"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    const bool d = p->dtype == FEMB200_F64, gd = p->geo_dtype == FEMB200_F64;
+    if (d && gd) return strain_rate_stress_impl<double, double>(h, p, tau_ip, out);
+    if (d) return strain_rate_stress_impl<double, float>(h, p, tau_ip, out);
+    if (gd) return strain_rate_stress_impl<float, double>(h, p, tau_ip, out);
+    return strain_rate_stress_impl<float, float>(h, p, tau_ip, out);
 }
 
 int femb200_extrapolate_state(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[3],

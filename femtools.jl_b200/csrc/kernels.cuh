@@ -171,6 +171,24 @@ cudaError_t launch_grid_fields(const T* vx, const T* vy, const T* P, const int32
 cudaError_t launch_net_input(const float* Fp, const float* Fc, const float* s, void* X, int64_t npix, cudaStream_t st);
 cudaError_t launch_net_target(const float* Fp, const float* Fc, const float* Fn, const float* s, float* tgt, int64_t npix,
                               cudaStream_t st);
+// Element-averaged strain-rate and stress diagnostics (postprocess.cu).
+template <class T, class TG>
+struct PostArgs {
+    const int32_t* el2n;
+    const TG* geo_v;
+    const T* v[3];
+    const T* tau[6];      // nq × nels each: 6 components in 3-D, (xx, yy, xy) in 2-D
+    T* out[14];           // nels each: 14 fields in 3-D, 10 in 2-D
+    int64_t nels;
+};
+template <class T, class TG>
+cudaError_t launch_strain_rate_stress(int dim, const PostArgs<T, TG>& a, cudaStream_t st);
+
+// Element geometry at the velocity integration points (geometry.cu).
+template <class TG>
+cudaError_t launch_geometry(int dim, const double* coords, const int32_t* el2n, int64_t nels, int64_t nnodes, TG* geo_v,
+                            TG* geo_P, int* bad, cudaStream_t st);
+
 template <class T>
 cudaError_t launch_extrapolate_guess(int dim, const T* const* vprev, const T* const* vcur, const T* Pprev,
                                      const T* Pcur, const uint8_t* mask, T* const* v, T* P, int64_t nnodes,

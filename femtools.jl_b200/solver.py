@@ -313,6 +313,51 @@ def solve_adjoint(dr: StokesDR, bc_v, dt, objective_v, lam_v=None, lam_P=None, t
     return lam_v, lam_P, prob.stats_dict(st)
 
 
+def _device_coords(coords, dim):
+    """Node coordinates as a contiguous FP64 device array, nnodes × dim (x fastest)."""
+    c = coords if isinstance(coords, torch.Tensor) else torch.as_tensor(np.asarray(coords, dtype=np.float64))
+    c = c.to(device="cuda", dtype=torch.float64).reshape(-1, dim).contiguous()
+    return c
+
+
+def precompute_geometry(coords, el2n, dim, geometry_dtype=None, with_P=True):
+    """precompute_geometry (src/mesh/mesh.jl:592-606) and the mixed-mesh geometry
+    (mixed_mesh.jl:358-392) on the device: returns (geo_v, geo_P), nels × nq × (dim² + 1)
+    and nels × nq, with J⁻¹ (column-major) and |det J|·ω at every velocity integration
+    point. `geometry_dtype` is the stored precision (torch.float64 or torch.float32, the
+    reference's geometry_precision); J is inverted in FP64 either way."""
+    lib, h = _Handle.get()
+    gdt = geometry_dtype or torch.float64
+    c = _device_coords(coords, dim)
+    e2n = el2n if isinstance(el2n, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(el2n, dtype=np.int32))
+    e2n = e2n.to(device="cuda", dtype=torch.int32).contiguous()
+    nv = 27 if dim == 3 else 9
+    nels = e2n.numel() // nv
+    geo_v = torch.empty((nels, nv, dim * dim + 1), dtype=gdt, device="cuda")
+    geo_P = torch.empty((nels, nv), dtype=gdt, device="cuda") if with_P else None
+    _check(lib, h, lib.femb200_precompute_geometry(h, dim, nels, c.shape[0], _ptr(c), _ptr(e2n), _ptr(geo_v),
+                                                   _ptr(geo_P), _DT[gdt]))
+    return geo_v, geo_P
+
+
+def update_geometry(state, coords):
+    """update_geometry!(mesh) (src/mesh/mesh.jl:640-650, mixed_mesh.jl:337-345): recompute
+    the geometry a StokesDR or ThermalDiffusionDR state holds, in place (the arrays keep
+    their identity), from moved node coordinates (host or device, nnodes × dim)."""
+    lib, h = _Handle.get()
+    mesh = state.mesh
+    c = _device_coords(coords, mesh.dim)
+    if c.shape[0] != mesh.nnodes:
+        raise ValueError(f"coords has {c.shape[0]} nodes; expected {mesh.nnodes}")
+    if isinstance(state, StokesDR):
+        e2n, geo_v, geo_P = state._mesh["el2n"], state._mesh["geo_v"], state._mesh["geo_P"]
+    else:
+        e2n, geo_v, geo_P = state.el2n, state.geo, None
+    _check(lib, h, lib.femb200_precompute_geometry(h, mesh.dim, mesh.nels, mesh.nnodes, _ptr(c), _ptr(e2n),
+                                                   _ptr(geo_v), _ptr(geo_P), _DT[geo_v.dtype]))
+    return state
+
+
 class ThermalDiffusionDR:
     """Thermal DR state on the device (heat_diffusion_types.jl:90-132)."""
 

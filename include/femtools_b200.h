@@ -384,6 +384,31 @@ int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p,
                              const void* const vcur[2], const void* Pprev, const void* Pcur, const float* out,
                              int32_t co, const float scale[3]);
 
+/* ---- element geometry (src/mesh/mesh.jl:592-682, src/mesh/mixed_mesh.jl:337-392) ---- */
+/* precompute_geometry / update_geometry!: at every velocity integration point of
+ * every element, J = Σ_a x_a ∂N_a/∂ξ from the node coordinates (precompute_geometry_kernel!,
+ * mesh.jl:674-682), stored as J⁻¹ (column-major) and |det J|·ω in geo_v (nels × nq ×
+ * (dim·dim + 1)) and |det J|·ω in geo_P (nels × nq; NULL skips it). coords is nnodes × dim,
+ * interleaved (the memory of Julia's Vector{SVector{dim,Float64}}); el2n is nv × nels,
+ * 1-based. J is inverted in FP64 and rounded once, on store, to geo_dtype (FEMB200_F64
+ * or FEMB200_F32: the reference's geometry_precision, mesh.jl:583-591). dim 3: Hex27
+ * (nv = nq = 27); dim 2: Q9 (nv = nq = 9). A connectivity entry outside 1..nnodes
+ * returns FEMB200_EINVAL (its points are written as NaN). Synchronises the stream. */
+int femb200_precompute_geometry(femb200_handle* h, int32_t dim, int64_t nels, int64_t nnodes,
+                                const double* coords, const int32_t* el2n, void* geo_v, void* geo_P,
+                                int32_t geo_dtype);
+
+/* ---- post-processing (src/postprocess/postprocess.jl:17-79, :168-215) ---- */
+/* compute_strain_rate_stress_postprocess from integration-point stresses: per element,
+ * the dΩ-weighted averages of the strain rate from p->v and of the deviatoric stress
+ * tau_ip (nq × nels arrays: (xx, yy, zz, xy, xz, yz) in 3-D, (xx, yy, xy) in 2-D with
+ * τzz = −(τxx + τyy)), and of their second invariants. out: nels arrays in p->dtype,
+ * 3-D (14): εxx, εyy, εzz, εxy, εxz, εyz, εII, τxx, τyy, τzz, τxy, τxz, τyz, τII (the
+ * invariants with the eps² floor of second_invariant, rheology.jl:395-400); 2-D (10):
+ * εxx, εyy, εzz (= 0), εxy, εII, τxx, τyy, τzz, τxy, τII. Uses p's mesh, geometry and v. */
+int femb200_strain_rate_stress(femb200_handle* h, const femb200_stokes_problem* p,
+                               const void* const tau_ip[6], void* const out[14]);
+
 /* Initial guess of the next time step by linear extrapolation of a 2-D or 3-D FP64
  * state: v = 2 v_cur − v_prev on the DoFs p's Dirichlet sets leave free, P = 2 P_cur −
  * P_prev on every pressure DoF. Writes p->v and p->P. */

@@ -1119,6 +1119,65 @@ int orc_geometry(int dim, int64_t nels, const double* coords, const int32_t* el2
     return 0;
 }
 
+// compute_strain_rate_stress_postprocess from integration-point stresses
+// (src/postprocess/postprocess.jl:17-79 in 2-D, :168-215 in 3-D): per element the
+// dΩ-weighted averages of ε (from ∂N∂x = ∂N∂ξ·J⁻¹, mesh.jl:504-507), its deviatoric
+// second invariant, τ and τII. 3-D invariants carry the eps² floor of
+// second_invariant (rheology.jl:395-400); the 2-D ones are formed without it (:52-53).
+int orc_strain_rate_stress(int dim, int64_t nels, const int32_t* el2n, const double* geo_v, const double* const* v,
+                           const double* const* tau, double* const* out) {
+    const Tables& t = tables_for(dim);
+    const int D = dim, NV = t.nv, NQ = t.nq, S = D * D + 1, NF = dim == 3 ? 14 : 10;
+    const double e2 = 2.220446049250313e-16 * 2.220446049250313e-16;
+    for (int64_t e = 0; e < nels; ++e) {
+        double tot[14] = {0}, vol = 0;
+        for (int q = 0; q < NQ; ++q) {
+            const double* g = geo_v + ((int64_t)e * NQ + q) * S;
+            double gv[3][3] = {{0}};
+            for (int a = 0; a < NV; ++a) {
+                const int64_t node = el2n[(int64_t)NV * e + a] - 1;
+                for (int k = 0; k < D; ++k) {
+                    double dNdx = 0;
+                    for (int j = 0; j < D; ++j) dNdx += t.dN[q][a][j] * g[j + D * k];
+                    for (int c = 0; c < D; ++c) gv[c][k] += dNdx * v[c][node];
+                }
+            }
+            const double dO = g[D * D];
+            const int64_t iq = (int64_t)e * NQ + q;
+            double f[14];
+            if (D == 3) {
+                const double eps_[6] = {gv[0][0], gv[1][1], gv[2][2], (gv[0][1] + gv[1][0]) / 2,
+                                        (gv[0][2] + gv[2][0]) / 2, (gv[1][2] + gv[2][1]) / 2};
+                const double tr = (eps_[0] + eps_[1] + eps_[2]) / 3;
+                const double dv[6] = {eps_[0] - tr, eps_[1] - tr, eps_[2] - tr, eps_[3], eps_[4], eps_[5]};
+                const double eII = std::sqrt((dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]) / 2 + dv[3] * dv[3] +
+                                             dv[4] * dv[4] + dv[5] * dv[5] + e2);
+                double tq[6];
+                for (int c = 0; c < 6; ++c) tq[c] = tau[c][iq];
+                const double tII = std::sqrt((tq[0] * tq[0] + tq[1] * tq[1] + tq[2] * tq[2]) / 2 + tq[3] * tq[3] +
+                                             tq[4] * tq[4] + tq[5] * tq[5] + e2);
+                for (int c = 0; c < 6; ++c) f[c] = eps_[c];
+                f[6] = eII;
+                for (int c = 0; c < 6; ++c) f[7 + c] = tq[c];
+                f[13] = tII;
+            } else {
+                const double exx = gv[0][0], eyy = gv[1][1], ezz = 0.0, exy = (gv[0][1] + gv[1][0]) / 2;
+                const double tr = (exx + eyy + ezz) / 3;
+                const double d0 = exx - tr, d1 = eyy - tr, d2 = ezz - tr;
+                const double eII = std::sqrt((d0 * d0 + d1 * d1 + d2 * d2) / 2 + exy * exy);
+                const double txx = tau[0][iq], tyy = tau[1][iq], txy = tau[2][iq], tzz = -(txx + tyy);
+                const double tII = std::sqrt((txx * txx + tyy * tyy + tzz * tzz) / 2 + txy * txy);
+                const double ff[10] = {exx, eyy, ezz, exy, eII, txx, tyy, tzz, txy, tII};
+                for (int k = 0; k < 10; ++k) f[k] = ff[k];
+            }
+            for (int k = 0; k < NF; ++k) tot[k] += f[k] * dO;
+            vol += dO;
+        }
+        for (int k = 0; k < NF; ++k) out[k][e] = tot[k] / vol;
+    }
+    return 0;
+}
+
 int orc_pressure_residual(const femb200_stokes_problem* p, double dt, int32_t finite_K) {
     int rc = check_problem(p); if (rc) return rc;
     pressure_residual_impl(p, dt, finite_K);

@@ -38,6 +38,7 @@ def lib():
             "orc_tables": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp]),
             "orc_structured_mesh": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
             "orc_geometry": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
+            "orc_strain_rate_stress": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp * 3, _vp * 6, _vp * 14]),
             "orc_pressure_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
             "orc_momentum_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
             "orc_stokes_residuals": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
@@ -289,3 +290,19 @@ def solve_coupled(thermal: HostThermal, stokes: HostStokes, Tref=273.0, shear_he
                                  ptr(phi), C.byref(st))
     check(rc)
     return problem.stats_dict(st), phi
+
+
+def strain_rate_stress(dim, el2n, geo_v, v, tau):
+    """Oracle element-averaged diagnostics: list of 14 (3-D) / 10 (2-D) arrays of nels."""
+    el2n = np.ascontiguousarray(el2n, dtype=np.int32)
+    geo_v = np.ascontiguousarray(geo_v, dtype=np.float64)
+    nels = el2n.shape[0]
+    vs = [np.ascontiguousarray(x, dtype=np.float64) for x in v]
+    ts = [np.ascontiguousarray(x, dtype=np.float64) for x in tau]
+    nf = 14 if dim == 3 else 10
+    out = [np.zeros(nels) for _ in range(nf)]
+    vp = (C.c_void_p * 3)(*([ptr(x) for x in vs] + [0] * (3 - len(vs))))
+    tp = (C.c_void_p * 6)(*([ptr(x) for x in ts] + [0] * (6 - len(ts))))
+    op = (C.c_void_p * 14)(*([ptr(x) for x in out] + [0] * (14 - nf)))
+    check(lib().orc_strain_rate_stress(dim, nels, ptr(el2n), ptr(geo_v), vp, tp, op))
+    return out
