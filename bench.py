@@ -339,6 +339,75 @@ def warmstart_mode(args, fem):
     return 0
 
 
+def cellpressure_mode(args, fem):
+    """Cell-pressure Hex27 Stokes (CellPressureStokesDR): the sinking block on an n³
+    structured mesh (configs.cell_pressure_case), solved from rest to the reference's
+    default absolute tolerance 1e-5 with its default steps. Prints one JSON line: the
+    solve time and iteration count, the per-launch time and algorithmic HBM bandwidth of
+    the momentum and pressure residual kernels, and the oracle's time per iteration on
+    all host cores (a bounded sample of 20 iterations) extrapolated to the GPU run's count."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    case = fem.configs.cell_pressure_case(n=args.n, seed=args.seed, distort=False)
+    mesh = case.mesh
+    dr = fem.CellPressureStokesDR(mesh, case.material, phases=case.phases)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # per-launch kernel times on the zero state (inputs larger than L2 at 64³: geometry 566 MB)
+    for _ in range(args.warmup):
+        fem.assemble_stokes_momentum_residual_3d(dr)
+        fem.assemble_stokes_pressure_residual_3d(dr)
+    k = max(args.steps, 5)
+    e0, e1, e2 = ev(), ev(), ev()
+    e0.record()
+    for _ in range(k):
+        fem.assemble_stokes_momentum_residual_3d(dr)
+    e1.record()
+    for _ in range(k):
+        fem.assemble_stokes_pressure_residual_3d(dr)
+    e2.record()
+    torch.cuda.synchronize()
+    t_mom = e0.elapsed_time(e1) / k     # includes the launch's Rv zero-fill and the device phase check
+    t_pres = e1.elapsed_time(e2) / k
+    ne, nn = mesh.nels, mesh.nnodes
+    # algorithmic bytes per launch: geometry (J⁻¹ + dΩ per point), connectivity, velocities
+    # gathered once per node, phase and pressure per cell, Rv read-modify-write / RP write
+    geo = ne * 27 * 10 * 8 + ne * 27 * 4
+    b_mom = geo + 3 * nn * 8 + ne * (4 + 32) + 3 * nn * 8 * 2
+    b_pres = geo + 3 * nn * 8 + ne * 32
+    peak, kind = measured_peaks()
+    # the solve
+    torch.cuda.synchronize()
+    s0, s1 = ev(), ev()
+    s0.record()
+    st = fem.solve_cell_pressure(dr, case.bc, tolerance=1e-5, max_iterations=args.max_iterations,
+                                 check_interval=100, throw_on_failure=False)
+    s1.record()
+    torch.cuda.synchronize()
+    t_solve = s0.elapsed_time(s1) / 1e3
+    cpu = None
+    if not args.no_cpu_baseline:
+        hs = oh.HostCellPressure(mesh, case.material.eta, case.material.rho0, case.material.g, case.phases)
+        sample = 20
+        t0 = time.perf_counter()
+        hs.solve(case.bc, tolerance=1e-300, max_iterations=sample, check_interval=sample, throw_on_failure=False)
+        per_it = (time.perf_counter() - t0) / sample
+        cpu = {"value": per_it * st["iterations"], "unit": "s", "cores": 1, "kind": "port",
+               "sample": f"{sample} oracle iterations at {mesh.nel} ({per_it:.3f} s each, serial), "
+                         f"extrapolated to {st['iterations']} iterations"}
+    print(json.dumps({
+        "mode": "cellpressure", "workload": f"sinking-block-hex27-cell-pressure-{args.n}^3", "nels": ne,
+        "nnodes": nn, "value": t_solve, "unit": "s", "iterations": st["iterations"], "converged": st["converged"],
+        "residual": st["residual"],
+        "kernels": {"momentum_ms": t_mom, "momentum_GBs": b_mom / (t_mom / 1e3) / 1e9,
+                    "momentum_frac": b_mom / (t_mom / 1e3) / 1e9 / peak, "momentum_bytes": b_mom,
+                    "pressure_ms": t_pres, "pressure_GBs": b_pres / (t_pres / 1e3) / 1e9,
+                    "pressure_frac": b_pres / (t_pres / 1e3) / 1e9 / peak, "pressure_bytes": b_pres,
+                    "peak_GBs": peak, "peak_kind": kind},
+        "cpu_baseline": cpu}), flush=True)
+    return 0
+
+
 def timeloop_mode(args, fem):
     """Time loop of the layered visco-elasto-plastic case (BASELINE config 2 shape): each
     step P0 ← P, solve to the tolerance, τ_old ← τ. Arms, each on its own trajectory:
@@ -439,7 +508,7 @@ def main():
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
     ap.add_argument("--tl-steps", type=int, default=10)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -477,6 +546,8 @@ def main():
         return warmstart_mode(args, fem)
     if args.mode == "timeloop":
         return timeloop_mode(args, fem)
+    if args.mode == "cellpressure":
+        return cellpressure_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()

@@ -31,3 +31,7 @@ from . import warmstart  # noqa: E402,F401
 from . import postprocess  # noqa: E402,F401
 from .postprocess import (compute_strain_rate_stress_postprocess, update_old_stress_from_cells,  # noqa: E402,F401
                           write_vtk, write_stokes_vtk, VtkMesh)
+from . import cellpressure  # noqa: E402,F401
+from .cellpressure import (CellPressureStokesDR, stokes_preconditioner_3d,  # noqa: E402,F401
+                           assemble_stokes_pressure_residual_3d, assemble_stokes_momentum_residual_3d,
+                           solve_cell_pressure)

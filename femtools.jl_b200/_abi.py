@@ -115,6 +115,31 @@ class ThermalStatsC(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int64), ("residual", C.c_double)]
 
 
+class CellPressureProblemC(C.Structure):
+    _fields_ = [
+        ("nels", C.c_int64), ("nnodes", C.c_int64),
+        ("el2n", _vp), ("geo_v", _vp), ("phases", _vp), ("nphases", C.c_int32),
+        ("eta", _dvec), ("rho", _dvec), ("g", C.c_double * 3),
+        ("v", _vp * 3), ("P", _vp), ("Rv", _vp * 3), ("RP", _vp), ("diagonal", _vp * 3), ("pressure_mass", _vp),
+        ("load", _vp * 3), ("bc_dofs", _vp * 3), ("bc_vals", _vp * 3), ("bc_n", C.c_int64 * 3),
+    ]
+
+
+class CellPressureControlsC(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double), ("max_iterations", C.c_int64), ("check_interval", C.c_int64),
+        ("velocity_step", C.c_double), ("pressure_step", C.c_double), ("throw_on_failure", C.c_int32),
+        ("history", C.POINTER(C.c_double)), ("history_capacity", C.c_int64),
+    ]
+
+
+class CellPressureStatsC(C.Structure):
+    _fields_ = [
+        ("converged", C.c_int32), ("reached_total_iter", C.c_int32), ("iterations", C.c_int64),
+        ("residual", C.c_double), ("err_v", C.c_double), ("err_P", C.c_double), ("history_len", C.c_int64),
+    ]
+
+
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libfemtools_b200.so")
 
@@ -160,6 +185,10 @@ SIGNATURES = {
     "femb200_extrapolate_state": (C.c_int, [_vp, _P(StokesProblemC), _vp * 3, _vp * 3, _vp, _vp]),
     "femb200_precompute_geometry": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int32]),
     "femb200_strain_rate_stress": (C.c_int, [_vp, _P(StokesProblemC), _vp * 6, _vp * 14]),
+    "femb200_cell_pressure_preconditioner": (C.c_int, [_vp, _P(CellPressureProblemC)]),
+    "femb200_cell_pressure_residuals": (C.c_int, [_vp, _P(CellPressureProblemC), C.c_int32]),
+    "femb200_solve_cell_pressure": (C.c_int, [_vp, _P(CellPressureProblemC), _P(CellPressureControlsC),
+                                              _P(CellPressureStatsC)]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

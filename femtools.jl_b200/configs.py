@@ -295,3 +295,40 @@ def shear_band_2d_case(n=256, seed=0, dt=0.1, eta_reg=1.0, Kb=10.0, bulk=10.0):
                       tau_old=[np.zeros(mesh.nq * mesh.nels) for _ in range(3)], bc=bc)
     case.meta = dict(center=(cx, cy))
     return case
+
+
+@dataclass
+class CellPressureCase:
+    """A sinking-block configuration of the cell-pressure Hex27 solver: mesh, material,
+    one phase per cell and free-slip walls (wall-normal velocity fixed to zero)."""
+    mesh: object
+    material: object
+    phases: np.ndarray
+    bc: list            # per component: (DoFs, vals)
+
+
+def cell_pressure_case(n=4, seed=0, distort=True, eta=(1.0, 100.0), rho=(1.0, 1.5), half_width=0.25):
+    """Hex27 n³ on the unit cube (interior nodes perturbed by up to 15 % of the node
+    spacing when `distort`), a dense viscous block |x − ½|, |y − ½|, |z − ½| < half_width
+    (phase 2, by cell centroid) in a phase-1 matrix, g = (0, 0, −1), free slip on every wall
+    (the setup of the reference's 3-D sinking-block example, on a structured mesh)."""
+    rng = np.random.default_rng(seed)
+    mesh = _mesh.structured_mixed_mesh(3, (n, n, n))
+    coords = mesh.coords.copy()
+    if distort:
+        h = 1.0 / (2 * n)
+        interior = np.all((coords > 1e-12) & (coords < 1 - 1e-12), axis=1)
+        coords[interior] += rng.uniform(-0.15 * h, 0.15 * h, size=(interior.sum(), 3))
+        geo_v, geo_P = _mesh.precompute_geometry(coords, mesh.el2n, _mesh.element_tables(3))
+        mesh.coords, mesh.geo_v, mesh.geo_P = coords, geo_v, geo_P
+    cen = _mesh.cell_centroids(mesh)
+    inside = np.all(np.abs(cen - 0.5) < half_width, axis=1)
+    phases = np.where(inside, 2, 1).astype(np.int32)
+    material = _problem.StokesMaterial(eta=eta, rho0=rho, g=(0.0, 0.0, -1.0))
+    tol = 32 * np.finfo(float).eps
+    bc = []
+    for d in range(3):
+        on = (np.abs(mesh.coords[:, d]) <= tol) | (np.abs(mesh.coords[:, d] - 1.0) <= tol)
+        dofs = (np.nonzero(on)[0] + 1).astype(np.int32)
+        bc.append((dofs, np.zeros(len(dofs))))
+    return CellPressureCase(mesh, material, phases, bc)

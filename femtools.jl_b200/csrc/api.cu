@@ -1425,6 +1425,74 @@ int check_controls(femb200_handle* h, const femb200_stokes_controls* c) {
 }  // namespace
 
 namespace {
+int check_cp_problem(femb200_handle* h, const femb200_cell_pressure_problem* p) {
+    if (!h) return FEMB200_EINVAL;
+    if (!p) { h->err = "null problem"; return FEMB200_EINVAL; }
+    if (p->nels <= 0 || p->nnodes <= 0) { h->err = "empty mesh"; return FEMB200_EINVAL; }
+    if (p->nphases < 1 || p->nphases > FEMB200_MAX_PHASES) { h->err = "nphases must lie in 1:16"; return FEMB200_EINVAL; }
+    if (!p->el2n || !p->geo_v || !p->phases || !p->P || !p->RP || !p->pressure_mass) {
+        h->err = "mesh, phase, pressure and scratch arrays are required";
+        return FEMB200_EINVAL;
+    }
+    for (int c = 0; c < 3; ++c)
+        if (!p->v[c] || !p->Rv[c] || !p->diagonal[c] || (p->bc_n[c] > 0 && !p->bc_dofs[c]) || p->bc_n[c] < 0) {
+            h->err = "velocity, residual and preconditioner components are required";
+            return FEMB200_EINVAL;
+        }
+    return FEMB200_OK;
+}
+
+CpArgs cp_args(const femb200_cell_pressure_problem* p) {
+    CpArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.nels = p->nels;
+    a.el2n = p->el2n;
+    a.geo_v = p->geo_v;
+    a.phases = p->phases;
+    for (int k = 0; k < FEMB200_MAX_PHASES; ++k) { a.eta[k] = p->eta[k]; a.rho[k] = p->rho[k]; }
+    for (int c = 0; c < 3; ++c) {
+        a.g[c] = p->g[c];
+        a.v[c] = p->v[c];
+        a.Rv[c] = p->Rv[c];
+        a.diagonal[c] = p->diagonal[c];
+    }
+    a.P = p->P;
+    a.RP = p->RP;
+    a.pressure_mass = p->pressure_mass;
+    return a;
+}
+
+// The device checks of the connectivity and the phases (one synchronisation).
+int cp_validate(femb200_handle* h, const femb200_cell_pressure_problem* p) {
+    if (!h->d_flag) {
+        CK(cudaMalloc(&h->d_flag, sizeof(int)));
+        CK(cudaMallocHost(&h->h_flag, sizeof(int)));
+    }
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    CK(launch_cp_validate(p->el2n, p->phases, p->nels, p->nnodes, p->nphases, h->d_flag, h->stream));
+    CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (*h->h_flag & 1) { h->err = "connectivity entry outside 1:nnodes"; return FEMB200_EINVAL; }
+    if (*h->h_flag & 2) { h->err = "phases must lie in 1:nphases"; return FEMB200_EINVAL; }
+    return FEMB200_OK;
+}
+
+int cp_preconditioner(femb200_handle* h, const femb200_cell_pressure_problem* p) {
+    for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(p->diagonal[c], 0, sizeof(double) * p->nnodes, h->stream));
+    CK(launch_cp_preconditioner(cp_args(p), h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
+int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int which) {
+    const CpArgs a = cp_args(p);
+    if (which & 1) CK(launch_cp_pressure_residual(a, h->num_sms, h->stream));
+    if (which & 2) {
+        for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(double) * p->nnodes, h->stream));
+        CK(launch_cp_momentum_residual(a, h->num_sms, h->stream));
+    }
+    return FEMB200_OK;
+}
+
 template <class T, class TG>
 int strain_rate_stress_impl(femb200_handle* h, const femb200_stokes_problem* p, const void* const tau_ip[6],
                             void* const out[14]) {
@@ -1709,6 +1777,90 @@ int femb200_precompute_geometry(femb200_handle* h, int32_t dim, int64_t nels, in
     return FEMB200_OK;
 }
 
+
+int femb200_cell_pressure_preconditioner(femb200_handle* h, const femb200_cell_pressure_problem* p) {
+    RC(check_cp_problem(h, p));
+    RC(ensure_tables(h));
+    RC(cp_validate(h, p));
+    return cp_preconditioner(h, p);
+}
+
+int femb200_cell_pressure_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int32_t which) {
+    RC(check_cp_problem(h, p));
+    if (which < 1 || which > 3) { h->err = "which: bit 0 pressure residual, bit 1 momentum residual"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    RC(cp_validate(h, p));
+    return cp_residuals(h, p, which);
+}
+
+int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_problem* p,
+                                const femb200_cell_pressure_controls* c, femb200_cell_pressure_stats* st) {
+    RC(check_cp_problem(h, p));
+    if (!c || !st) { h->err = "controls and stats are required"; return FEMB200_EINVAL; }
+    if (!(c->tolerance > 0) || c->max_iterations < 1 || c->check_interval < 1 || !std::isfinite(c->velocity_step) ||
+        !std::isfinite(c->pressure_step)) {
+        h->err = "tolerance, max_iterations, check_interval and the step sizes must be positive and finite";
+        return FEMB200_EINVAL;
+    }
+    RC(ensure_tables(h));
+    RC(cp_validate(h, p));
+    std::memset(st, 0, sizeof(*st));
+    const int64_t nn = p->nnodes, nels = p->nels;
+    const cudaStream_t s = h->stream;
+    RC(cp_preconditioner(h, p));
+    // the first residual sees the prescribed boundary velocities too
+    for (int k = 0; k < 3; ++k) CK(launch_dirichlet<double>(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k], s));
+    const int nb = cp_mean_blocks(h->num_sms);
+    RC(ensure_partials(h, nb));
+    double err_v = INFINITY, err_P = INFINITY, err = INFINITY;
+    int64_t iter = 0, hist = 0;
+    for (int64_t it = 1; it <= c->max_iterations; ++it) {
+        iter = it;
+        RC(cp_residuals(h, p, 1));
+        CK(launch_cp_pressure_update(p->P, p->RP, p->pressure_mass, nels, c->pressure_step, h->d_partials, nb, s));
+        RC(cp_residuals(h, p, 2));
+        for (int k = 0; k < 3; ++k) {
+            if (p->load[k]) CK(launch_cp_subtract(p->Rv[k], p->load[k], nn, s));
+            CK(launch_dirichlet<double>(p->Rv[k], p->bc_dofs[k], nullptr, p->bc_n[k], s));
+            CK(launch_cp_velocity_update(p->v[k], p->Rv[k], p->diagonal[k], nn, c->velocity_step, s));
+            CK(launch_dirichlet<double>(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k], s));
+        }
+        if (!(it % c->check_interval == 0 || it == c->max_iterations)) continue;
+        err_v = 0;
+        for (int k = 0; k < 3; ++k) {
+            double ss = 0;
+            RC(sumsq<double>(h, p->Rv[k], nullptr, nn, ss));
+            err_v = std::max(err_v, std::sqrt(ss));
+        }
+        double sp = 0;
+        RC(sumsq<double>(h, p->RP, nullptr, 4 * nels, sp));
+        err_P = std::sqrt(sp);
+        err = std::max(err_v, err_P);
+        if (!std::isfinite(err)) { h->err = "non-finite residual in 3-D Stokes solve"; return FEMB200_ENONFINITE; }
+        if (c->history && hist < c->history_capacity) {
+            c->history[3 * hist] = (double)it;
+            c->history[3 * hist + 1] = err_v;
+            c->history[3 * hist + 2] = err_P;
+            ++hist;
+        }
+        if (err < c->tolerance) break;
+    }
+    st->converged = err < c->tolerance;
+    st->iterations = iter;
+    st->residual = err;
+    st->err_v = err_v;
+    st->err_P = err_P;
+    st->reached_total_iter = iter >= c->max_iterations && !st->converged;
+    st->history_len = hist;
+    if (!st->converged && c->throw_on_failure) {
+        char b[160];
+        std::snprintf(b, sizeof b, "3-D Stokes solve did not converge after %lld iterations (residual = %g, tolerance = %g)",
+                      (long long)iter, err, c->tolerance);
+        h->err = b;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
+}
 
 int femb200_strain_rate_stress(femb200_handle* h, const femb200_stokes_problem* p, const void* const tau_ip[6],
                                void* const out[14]) {

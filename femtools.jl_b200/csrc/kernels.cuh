@@ -171,6 +171,32 @@ cudaError_t launch_grid_fields(const T* vx, const T* vy, const T* P, const int32
 cudaError_t launch_net_input(const float* Fp, const float* Fc, const float* s, void* X, int64_t npix, cudaStream_t st);
 cudaError_t launch_net_target(const float* Fp, const float* Fc, const float* Fn, const float* s, float* tgt, int64_t npix,
                               cudaStream_t st);
+// Cell-pressure Hex27 Stokes (cellpressure.cu): FP64, P / RP / pressure_mass 4 × nels.
+struct CpArgs {
+    int64_t nels;
+    const int32_t* el2n;
+    const double* geo_v;
+    const int32_t* phases;
+    double eta[FEMB200_MAX_PHASES], rho[FEMB200_MAX_PHASES], g[3];
+    const double* v[3];
+    const double* P;
+    double* Rv[3];
+    double* RP;
+    double* diagonal[3];
+    double* pressure_mass;
+};
+cudaError_t launch_cp_pressure_residual(const CpArgs& a, int num_sms, cudaStream_t st);
+cudaError_t launch_cp_momentum_residual(const CpArgs& a, int num_sms, cudaStream_t st);
+cudaError_t launch_cp_preconditioner(const CpArgs& a, int num_sms, cudaStream_t st);
+int cp_mean_blocks(int num_sms);
+cudaError_t launch_cp_validate(const int32_t* el2n, const int32_t* phases, int64_t nels, int64_t nnodes, int nphases,
+                               int* bad, cudaStream_t st);
+cudaError_t launch_cp_pressure_update(double* P, const double* RP, const double* M, int64_t nels, double step,
+                                      double* partials, int nb, cudaStream_t st);
+cudaError_t launch_cp_velocity_update(double* v, const double* R, const double* diag, int64_t n, double step,
+                                      cudaStream_t st);
+cudaError_t launch_cp_subtract(double* R, const double* load, int64_t n, cudaStream_t st);
+
 // Element-averaged strain-rate and stress diagnostics (postprocess.cu).
 template <class T, class TG>
 struct PostArgs {

@@ -11,11 +11,11 @@ namespace {
 
 template <int DIM> struct PpTabs;
 template <> struct PpTabs<3> {
-    static constexpr int NV = 27, NF = 14, NT = 6;
+    static constexpr int NV = 27, NF = 14;
     FEMB_D static double dN(int q, int a, int j) { return c_tab.dN3[q][a][j]; }
 };
 template <> struct PpTabs<2> {
-    static constexpr int NV = 9, NF = 10, NT = 3;
+    static constexpr int NV = 9, NF = 10;
     FEMB_D static double dN(int q, int a, int j) { return c_tab.dN2[q][a][j]; }
 };
 

@@ -230,6 +230,50 @@ typedef struct femb200_thermal_stats {
     double residual;
 } femb200_thermal_stats;
 
+/* Viscous incompressible Hex27 Stokes with four cell-local pressure modes (1, ξ, η, ζ)
+ * per cell (CellPressureStokesDR, src/stokes/types/stokes_types.jl:567-613). FP64
+ * device arrays; P, RP and pressure_mass are 4 × nels (column-major: mode fastest). */
+typedef struct femb200_cell_pressure_problem {
+    int64_t nels, nnodes;
+    const int32_t* el2n;          /* 27 × nels, 1-based */
+    const double* geo_v;          /* nels × 27 × 10: J⁻¹ (column-major), |det J|·ω */
+    const int32_t* phases;        /* one phase per cell, 1-based */
+    int32_t nphases;
+    double eta[FEMB200_MAX_PHASES];
+    double rho[FEMB200_MAX_PHASES];
+    double g[3];
+    double* v[3];
+    double* P;
+    double* Rv[3];
+    double* RP;
+    double* diagonal[3];          /* Jacobi preconditioner */
+    double* pressure_mass;        /* lumped mass of the pressure modes */
+    const double* load[3];        /* NULL, or a momentum right-hand side subtracted from Rv */
+    const int32_t* bc_dofs[3];
+    const double* bc_vals[3];     /* NULL → homogeneous */
+    int64_t bc_n[3];
+} femb200_cell_pressure_problem;
+
+/* Controls of solve!(dr::CellPressureStokesDR, mesh, bc_v; …) (src/stokes/solvers/DR.jl:980-1002). */
+typedef struct femb200_cell_pressure_controls {
+    double tolerance;             /* 1e-5 */
+    int64_t max_iterations;       /* 3000 */
+    int64_t check_interval;       /* 100 */
+    double velocity_step;         /* 0.6 */
+    double pressure_step;         /* 0.2 */
+    int32_t throw_on_failure;     /* nonzero: FEMB200_ENOTCONV when not converged */
+    double* history;              /* optional (iter, err_v, err_P) per check */
+    int64_t history_capacity;
+} femb200_cell_pressure_controls;
+
+typedef struct femb200_cell_pressure_stats {
+    int32_t converged;
+    int32_t reached_total_iter;
+    int64_t iterations;
+    double residual, err_v, err_P;
+    int64_t history_len;
+} femb200_cell_pressure_stats;
+
 /* ---- handle -------------------------------------------------------------- */
 typedef struct femb200_handle femb200_handle;
 
@@ -397,6 +441,25 @@ int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p,
 int femb200_precompute_geometry(femb200_handle* h, int32_t dim, int64_t nels, int64_t nnodes,
                                 const double* coords, const int32_t* el2n, void* geo_v, void* geo_P,
                                 int32_t geo_dtype);
+
+/* ---- cell-pressure Hex27 Stokes (src/stokes/solvers/DR.jl:980-1057) ---- */
+/* stokes_preconditioner_3d! (momentum_residuals.jl:703-745): diagonal_c(a) =
+ * Σ η_phase (|∇N_a|² + (∂_c N_a)²/3) dΩ and pressure_mass(m, e) = Σ mode_m² dΩ. */
+int femb200_cell_pressure_preconditioner(femb200_handle* h, const femb200_cell_pressure_problem* p);
+/* which bit 0: assemble_stokes_pressure_residual_3d! (pressure_residual.jl:330-364),
+ * RP(m, e) = −Σ_q mode_m ∇·v dΩ; bit 1: assemble_stokes_momentum_residual_3d!
+ * (momentum_residuals.jl:644-700), Rv = ∫ ∇N·(2η ε̇′ − P I) − N ρ g dΩ with η and ρ
+ * interpolated over the cell (the reference's interp2ip_phase). The load is not
+ * subtracted here. Connectivity outside 1..nnodes or phases outside 1..nphases return
+ * FEMB200_EINVAL before any kernel reads by them. */
+int femb200_cell_pressure_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int32_t which);
+/* The Arrow–Hurwicz dynamic relaxation of _relax_cell_pressure_stokes! (DR.jl:1004-1057):
+ * P += pressure_step·RP/M, mean of mode 1 removed, v −= velocity_step·Rv/diagonal with
+ * the Dirichlet values reapplied; every check_interval iterations (and at the last)
+ * err = max(max_c ‖Rv_c‖, ‖RP‖) against the tolerance. The mean removal stays on the
+ * device; only checks synchronise. */
+int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_problem* p,
+                                const femb200_cell_pressure_controls* c, femb200_cell_pressure_stats* st);
 
 /* ---- post-processing (src/postprocess/postprocess.jl:17-79, :168-215) ---- */
 /* compute_strain_rate_stress_postprocess from integration-point stresses: per element,

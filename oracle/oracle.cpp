@@ -1044,6 +1044,169 @@ int solve_stokes_impl(const femb200_stokes_problem* p, const femb200_stokes_cont
     return FEMB200_OK;
 }
 
+// ---- CellPressureStokesDR (viscous Hex27, four cell-local pressure modes) ----
+// The modes (1, ξ, η, ζ) at the Gauss points (pressure_mode_table,
+// momentum_residuals.jl:618-621); ξ, η, ζ are the P1 rows 2..4 of the tables.
+inline double cp_mode(const Tables& t, int q, int m) { return m == 0 ? 1.0 : t.NP[q][m]; }
+
+// ∂N_a/∂x_k at q from the element geometry (element_geometry, mesh.jl:504-507).
+inline void cp_dNdx(const Tables& t, const double* g, int q, int a, double out[3]) {
+    for (int k = 0; k < 3; ++k) out[k] = t.dN[q][a][0] * g[3 * k] + t.dN[q][a][1] * g[1 + 3 * k] + t.dN[q][a][2] * g[2 + 3 * k];
+}
+
+// stokes_preconditioner_3d_kernel! (momentum_residuals.jl:728-745)
+void cp_preconditioner_impl(const femb200_cell_pressure_problem* p) {
+    const Tables& t = tables_for(3);
+    for (int c = 0; c < 3; ++c) std::fill(p->diagonal[c], p->diagonal[c] + p->nnodes, 0.0);
+    std::fill(p->pressure_mass, p->pressure_mass + 4 * p->nels, 0.0);
+    for (int64_t e = 0; e < p->nels; ++e) {
+        const double eta = p->eta[p->phases[e] - 1];
+        for (int q = 0; q < 27; ++q) {
+            const double* g = p->geo_v + (e * 27 + q) * 10;
+            const double dO = g[9];
+            for (int a = 0; a < 27; ++a) {
+                double gr[3];
+                cp_dNdx(t, g, q, a, gr);
+                const int64_t node = p->el2n[27 * e + a] - 1;
+                const double n2 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+                for (int c = 0; c < 3; ++c) p->diagonal[c][node] += eta * (n2 + gr[c] * gr[c] / 3) * dO;
+            }
+            for (int m = 0; m < 4; ++m) p->pressure_mass[4 * e + m] += cp_mode(t, q, m) * cp_mode(t, q, m) * dO;
+        }
+    }
+}
+
+// velocity gradient ∂v_c/∂x_k at q
+inline void cp_grad(const Tables& t, const femb200_cell_pressure_problem* p, int64_t e, int q, double gv[3][3]) {
+    const double* g = p->geo_v + (e * 27 + q) * 10;
+    for (int c = 0; c < 3; ++c)
+        for (int k = 0; k < 3; ++k) gv[c][k] = 0;
+    for (int a = 0; a < 27; ++a) {
+        double gr[3];
+        cp_dNdx(t, g, q, a, gr);
+        const int64_t node = p->el2n[27 * e + a] - 1;
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 3; ++k) gv[c][k] += p->v[c][node] * gr[k];
+    }
+}
+
+// stokes_pressure_residual_3d_kernel! (pressure_residual.jl:352-364): RP = −Σ mode ∇·v dΩ
+void cp_pressure_residual_impl(const femb200_cell_pressure_problem* p) {
+    const Tables& t = tables_for(3);
+    for (int64_t e = 0; e < p->nels; ++e) {
+        double r[4] = {0, 0, 0, 0};
+        for (int q = 0; q < 27; ++q) {
+            double gv[3][3];
+            cp_grad(t, p, e, q, gv);
+            const double dO = p->geo_v[(e * 27 + q) * 10 + 9];
+            const double div = gv[0][0] + gv[1][1] + gv[2][2];
+            for (int m = 0; m < 4; ++m) r[m] -= cp_mode(t, q, m) * (div * dO);
+        }
+        for (int m = 0; m < 4; ++m) p->RP[4 * e + m] = r[m];
+    }
+}
+
+// stokes_momentum_residual_3d_kernel! (momentum_residuals.jl:675-700) through
+// integrate_momentum_residual (:221-258) with G = K = ∞, α = 0: viscous stress 2ηε̇′,
+// pressure from the modes, ρ = interp(ρ0), accumulate_momentum (:28-33).
+void cp_momentum_residual_impl(const femb200_cell_pressure_problem* p) {
+    const Tables& t = tables_for(3);
+    for (int c = 0; c < 3; ++c) std::fill(p->Rv[c], p->Rv[c] + p->nnodes, 0.0);
+    for (int64_t e = 0; e < p->nels; ++e) {
+        const int ph = p->phases[e] - 1;
+        double R[3][27] = {{0}};
+        for (int q = 0; q < 27; ++q) {
+            const double* g = p->geo_v + (e * 27 + q) * 10;
+            const double dO = g[9];
+            double gv[3][3];
+            cp_grad(t, p, e, q, gv);
+            double eta_q = 0, rho_q = 0;     // interp2ip_phase over the cell's (single) phase
+            for (int a = 0; a < 27; ++a) { eta_q += t.N[q][a] * p->eta[ph]; rho_q += t.N[q][a] * p->rho[ph]; }
+            const double tr = (gv[0][0] + gv[1][1] + gv[2][2]) / 3;
+            double Pq = 0;
+            for (int m = 0; m < 4; ++m) Pq += cp_mode(t, q, m) * p->P[4 * e + m];
+            double sig[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    sig[i][j] = 2 * eta_q * ((gv[i][j] + gv[j][i]) / 2 - (i == j ? tr : 0.0)) - (i == j ? Pq : 0.0);
+            for (int a = 0; a < 27; ++a) {
+                double gr[3];
+                cp_dNdx(t, g, q, a, gr);
+                for (int i = 0; i < 3; ++i) {
+                    double f = 0;
+                    for (int j = 0; j < 3; ++j) f += gr[j] * sig[j][i];
+                    R[i][a] += (f - t.N[q][a] * (rho_q * p->g[i])) * dO;
+                }
+            }
+        }
+        for (int a = 0; a < 27; ++a) {
+            const int64_t node = p->el2n[27 * e + a] - 1;
+            for (int i = 0; i < 3; ++i) p->Rv[i][node] += R[i][a];
+        }
+    }
+}
+
+inline void cp_dirichlet(double* x, const int32_t* dofs, const double* vals, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) x[dofs[i] - 1] = vals ? vals[i] : 0.0;
+}
+
+// _relax_cell_pressure_stokes! (DR.jl:1004-1057)
+int cp_solve_impl(const femb200_cell_pressure_problem* p, const femb200_cell_pressure_controls* c,
+                  femb200_cell_pressure_stats* st) {
+    std::memset(st, 0, sizeof(*st));
+    cp_preconditioner_impl(p);
+    for (int k = 0; k < 3; ++k) cp_dirichlet(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k]);
+    double err_v = INFINITY, err_P = INFINITY, err = INFINITY;
+    int64_t iter = 0, hist = 0;
+    for (int64_t it = 1; it <= c->max_iterations; ++it) {
+        iter = it;
+        cp_pressure_residual_impl(p);
+        for (int64_t i = 0; i < 4 * p->nels; ++i) p->P[i] += c->pressure_step * p->RP[i] / p->pressure_mass[i];
+        double s0 = 0, s1 = 0;
+        for (int64_t e = 0; e < p->nels; ++e) { s0 += p->P[4 * e] * p->pressure_mass[4 * e]; s1 += p->pressure_mass[4 * e]; }
+        const double pmean = s0 / s1;
+        for (int64_t e = 0; e < p->nels; ++e) p->P[4 * e] -= pmean;
+        cp_momentum_residual_impl(p);
+        for (int k = 0; k < 3; ++k) {
+            if (p->load[k])
+                for (int64_t i = 0; i < p->nnodes; ++i) p->Rv[k][i] -= p->load[k][i];
+            cp_dirichlet(p->Rv[k], p->bc_dofs[k], nullptr, p->bc_n[k]);
+            for (int64_t i = 0; i < p->nnodes; ++i) p->v[k][i] -= c->velocity_step * p->Rv[k][i] / p->diagonal[k][i];
+            cp_dirichlet(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k]);
+        }
+        if (!(it % c->check_interval == 0 || it == c->max_iterations)) continue;
+        err_v = 0;
+        for (int k = 0; k < 3; ++k) {
+            double ss = 0;
+            for (int64_t i = 0; i < p->nnodes; ++i) ss += p->Rv[k][i] * p->Rv[k][i];
+            err_v = std::max(err_v, std::sqrt(ss));
+        }
+        double sp = 0;
+        for (int64_t i = 0; i < 4 * p->nels; ++i) sp += p->RP[i] * p->RP[i];
+        err_P = std::sqrt(sp);
+        err = std::max(err_v, err_P);
+        if (!std::isfinite(err)) { g_last_error = "non-finite residual in 3-D Stokes solve"; return FEMB200_ENONFINITE; }
+        if (c->history && hist < c->history_capacity) {
+            c->history[3 * hist] = (double)it; c->history[3 * hist + 1] = err_v; c->history[3 * hist + 2] = err_P;
+            ++hist;
+        }
+        if (err < c->tolerance) break;
+    }
+    st->converged = err < c->tolerance;
+    st->iterations = iter;
+    st->residual = err; st->err_v = err_v; st->err_P = err_P;
+    st->reached_total_iter = iter >= c->max_iterations && !st->converged;
+    st->history_len = hist;
+    if (!st->converged && c->throw_on_failure) {
+        char b[160];
+        std::snprintf(b, sizeof b, "3-D Stokes solve did not converge after %lld iterations (residual = %g, tolerance = %g)",
+                      (long long)iter, err, c->tolerance);
+        g_last_error = b;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1313,6 +1476,22 @@ int orc_solve_coupled(femb200_thermal_problem* t, const femb200_stokes_problem* 
     Coupled cp{t, Tref, shear_heating ? phi : nullptr};
     rc = solve_stokes_impl(p, c, st, &cp);
     return rc;
+}
+
+int orc_cell_pressure_preconditioner(const femb200_cell_pressure_problem* p) {
+    cp_preconditioner_impl(p);
+    return 0;
+}
+
+int orc_cell_pressure_residuals(const femb200_cell_pressure_problem* p, int32_t which) {
+    if (which & 1) cp_pressure_residual_impl(p);
+    if (which & 2) cp_momentum_residual_impl(p);
+    return 0;
+}
+
+int orc_solve_cell_pressure(const femb200_cell_pressure_problem* p, const femb200_cell_pressure_controls* c,
+                            femb200_cell_pressure_stats* st) {
+    return cp_solve_impl(p, c, st);
 }
 
 }  // extern "C"

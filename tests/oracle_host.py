@@ -39,6 +39,10 @@ def lib():
             "orc_structured_mesh": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
             "orc_geometry": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
             "orc_strain_rate_stress": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp * 3, _vp * 6, _vp * 14]),
+            "orc_cell_pressure_preconditioner": (C.c_int, [_P(abi.CellPressureProblemC)]),
+            "orc_cell_pressure_residuals": (C.c_int, [_P(abi.CellPressureProblemC), C.c_int32]),
+            "orc_solve_cell_pressure": (C.c_int, [_P(abi.CellPressureProblemC), _P(abi.CellPressureControlsC),
+                                                  _P(abi.CellPressureStatsC)]),
             "orc_pressure_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
             "orc_momentum_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
             "orc_stokes_residuals": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32]),
@@ -306,3 +310,63 @@ def strain_rate_stress(dim, el2n, geo_v, v, tau):
     op = (C.c_void_p * 14)(*([ptr(x) for x in out] + [0] * (14 - nf)))
     check(lib().orc_strain_rate_stress(dim, nels, ptr(el2n), ptr(geo_v), vp, tp, op))
     return out
+
+
+class HostCellPressure:
+    """Oracle state of the cell-pressure Hex27 Stokes problem (host numpy arrays)."""
+
+    def __init__(self, mesh, eta, rho, g, phases, v=None, P=None):
+        self.mesh = mesh
+        nn, ne = mesh.nnodes, mesh.nels
+        self.el2n = np.ascontiguousarray(mesh.el2n, dtype=np.int32)
+        self.geo_v = np.ascontiguousarray(mesh.geo_v, dtype=np.float64)
+        self.phases = np.ascontiguousarray(phases, dtype=np.int32)
+        self.eta, self.rho, self.g = tuple(eta), tuple(rho), tuple(g)
+        self.v = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in v] if v is not None else \
+            [np.zeros(nn) for _ in range(3)]
+        self.P = np.ascontiguousarray(P, dtype=np.float64).copy() if P is not None else np.zeros(4 * ne)
+        self.Rv = [np.zeros(nn) for _ in range(3)]
+        self.RP = np.zeros(4 * ne)
+        self.diagonal = [np.zeros(nn) for _ in range(3)]
+        self.pressure_mass = np.zeros(4 * ne)
+        self._keep = []
+
+    def struct(self, bc=None, load=None):
+        p = abi.CellPressureProblemC()
+        p.nels, p.nnodes = self.mesh.nels, self.mesh.nnodes
+        p.el2n, p.geo_v, p.phases = ptr(self.el2n), ptr(self.geo_v), ptr(self.phases)
+        p.nphases = len(self.eta)
+        for i in range(len(self.eta)):
+            p.eta[i], p.rho[i] = self.eta[i], self.rho[i]
+        keep = []
+        for c in range(3):
+            p.g[c] = self.g[c]
+            p.v[c], p.Rv[c], p.diagonal[c] = ptr(self.v[c]), ptr(self.Rv[c]), ptr(self.diagonal[c])
+            if load is not None:
+                ld = np.ascontiguousarray(load[c], dtype=np.float64)
+                keep.append(ld)
+                p.load[c] = ptr(ld)
+            if bc is not None and bc[c] is not None:
+                d = np.ascontiguousarray(bc[c][0], dtype=np.int32)
+                vv = np.ascontiguousarray(np.broadcast_to(np.asarray(bc[c][1], dtype=np.float64), d.shape))
+                keep += [d, vv]
+                p.bc_dofs[c], p.bc_vals[c], p.bc_n[c] = ptr(d), ptr(vv), len(d)
+        p.P, p.RP, p.pressure_mass = ptr(self.P), ptr(self.RP), ptr(self.pressure_mass)
+        self._keep = keep
+        return p
+
+    def preconditioner(self):
+        check(lib().orc_cell_pressure_preconditioner(C.byref(self.struct())))
+
+    def residuals(self, which=3):
+        check(lib().orc_cell_pressure_residuals(C.byref(self.struct()), which))
+
+    def solve(self, bc, tolerance=1e-5, max_iterations=3000, check_interval=100, velocity_step=0.6,
+              pressure_step=0.2, throw_on_failure=True, load=None):
+        p = self.struct(bc, load)
+        c = abi.CellPressureControlsC()
+        c.tolerance, c.max_iterations, c.check_interval = tolerance, max_iterations, check_interval
+        c.velocity_step, c.pressure_step, c.throw_on_failure = velocity_step, pressure_step, int(throw_on_failure)
+        st = abi.CellPressureStatsC()
+        check(lib().orc_solve_cell_pressure(C.byref(p), C.byref(c), C.byref(st)))
+        return st

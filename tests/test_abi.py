@@ -46,6 +46,9 @@ STRUCTS = {
     "femb200_thermal_problem": abi.ThermalProblemC,
     "femb200_thermal_controls": abi.ThermalControlsC,
     "femb200_thermal_stats": abi.ThermalStatsC,
+    "femb200_cell_pressure_problem": abi.CellPressureProblemC,
+    "femb200_cell_pressure_controls": abi.CellPressureControlsC,
+    "femb200_cell_pressure_stats": abi.CellPressureStatsC,
 }
 
 

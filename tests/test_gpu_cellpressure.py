@@ -1,0 +1,106 @@
+"""Cell-pressure Hex27 Stokes (CellPressureStokesDR) through the C ABI against the CPU
+oracle (itself pinned to the sparse saddle-point system in test_cellpressure_oracle.py).
+Element sums run in a different order on the device (warp reductions, FP64 atomics),
+so assemblies agree to 1e-12 of their largest entry; full relaxations take the same
+number of iterations and agree to 1e-9 relative."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_host as oh
+from conftest import fem
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+abi = fem._abi
+
+
+def host(x):
+    return x.detach().cpu().numpy()
+
+
+def close(got, want, rel):
+    np.testing.assert_allclose(host(got), want, rtol=0, atol=rel * max(np.abs(want).max(), 1e-300))
+
+
+def states(n=3, seed=4, distort=True, random=True):
+    case = fem.configs.cell_pressure_case(n=n, seed=seed, distort=distort)
+    rng = np.random.default_rng(seed + 10)
+    v = [rng.standard_normal(case.mesh.nnodes) for _ in range(3)] if random else None
+    P = rng.standard_normal(4 * case.mesh.nels) if random else None
+    dr = fem.CellPressureStokesDR(case.mesh, case.material, phases=case.phases)
+    if random:
+        for c in range(3):
+            dr.v[c].copy_(torch.as_tensor(v[c], device="cuda"))
+        dr.P.copy_(torch.as_tensor(P, device="cuda"))
+    hs = oh.HostCellPressure(case.mesh, case.material.eta, case.material.rho0, case.material.g, case.phases, v, P)
+    return case, dr, hs
+
+
+@pytest.mark.parametrize("distort", [False, True])
+def test_assemblies_match_oracle(distort):
+    case, dr, hs = states(distort=distort)
+    fem.stokes_preconditioner_3d(dr)
+    fem.assemble_stokes_pressure_residual_3d(dr)
+    fem.assemble_stokes_momentum_residual_3d(dr)
+    hs.preconditioner()
+    hs.residuals(3)
+    for c in range(3):
+        close(dr.diagonal[c], hs.diagonal[c], 1e-12)
+        close(dr.Rv[c], hs.Rv[c], 1e-12)
+    close(dr.pressure_mass, hs.pressure_mass, 1e-12)
+    close(dr.RP, hs.RP, 1e-12)
+
+
+def test_solve_matches_oracle():
+    case, dr, hs = states(n=3, seed=2, random=False)
+    kw = dict(tolerance=1e-8, max_iterations=100000, check_interval=100)
+    st = fem.solve_cell_pressure(dr, case.bc, collect_history=True, **kw)
+    ref = hs.solve(case.bc, **kw)
+    assert st["converged"] and ref.converged
+    assert st["iterations"] == ref.iterations
+    assert len(st["history"]) == ref.iterations // 100
+    for c in range(3):
+        close(dr.v[c], hs.v[c], 1e-9)
+    close(dr.P, hs.P, 1e-9)
+    # boundary velocities pinned, the mean of the constant mode removed
+    for c in range(3):
+        assert torch.all(dr.v[c][torch.as_tensor(case.bc[c][0] - 1, device="cuda").long()] == 0)
+    M0 = host(dr.pressure_mass)[0::4]
+    assert abs((host(dr.P)[0::4] * M0).sum()) <= 1e-12 * np.abs(host(dr.P)).max() * M0.sum()
+
+
+def test_load_stands_in_for_gravity():
+    # the same block driven by a momentum load instead of gravity reaches the same state
+    case, dr, _ = states(n=2, seed=3, random=False)
+    fem.assemble_stokes_momentum_residual_3d(dr)                  # v = 0, P = 0: Rv = −∫ N ρ g
+    load = [(-r).clone() for r in dr.Rv]
+    kw = dict(tolerance=1e-9, max_iterations=100000, check_interval=100)
+    fem.solve_cell_pressure(dr, case.bc, **kw)
+    mat0 = fem.StokesMaterial(eta=case.material.eta, rho0=case.material.rho0, g=(0.0, 0.0, 0.0))
+    dr0 = fem.CellPressureStokesDR(case.mesh, mat0, phases=case.phases)
+    fem.solve_cell_pressure(dr0, case.bc, load=load, **kw)
+    for c in range(3):
+        close(dr0.v[c], host(dr.v[c]), 1e-6)
+
+
+def test_non_convergence_and_validation():
+    case, dr, _ = states(n=2, seed=1, random=False)
+    with pytest.raises(abi.FemB200Error, match="3-D Stokes solve did not converge after 200 iterations"):
+        fem.solve_cell_pressure(dr, case.bc, tolerance=1e-14, max_iterations=200)
+    st = fem.solve_cell_pressure(dr, case.bc, tolerance=1e-14, max_iterations=150, throw_on_failure=False)
+    assert not st["converged"] and st["reached_total_iter"] and st["iterations"] == 150
+    with pytest.raises(ValueError, match="phases must lie in 1:2"):
+        fem.CellPressureStokesDR(case.mesh, case.material, phases=np.full(case.mesh.nels, 3))
+    with pytest.raises(ValueError, match="purely viscous"):
+        fem.CellPressureStokesDR(case.mesh, fem.StokesMaterial(eta=(1.0,), G=(1.0,), g=(0.0, 0.0, -1.0)))
+    # the library checks phases and connectivity on the device before any gather by them
+    lib, h = fem.solver._Handle.get()
+    dr.phases.fill_(5)
+    with pytest.raises(abi.FemB200Error, match="phases must lie in 1:nphases"):
+        fem.solver._check(lib, h, lib.femb200_cell_pressure_residuals(h, C.byref(dr.problem()), 3))
+    dr.phases.fill_(1)
+    dr.el2n[0, 3] = case.mesh.nnodes + 7
+    with pytest.raises(abi.FemB200Error, match="connectivity entry outside"):
+        fem.solve_cell_pressure(dr, case.bc)
