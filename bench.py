@@ -408,6 +408,75 @@ def cellpressure_mode(args, fem):
     return 0
 
 
+def lithostatic_mode(args, fem):
+    """Lithostatic pressure (LithostaticPressureDR) on a structured Hex27 n³ mesh: two
+    phases in horizontal layers, a temperature that falls with height, the EOS with a
+    finite bulk modulus, P = 0 on the top; solved from zero to the reference's default
+    relative tolerance 1e-6. Prints one JSON line: solve time and iterations, the
+    residual kernel's per-launch time (with and without the Jacobian diagnostics), and
+    the oracle's time per iteration on a bounded sample extrapolated to the GPU count."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    n = args.n
+    mesh = fem.structured_mixed_mesh(3, (n, n, n))
+    z = mesh.coords[:, 2]
+    ph = np.where(z < 0.5, 1, 2).astype(np.int32)
+    mat = dict(rho0=(3.3, 2.8), alpha=(3e-2, 3e-2), K=(100.0, 80.0))
+    T = 1.0 - z
+    top = (np.nonzero(np.abs(z - 1.0) < 1e-12)[0] + 1).astype(np.int32)
+    bc = (top, np.zeros(len(top)))
+    g = (0.0, 0.0, -1.0)
+    dr = fem.LithostaticPressureDR(mesh, phases=ph, **mat)
+    dr.T.copy_(torch.as_tensor(T, device="cuda"))
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        fem.assemble_lithostatic_pressure(dr, Tref=0.0, g=g, compute_jacobian=True)
+    k = max(args.steps, 5)
+    e0, e1, e2 = ev(), ev(), ev()
+    e0.record()
+    for _ in range(k):
+        fem.assemble_lithostatic_pressure(dr, Tref=0.0, g=g)
+    e1.record()
+    for _ in range(k):
+        fem.assemble_lithostatic_pressure(dr, Tref=0.0, g=g, compute_jacobian=True)
+    e2.record()
+    torch.cuda.synchronize()
+    t_res, t_jac = e0.elapsed_time(e1) / k, e1.elapsed_time(e2) / k
+    dr.P.zero_()
+    dr.rate.zero_()
+    s0, s1 = ev(), ev()
+    s0.record()
+    st = fem.solve_lithostatic(dr, bc, Tref=0.0, g=g, tolerance=1e-6, max_iterations=args.max_iterations,
+                               throw_on_failure=False)
+    s1.record()
+    torch.cuda.synchronize()
+    t_solve = s0.elapsed_time(s1) / 1e3
+    ne, nn = mesh.nels, mesh.nnodes
+    nbytes = ne * 27 * 10 * 8 + ne * 27 * 4 + nn * 8 * 3 + nn * 4 + nn * 8 * 2   # geometry, el2n, P/T + phase, R RMW
+    peak, kind = measured_peaks()
+    cpu = None
+    if not args.no_cpu_baseline:
+        hs = oh.HostLithostatic(mesh, phases=ph, T=T, **mat)
+        sample = 10
+        t0 = time.perf_counter()
+        hs.solve(bc, Tref=0.0, g=g, tolerance=0.0, max_iterations=sample, check_interval=sample,
+                 throw_on_failure=False)
+        per_it = (time.perf_counter() - t0) / sample
+        cpu = {"value": per_it * st["iterations"], "unit": "s", "cores": 1, "kind": "port",
+               "sample": f"{sample} oracle iterations at {mesh.nel} ({per_it:.3f} s each, serial, one with the "
+                         f"Jacobian), extrapolated to {st['iterations']} iterations"}
+    print(json.dumps({
+        "mode": "lithostatic", "workload": f"layered-lithostatic-hex27-{n}^3", "nels": ne, "nnodes": nn,
+        "value": t_solve, "unit": "s", "iterations": st["iterations"], "converged": st["converged"],
+        "residual": st["residual"],
+        "kernels": {"residual_ms": t_res, "residual_GBs": nbytes / (t_res / 1e3) / 1e9,
+                    "residual_frac": nbytes / (t_res / 1e3) / 1e9 / peak, "residual_bytes": nbytes,
+                    "residual_with_jacobian_ms": t_jac, "peak_GBs": peak, "peak_kind": kind},
+        "cpu_baseline": cpu}), flush=True)
+    return 0
+
+
 def timeloop_mode(args, fem):
     """Time loop of the layered visco-elasto-plastic case (BASELINE config 2 shape): each
     step P0 ← P, solve to the tolerance, τ_old ← τ. Arms, each on its own trajectory:
@@ -508,7 +577,7 @@ def main():
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
     ap.add_argument("--tl-steps", type=int, default=10)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -548,6 +617,8 @@ def main():
         return timeloop_mode(args, fem)
     if args.mode == "cellpressure":
         return cellpressure_mode(args, fem)
+    if args.mode == "lithostatic":
+        return lithostatic_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()

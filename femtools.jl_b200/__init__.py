@@ -35,3 +35,5 @@ from . import cellpressure  # noqa: E402,F401
 from .cellpressure import (CellPressureStokesDR, stokes_preconditioner_3d,  # noqa: E402,F401
                            assemble_stokes_pressure_residual_3d, assemble_stokes_momentum_residual_3d,
                            solve_cell_pressure)
+from . import lithostatic  # noqa: E402,F401
+from .lithostatic import LithostaticPressureDR, assemble_lithostatic_pressure, solve_lithostatic  # noqa: E402,F401

@@ -115,6 +115,26 @@ class ThermalStatsC(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int64), ("residual", C.c_double)]
 
 
+class LithostaticProblemC(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("nv", C.c_int32), ("nq", C.c_int32),
+        ("nels", C.c_int64), ("nnodes", C.c_int64),
+        ("el2n", _vp), ("geo", _vp),
+        ("P", _vp), ("rate", _vp), ("R", _vp), ("R0", _vp), ("dRdP", _vp), ("PC", _vp),
+        ("T", _vp), ("phases", _vp), ("phases_layout", C.c_int32),
+        ("nphases", C.c_int32), ("rho0", _dvec), ("alpha", _dvec), ("K", _dvec),
+        ("bc_dofs", _vp), ("bc_vals", _vp), ("bc_n", C.c_int64),
+        ("cfl", C.c_double), ("c_fact", C.c_double), ("eps", C.c_double),
+    ]
+
+
+class LithostaticControlsC(C.Structure):
+    _fields_ = [
+        ("Tref", C.c_double), ("g", C.c_double * 3), ("tolerance", C.c_double),
+        ("max_iterations", C.c_int64), ("check_interval", C.c_int64), ("throw_on_failure", C.c_int32),
+    ]
+
+
 class CellPressureProblemC(C.Structure):
     _fields_ = [
         ("nels", C.c_int64), ("nnodes", C.c_int64),
@@ -185,6 +205,10 @@ SIGNATURES = {
     "femb200_extrapolate_state": (C.c_int, [_vp, _P(StokesProblemC), _vp * 3, _vp * 3, _vp, _vp]),
     "femb200_precompute_geometry": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int32]),
     "femb200_strain_rate_stress": (C.c_int, [_vp, _P(StokesProblemC), _vp * 6, _vp * 14]),
+    "femb200_lithostatic_residual": (C.c_int, [_vp, _P(LithostaticProblemC), C.c_double, C.c_double * 3,
+                                               C.c_int32]),
+    "femb200_solve_lithostatic": (C.c_int, [_vp, _P(LithostaticProblemC), _P(LithostaticControlsC),
+                                            _P(ThermalStatsC)]),
     "femb200_cell_pressure_preconditioner": (C.c_int, [_vp, _P(CellPressureProblemC)]),
     "femb200_cell_pressure_residuals": (C.c_int, [_vp, _P(CellPressureProblemC), C.c_int32]),
     "femb200_solve_cell_pressure": (C.c_int, [_vp, _P(CellPressureProblemC), _P(CellPressureControlsC),

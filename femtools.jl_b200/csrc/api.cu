@@ -1493,6 +1493,107 @@ int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int 
     return FEMB200_OK;
 }
 
+// solve_dynamic_relaxation! (src/dynamic_relaxation/solver.jl:61-122) for one nodal
+// unknown u with a diagonal preconditioner: the thermal and lithostatic DR solves.
+// `assemble(jac)` fills R (and on check iterations the Jacobian row sums and |diag|);
+// the Dirichlet pins of R and the rate are folded into the update through `mask`.
+struct DrNodal {
+    double *u, *rate, *R, *R0;
+    const double *dRdu, *PC;
+    int64_t n;
+    const int32_t* bc_dofs;
+    const double* bc_vals;
+    int64_t bc_n;
+    double cfl, c_fact;
+};
+
+template <class Asm>
+int dr_nodal_solve(femb200_handle* h, const DrNodal& f, const uint8_t* mask, double tolerance, int64_t max_it,
+                   int64_t check, int32_t throw_on_failure, const char* label, const char* title, Asm assemble,
+                   femb200_thermal_stats* st) {
+    using T = double;
+    double a = 0, b = 0, nr0 = 0, last = NAN, lmax = 0;
+    const int nbk = red_blocks(h, f.n);
+    RC(ensure_partials(h, nbk));
+    for (int64_t it = 1; it <= max_it; ++it) {
+        const bool dj = (it % check == 0) || it == 1;
+        if (dj) CK(launch_copy<T>(f.R0, f.R, f.n, h->stream));
+        RC(assemble(dj));
+        if (dj) RC(checked_lmax<T>(h, f.dRdu, f.PC, f.n, label, lmax));
+        CK(launch_thermal_update<T>(f.u, f.rate, f.R, f.PC, mask, f.n, a, b, h->stream));
+        if (f.bc_n > 0) CK(launch_dirichlet<T>(f.u, f.bc_dofs, f.bc_vals, f.bc_n, h->stream));
+        if (dj) {
+            const double dtau = 2 / std::sqrt(lmax) * f.cfl;
+            CK(launch_lmin_sums<T>(f.rate, f.R, f.R0, f.PC, f.n, dtau, h->d_partials, nbk, h->stream));
+            double s[3];
+            RC(fetch_sums(h, nbk, 3, s));
+            const double nr = std::sqrt(s[2]);
+            if (it == 1) nr0 = std::max(nr, julia_eps(nr));
+            if (std::isnan(nr / nr0)) { char bb[64]; std::snprintf(bb, sizeof bb, "NaNs at PT iter %lld", (long long)it); h->err = bb; return FEMB200_ENAN; }
+            const double lmin = (it == 1 || s[0] == 0) ? 0.0 : std::fabs(s[1]) / s[0];
+            cheb(dtau, lmin, f.c_fact, a, b);
+            last = nr / nr0;
+            if (last < tolerance) { st->converged = 1; st->iterations = it; st->residual = last; return FEMB200_OK; }
+        }
+    }
+    st->converged = 0; st->iterations = max_it; st->residual = last;
+    if (throw_on_failure) {
+        char bb[256];
+        std::snprintf(bb, sizeof bb, "%s DR solver did not converge after %lld pseudo-transient iterations (relative residual = %g)",
+                      title, (long long)max_it, last);
+        h->err = bb;
+        return FEMB200_ENOTCONV;
+    }
+    return FEMB200_OK;
+}
+
+int build_node_mask(femb200_handle* h, const int32_t* dofs, int64_t bc_n, int64_t nnodes) {
+    const size_t n = (size_t)nnodes;
+    if (n > h->tmask_cap) {
+        if (h->d_tmask) cudaFree(h->d_tmask);
+        h->d_tmask = nullptr;
+        CK(cudaMalloc(&h->d_tmask, n));
+        h->tmask_cap = n;
+    }
+    CK(cudaMemsetAsync(h->d_tmask, 0, n, h->stream));
+    if (bc_n > 0) CK(launch_build_mask(h->d_tmask, dofs, bc_n, 0, h->stream));
+    return FEMB200_OK;
+}
+
+int check_litho_problem(femb200_handle* h, const femb200_lithostatic_problem* p) {
+    if (!h) return FEMB200_EINVAL;
+    if (!p) { h->err = "null problem"; return FEMB200_EINVAL; }
+    const bool h27 = p->dim == 3 && p->nv == 27 && p->nq == 27, q9 = p->dim == 2 && p->nv == 9 && p->nq == 9;
+    if (!h27 && !q9) { h->err = "lithostatic pressure: Hex27 (3-D) or Q9 (2-D) meshes"; return FEMB200_EUNSUPPORTED; }
+    if (p->nels <= 0 || p->nnodes <= 0) { h->err = "empty mesh"; return FEMB200_EINVAL; }
+    if (p->nphases < 1 || p->nphases > FEMB200_MAX_PHASES) { h->err = "nphases must lie in 1:16"; return FEMB200_EINVAL; }
+    if (!p->el2n || !p->geo || !p->P || !p->rate || !p->R || !p->R0 || !p->dRdP || !p->PC || !p->phases ||
+        (p->bc_n > 0 && !p->bc_dofs) || p->bc_n < 0) {
+        h->err = "lithostatic pressure: mesh, state and phase arrays are required";
+        return FEMB200_EINVAL;
+    }
+    return FEMB200_OK;
+}
+
+int litho_assemble(femb200_handle* h, const femb200_lithostatic_problem* p, double Tref, const double* g, bool jac) {
+    LithoArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.dim = p->dim; a.el2n = p->el2n; a.geo = p->geo; a.P = p->P; a.Tn = p->T;
+    a.ph = p->phases; a.ph_layout = p->phases_layout;
+    a.R = p->R; a.dRdP = p->dRdP; a.PC = p->PC; a.nels = p->nels; a.Tref = Tref; a.jac = jac ? 1 : 0;
+    for (int k = 0; k < p->dim; ++k) a.g[k] = g[k];
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) {
+        a.rho0[i] = p->rho0[i]; a.alpha[i] = p->alpha[i]; a.beta[i] = 1.0 / p->K[i];   // β = 1/K: 0 for K = ∞
+    }
+    CK(cudaMemsetAsync(p->R, 0, sizeof(double) * p->nnodes, h->stream));
+    if (jac) {
+        CK(cudaMemsetAsync(p->dRdP, 0, sizeof(double) * p->nnodes, h->stream));
+        CK(cudaMemsetAsync(p->PC, 0, sizeof(double) * p->nnodes, h->stream));
+    }
+    CK(launch_lithostatic(a, h->stream));
+    return FEMB200_OK;
+}
+
 template <class T, class TG>
 int strain_rate_stress_impl(femb200_handle* h, const femb200_stokes_problem* p, const void* const tau_ip[6],
                             void* const out[14]) {
@@ -1993,42 +2094,34 @@ int femb200_solve_thermal(femb200_handle* h, const femb200_thermal_problem* t, c
     using T = double;
     RC(upload_thermal_material(h, t));
     RC(build_tmask(h, t));
-    const int64_t n = t->nnodes;
-    double a = 0, b = 0, nr0 = 0, last = NAN, lmax = 0;
-    const int nbk = red_blocks(h, n);
-    RC(ensure_partials(h, nbk));
-    for (int64_t it = 1; it <= c->max_iterations; ++it) {
-        const bool dj = (it % c->check_interval == 0) || it == 1;
-        if (dj) CK(launch_copy<T>(static_cast<T*>(t->R0), static_cast<const T*>(t->R), n, h->stream));
-        RC((thermal_assemble<T, T>(h, t, c->dt, c->Tref, dj, t->source_ip)));
-        if (dj) RC(checked_lmax<T>(h, static_cast<const T*>(t->dRdT), static_cast<const T*>(t->PC), n, "thermal diffusion", lmax));
-        CK(launch_thermal_update<T>(static_cast<T*>(t->T), static_cast<T*>(t->rate), static_cast<T*>(t->R),
-                                    static_cast<const T*>(t->PC), h->d_tmask, n, a, b, h->stream));
-        if (t->bc_n > 0) CK(launch_dirichlet<T>(static_cast<T*>(t->T), t->bc_dofs, static_cast<const T*>(t->bc_vals), t->bc_n, h->stream));
-        if (dj) {
-            const double dtau = 2 / std::sqrt(lmax) * t->cfl;
-            CK(launch_lmin_sums<T>(static_cast<const T*>(t->rate), static_cast<const T*>(t->R), static_cast<const T*>(t->R0),
-                                   static_cast<const T*>(t->PC), n, dtau, h->d_partials, nbk, h->stream));
-            double s[3];
-            RC(fetch_sums(h, nbk, 3, s));
-            const double nr = std::sqrt(s[2]);
-            if (it == 1) nr0 = std::max(nr, julia_eps(nr));
-            if (std::isnan(nr / nr0)) { char bb[64]; std::snprintf(bb, sizeof bb, "NaNs at PT iter %lld", (long long)it); h->err = bb; return FEMB200_ENAN; }
-            const double lmin = (it == 1 || s[0] == 0) ? 0.0 : std::fabs(s[1]) / s[0];
-            cheb(dtau, lmin, t->c_fact, a, b);
-            last = nr / nr0;
-            if (last < c->tolerance) { st->converged = 1; st->iterations = it; st->residual = last; return FEMB200_OK; }
-        }
-    }
-    st->converged = 0; st->iterations = c->max_iterations; st->residual = last;
-    if (c->throw_on_failure) {
-        char bb[256];
-        std::snprintf(bb, sizeof bb, "Thermal diffusion DR solver did not converge after %lld pseudo-transient iterations (relative residual = %g)",
-                      (long long)c->max_iterations, last);
-        h->err = bb;
-        return FEMB200_ENOTCONV;
-    }
-    return FEMB200_OK;
+    DrNodal f{static_cast<T*>(t->T), static_cast<T*>(t->rate), static_cast<T*>(t->R), static_cast<T*>(t->R0),
+              static_cast<const T*>(t->dRdT), static_cast<const T*>(t->PC), t->nnodes, t->bc_dofs,
+              static_cast<const T*>(t->bc_vals), t->bc_n, t->cfl, t->c_fact};
+    auto assemble = [&](bool dj) { return thermal_assemble<T, T>(h, t, c->dt, c->Tref, dj, t->source_ip); };
+    return dr_nodal_solve(h, f, h->d_tmask, c->tolerance, c->max_iterations, c->check_interval, c->throw_on_failure,
+                          "thermal diffusion", "Thermal diffusion", assemble, st);
+}
+
+int femb200_lithostatic_residual(femb200_handle* h, const femb200_lithostatic_problem* p, double Tref,
+                                 const double g[3], int32_t jac) {
+    RC(check_litho_problem(h, p));
+    if (!g) { h->err = "lithostatic pressure: g is required"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    return litho_assemble(h, p, Tref, g, jac != 0);
+}
+
+int femb200_solve_lithostatic(femb200_handle* h, const femb200_lithostatic_problem* p,
+                              const femb200_lithostatic_controls* c, femb200_thermal_stats* st) {
+    RC(check_litho_problem(h, p));
+    if (!c || !st) { h->err = "controls and stats are required"; return FEMB200_EINVAL; }
+    if (c->max_iterations < 1 || c->check_interval < 1) { h->err = "max_iterations and check_interval must be positive"; return FEMB200_EINVAL; }
+    RC(ensure_tables(h));
+    RC(build_node_mask(h, p->bc_dofs, p->bc_n, p->nnodes));
+    std::memset(st, 0, sizeof(*st));
+    DrNodal f{p->P, p->rate, p->R, p->R0, p->dRdP, p->PC, p->nnodes, p->bc_dofs, p->bc_vals, p->bc_n, p->cfl, p->c_fact};
+    auto assemble = [&](bool dj) { return litho_assemble(h, p, c->Tref, c->g, dj); };
+    return dr_nodal_solve(h, f, h->d_tmask, c->tolerance, c->max_iterations, c->check_interval, c->throw_on_failure,
+                          "lithostatic pressure", "Lithostatic pressure", assemble, st);
 }
 
 int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t, const femb200_stokes_problem* p,

@@ -351,6 +351,26 @@ struct ThermalArgs {
 template <class T, class TG>
 cudaError_t launch_thermal(const ThermalArgs<T, TG>& a, int num_sms, cudaStream_t st);
 
+// Lithostatic pressure (simple.cu): FP64, per-phase constants by value.
+struct LithoArgs {
+    int dim;
+    const int32_t* el2n;
+    const double* geo;
+    const double* P;
+    const double* Tn;
+    const int32_t* ph;
+    int ph_layout;
+    double* R;
+    double* dRdP;
+    double* PC;
+    int64_t nels;
+    double Tref;
+    double g[3];
+    int jac;
+    double rho0[MAXPH], alpha[MAXPH], beta[MAXPH];
+};
+cudaError_t launch_lithostatic(const LithoArgs& a, cudaStream_t st);
+
 // Thermal DR node update: rate = R/PC + β rate; T += α rate, masked by Dirichlet.
 template <class T>
 cudaError_t launch_thermal_update(T* Tn, T* rate, T* R, const T* PC, const uint8_t* mask, int64_t n, double alpha,

@@ -485,9 +485,102 @@ __global__ void thermal_kernel(ThermalArgs<T, TG> a) {
     }
 }
 
+// Lithostatic-pressure element residual (lp_integrate_residual,
+// src/lithostatic_pressure/assembly/residual.jl:48-63): R_i = Σ_q (ρ_q ∇N_i·g − ∇N_i·∇P) dΩ
+// with ρ_q = ρ0_q (1 − α_q (T_q − Tref) + β_q P_q), and the row sums and diagonal of its
+// Jacobian (the ForwardDiff diagnostics of lp_element_jacobian, :22-36), in closed form:
+// ∂R_i/∂P_b = Σ_q (ρ0_q β_q N_b ∇N_i·g − ∇N_i·∇N_b) dΩ.
+template <int DIM>
+__global__ void lithostatic_kernel(LithoArgs a) {
+    using TB = Tabs<DIM>;
+    constexpr int NV = TB::NV, NQ = TB::NQ, S = DIM * DIM + 1;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.nels) return;
+    int node[NV], ph[NV];
+    double Pl[NV], Tl[NV];
+    for (int i = 0; i < NV; ++i) {
+        node[i] = __ldg(a.el2n + NV * e + i) - 1;
+        Pl[i] = a.P[node[i]];
+        Tl[i] = a.Tn ? __ldg(a.Tn + node[i]) : 0.0;
+        ph[i] = phase_of(a.ph, a.ph_layout, (int64_t)node[i] + 1, i, e, NV);
+    }
+    const double* G = a.geo + e * NQ * S;
+    double R[NV];
+    for (int i = 0; i < NV; ++i) R[i] = 0.0;
+    for (int q = 0; q < NQ; ++q) {
+        const double* g = G + q * S;
+        const double dO = g[DIM * DIM];
+        double Tq = 0, Pq = 0, aq = 0, bq = 0, rq = 0;
+        for (int i = 0; i < NV; ++i) {
+            const double N = TB::N(q, i);
+            Tq += N * Tl[i]; Pq += N * Pl[i];
+            aq += N * a.alpha[ph[i]]; bq += N * a.beta[ph[i]]; rq += N * a.rho0[ph[i]];
+        }
+        const double rho = rq * (1.0 - aq * (Tq - a.Tref) + bq * Pq);
+        double dn[NV][DIM], gP[DIM];
+        for (int k = 0; k < DIM; ++k) gP[k] = 0.0;
+        for (int i = 0; i < NV; ++i)
+            for (int k = 0; k < DIM; ++k) {
+                double s = 0;
+                for (int j = 0; j < DIM; ++j) s += TB::dN(q, i, j) * g[j + DIM * k];
+                dn[i][k] = s;
+                gP[k] += s * Pl[i];
+            }
+        for (int i = 0; i < NV; ++i) {
+            double ng = 0, np = 0;
+            for (int k = 0; k < DIM; ++k) { ng += dn[i][k] * a.g[k]; np += dn[i][k] * gP[k]; }
+            R[i] += (rho * ng - np) * dO;
+        }
+    }
+    for (int i = 0; i < NV; ++i) atomicAdd(a.R + node[i], R[i]);
+    if (!a.jac) return;
+    for (int i = 0; i < NV; ++i) {
+        double Jrow[NV];
+        for (int b = 0; b < NV; ++b) Jrow[b] = 0.0;
+        for (int q = 0; q < NQ; ++q) {
+            const double* g = G + q * S;
+            const double dO = g[DIM * DIM];
+            double bq = 0, rq = 0;
+            for (int m = 0; m < NV; ++m) {
+                const double N = TB::N(q, m);
+                bq += N * a.beta[ph[m]]; rq += N * a.rho0[ph[m]];
+            }
+            double dni[DIM], ng = 0;
+            for (int k = 0; k < DIM; ++k) {
+                double s = 0;
+                for (int j = 0; j < DIM; ++j) s += TB::dN(q, i, j) * g[j + DIM * k];
+                dni[k] = s;
+                ng += s * a.g[k];
+            }
+            const double cf = rq * bq * ng;
+            for (int b = 0; b < NV; ++b) {
+                double kk = 0;
+                for (int k = 0; k < DIM; ++k) {
+                    double s = 0;
+                    for (int j = 0; j < DIM; ++j) s += TB::dN(q, b, j) * g[j + DIM * k];
+                    kk += dni[k] * s;
+                }
+                Jrow[b] += (cf * TB::N(q, b) - kk) * dO;
+            }
+        }
+        double row = 0;
+        for (int b = 0; b < NV; ++b) row += fabs(Jrow[b]);
+        atomicAdd(a.dRdP + node[i], row);
+        atomicAdd(a.PC + node[i], fabs(Jrow[i]));
+    }
+}
+
 inline unsigned nb(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+cudaError_t launch_lithostatic(const LithoArgs& a, cudaStream_t st) {
+    if (a.nels <= 0) return cudaSuccess;
+    count_launch();
+    if (a.dim == 3) lithostatic_kernel<3><<<nb(a.nels, 64), 64, 0, st>>>(a);
+    else lithostatic_kernel<2><<<nb(a.nels, 128), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
 
 template <class T, class TG>
 cudaError_t launch_pressure_scaling(int dim, const int32_t* el2n, const int32_t* dofsP, const TG* geo_P,

@@ -230,6 +230,36 @@ typedef struct femb200_thermal_stats {
     double residual;
 } femb200_thermal_stats;
 
+/* Lithostatic pressure (LithostaticPressureDR,
+ * src/lithostatic_pressure/types/lithostatic_pressure_types.jl:1-104): the steady
+ * Poisson problem ∫ ∇P·∇v dΩ = ∫ ρ(T, P) g·∇v dΩ for a nodal P on the velocity mesh
+ * (Hex27 or Q9), ρ = ρ0(1 − α(T − Tref) + P/K); solved by the same dynamic relaxation
+ * as the thermal problem. FP64 device arrays of nnodes entries. */
+typedef struct femb200_lithostatic_problem {
+    int32_t dim, nv, nq;      /* 3, 27, 27 or 2, 9, 9 */
+    int64_t nels, nnodes;
+    const int32_t* el2n;
+    const double* geo;        /* nels × nq × (dim·dim + 1) */
+    double* P;                /* the unknown, updated in place */
+    double* rate;             /* ∂P∂τ */
+    double* R; double* R0; double* dRdP; double* PC;
+    const double* T;          /* temperature (EOS coefficient); NULL → 0 */
+    const int32_t* phases; int32_t phases_layout;
+    int32_t nphases;
+    double rho0[FEMB200_MAX_PHASES], alpha[FEMB200_MAX_PHASES], K[FEMB200_MAX_PHASES];
+    const int32_t* bc_dofs; const double* bc_vals; int64_t bc_n;
+    double cfl, c_fact, eps;  /* CFL (0.98), c_fact (0.9), ϵ (1e-6) */
+} femb200_lithostatic_problem;
+
+typedef struct femb200_lithostatic_controls {
+    double Tref;              /* 273 */
+    double g[3];              /* body force; (0, −9.81) in 2-D by default */
+    double tolerance;         /* relative ‖R‖/‖R⁰‖ (default ϵ) */
+    int64_t max_iterations;   /* 10 000 */
+    int64_t check_interval;   /* 100 */
+    int32_t throw_on_failure;
+} femb200_lithostatic_controls;
+
 /* Viscous incompressible Hex27 Stokes with four cell-local pressure modes (1, ξ, η, ζ)
  * per cell (CellPressureStokesDR, src/stokes/types/stokes_types.jl:567-613). FP64
  * device arrays; P, RP and pressure_mass are 4 × nels (column-major: mode fastest). */
@@ -441,6 +471,17 @@ int femb200_apply_warm_start(femb200_handle* h, const femb200_stokes_problem* p,
 int femb200_precompute_geometry(femb200_handle* h, int32_t dim, int64_t nels, int64_t nnodes,
                                 const double* coords, const int32_t* el2n, void* geo_v, void* geo_P,
                                 int32_t geo_dtype);
+
+/* ---- lithostatic pressure (src/lithostatic_pressure/) ---- */
+/* assemble_lithostatic_pressure_matrices_atomix! (assembly/residual_atomics.jl:1-19):
+ * R = Σ_q (ρ ∇N·g − ∇N·∇P) dΩ, and with jac ≠ 0 the Jacobian's absolute row sums
+ * (dRdP) and |diagonal| (PC). g has dim components. */
+int femb200_lithostatic_residual(femb200_handle* h, const femb200_lithostatic_problem* p, double Tref,
+                                 const double g[3], int32_t jac);
+/* solve!(dr::LithostaticPressureDR, mesh, bc; …) (solvers/DR.jl:1-44) through
+ * solve_dynamic_relaxation! (src/dynamic_relaxation/solver.jl:61-122). */
+int femb200_solve_lithostatic(femb200_handle* h, const femb200_lithostatic_problem* p,
+                              const femb200_lithostatic_controls* c, femb200_thermal_stats* st);
 
 /* ---- cell-pressure Hex27 Stokes (src/stokes/solvers/DR.jl:980-1057) ---- */
 /* stokes_preconditioner_3d! (momentum_residuals.jl:703-745): diagonal_c(a) =

@@ -1044,6 +1044,135 @@ int solve_stokes_impl(const femb200_stokes_problem* p, const femb200_stokes_cont
     return FEMB200_OK;
 }
 
+// ---- LithostaticPressureDR ----------------------------------------------------
+// lp_integrate_residual (src/lithostatic_pressure/assembly/residual.jl:48-63) on one
+// element given its shape functions N[q][a], physical gradients dNdx[q][a][k] and
+// weights dO[q]: R_i = Σ_q (ρ_q ∇N_i·g − ∇N_i·∇P) dΩ, ρ_q = ρ0_q (1 − α_q (T_q − Tref) + β_q P_q).
+template <class S>
+void lp_element(int NV, int D, int NQ, const double* N, const double* dNdx, const double* dO, const S* P,
+                const double* T, const int* ph, const double* rho0, const double* alpha, const double* beta,
+                double Tref, const double* g, S* Re) {
+    for (int a = 0; a < NV; ++a) Re[a] = S(0.0);
+    for (int q = 0; q < NQ; ++q) {
+        const double* Nq = N + q * NV;
+        const double* G = dNdx + (size_t)q * NV * D;
+        double Tq = 0;
+        for (int a = 0; a < NV; ++a) Tq += Nq[a] * T[a];
+        S Pq(0.0);
+        for (int a = 0; a < NV; ++a) Pq = Pq + Nq[a] * P[a];
+        const double aq = interp_phase(Nq, alpha, ph, NV), bq = interp_phase(Nq, beta, ph, NV);
+        const S rho = interp_phase(Nq, rho0, ph, NV) * (1.0 - aq * (Tq - Tref) + bq * Pq);
+        S gP[3] = {S(0.0), S(0.0), S(0.0)};
+        for (int k = 0; k < D; ++k)
+            for (int b = 0; b < NV; ++b) gP[k] = gP[k] + G[b * D + k] * P[b];
+        for (int i = 0; i < NV; ++i) {
+            double ng = 0;
+            S np(0.0);
+            for (int k = 0; k < D; ++k) { ng += G[i * D + k] * g[k]; np = np + G[i * D + k] * gP[k]; }
+            Re[i] = Re[i] + (rho * ng - np) * dO[q];
+        }
+    }
+}
+
+// Residual of one element and, with jac, the absolute row sums and diagonal of its
+// ForwardDiff Jacobian in P (lp_element_jacobian, residual.jl:22-36).
+template <int NVT>
+void lp_element_all(int NV, int D, int NQ, const double* N, const double* dNdx, const double* dO, const double* P,
+                    const double* T, const int* ph, const double* rho0, const double* alpha, const double* beta,
+                    double Tref, const double* g, bool jac, double* R, double* rows, double* diag) {
+    lp_element<double>(NV, D, NQ, N, dNdx, dO, P, T, ph, rho0, alpha, beta, Tref, g, R);
+    if (!jac) return;
+    Dual<NVT> Pd[27], Rd[27];
+    for (int a = 0; a < NV; ++a) { Pd[a] = Dual<NVT>(P[a]); Pd[a].d[a] = 1.0; }
+    lp_element<Dual<NVT>>(NV, D, NQ, N, dNdx, dO, Pd, T, ph, rho0, alpha, beta, Tref, g, Rd);
+    for (int a = 0; a < NV; ++a) {
+        double sum = 0;
+        for (int b = 0; b < NV; ++b) sum += std::fabs(Rd[a].d[b]);
+        rows[a] = sum;
+        diag[a] = std::fabs(Rd[a].d[a]);
+    }
+}
+
+void lp_assemble(const femb200_lithostatic_problem* p, double Tref, const double* g, bool jac) {
+    const Tables& t = tables_for(p->dim);
+    const int NV = t.nv, NQ = t.nq, D = p->dim;
+    double beta[FEMB200_MAX_PHASES];
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) beta[i] = 1.0 / p->K[i];
+    std::fill(p->R, p->R + p->nnodes, 0.0);
+    if (jac) { std::fill(p->dRdP, p->dRdP + p->nnodes, 0.0); std::fill(p->PC, p->PC + p->nnodes, 0.0); }
+    for (int64_t e = 0; e < p->nels; ++e) {
+        double N[27 * 27], G[27 * 27 * 3], dO[27], P[27], T[27], R[27], rows[27], diag[27];
+        int ph[27];
+        const double* geo = p->geo + (size_t)e * NQ * (D * D + 1);
+        for (int q = 0; q < NQ; ++q) {
+            double d[27][3];
+            dNdx_at(t, geo, D, q, d);
+            for (int a = 0; a < NV; ++a) {
+                N[q * NV + a] = t.N[q][a];
+                for (int k = 0; k < D; ++k) G[((size_t)q * NV + a) * D + k] = d[a][k];
+            }
+            dO[q] = geo[q * (D * D + 1) + D * D];
+        }
+        for (int a = 0; a < NV; ++a) {
+            const int64_t node = p->el2n[(int64_t)NV * e + a];
+            P[a] = p->P[node - 1];
+            T[a] = p->T ? p->T[node - 1] : 0.0;
+            ph[a] = phase_at(p->phases, p->phases_layout, node, a, e, NV);
+        }
+        if (NV == 27) lp_element_all<27>(NV, D, NQ, N, G, dO, P, T, ph, p->rho0, p->alpha, beta, Tref, g, jac, R, rows, diag);
+        else lp_element_all<9>(NV, D, NQ, N, G, dO, P, T, ph, p->rho0, p->alpha, beta, Tref, g, jac, R, rows, diag);
+        for (int a = 0; a < NV; ++a) {
+            const int64_t n = p->el2n[(int64_t)NV * e + a] - 1;
+            p->R[n] += R[a];
+            if (jac) { p->dRdP[n] += rows[a]; p->PC[n] += diag[a]; }
+        }
+    }
+}
+
+// solve_dynamic_relaxation! (src/dynamic_relaxation/solver.jl:61-122) for P.
+int lp_solve_impl(const femb200_lithostatic_problem* p, const femb200_lithostatic_controls* c, femb200_thermal_stats* st) {
+    const int64_t n = p->nnodes;
+    double aT = 0, bT = 0, nr0 = 0, last_rel = NAN, lmax = 0;
+    for (int64_t it = 1; it <= c->max_iterations; ++it) {
+        bool dj = (it % c->check_interval == 0) || it == 1;
+        if (dj) std::copy(p->R, p->R + n, p->R0);
+        lp_assemble(p, c->Tref, c->g, dj);
+        dirichlet(p->R, p->bc_dofs, nullptr, p->bc_n);
+        dirichlet(p->rate, p->bc_dofs, nullptr, p->bc_n);
+        if (dj) { int rc = checked_lmax(p->dRdP, p->PC, n, "lithostatic pressure", lmax); if (rc) return rc; }
+        for (int64_t i = 0; i < n; ++i) p->rate[i] = p->R[i] / p->PC[i] + bT * p->rate[i];
+        for (int64_t i = 0; i < n; ++i) p->P[i] += aT * p->rate[i];
+        dirichlet(p->P, p->bc_dofs, p->bc_vals, p->bc_n);
+        if (dj) {
+            double nr = norm2(p->R, n);
+            if (it == 1) nr0 = std::max(nr, julia_eps(nr));
+            if (std::isnan(nr / nr0)) { char b[64]; std::snprintf(b, sizeof b, "NaNs at PT iter %lld", (long long)it); g_last_error = b; return FEMB200_ENAN; }
+            double dtau = 2 / std::sqrt(lmax) * p->cfl;
+            double den = 0; for (int64_t i = 0; i < n; ++i) { double r = dtau * p->rate[i]; den += r * r; }
+            double lmin = 0;
+            if (!(it == 1 || den == 0)) {
+                double num = 0;
+                for (int64_t i = 0; i < n; ++i) num += dtau * p->rate[i] * ((p->R[i] - p->R0[i]) / p->PC[i]);
+                lmin = std::fabs(num) / den;
+            }
+            double cc = 2 * std::sqrt(lmin) * p->c_fact;
+            aT = 2 * dtau * dtau / (2 + cc * dtau);
+            bT = (2 - cc * dtau) / (2 + cc * dtau);
+            last_rel = nr / nr0;
+            if (last_rel < c->tolerance) { st->converged = 1; st->iterations = it; st->residual = last_rel; return 0; }
+        }
+    }
+    st->converged = 0; st->iterations = c->max_iterations; st->residual = last_rel;
+    if (c->throw_on_failure) {
+        char b[256];
+        std::snprintf(b, sizeof b, "Lithostatic pressure DR solver did not converge after %lld pseudo-transient iterations (relative residual = %g)",
+                      (long long)c->max_iterations, last_rel);
+        g_last_error = b;
+        return FEMB200_ENOTCONV;
+    }
+    return 0;
+}
+
 // ---- CellPressureStokesDR (viscous Hex27, four cell-local pressure modes) ----
 // The modes (1, ξ, η, ζ) at the Gauss points (pressure_mode_table,
 // momentum_residuals.jl:618-621); ξ, η, ζ are the P1 rows 2..4 of the tables.
@@ -1492,6 +1621,32 @@ int orc_cell_pressure_residuals(const femb200_cell_pressure_problem* p, int32_t 
 int orc_solve_cell_pressure(const femb200_cell_pressure_problem* p, const femb200_cell_pressure_controls* c,
                             femb200_cell_pressure_stats* st) {
     return cp_solve_impl(p, c, st);
+}
+
+int orc_lithostatic_residual(const femb200_lithostatic_problem* p, double Tref, const double* g, int32_t jac) {
+    lp_assemble(p, Tref, g, jac != 0);
+    return 0;
+}
+
+int orc_solve_lithostatic(const femb200_lithostatic_problem* p, const femb200_lithostatic_controls* c,
+                          femb200_thermal_stats* st) {
+    return lp_solve_impl(p, c, st);
+}
+
+// One element of the lithostatic residual from given shape functions N (nq × nv),
+// physical gradients dNdx (nq × nv × dim) and weights dΩ (nq): the element-level
+// checks of the reference's tests are stated this way.
+int orc_lithostatic_element_custom(int dim, int nv, int nq, const double* N, const double* dNdx, const double* dO,
+                                   const double* P, const double* T, const int32_t* ph, const double* rho0,
+                                   const double* alpha, const double* K, double Tref, const double* g,
+                                   double* R, double* rows, double* diag) {
+    if (nv > 9 || nq > 27 || (dim != 2 && dim != 3)) return FEMB200_EINVAL;
+    double beta[FEMB200_MAX_PHASES];
+    for (int i = 0; i < FEMB200_MAX_PHASES; ++i) beta[i] = 1.0 / K[i];
+    int p0[27];
+    for (int a = 0; a < nv; ++a) p0[a] = ph[a] - 1;
+    lp_element_all<9>(nv, dim, nq, N, dNdx, dO, P, T, p0, rho0, alpha, beta, Tref, g, true, R, rows, diag);
+    return 0;
 }
 
 }  // extern "C"

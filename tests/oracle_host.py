@@ -39,6 +39,10 @@ def lib():
             "orc_structured_mesh": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
             "orc_geometry": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
             "orc_strain_rate_stress": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp * 3, _vp * 6, _vp * 14]),
+            "orc_lithostatic_residual": (C.c_int, [_P(abi.LithostaticProblemC), C.c_double, _vp, C.c_int32]),
+            "orc_solve_lithostatic": (C.c_int, [_P(abi.LithostaticProblemC), _P(abi.LithostaticControlsC),
+                                                _P(abi.ThermalStatsC)]),
+            "orc_lithostatic_element_custom": (C.c_int, [C.c_int] * 3 + [_vp] * 9 + [C.c_double] + [_vp] * 4),
             "orc_cell_pressure_preconditioner": (C.c_int, [_P(abi.CellPressureProblemC)]),
             "orc_cell_pressure_residuals": (C.c_int, [_P(abi.CellPressureProblemC), C.c_int32]),
             "orc_solve_cell_pressure": (C.c_int, [_P(abi.CellPressureProblemC), _P(abi.CellPressureControlsC),
@@ -370,3 +374,80 @@ class HostCellPressure:
         st = abi.CellPressureStatsC()
         check(lib().orc_solve_cell_pressure(C.byref(p), C.byref(c), C.byref(st)))
         return st
+
+
+class HostLithostatic:
+    """Oracle state of the lithostatic-pressure problem (host numpy arrays)."""
+
+    def __init__(self, mesh, rho0=(1.0,), alpha=(0.0,), K=(float("inf"),), phases=None, T=None, P=None,
+                 cfl=0.98, c_fact=0.9, eps=1e-6):
+        nn = mesh.nnodes
+        self.mesh = mesh
+        self.el2n = np.ascontiguousarray(mesh.el2n, dtype=np.int32)
+        self.geo = np.ascontiguousarray(mesh.geo_v, dtype=np.float64)
+        self.phases = np.ascontiguousarray(np.ones(nn) if phases is None else phases, dtype=np.int32)
+        self.T = np.ascontiguousarray(np.zeros(nn) if T is None else T, dtype=np.float64)
+        self.P = np.ascontiguousarray(np.zeros(nn) if P is None else P, dtype=np.float64).copy()
+        for name in ("rate", "R", "R0", "dRdP", "PC"):
+            setattr(self, name, np.zeros(nn))
+        self.rho0, self.alpha, self.K = rho0, alpha, K
+        self.cfl, self.c_fact, self.eps = cfl, c_fact, eps
+        self._keep = []
+
+    def struct(self, bc=None):
+        p = abi.LithostaticProblemC()
+        d = self.mesh.dim
+        p.dim, p.nv, p.nq = (3, 27, 27) if d == 3 else (2, 9, 9)
+        p.nels, p.nnodes = self.mesh.nels, self.mesh.nnodes
+        p.el2n, p.geo = ptr(self.el2n), ptr(self.geo)
+        for name in ("P", "rate", "R", "R0", "dRdP", "PC", "T"):
+            setattr(p, name, ptr(getattr(self, name)))
+        p.phases, p.phases_layout, p.nphases = ptr(self.phases), abi.PHASE_NODAL, len(self.rho0)
+        for i in range(abi.MAX_PHASES):
+            p.rho0[i] = self.rho0[i] if i < len(self.rho0) else 1.0
+            p.alpha[i] = self.alpha[i] if i < len(self.alpha) else 0.0
+            p.K[i] = self.K[i] if i < len(self.K) else float("inf")
+        self._keep = []
+        if bc is not None:
+            dd = np.ascontiguousarray(bc[0], dtype=np.int32)
+            vv = np.ascontiguousarray(bc[1], dtype=np.float64)
+            self._keep = [dd, vv]
+            p.bc_dofs, p.bc_vals, p.bc_n = ptr(dd), ptr(vv), len(dd)
+        p.cfl, p.c_fact, p.eps = self.cfl, self.c_fact, self.eps
+        return p
+
+    def residual(self, Tref, g, jac=False):
+        gg = np.zeros(3)
+        gg[:len(g)] = g
+        check(lib().orc_lithostatic_residual(C.byref(self.struct()), Tref, ptr(gg), int(jac)))
+
+    def solve(self, bc, Tref, g, tolerance=None, max_iterations=10_000, check_interval=100, throw_on_failure=True):
+        p = self.struct(bc)
+        c = abi.LithostaticControlsC()
+        c.Tref = Tref
+        for k, x in enumerate(g):
+            c.g[k] = x
+        c.tolerance = self.eps if tolerance is None else tolerance
+        c.max_iterations, c.check_interval, c.throw_on_failure = max_iterations, check_interval, int(throw_on_failure)
+        st = abi.ThermalStatsC()
+        check(lib().orc_solve_lithostatic(C.byref(p), C.byref(c), C.byref(st)))
+        return st
+
+
+def lithostatic_element(N, dNdx, dO, P, T, phases, rho0, alpha, K, Tref, g):
+    """Oracle element residual, Jacobian row sums and |diagonal| for given N (nq × nv),
+    physical gradients dNdx (nq × nv × dim) and weights dO (nq)."""
+    N = np.ascontiguousarray(N, dtype=np.float64)
+    dNdx = np.ascontiguousarray(dNdx, dtype=np.float64)
+    nq, nv, dim = dNdx.shape
+    arr = lambda x, t=np.float64: np.ascontiguousarray(x, dtype=t)
+    dO, P, T = arr(dO), arr(P), arr(T)
+    ph = arr(phases, np.int32)
+    pad = lambda x, fill: arr(list(x) + [fill] * (abi.MAX_PHASES - len(x)))
+    r0, al, KK = pad(rho0, 1.0), pad(alpha, 0.0), pad(K, float("inf"))
+    gg = arr(list(g) + [0.0] * (3 - len(g)))
+    R, rows, diag = np.zeros(nv), np.zeros(nv), np.zeros(nv)
+    check(lib().orc_lithostatic_element_custom(dim, nv, nq, ptr(N), ptr(dNdx), ptr(dO), ptr(P), ptr(T), ptr(ph),
+                                               ptr(r0), ptr(al), ptr(KK), Tref, ptr(gg), ptr(R), ptr(rows),
+                                               ptr(diag)))
+    return R, rows, diag

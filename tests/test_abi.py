@@ -46,6 +46,8 @@ STRUCTS = {
     "femb200_thermal_problem": abi.ThermalProblemC,
     "femb200_thermal_controls": abi.ThermalControlsC,
     "femb200_thermal_stats": abi.ThermalStatsC,
+    "femb200_lithostatic_problem": abi.LithostaticProblemC,
+    "femb200_lithostatic_controls": abi.LithostaticControlsC,
     "femb200_cell_pressure_problem": abi.CellPressureProblemC,
     "femb200_cell_pressure_controls": abi.CellPressureControlsC,
     "femb200_cell_pressure_stats": abi.CellPressureStatsC,
