@@ -457,15 +457,23 @@ def lithostatic_mode(args, fem):
     peak, kind = measured_peaks()
     cpu = None
     if not args.no_cpu_baseline:
+        # the oracle's first iteration assembles the Jacobian diagnostics; the next ones do not
+        hs = oh.HostLithostatic(mesh, phases=ph, T=T, **mat)
+        t0 = time.perf_counter()
+        hs.solve(bc, Tref=0.0, g=g, tolerance=0.0, max_iterations=1, check_interval=1000, throw_on_failure=False)
+        t_jac_it = time.perf_counter() - t0
         hs = oh.HostLithostatic(mesh, phases=ph, T=T, **mat)
         sample = 10
         t0 = time.perf_counter()
-        hs.solve(bc, Tref=0.0, g=g, tolerance=0.0, max_iterations=sample, check_interval=sample,
+        hs.solve(bc, Tref=0.0, g=g, tolerance=0.0, max_iterations=sample + 1, check_interval=1000,
                  throw_on_failure=False)
-        per_it = (time.perf_counter() - t0) / sample
-        cpu = {"value": per_it * st["iterations"], "unit": "s", "cores": 1, "kind": "port",
-               "sample": f"{sample} oracle iterations at {mesh.nel} ({per_it:.3f} s each, serial, one with the "
-                         f"Jacobian), extrapolated to {st['iterations']} iterations"}
+        t_it = max(time.perf_counter() - t0 - t_jac_it, 0.0) / sample
+        n_jac = st["iterations"] // 100 + 1
+        cpu = {"value": n_jac * t_jac_it + (st["iterations"] - n_jac) * t_it, "unit": "s", "cores": 1,
+               "kind": "port",
+               "sample": f"oracle at {mesh.nel}, serial: one iteration with the Jacobian diagnostics "
+                         f"({t_jac_it:.3f} s) and {sample} without ({t_it:.4f} s each), extrapolated to "
+                         f"{st['iterations']} iterations with {n_jac} Jacobian assemblies"}
     print(json.dumps({
         "mode": "lithostatic", "workload": f"layered-lithostatic-hex27-{n}^3", "nels": ne, "nnodes": nn,
         "value": t_solve, "unit": "s", "iterations": st["iterations"], "converged": st["converged"],
