@@ -445,6 +445,19 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
         CK(cudaMemsetAsync(p->PC[c], 0, sizeof(T) * p->nnodes, h->stream));
     }
     if (!p->gammaP || !p->M_P) { h->err = "γP and M_P are required by the augmented Jacobian"; return FEMB200_EINVAL; }
+    if (p->dim == 3) {
+        // axis-aligned cells (the structured boxes) take the diagonal-J⁻¹ kernel; one
+        // read of the geometry and a synchronisation, at check iterations that synchronise anyway
+        if (!h->d_flag) {
+            CK(cudaMalloc(&h->d_flag, sizeof(int)));
+            CK(cudaMallocHost(&h->h_flag, sizeof(int)));
+        }
+        CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+        CK(launch_geo_offdiag<TG>(a.geo_v, p->nels, h->d_flag, h->stream));
+        CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        a.diag_geometry = *h->h_flag == 0;
+    }
     RC(prof_begin(h, FEMB200_PROF_JACOBIAN));
     if (p->dim == 3) CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
     else CK(launch_q9_jacobian<T, TG>(a, h->stream));

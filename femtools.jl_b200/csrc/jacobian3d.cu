@@ -10,6 +10,7 @@
 // Maxwell stress and Drucker–Prager return, rheology.jl:441-472), pushed through
 // the sum-factorised transposed contraction. Line threads own fixed rows, so the
 // row sums accumulate in registers without cross-thread reduction.
+#include <algorithm>
 #include "kernels.cuh"
 #include "hex27.cuh"
 
@@ -85,7 +86,9 @@ FEMB_D void jac_transpose(const Tab1D<T>& t, const T F[3][3][3], T* E, int m1, i
     __syncwarp();
 }
 
-template <class T, class TG>
+// DIAG: every J⁻¹ is diagonal (axis-aligned boxes); the gradient and flux transforms
+// are one product per entry.
+template <class T, class TG, bool DIAG>
 __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<T, TG> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -194,7 +197,9 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) gq[c][k] = g[c][0][qz] * Ji[0 + 3 * k] + g[c][1][qz] * Ji[1 + 3 * k] + g[c][2][qz] * Ji[2 + 3 * k];
+                for (int k = 0; k < 3; ++k)
+                    gq[c][k] = DIAG ? g[c][k][qz] * Ji[4 * k]
+                                    : g[c][0][qz] * Ji[0 + 3 * k] + g[c][1][qz] * Ji[1 + 3 * k] + g[c][2][qz] * Ji[2 + 3 * k];
             const T sN = (T)c_tab.sumN3[q];
             T invG, cphi = 0, sphi = 0, spsi = 0, C = 0, ereg = 0, Kb = 0;
             if (uniform) {
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) Fp[c][d][qz] = w * Ji[d + 3 * c];
+                    for (int d = 0; d < 3; ++d) Fp[c][d][qz] = DIAG ? (c == d ? w * Ji[4 * c] : T(0)) : w * Ji[d + 3 * c];
             }
             T Rp[3][3];
             if constexpr (L::strided) jac_transpose<T>(tb, Fp, E, m1, m2, Rp);
@@ -294,8 +299,12 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 const T rx = tb.Dd[m1][bx] * tb.B[m2][by] * tb.B[qz][bz];
                 const T ry = tb.B[m1][bx] * tb.Dd[m2][by] * tb.B[qz][bz];
                 const T rz = tb.B[m1][bx] * tb.B[m2][by] * tb.Dd[qz][bz];
+                if (DIAG) {
+                    dnb[qz][0] = rx * Ji[0]; dnb[qz][1] = ry * Ji[4]; dnb[qz][2] = rz * Ji[8];
+                } else {
 #pragma unroll
-                for (int k = 0; k < 3; ++k) dnb[qz][k] = rx * Ji[0 + 3 * k] + ry * Ji[1 + 3 * k] + rz * Ji[2 + 3 * k];
+                    for (int k = 0; k < 3; ++k) dnb[qz][k] = rx * Ji[0 + 3 * k] + ry * Ji[1 + 3 * k] + rz * Ji[2 + 3 * k];
+                }
             }
 #pragma unroll 1
             for (int j = 0; j < 3; ++j) {
@@ -350,7 +359,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                     for (int c = 0; c < 3; ++c)
 #pragma unroll
                         for (int d = 0; d < 3; ++d)
-                            Fd[c][d][qz] = dOq * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
+                            Fd[c][d][qz] = DIAG ? dOq * Ji[4 * d] * sg[d][c]
+                                                : dOq * (Ji[d + 0] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
                 }
                 T dR[3][3];
                 if constexpr (L::strided) jac_transpose<T>(tb, Fd, E, m1, m2, dR);
@@ -377,6 +387,29 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     }
 }
 
+namespace {
+// Sets *flag when any integration point's J⁻¹ has a nonzero off-diagonal entry.
+template <class TG>
+__global__ void geo_offdiag_kernel(const TG* geo_v, int64_t npts, int* flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
+        const TG* g = geo_v + i * 10;
+        if (g[1] != TG(0) || g[2] != TG(0) || g[3] != TG(0) || g[5] != TG(0) || g[6] != TG(0) || g[7] != TG(0))
+            *flag = 1;
+    }
+}
+}  // namespace
+
+template <class TG>
+cudaError_t launch_geo_offdiag(const TG* geo_v, int64_t nels, int* flag, cudaStream_t st) {
+    const int64_t n = nels * 27;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    count_launch();
+    geo_offdiag_kernel<TG><<<(unsigned)blocks, 256, 0, st>>>(geo_v, n, flag);
+    return cudaGetLastError();
+}
+template cudaError_t launch_geo_offdiag<double>(const double*, int64_t, int*, cudaStream_t);
+template cudaError_t launch_geo_offdiag<float>(const float*, int64_t, int*, cudaStream_t);
+
 template <class T, class TG>
 cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st) {
     const int wpb = JAC_THREADS / 32;
@@ -384,7 +417,8 @@ cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cu
                         (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
     const int64_t groups = (args.nels + 2) / 3;
@@ -393,7 +427,8 @@ cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cu
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     count_launch();
-    hex27_jacobian_kernel<T, TG><<<(unsigned)blocks, JAC_THREADS, smem, st>>>(args);
+    if (args.diag_geometry) hex27_jacobian_kernel<T, TG, true><<<(unsigned)blocks, JAC_THREADS, smem, st>>>(args);
+    else hex27_jacobian_kernel<T, TG, false><<<(unsigned)blocks, JAC_THREADS, smem, st>>>(args);
     return cudaGetLastError();
 }
 

@@ -247,7 +247,10 @@ struct H27JacArgs {
     T* PC[3];
     int64_t nels;
     T dt;
+    int diag_geometry;    // every J⁻¹ diagonal (the Hex27 kernel's DIAG specialisation)
 };
+template <class TG>
+cudaError_t launch_geo_offdiag(const TG* geo_v, int64_t nels, int* flag, cudaStream_t st);
 
 template <class T, class TG>
 cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st);

@@ -95,6 +95,23 @@ def test_jacobian_diagnostics(dim, plastic, phases):
         close(dr.PC[c], hs.PC[c], rtol=1e-9, what=f"PC[{c}]")
 
 
+@pytest.mark.parametrize("plastic", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_jacobian_diagnostics_on_axis_aligned_cells(plastic, precision):
+    # a box mesh: every J⁻¹ is diagonal and the library takes its diagonal-geometry kernel
+    case = random_state_case(dim=3, n=3, seed=9, phases="cell", plastic=plastic, distort=False)
+    straight = fem.structured_mixed_mesh(3, (3, 3, 3), hi=(1.0, 2.0, 0.5))
+    case.mesh.coords, case.mesh.geo_v, case.mesh.geo_P = straight.coords, straight.geo_v, straight.geo_P
+    dt_ = torch.float64 if precision == "fp64" else torch.float32
+    dr, hs = case.device_state(fem, dtype=dt_, geometry_dtype=dt_), case.host_state(oh)
+    fem.assemble_augmented_momentum_jacobian(dr, case.dt)
+    hs.jacobian_diagnostics(case.dt)
+    tol = 1e-9 if precision == "fp64" else 2e-5
+    for c in range(3):
+        close(dr.dRdv[c], hs.dRdv[c], rtol=tol, atol_rel=tol, what=f"dRdv[{c}]")
+        close(dr.PC[c], hs.PC[c], rtol=tol, atol_rel=tol, what=f"PC[{c}]")
+
+
 @pytest.mark.parametrize("dim", [3, 2])
 @pytest.mark.parametrize("finite_K", [False, True])
 def test_pressure_scaling(dim, finite_K):
