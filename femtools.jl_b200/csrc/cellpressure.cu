@@ -5,18 +5,21 @@
 // momentum residual (assemble_stokes_momentum_residual_3d!, momentum_residuals.jl:644-700)
 // and the node/cell updates of the Arrow–Hurwicz relaxation (DR.jl:1004-1057).
 //
-// One warp per element: lane q < 27 evaluates integration point q, lane a < 27 owns node
-// a, and the element's velocities and per-point fluxes pass through the warp's shared
-// memory. The Hex27 tables are staged once per block in shared memory, because the
-// lanes index them by their own point or node.
+// The residuals, evaluated every iteration, use the sum-factorised line-thread stages
+// of the StokesDR sweeps (three elements per warp). The preconditioner, once per solve,
+// is one warp per element: lane a < 27 owns node a and lane q < 27 point q, with the
+// Hex27 tables staged once per block in shared memory because the lanes index them by
+// their own point or node.
 #include <algorithm>
 #include "kernels.cuh"
+#include "hex27.cuh"
 
 namespace femb {
 namespace {
 
 constexpr int CP_WARPS = 4;
 constexpr int CP_THREADS = CP_WARPS * 32;
+constexpr int CPS_THREADS = 128;   // sum-factorised residuals: 4 warps × 3 elements
 
 struct CpTabs {
     double dN[27][27][3];   // ∂N_a/∂ξ_j at q
@@ -43,116 +46,109 @@ FEMB_D double warp_sum_d(double x) {
     return x;
 }
 
-// Velocity gradient ∂v_c/∂x_k at point q from the element's staged velocities V[c·27 + a].
-FEMB_D void grad_at(const CpTabs& T, const double* V, int q, const double* Ji, double gv[3][3]) {
-    double gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int a = 0; a < 27; ++a) {
-        const double d0 = T.dN[q][a][0], d1 = T.dN[q][a][1], d2 = T.dN[q][a][2];
+// Sum-factorised residuals (the line-thread stages of hex27.cuh): a warp holds three
+// elements, nine lanes per element, each owning one tensor line of the 3×3×3 node and
+// point grids. PRES: RP(m, e) = −Σ_q mode_m ∇·v dΩ, reduced over the element's lanes
+// through shared memory; MOM: the viscous stress 2ηε̇′ − P·I and the body force −ρg at
+// the owned points, pushed back to the nodes by the transposed contraction and
+// scattered with FP64 atomics.
+template <bool MOM>
+__global__ void __launch_bounds__(CPS_THREADS) cp_residual_sf_kernel(const CpArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const bool lane_ok = lane < 27;
+    // lanes 27..31 carry no element; they work in a private scratch slot (3)
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
+    double* E = reinterpret_cast<double*>(smem_raw) + ((size_t)warp * 4 + s) * H27_ELEM_SMEM;
+    Tab1D<double> tb; tb.load();
+    const double gvec[3] = {a.g[0], a.g[1], a.g[2]};
+    const double xi = c_tab.qx[m1], et = c_tab.qx[m2];
+    const int64_t stride = (int64_t)gridDim.x * wpb * 3;
+    for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
+        const int64_t e = base + (lane_ok ? s : 0);
+        const bool act = lane_ok && e < a.nels;
+        const int64_t ec = act ? e : 0;
+        int node[3];
+        double v[3][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const double va = V[c * 27 + a];
-            gr[c][0] = fma(va, d0, gr[c][0]);
-            gr[c][1] = fma(va, d1, gr[c][1]);
-            gr[c][2] = fma(va, d2, gr[c][2]);
+        for (int i = 0; i < 3; ++i) {
+            node[i] = act ? __ldg(a.el2n + 27 * ec + c_tab.tn3[tidx(i, m1, m2)]) - 1 : 0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c][i] = act ? a.v[c][node[i]] : 0.0;
         }
-    }
-    // ∂v_c/∂x_k = Σ_j gr[c][j] J⁻¹[j][k], J⁻¹ column-major: (j, k) at j + 3k
+        double g[3][3][3];
+        h27_gradient(tb, v, E, m1, m2, g);
+        if constexpr (!MOM) {
+            double rp[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+            for (int qz = 0; qz < 3; ++qz) {
+                const double* G = a.geo_v + (ec * 27 + tidx(m1, m2, qz)) * 10;
+                double div = 0.0;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) gv[c][k] = gr[c][0] * Ji[3 * k] + gr[c][1] * Ji[1 + 3 * k] + gr[c][2] * Ji[2 + 3 * k];
-}
-
-FEMB_D void stage_velocity(const CpArgs& a, int64_t e, int lane, double* V, int& node) {
-    node = lane < 27 ? __ldg(a.el2n + e * 27 + lane) - 1 : 0;
-    if (lane < 27) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) V[c * 27 + lane] = a.v[c][node];
-    }
-    __syncwarp();
-}
-
-__global__ void __launch_bounds__(CP_THREADS) cp_pressure_residual_kernel(const CpArgs a) {
-    __shared__ CpTabs T;
-    __shared__ double Vs[CP_WARPS][81];
-    stage_tables(T);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int64_t e = (int64_t)blockIdx.x * CP_WARPS + w; e < a.nels; e += (int64_t)gridDim.x * CP_WARPS) {
-        int node;
-        stage_velocity(a, e, lane, Vs[w], node);
-        double r[4] = {0, 0, 0, 0};
-        if (lane < 27) {
-            const int q = lane;
-            const double* g = a.geo_v + (e * 27 + q) * 10;
-            double Ji[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) Ji[i] = __ldg(g + i);
-            double gv[3][3];
-            grad_at(T, Vs[w], q, Ji, gv);
-            const double f = (gv[0][0] + gv[1][1] + gv[2][2]) * __ldg(g + 9);
-            r[0] = f; r[1] = T.x[q][0] * f; r[2] = T.x[q][1] * f; r[3] = T.x[q][2] * f;
-        }
-#pragma unroll
-        for (int m = 0; m < 4; ++m) r[m] = warp_sum_d(r[m]);
-        if (lane < 4) a.RP[4 * e + lane] = -(lane == 0 ? r[0] : lane == 1 ? r[1] : lane == 2 ? r[2] : r[3]);
-        __syncwarp();
-    }
-}
-
-__global__ void __launch_bounds__(CP_THREADS) cp_momentum_residual_kernel(const CpArgs a) {
-    __shared__ CpTabs T;
-    __shared__ double Vs[CP_WARPS][81];
-    __shared__ double Fs[CP_WARPS][27][10];
-    stage_tables(T);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int64_t e = (int64_t)blockIdx.x * CP_WARPS + w; e < a.nels; e += (int64_t)gridDim.x * CP_WARPS) {
-        int node;
-        stage_velocity(a, e, lane, Vs[w], node);
-        const int ph = __ldg(a.phases + e) - 1;
-        if (lane < 27) {
-            const int q = lane;
-            const double* g = a.geo_v + (e * 27 + q) * 10;
-            double Ji[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) Ji[i] = __ldg(g + i);
-            const double dO = __ldg(g + 9);
-            double gv[3][3];
-            grad_at(T, Vs[w], q, Ji, gv);
-            // deviatoric strain rate and the viscous stress 2ηε̇′ (η interpolated over the cell)
-            const double tr = (gv[0][0] + gv[1][1] + gv[2][2]) / 3.0;
-            const double eta_q = a.eta[ph] * T.sumN[q];
-            double s[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) s[i][j] = 2.0 * eta_q * (0.5 * (gv[i][j] + gv[j][i]) - (i == j ? tr : 0.0));
-            const double* P = a.P + 4 * e;
-            const double Pq = P[0] + P[1] * T.x[q][0] + P[2] * T.x[q][1] + P[3] * T.x[q][2];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) s[i][i] -= Pq;
-            // reference-frame flux F[c][d] = dΩ Σ_k J⁻¹[d][k] σ[k][c]
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    Fs[w][q][c * 3 + d] = dO * (Ji[d] * s[0][c] + Ji[d + 3] * s[1][c] + Ji[d + 6] * s[2][c]);
-            Fs[w][q][9] = a.rho[ph] * T.sumN[q] * dO;
-        }
-        __syncwarp();
-        if (lane < 27) {
-            const int an = lane;
-            double R[3] = {0, 0, 0}, B = 0;
-            for (int q = 0; q < 27; ++q) {
-                const double d0 = T.dN[q][an][0], d1 = T.dN[q][an][1], d2 = T.dN[q][an][2];
-                const double* F = Fs[w][q];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) R[c] += d0 * F[c * 3] + d1 * F[c * 3 + 1] + d2 * F[c * 3 + 2];
-                B += T.N[q][an] * F[9];
+                for (int c = 0; c < 3; ++c) div += g[c][0][qz] * __ldg(G + 3 * c) + g[c][1][qz] * __ldg(G + 1 + 3 * c) +
+                                                   g[c][2][qz] * __ldg(G + 2 + 3 * c);
+                const double f = act ? -div * __ldg(G + 9) : 0.0;
+                const double ze = c_tab.qx[qz];
+                rp[0] += f; rp[1] += xi * f; rp[2] += et * f; rp[3] += ze * f;
             }
+            double* RPs = E + 460;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) atomicAdd(a.Rv[c] + node, R[c] - a.g[c] * B);
+            for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = rp[p];
+            __syncwarp();
+            if (act && m < 4) {
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) acc += RPs[t * 4 + m];
+                a.RP[4 * e + m] = acc;
+            }
+            __syncwarp();
+        } else {
+            const int ph = act ? __ldg(a.phases + ec) - 1 : 0;
+            double Pl[4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) Pl[p] = act ? a.P[4 * ec + p] : 0.0;
+            double F[3][3][3], beta_q[3];
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) {
+                const int q = tidx(m1, m2, qz);
+                const double* G = a.geo_v + (ec * 27 + q) * 10;
+                double Ji[9];
+#pragma unroll
+                for (int r = 0; r < 9; ++r) Ji[r] = act ? __ldg(G + r) : 0.0;
+                const double dO = act ? __ldg(G + 9) : 0.0;
+                double gq[3][3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        gq[c][k] = g[c][0][qz] * Ji[3 * k] + g[c][1][qz] * Ji[1 + 3 * k] + g[c][2][qz] * Ji[2 + 3 * k];
+                // η and ρ interpolated over the cell's single phase (interp2ip_phase)
+                const double sN = c_tab.sumN3[q];
+                const double eta_q = a.eta[ph] * sN;
+                const double tr = (gq[0][0] + gq[1][1] + gq[2][2]) / 3.0;
+                const double Pq = Pl[0] + Pl[1] * xi + Pl[2] * et + Pl[3] * c_tab.qx[qz];
+                double sg[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        sg[i][j] = 2.0 * eta_q * (0.5 * (gq[i][j] + gq[j][i]) - (i == j ? tr : 0.0)) - (i == j ? Pq : 0.0);
+                beta_q[qz] = a.rho[ph] * sN * dO;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) F[c][d][qz] = dO * (Ji[d] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
+            }
+            double R[3][3];
+            h27_transpose(tb, F, beta_q, gvec, E, m1, m2, R);
+            if (act) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) atomicAdd(a.Rv[c] + node[i], R[c][i]);
+            }
         }
-        __syncwarp();
     }
 }
 
@@ -267,16 +263,33 @@ inline unsigned grid_for(int64_t n, int t, int cap) {
 
 }  // namespace
 
-cudaError_t launch_cp_pressure_residual(const CpArgs& a, int num_sms, cudaStream_t st) {
+namespace {
+size_t cps_smem() { return (size_t)(CPS_THREADS / 32) * 4 * H27_ELEM_SMEM * sizeof(double); }
+
+template <bool MOM>
+cudaError_t launch_cp_sf(const CpArgs& a, int num_sms, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(cp_residual_sf_kernel<MOM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)cps_smem());
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const int wpb = CPS_THREADS / 32;
+    const int64_t groups = (a.nels + 2) / 3;
+    const unsigned blocks = grid_for(groups, wpb, num_sms * 16);
     count_launch();
-    cp_pressure_residual_kernel<<<grid_for(a.nels, CP_WARPS, num_sms * 8), CP_THREADS, 0, st>>>(a);
+    cp_residual_sf_kernel<MOM><<<blocks, CPS_THREADS, cps_smem(), st>>>(a);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_cp_pressure_residual(const CpArgs& a, int num_sms, cudaStream_t st) {
+    return launch_cp_sf<false>(a, num_sms, st);
 }
 
 cudaError_t launch_cp_momentum_residual(const CpArgs& a, int num_sms, cudaStream_t st) {
-    count_launch();
-    cp_momentum_residual_kernel<<<grid_for(a.nels, CP_WARPS, num_sms * 8), CP_THREADS, 0, st>>>(a);
-    return cudaGetLastError();
+    return launch_cp_sf<true>(a, num_sms, st);
 }
 
 cudaError_t launch_cp_preconditioner(const CpArgs& a, int num_sms, cudaStream_t st) {
