@@ -161,6 +161,18 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest of a per-rank value over all ranks (every multi-GPU time is the max over
+    ranks); the value itself on one rank. Every rank must call it, in the same order."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
 def cpu_baseline_estimate(case, iterations, jac_assemblies, threads=None):
     """Time-to-solution of the CPU restatement of the reference (the oracle), from a
     bounded sample: two fused residual sweeps on the full mesh, one Jacobian-diagnostics
@@ -563,7 +575,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--n", "--size", dest="n", type=int, default=64,
+                    help="elements per direction (--size spells it under torchrun, whose own options --n abbreviates)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
@@ -686,10 +699,7 @@ def main():
     lib.femb200_profile_read(h, prof_ms, prof_n)
     lib.femb200_profile(h, 0)
     t_step = ms_total / 1e3 / args.steps
-    if world > 1:
-        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = tt.item()
+    t_step = max_over_ranks(t_step, world)
 
     # ---- end to end: host inputs in pinned memory, copies inside the timed region ----
     host_in = {k: ([x.cpu().pin_memory() for x in v] if isinstance(v, list) else v.cpu().pin_memory())
@@ -715,10 +725,7 @@ def main():
     ev1.record(stream)
     barrier()
     t_e2e = ev0.elapsed_time(ev1) / 1e3 / e2e_steps
-    if world > 1:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = tt.item()
+    t_e2e = max_over_ranks(t_e2e, world)
 
     st = step_stats[-1]
     iters = st["iter"]
@@ -749,10 +756,7 @@ def main():
         ev1.record(stream)
         barrier()
         t64 = ev0.elapsed_time(ev1) / 1e3
-        if world > 1:
-            tt = torch.tensor([t64], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t64 = tt.item()
+        t64 = max_over_ranks(t64, world)
         f64 = snapshot()
         err = {k: float(torch.linalg.norm(chosen_fields[k] - f64[k]) / torch.linalg.norm(f64[k])) for k in f64}
         plain = {"value": t64, "unit": "s", "iterations": st64["iter"], "itPH": st64["itPH"],
