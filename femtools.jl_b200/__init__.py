@@ -34,6 +34,6 @@ from .postprocess import (compute_strain_rate_stress_postprocess, update_old_str
 from . import cellpressure  # noqa: E402,F401
 from .cellpressure import (CellPressureStokesDR, stokes_preconditioner_3d,  # noqa: E402,F401
                            assemble_stokes_pressure_residual_3d, assemble_stokes_momentum_residual_3d,
-                           solve_cell_pressure)
+                           solve_cell_pressure, solve_adjoint_cell_pressure, stokes_material_gradient_3d)
 from . import lithostatic  # noqa: E402,F401
 from .lithostatic import LithostaticPressureDR, assemble_lithostatic_pressure, solve_lithostatic  # noqa: E402,F401

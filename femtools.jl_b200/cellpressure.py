@@ -158,3 +158,82 @@ def solve_cell_pressure(dr: CellPressureStokesDR, bc_v, tolerance=1e-5, max_iter
     return {"converged": bool(st.converged), "iterations": st.iterations, "residual": st.residual,
             "history": history, "err_v": st.err_v, "err_P": st.err_P, "iter": st.iterations, "err": st.residual,
             "reached_total_iter": bool(st.reached_total_iter)}
+
+
+def solve_adjoint_cell_pressure(dr: CellPressureStokesDR, bc_v, objective_v, lam_v=None, lam_P=None,
+                                throw_on_failure=True, tolerance=1e-5, max_iterations=3000, check_interval=100,
+                                velocity_step=0.6, pressure_step=0.2):
+    """solve_adjoint!(dr::CellPressureStokesDR, mesh, bc_v; objective_v, λv, λP)
+    (src/stokes/solvers/DR_adjoint.jl:446-484): the viscous operator is symmetric and linear,
+    so the adjoint (∂R/∂u)ᵀλ = ∂J/∂u is the forward relaxation with `objective_v` (three nodal
+    arrays) as the momentum load, zero density and gravity and homogeneous conditions on
+    the nodes of `bc_v`. `lam_v` (three nodal arrays) and `lam_P` (4·nels) are the initial
+    iterate and are overwritten (zeros when omitted); dr.v and dr.P are left unchanged.
+    Returns (lam_v, lam_P, stats)."""
+    import torch
+    from . import solver
+    dev = dr.device
+    lam_v = [torch.zeros(dr.mesh.nnodes, dtype=torch.float64, device=dev) for _ in range(3)] if lam_v is None else lam_v
+    lam_P = torch.zeros(4 * dr.mesh.nels, dtype=torch.float64, device=dev) if lam_P is None else lam_P
+    if len(objective_v) != 3 or any(len(o) != dr.mesh.nnodes for o in objective_v):
+        raise ValueError("objective_v must have mesh.nnodes entries per component")
+    lib, h = solver._Handle.get()
+    zero_bc = []
+    for c in range(3):
+        bc = bc_v[c]
+        dofs = bc.DoFs if isinstance(bc, prob.DirichletBoundaryCondition) else bc[0]
+        zero_bc.append((np.asarray(dofs.cpu() if hasattr(dofs, "cpu") else dofs), np.zeros(len(dofs))))
+    p = dr.problem(zero_bc, load=objective_v)
+    for i in range(abi.MAX_PHASES):
+        p.rho[i] = 0.0
+    for c in range(3):
+        p.g[c] = 0.0
+        p.v[c] = solver._ptr(lam_v[c])
+    p.P = solver._ptr(lam_P)
+    c = abi.CellPressureControlsC()
+    c.tolerance, c.max_iterations, c.check_interval = tolerance, max_iterations, check_interval
+    c.velocity_step, c.pressure_step, c.throw_on_failure = velocity_step, pressure_step, 0
+    st = abi.CellPressureStatsC()
+    solver._check(lib, h, lib.femb200_solve_cell_pressure(h, C.byref(p), C.byref(c), C.byref(st)))
+    stats = {"converged": bool(st.converged), "iterations": st.iterations, "residual": st.residual,
+             "err_v": st.err_v, "err_P": st.err_P, "iter": st.iterations, "err": st.residual,
+             "reached_total_iter": bool(st.reached_total_iter)}
+    if not st.converged and throw_on_failure:
+        raise abi.FemB200Error(abi.ENOTCONV, f"3-D Stokes adjoint solve did not converge after {st.iterations} "
+                                             f"iterations (residual = {st.residual:g}, tolerance = {tolerance:g})")
+    return lam_v, lam_P, stats
+
+
+def stokes_material_gradient_3d(dr: CellPressureStokesDR, adjoint_velocity):
+    """stokes_material_gradient_3d(dr::CellPressureStokesDR, mesh, adjoint_velocity)
+    (src/stokes/solvers/DR_adjoint.jl:486-531): per phase, the adjoint contracted with the
+    derivative of the momentum residual in that phase's density (the load at v = 0, P = 0
+    with ρ = e_phase) and in its viscosity (the viscous residual of dr.v with η = e_phase,
+    no load): density_gradient[p] = −λ·∂R/∂ρ_p, viscosity_gradient[p] = −λ·∂R/∂η_p.
+    Both residuals are device assemblies; the contractions are device dot products."""
+    import torch
+    from . import solver
+    lib, h = solver._Handle.get()
+    n = len(dr.material.eta)
+    nn, ne = dr.mesh.nnodes, dr.mesh.nels
+    zero_v = [torch.zeros(nn, dtype=torch.float64, device=dr.device) for _ in range(3)]
+    zero_P = torch.zeros(4 * ne, dtype=torch.float64, device=dr.device)
+    R = [torch.empty(nn, dtype=torch.float64, device=dr.device) for _ in range(3)]
+    lam = [torch.as_tensor(x, dtype=torch.float64, device=dr.device).reshape(-1) for x in adjoint_velocity]
+
+    def contract(v, eta, rho, g):
+        p = dr.problem()
+        for i in range(abi.MAX_PHASES):
+            p.eta[i] = eta[i] if i < n else 0.0
+            p.rho[i] = rho[i] if i < n else 0.0
+        for c in range(3):
+            p.g[c] = g[c]
+            p.v[c], p.Rv[c] = solver._ptr(v[c]), solver._ptr(R[c])
+        p.P = solver._ptr(zero_P)
+        solver._check(lib, h, lib.femb200_cell_pressure_residuals(h, C.byref(p), 2))
+        return -float(sum(torch.dot(lam[c], R[c]) for c in range(3)))
+
+    unit = lambda k: [1.0 if i == k else 0.0 for i in range(n)]
+    dens = tuple(contract(zero_v, dr.material.eta, unit(k), dr.material.g) for k in range(n))
+    visc = tuple(contract(dr.v, unit(k), [0.0] * n, (0.0, 0.0, 0.0)) for k in range(n))
+    return {"density_gradient": dens, "viscosity_gradient": visc}

@@ -111,3 +111,26 @@ def test_non_convergence_is_reported():
         hs.solve(case.bc, tolerance=1e-12, max_iterations=200, check_interval=100)
     st = hs.solve(case.bc, tolerance=1e-12, max_iterations=150, check_interval=100, throw_on_failure=False)
     assert not st.converged and st.reached_total_iter and st.iterations == 150
+
+
+def test_oracle_adjoint_is_the_transposed_sparse_solve():
+    # the adjoint of the symmetric operator is the forward relaxation with the objective
+    # as load, no gravity and homogeneous conditions (DR_adjoint.jl:446-484)
+    import scipy.sparse.linalg as spla
+    case = fem.configs.cell_pressure_case(n=2, seed=4, distort=True)
+    nn = case.mesh.nnodes
+    rng = np.random.default_rng(2)
+    obj = [rng.standard_normal(nn) for _ in range(3)]
+    for c in range(3):
+        obj[c][case.bc[c][0] - 1] = 0.0
+    hs = oh.HostCellPressure(case.mesh, case.material.eta, (0.0,) * len(case.material.eta), (0.0, 0.0, 0.0),
+                             case.phases)
+    st = hs.solve([(b[0], np.zeros(len(b[0]))) for b in case.bc], tolerance=1e-11, max_iterations=400_000,
+                  load=obj)
+    assert st.converged
+    A, rhs, free = sparse_stokes_reference(case)
+    objective = np.concatenate([np.stack(obj, axis=1).ravel(), np.zeros(4 * case.mesh.nels)])
+    lam = np.zeros(len(rhs))
+    lam[free] = spla.spsolve(A[free][:, free].T.tocsc(), objective[free])
+    lv = lam[: 3 * nn].reshape(-1, 3)
+    assert np.linalg.norm(np.stack(hs.v, axis=1) - lv) <= 1e-6 * np.linalg.norm(lv)

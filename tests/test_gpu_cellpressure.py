@@ -104,3 +104,60 @@ def test_non_convergence_and_validation():
     dr.el2n[0, 3] = case.mesh.nnodes + 7
     with pytest.raises(abi.FemB200Error, match="connectivity entry outside"):
         fem.solve_cell_pressure(dr, case.bc)
+
+
+def _sparse_solution(case, objective=None):
+    import dataclasses  # noqa: F401
+    import scipy.sparse.linalg as spla
+    from test_cellpressure_oracle import sparse_stokes_reference
+    A, rhs, free = sparse_stokes_reference(case)
+    x = np.zeros(len(rhs))
+    Af = A[free][:, free].tocsc()
+    x[free] = spla.spsolve(Af, rhs[free])
+    lam = None
+    if objective is not None:
+        lam = np.zeros(len(rhs))
+        lam[free] = spla.spsolve(Af.T.tocsc(), objective[free])
+    return x, lam
+
+
+def test_adjoint_and_material_gradients_match_the_sparse_system():
+    # solve_adjoint! and stokes_material_gradient_3d (DR_adjoint.jl:446-531) against the
+    # transposed sparse system and central differences of its solutions
+    import dataclasses
+    case = fem.configs.cell_pressure_case(n=2, seed=5, distort=True)
+    mesh = case.mesh
+    nn, nv = mesh.nnodes, 3 * mesh.nnodes
+    rng = np.random.default_rng(12)
+    obj = [rng.standard_normal(nn) for _ in range(3)]
+    for c in range(3):
+        obj[c][case.bc[c][0] - 1] = 0.0
+    objective = np.concatenate([np.stack(obj, axis=1).ravel(), np.zeros(4 * mesh.nels)])
+    x, lam = _sparse_solution(case, objective)
+    dr = fem.CellPressureStokesDR(mesh, case.material, phases=case.phases)
+    fem.solve_cell_pressure(dr, case.bc, tolerance=1e-11, max_iterations=400_000)
+    lv, lP, st = fem.solve_adjoint_cell_pressure(dr, case.bc, obj, tolerance=1e-11, max_iterations=400_000)
+    assert st["converged"]
+    lam_v = lam[:nv].reshape(-1, 3)
+    got = np.stack([host(t) for t in lv], axis=1)
+    assert np.linalg.norm(got - lam_v) <= 1e-6 * np.linalg.norm(lam_v)
+    assert np.allclose(host(dr.v[2]), x[:nv].reshape(-1, 3)[:, 2], atol=1e-6 * np.abs(x[:nv]).max())
+    grads = fem.stokes_material_gradient_3d(dr, lv)
+    J = lambda cs: float(objective @ _sparse_solution(cs)[0])
+    h = 1e-5
+    for p in range(len(case.material.eta)):
+        rho = list(case.material.rho0)
+        rp, rm = list(rho), list(rho)
+        rp[p] += h
+        rm[p] -= h
+        mat = lambda r=None, e=None: fem.StokesMaterial(eta=e or case.material.eta, rho0=r or rho, g=case.material.g)
+        fd_rho = (J(dataclasses.replace(case, material=mat(r=rp))) - J(dataclasses.replace(case, material=mat(r=rm)))) / (2 * h)
+        eta = list(case.material.eta)
+        ep, em = list(eta), list(eta)
+        ep[p] *= 1 + h
+        em[p] *= 1 - h
+        fd_eta = (J(dataclasses.replace(case, material=mat(e=ep))) - J(dataclasses.replace(case, material=mat(e=em)))) / (2 * h * eta[p])
+        assert abs(grads["density_gradient"][p] - fd_rho) <= 1e-4 * max(abs(fd_rho), 1e-12)
+        assert abs(grads["viscosity_gradient"][p] - fd_eta) <= 1e-4 * max(abs(fd_eta), 1e-12)
+    # the forward state is untouched by the adjoint solve
+    assert np.allclose(host(dr.v[2]), x[:nv].reshape(-1, 3)[:, 2], atol=1e-6 * np.abs(x[:nv]).max())
