@@ -1496,8 +1496,9 @@ int cp_preconditioner(femb200_handle* h, const femb200_cell_pressure_problem* p)
     return FEMB200_OK;
 }
 
-int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int which) {
-    const CpArgs a = cp_args(p);
+int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int which, const double* geo_c = nullptr) {
+    CpArgs a = cp_args(p);
+    a.geo_c = geo_c;
     if (which & 1) CK(launch_cp_pressure_residual(a, h->num_sms, h->stream));
     if (which & 2) {
         for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(double) * p->nnodes, h->stream));
@@ -1922,6 +1923,24 @@ int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_p
     const int64_t nn = p->nnodes, nels = p->nels;
     const cudaStream_t s = h->stream;
     RC(cp_preconditioner(h, p));
+    // affine cells (a box or sheared mesh): the residuals read one J⁻¹ and |det J| per
+    // cell, built here once per solve in the handle's geometry scratch
+    const double* geo_c = nullptr;
+    {
+        const size_t need = (size_t)nels * 10 * sizeof(double);
+        if (need > h->geo_c_cap) {
+            if (h->d_geo_c) cudaFree(h->d_geo_c);
+            h->d_geo_c = nullptr;
+            CK(cudaMalloc(&h->d_geo_c, need));
+            h->geo_c_cap = need;
+        }
+        h->geo_c_valid = false;   // the StokesDR sweeps rebuild theirs at their next solve
+        CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+        CK(launch_cp_compress_geometry(p->geo_v, nels, static_cast<double*>(h->d_geo_c), h->d_flag, s));
+        CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (*h->h_flag == 0) geo_c = static_cast<const double*>(h->d_geo_c);
+    }
     // the first residual sees the prescribed boundary velocities too
     for (int k = 0; k < 3; ++k) CK(launch_dirichlet<double>(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k], s));
     const int nb = cp_mean_blocks(h->num_sms);
@@ -1930,9 +1949,9 @@ int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_p
     int64_t iter = 0, hist = 0;
     for (int64_t it = 1; it <= c->max_iterations; ++it) {
         iter = it;
-        RC(cp_residuals(h, p, 1));
+        RC(cp_residuals(h, p, 1, geo_c));
         CK(launch_cp_pressure_update(p->P, p->RP, p->pressure_mass, nels, c->pressure_step, h->d_partials, nb, s));
-        RC(cp_residuals(h, p, 2));
+        RC(cp_residuals(h, p, 2, geo_c));
         for (int k = 0; k < 3; ++k) {
             if (p->load[k]) CK(launch_cp_subtract(p->Rv[k], p->load[k], nn, s));
             CK(launch_dirichlet<double>(p->Rv[k], p->bc_dofs[k], nullptr, p->bc_n[k], s));

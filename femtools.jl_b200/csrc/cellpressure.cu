@@ -52,7 +52,9 @@ FEMB_D double warp_sum_d(double x) {
 // through shared memory; MOM: the viscous stress 2ηε̇′ − P·I and the body force −ρg at
 // the owned points, pushed back to the nodes by the transposed contraction and
 // scattered with FP64 atomics.
-template <bool MOM>
+// AFF: every cell is affine and a.geo_c holds one J⁻¹ and |det J| per cell (dΩ_q =
+// |det J|·ω_q), read once per element instead of at every point.
+template <bool MOM, bool AFF>
 __global__ void __launch_bounds__(CPS_THREADS) cp_residual_sf_kernel(const CpArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -83,12 +85,14 @@ __global__ void __launch_bounds__(CPS_THREADS) cp_residual_sf_kernel(const CpArg
             double rp[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
             for (int qz = 0; qz < 3; ++qz) {
-                const double* G = a.geo_v + (ec * 27 + tidx(m1, m2, qz)) * 10;
+                const int q = tidx(m1, m2, qz);
+                const double* G = AFF ? a.geo_c + ec * 10 : a.geo_v + (ec * 27 + q) * 10;
                 double div = 0.0;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) div += g[c][0][qz] * __ldg(G + 3 * c) + g[c][1][qz] * __ldg(G + 1 + 3 * c) +
                                                    g[c][2][qz] * __ldg(G + 2 + 3 * c);
-                const double f = act ? -div * __ldg(G + 9) : 0.0;
+                const double dOq = AFF ? __ldg(G + 9) * c_tab.w3[q] : __ldg(G + 9);
+                const double f = act ? -div * dOq : 0.0;
                 const double ze = c_tab.qx[qz];
                 rp[0] += f; rp[1] += xi * f; rp[2] += et * f; rp[3] += ze * f;
             }
@@ -112,11 +116,11 @@ __global__ void __launch_bounds__(CPS_THREADS) cp_residual_sf_kernel(const CpArg
 #pragma unroll
             for (int qz = 0; qz < 3; ++qz) {
                 const int q = tidx(m1, m2, qz);
-                const double* G = a.geo_v + (ec * 27 + q) * 10;
+                const double* G = AFF ? a.geo_c + ec * 10 : a.geo_v + (ec * 27 + q) * 10;
                 double Ji[9];
 #pragma unroll
                 for (int r = 0; r < 9; ++r) Ji[r] = act ? __ldg(G + r) : 0.0;
-                const double dO = act ? __ldg(G + 9) : 0.0;
+                const double dO = act ? (AFF ? __ldg(G + 9) * c_tab.w3[q] : __ldg(G + 9)) : 0.0;
                 double gq[3][3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
@@ -266,11 +270,11 @@ inline unsigned grid_for(int64_t n, int t, int cap) {
 namespace {
 size_t cps_smem() { return (size_t)(CPS_THREADS / 32) * 4 * H27_ELEM_SMEM * sizeof(double); }
 
-template <bool MOM>
+template <bool MOM, bool AFF>
 cudaError_t launch_cp_sf(const CpArgs& a, int num_sms, cudaStream_t st) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(cp_residual_sf_kernel<MOM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(cp_residual_sf_kernel<MOM, AFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)cps_smem());
         if (e != cudaSuccess) return e;
         configured = true;
@@ -279,17 +283,44 @@ cudaError_t launch_cp_sf(const CpArgs& a, int num_sms, cudaStream_t st) {
     const int64_t groups = (a.nels + 2) / 3;
     const unsigned blocks = grid_for(groups, wpb, num_sms * 16);
     count_launch();
-    cp_residual_sf_kernel<MOM><<<blocks, CPS_THREADS, cps_smem(), st>>>(a);
+    cp_residual_sf_kernel<MOM, AFF><<<blocks, CPS_THREADS, cps_smem(), st>>>(a);
     return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t launch_cp_pressure_residual(const CpArgs& a, int num_sms, cudaStream_t st) {
-    return launch_cp_sf<false>(a, num_sms, st);
+    return a.geo_c ? launch_cp_sf<false, true>(a, num_sms, st) : launch_cp_sf<false, false>(a, num_sms, st);
 }
 
 cudaError_t launch_cp_momentum_residual(const CpArgs& a, int num_sms, cudaStream_t st) {
-    return launch_cp_sf<true>(a, num_sms, st);
+    return a.geo_c ? launch_cp_sf<true, true>(a, num_sms, st) : launch_cp_sf<true, false>(a, num_sms, st);
+}
+
+namespace {
+// One J⁻¹ and |det J| = dΩ_q/ω_q per cell from its centre point; *not_affine is set when
+// any point of a cell differs from them by more than 1e-12 of their scale.
+__global__ void cp_compress_geometry_kernel(const double* geo_v, int64_t nels, double* out, int* not_affine) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nels) return;
+    const double* G = geo_v + e * 270;
+    double Jc[9], sc = 0;
+    for (int r = 0; r < 9; ++r) { Jc[r] = G[13 * 10 + r]; sc = fmax(sc, fabs(Jc[r])); }
+    const double dc = G[13 * 10 + 9] / c_tab.w3[13];
+    bool ok = true;
+    for (int q = 0; q < 27; ++q) {
+        for (int r = 0; r < 9; ++r) ok = ok && fabs(G[q * 10 + r] - Jc[r]) <= 1e-12 * sc;
+        ok = ok && fabs(G[q * 10 + 9] / c_tab.w3[q] - dc) <= 1e-12 * fabs(dc);
+    }
+    if (!ok) atomicOr(not_affine, 1);
+    for (int r = 0; r < 9; ++r) out[e * 10 + r] = Jc[r];
+    out[e * 10 + 9] = dc;
+}
+}  // namespace
+
+cudaError_t launch_cp_compress_geometry(const double* geo_v, int64_t nels, double* out, int* not_affine, cudaStream_t st) {
+    count_launch();
+    cp_compress_geometry_kernel<<<grid_for(nels, 128, 1 << 30), 128, 0, st>>>(geo_v, nels, out, not_affine);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cp_preconditioner(const CpArgs& a, int num_sms, cudaStream_t st) {

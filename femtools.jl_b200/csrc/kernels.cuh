@@ -184,7 +184,9 @@ struct CpArgs {
     double* RP;
     double* diagonal[3];
     double* pressure_mass;
+    const double* geo_c;     // per-cell affine geometry (J⁻¹, |det J|) or null: per-point geo_v
 };
+cudaError_t launch_cp_compress_geometry(const double* geo_v, int64_t nels, double* out, int* not_affine, cudaStream_t st);
 cudaError_t launch_cp_pressure_residual(const CpArgs& a, int num_sms, cudaStream_t st);
 cudaError_t launch_cp_momentum_residual(const CpArgs& a, int num_sms, cudaStream_t st);
 cudaError_t launch_cp_preconditioner(const CpArgs& a, int num_sms, cudaStream_t st);
