@@ -421,6 +421,74 @@ def cellpressure_mode(args, fem):
     return 0
 
 
+def cap_mode(args, fem):
+    """Tensile-cap local updates (femb200_cap_update, ncomp 6): one 3-D cap_local_update
+    per integration point of an n³ Hex27 mesh (27·n³ points; 7.1 M at n = 64) with random
+    trial stresses, pressures and per-point materials around the cap (elastic, shear and
+    cap branches mixed in every warp). Prints one JSON line: points per second, the
+    per-launch time and its algorithmic HBM bandwidth (14 FP64 inputs, 9 FP64 outputs and
+    the converged flag per point), and the serial oracle on a 100 000-point sample."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    n = 27 * args.n ** 3
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    u = lambda lo, hi: torch.rand(n, generator=g, device="cuda", dtype=torch.float64) * (hi - lo) + lo
+    phi = u(math.radians(10), math.radians(40))
+    psi = u(0.0, 1.0) * phi * (u(0.0, 1.0) < 0.8)
+    k, kq = torch.sin(phi), torch.sin(psi)
+    c = u(0.5, 3.0) * torch.cos(phi)
+    pT = -u(0.05, 0.9) * c / k
+    tau = torch.randn(n, 6, generator=g, device="cuda", dtype=torch.float64) * 1.5
+    P, eve, kdt = u(-3.0, 4.0), u(0.2, 3.0), u(0.5, 8.0)
+    ereg = u(0.0, 0.5) * (u(0.0, 1.0) < 0.7)
+    out_tau = torch.empty_like(tau)
+    out = [torch.empty(n, device="cuda", dtype=torch.float64) for _ in range(3)]
+    conv = torch.empty(n, device="cuda", dtype=torch.int32)
+    del phi, psi
+    lib, h = fem.solver._Handle.get()
+    pr = fem._abi.CapProblemC()
+    pr.n, pr.ncomp, pr.maxiter = n, 6, 40
+    pr.tau_trial, pr.P_trial, pr.eta_ve, pr.K_dt = tau.data_ptr(), P.data_ptr(), eve.data_ptr(), kdt.data_ptr()
+    pr.k, pr.kq, pr.c, pr.pT, pr.eta_reg = k.data_ptr(), kq.data_ptr(), c.data_ptr(), pT.data_ptr(), ereg.data_ptr()
+    pr.tau, pr.P, pr.gamma_dot, pr.theta_dot = out_tau.data_ptr(), out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr()
+    pr.converged = conv.data_ptr()
+    call = lambda: fem.solver._check(lib, h, lib.femb200_cap_update(h, C.byref(pr)))
+    for _ in range(args.warmup):
+        call()
+    k_steps = max(args.steps, 5)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(k_steps):
+        call()                    # inputs (1.3 GB at n = 64) exceed L2 between launches
+    ev[1].record()
+    torch.cuda.synchronize()
+    t = ev[0].elapsed_time(ev[1]) / k_steps / 1e3
+    nbytes = n * (14 * 8 + 9 * 8 + 4)
+    peak, kind = measured_peaks()
+    cv = conv.bool()
+    cpu = None
+    if not args.no_cpu_baseline:
+        m = 100_000
+        host = lambda x: x[:m].cpu().numpy().copy()
+        args_h = [host(x) for x in (tau, P, eve, kdt, k, kq, c, pT, ereg)]
+        t0 = time.perf_counter()
+        oh.cap_update(6, *args_h)
+        per = (time.perf_counter() - t0) / m
+        cpu = {"value": 1.0 / per, "unit": "points/s", "cores": 1, "kind": "port",
+               "sample": f"{m} points of the same batch through the serial oracle ({per * 1e6:.2f} us each)"}
+    print(json.dumps({
+        "mode": "cap", "workload": f"tensile-cap-local-update-3d-{n}-points", "points": n,
+        "value": n / t, "unit": "points/s", "ms_per_launch": t * 1e3, "steps": k_steps, "warmup": args.warmup,
+        "converged_frac": float(cv.double().mean()),
+        "plastic_frac": float(((out[1] > 0) & cv).double().mean()),
+        "roofline": {"bound": "hbm", "achieved": nbytes / t / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": nbytes / t / 1e9 / peak, "bytes_per_launch": nbytes, "peak_kind": kind},
+        "cpu_baseline": cpu}), flush=True)
+    return 0
+
+
 def lithostatic_mode(args, fem):
     """Lithostatic pressure (LithostaticPressureDR) on a structured Hex27 n³ mesh: two
     phases in horizontal layers, a temperature that falls with height, the EOS with a
@@ -599,7 +667,7 @@ def main():
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
     ap.add_argument("--tl-steps", type=int, default=10)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic"],
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -641,6 +709,8 @@ def main():
         return cellpressure_mode(args, fem)
     if args.mode == "lithostatic":
         return lithostatic_mode(args, fem)
+    if args.mode == "cap":
+        return cap_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()

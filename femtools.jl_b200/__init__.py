@@ -37,3 +37,6 @@ from .cellpressure import (CellPressureStokesDR, stokes_preconditioner_3d,  # no
                            solve_cell_pressure, solve_adjoint_cell_pressure, stokes_material_gradient_3d)
 from . import lithostatic  # noqa: E402,F401
 from .lithostatic import LithostaticPressureDR, assemble_lithostatic_pressure, solve_lithostatic  # noqa: E402,F401
+from . import cap  # noqa: E402,F401
+from .cap import (DruckerPragerCap, cap_geometry, cap_yield_function, cap_invariants,  # noqa: E402,F401
+                  cap_invariants_phase, softened_cohesion, cap_return_map, cap_local_update)

@@ -160,6 +160,16 @@ class CellPressureStatsC(C.Structure):
     ]
 
 
+class CapProblemC(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64), ("ncomp", C.c_int32), ("maxiter", C.c_int32),
+        ("tau_trial", _vp), ("s_trial", _vp), ("P_trial", _vp), ("eta_ve", _vp), ("K_dt", _vp),
+        ("k", _vp), ("kq", _vp), ("c", _vp), ("pT", _vp), ("eta_reg", _vp),
+        ("tau", _vp), ("tau_II", _vp), ("P", _vp), ("lambda_", _vp), ("A_tau", _vp), ("A_p", _vp),
+        ("gamma_dot", _vp), ("theta_dot", _vp), ("converged", _vp),
+    ]
+
+
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libfemtools_b200.so")
 
@@ -213,6 +223,7 @@ SIGNATURES = {
     "femb200_cell_pressure_residuals": (C.c_int, [_vp, _P(CellPressureProblemC), C.c_int32]),
     "femb200_solve_cell_pressure": (C.c_int, [_vp, _P(CellPressureProblemC), _P(CellPressureControlsC),
                                               _P(CellPressureStatsC)]),
+    "femb200_cap_update": (C.c_int, [_vp, _P(CapProblemC)]),
     "femb200_thermal_residual": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
     "femb200_solve_thermal": (C.c_int, [_vp, _P(ThermalProblemC), _P(ThermalControlsC), _P(ThermalStatsC)]),
     "femb200_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32]),

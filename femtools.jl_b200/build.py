@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfemtools_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["api.cu", "stokes3d.cu", "stokes3d_pipe.cu", "stokes3d_incr.cu", "adjoint3d.cu", "conv_bf16.cu", "warmstart_fields.cu", "geometry.cu", "postprocess.cu", "cellpressure.cu", "jacobian3d.cu", "simple.cu", "node.cu", "coloring.cpp"]
+SOURCES = ["api.cu", "stokes3d.cu", "stokes3d_pipe.cu", "stokes3d_incr.cu", "adjoint3d.cu", "conv_bf16.cu", "warmstart_fields.cu", "geometry.cu", "postprocess.cu", "cellpressure.cu", "jacobian3d.cu", "simple.cu", "node.cu", "cap.cu", "coloring.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-rdc=true"]

@@ -2012,6 +2012,25 @@ int femb200_strain_rate_stress(femb200_handle* h, const femb200_stokes_problem* 
     return strain_rate_stress_impl<float, float>(h, p, tau_ip, out);
 }
 
+int femb200_cap_update(femb200_handle* h, const femb200_cap_problem* p) {
+    if (!h) return FEMB200_EINVAL;
+    if (!p) { h->err = "cap_update: problem is required"; return FEMB200_EINVAL; }
+    if (p->n < 0) { h->err = "cap_update: negative point count"; return FEMB200_EINVAL; }
+    if (p->ncomp != 0 && p->ncomp != 3 && p->ncomp != 6) {
+        h->err = "cap_update: ncomp must be 0 (scalar return map), 3 (plane strain) or 6 (3-D)";
+        return FEMB200_EINVAL;
+    }
+    if (p->maxiter < 0) { h->err = "cap_update: maxiter must be >= 0"; return FEMB200_EINVAL; }
+    if (p->n == 0) return FEMB200_OK;
+    const bool trial = p->ncomp > 0 ? p->tau_trial != nullptr : p->s_trial != nullptr;
+    if (!trial || !p->P_trial || !p->eta_ve || !p->K_dt || !p->k || !p->kq || !p->c || !p->pT || !p->eta_reg) {
+        h->err = "cap_update: the trial state and every material array are required";
+        return FEMB200_EINVAL;
+    }
+    CK(launch_cap_update(*p, h->num_sms, h->stream));
+    return FEMB200_OK;
+}
+
 int femb200_extrapolate_state(femb200_handle* h, const femb200_stokes_problem* p, const void* const vprev[3],
                               const void* const vcur[3], const void* Pprev, const void* Pcur) {
     RC(check_problem(h, p));

@@ -376,6 +376,9 @@ struct LithoArgs {
 };
 cudaError_t launch_lithostatic(const LithoArgs& a, cudaStream_t st);
 
+// Tensile-cap local updates, one thread per point (cap.cu).
+cudaError_t launch_cap_update(const femb200_cap_problem& p, int num_sms, cudaStream_t st);
+
 // Thermal DR node update: rate = R/PC + β rate; T += α rate, masked by Dirichlet.
 template <class T>
 cudaError_t launch_thermal_update(T* Tn, T* rate, T* R, const T* PC, const uint8_t* mask, int64_t n, double alpha,

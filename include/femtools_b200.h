@@ -304,6 +304,40 @@ typedef struct femb200_cell_pressure_stats {
     int64_t history_len;
 } femb200_cell_pressure_stats;
 
+/* One batch of Drucker–Prager tensile-cap local updates (DruckerPragerCap,
+ * src/stokes/types/stokes_types.jl:426-545; Popov, Berlie & Kaus 2025). FP64 device
+ * arrays of n points; the material arrays hold each point's parameters as the
+ * reference interpolates them to the point: k = sin ϕ, kq = sin Ψ, c = C·cos ϕ (the
+ * softened cohesion), pT ≤ 0 (compression-positive pressure), η_reg, and the Maxwell
+ * viscosity ηve and Kb·Δt. */
+typedef struct femb200_cap_problem {
+    int64_t n;
+    int32_t ncomp;            /* 0: cap_return_map of s_trial; 3: cap_local_update of a
+                                 plane-strain (xx, yy, xy) stress; 6: of a 3-D
+                                 (xx, yy, zz, xy, xz, yz) stress */
+    int32_t maxiter;          /* Newton budget (40 in the reference) */
+    const double* tau_trial;  /* n × ncomp, point-major (ncomp > 0) */
+    const double* s_trial;    /* n (ncomp == 0) */
+    const double* P_trial;
+    const double* eta_ve;
+    const double* K_dt;
+    const double* k;
+    const double* kq;
+    const double* c;
+    const double* pT;
+    const double* eta_reg;
+    /* outputs, each optional (NULL: not written) */
+    double* tau;              /* n × ncomp: τ_trial − 2ηve·γdot·τ_trial/s_trial */
+    double* tau_II;           /* s of the return (s_trial when elastic or failed) */
+    double* P;                /* ncomp == 0: p of the return; ncomp > 0: P_trial + Kb·Δt·θdot */
+    double* lambda;
+    double* A_tau;            /* ½ ∂Q/∂s at the returned state */
+    double* A_p;              /* −∂Q/∂p at the returned state */
+    double* gamma_dot;        /* λ·A_tau (NaN when the local solve failed) */
+    double* theta_dot;        /* λ·A_p (NaN when the local solve failed) */
+    int32_t* converged;
+} femb200_cap_problem;
+
 /* ---- handle -------------------------------------------------------------- */
 typedef struct femb200_handle femb200_handle;
 
@@ -512,6 +546,19 @@ int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_p
  * εxx, εyy, εzz (= 0), εxy, εII, τxx, τyy, τzz, τxy, τII. Uses p's mesh, geometry and v. */
 int femb200_strain_rate_stress(femb200_handle* h, const femb200_stokes_problem* p,
                                const void* const tau_ip[6], void* const out[14]);
+
+/* ---- Drucker–Prager tensile cap (src/stokes/assemblers/rheology.jl:510-724) ---- */
+/* cap_return_map / cap_local_update at every point of p: the composite yield
+ * function (shear line τII = k·P + c closed by a circular cap through pT, tangent to
+ * it) and the coupled return for x = (s, p, λ),
+ *     s − s_trial + 2ηve·λ·Aτ = 0,  p − p_trial − Kb·Δt·λ·Ap = 0,  F − η_reg·λ = 0,
+ * by Newton on residuals scaled by max(|s_trial|, |p_trial|, |F_trial|, eps) with
+ * backtracking (at most 24 halvings, s ≥ 0, λ ≥ 0, Armijo decrease) to a scaled
+ * infinity norm ≤ 100·eps, then one more full Newton step. An elastic trial state
+ * (F ≤ 0) returns unchanged with λ = 0; a failure (ηve or Kb·Δt not positive and
+ * finite, a non-finite step, a failed line search, an exhausted budget) returns the
+ * trial state with converged = 0, and NaN γdot, θdot, τ and (ncomp > 0) P. */
+int femb200_cap_update(femb200_handle* h, const femb200_cap_problem* p);
 
 /* Initial guess of the next time step by linear extrapolation of a 2-D or 3-D FP64
  * state: v = 2 v_cur − v_prev on the DoFs p's Dirichlet sets leave free, P = 2 P_cur −

@@ -43,6 +43,8 @@ def lib():
             "orc_solve_lithostatic": (C.c_int, [_P(abi.LithostaticProblemC), _P(abi.LithostaticControlsC),
                                                 _P(abi.ThermalStatsC)]),
             "orc_lithostatic_element_custom": (C.c_int, [C.c_int] * 3 + [_vp] * 9 + [C.c_double] + [_vp] * 4),
+            "orc_cap_update": (C.c_int, [_P(abi.CapProblemC)]),
+            "orc_cap_invariants": (C.c_int, [C.c_int64, _vp, _vp] + [C.c_double] * 4 + [_vp] * 3),
             "orc_cell_pressure_preconditioner": (C.c_int, [_P(abi.CellPressureProblemC)]),
             "orc_cell_pressure_residuals": (C.c_int, [_P(abi.CellPressureProblemC), C.c_int32]),
             "orc_solve_cell_pressure": (C.c_int, [_P(abi.CellPressureProblemC), _P(abi.CellPressureControlsC),
@@ -451,3 +453,47 @@ def lithostatic_element(N, dNdx, dO, P, T, phases, rho0, alpha, K, Tref, g):
                                                ptr(r0), ptr(al), ptr(KK), Tref, ptr(gg), ptr(R), ptr(rows),
                                                ptr(diag)))
     return R, rows, diag
+
+
+def cap_update(ncomp, trial, P_trial, eta_ve, K_dt, k, kq, c, pT, eta_reg, maxiter=40):
+    """orc_cap_update on host arrays broadcast to one length: cap_return_map (ncomp 0,
+    trial = s_trial) or cap_local_update (ncomp 3 or 6, trial = n × ncomp stresses).
+    Returns a dict of numpy arrays named like femb200_cap_problem's outputs."""
+    if ncomp:
+        trial = np.ascontiguousarray(trial, dtype=np.float64).reshape(-1, ncomp)
+        n = trial.shape[0]
+        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (n,)))
+                for a in (P_trial, eta_ve, K_dt, k, kq, c, pT, eta_reg)]
+    else:
+        arrs = np.broadcast_arrays(*[np.asarray(a, dtype=np.float64)
+                                     for a in (trial, P_trial, eta_ve, K_dt, k, kq, c, pT, eta_reg)])
+        arrs = [np.ascontiguousarray(a).reshape(-1) for a in arrs]
+        trial, arrs = arrs[0], arrs[1:]
+        n = trial.shape[0]
+    out = {name: np.empty(n) for name in ("tau_II", "P", "lambda", "A_tau", "A_p", "gamma_dot", "theta_dot")}
+    out["converged"] = np.empty(n, dtype=np.int32)
+    if ncomp:
+        out["tau"] = np.empty((n, ncomp))
+    pr = abi.CapProblemC()
+    pr.n, pr.ncomp, pr.maxiter = n, ncomp, maxiter
+    if ncomp:
+        pr.tau_trial = ptr(trial)
+    else:
+        pr.s_trial = ptr(trial)
+    pr.P_trial, pr.eta_ve, pr.K_dt, pr.k, pr.kq, pr.c, pr.pT, pr.eta_reg = [ptr(a) for a in arrs]
+    pr.tau = ptr(out.get("tau"))
+    pr.tau_II, pr.P, pr.lambda_ = ptr(out["tau_II"]), ptr(out["P"]), ptr(out["lambda"])
+    pr.A_tau, pr.A_p = ptr(out["A_tau"]), ptr(out["A_p"])
+    pr.gamma_dot, pr.theta_dot, pr.converged = ptr(out["gamma_dot"]), ptr(out["theta_dot"]), ptr(out["converged"])
+    assert lib().orc_cap_update(C.byref(pr)) == 0
+    out["converged"] = out["converged"].astype(bool)
+    out["_keep"] = (trial, arrs)
+    return out
+
+
+def cap_invariants(s, p, k, kq, c, pT):
+    """orc_cap_invariants at the points (s, p) of one material: (F, Aτ, Ap) arrays."""
+    s, p = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in np.broadcast_arrays(s, p)]
+    F, At, Ap = np.empty(len(s)), np.empty(len(s)), np.empty(len(s))
+    assert lib().orc_cap_invariants(len(s), ptr(s), ptr(p), k, kq, c, pT, ptr(F), ptr(At), ptr(Ap)) == 0
+    return F, At, Ap

@@ -51,6 +51,7 @@ STRUCTS = {
     "femb200_cell_pressure_problem": abi.CellPressureProblemC,
     "femb200_cell_pressure_controls": abi.CellPressureControlsC,
     "femb200_cell_pressure_stats": abi.CellPressureStatsC,
+    "femb200_cap_problem": abi.CapProblemC,
 }
 
 
