@@ -9,12 +9,14 @@ namespace {
 
 constexpr int CAP_THREADS = 128;
 
+template <int NC>
 __global__ void __launch_bounds__(CAP_THREADS) cap_update_kernel(const femb200_cap_problem p) {
-    const int nc = p.ncomp;
+    constexpr int nc = NC;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += (int64_t)gridDim.x * blockDim.x) {
-        double tt[6];
+        double tt[NC > 0 ? NC : 1];
         double st;
         if (nc > 0) {
+#pragma unroll
             for (int j = 0; j < nc; ++j) tt[j] = __ldg(p.tau_trial + i * nc + j);
             st = cap_second_invariant(tt, nc);
         } else {
@@ -27,6 +29,7 @@ __global__ void __launch_bounds__(CAP_THREADS) cap_update_kernel(const femb200_c
         const double lam = r.converged ? r.lam : __longlong_as_double(0x7ff8000000000000ll);
         const double gdot = lam * r.At, tdot = lam * r.Ap;
         if (p.tau && nc > 0)
+#pragma unroll
             for (int j = 0; j < nc; ++j) p.tau[i * nc + j] = tt[j] - 2.0 * eve * gdot * tt[j] / st;
         if (p.tau_II) p.tau_II[i] = r.s;
         if (p.P) p.P[i] = nc > 0 ? Pt + Kdt * tdot : r.p;
@@ -46,7 +49,9 @@ cudaError_t launch_cap_update(const femb200_cap_problem& p, int num_sms, cudaStr
     count_launch();
     const int64_t want = (p.n + CAP_THREADS - 1) / CAP_THREADS;
     const int blocks = (int)std::min<int64_t>(want, (int64_t)num_sms * 16);
-    cap_update_kernel<<<blocks, CAP_THREADS, 0, st>>>(p);
+    if (p.ncomp == 6) cap_update_kernel<6><<<blocks, CAP_THREADS, 0, st>>>(p);
+    else if (p.ncomp == 3) cap_update_kernel<3><<<blocks, CAP_THREADS, 0, st>>>(p);
+    else cap_update_kernel<0><<<blocks, CAP_THREADS, 0, st>>>(p);
     return cudaGetLastError();
 }
 

@@ -51,9 +51,10 @@ FEMB_HD CapFlow<T> cap_flow(T s, T p, T k, T kq, T c, const CapGeom<T>& g) {
     } else {
         const T dp = p - g.p_y;
         const T R = sqrt(s * s + dp * dp + cap_eps<T>() * cap_eps<T>());
+        const T aR = g.a / R;
         f.F = g.a * (R - g.R_y);
-        f.dF[0] = g.a * s / R;
-        f.dF[1] = g.a * dp / R;
+        f.dF[0] = aR * s;
+        f.dF[1] = aR * dp;
     }
     f.dAt[0] = f.dAt[1] = f.dAp[0] = f.dAp[1] = T(0);
     if (p + kq * s >= g.p_q) {
@@ -67,10 +68,12 @@ FEMB_HD CapFlow<T> cap_flow(T s, T p, T k, T kq, T c, const CapGeom<T>& g) {
         f.At = f.Ap = T(0);
         return f;
     }
-    f.At = g.b * s / (T(2) * R);
-    f.Ap = -g.b * d / R;
-    // with u = s/R, w = d/R: ∂Aτ = b/(2R)·(w², −u·w), ∂Ap = b/R·(u·w, −u²)
-    const T u = s / R, w = d / R, bR = g.b / R;
+    // with u = s/R, w = d/R: Aτ = b·u/2, Ap = −b·w, ∂Aτ = b/(2R)·(w², −u·w),
+    // ∂Ap = b/R·(u·w, −u²)
+    const T iR = T(1) / R;
+    const T u = s * iR, w = d * iR, bR = g.b * iR;
+    f.At = T(0.5) * g.b * u;
+    f.Ap = -g.b * w;
     f.dAt[0] = T(0.5) * bR * w * w;
     f.dAt[1] = -T(0.5) * bR * u * w;
     f.dAp[0] = bR * u * w;
@@ -102,28 +105,37 @@ FEMB_HD void cap_residual(const T y[3], T st, T pt, T eve, T Kdt, T k, T kq, T c
 }
 
 // x = A⁻¹ b for a 3×3 system by Gaussian elimination with partial pivoting (A is
-// overwritten). A singular pivot gives non-finite entries.
+// overwritten). The pivot row is found by conditional swaps with compile-time row
+// indices, so the system stays in registers. A singular pivot gives non-finite entries.
 template <class T>
 FEMB_HD void cap_solve3(T A[3][3], const T b[3], T x[3]) {
     T r[3] = {b[0], b[1], b[2]};
+    T ip[3];   // reciprocal pivots
+#pragma unroll
     for (int col = 0; col < 3; ++col) {
-        int piv = col;
-        for (int i = col + 1; i < 3; ++i)
-            if (fabs(A[i][col]) > fabs(A[piv][col])) piv = i;
-        if (piv != col) {
-            for (int j = 0; j < 3; ++j) { const T t = A[col][j]; A[col][j] = A[piv][j]; A[piv][j] = t; }
-            const T t = r[col]; r[col] = r[piv]; r[piv] = t;
-        }
+#pragma unroll
         for (int i = col + 1; i < 3; ++i) {
-            const T m = A[i][col] / A[col][col];
+            if (fabs(A[i][col]) > fabs(A[col][col])) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) { const T t = A[col][j]; A[col][j] = A[i][j]; A[i][j] = t; }
+                const T t = r[col]; r[col] = r[i]; r[i] = t;
+            }
+        }
+        ip[col] = T(1) / A[col][col];
+#pragma unroll
+        for (int i = col + 1; i < 3; ++i) {
+            const T m = A[i][col] * ip[col];
+#pragma unroll
             for (int j = col; j < 3; ++j) A[i][j] -= m * A[col][j];
             r[i] -= m * r[col];
         }
     }
+#pragma unroll
     for (int i = 2; i >= 0; --i) {
         T acc = r[i];
+#pragma unroll
         for (int j = i + 1; j < 3; ++j) acc -= A[i][j] * x[j];
-        x[i] = acc / A[i][i];
+        x[i] = acc * ip[i];
     }
 }
 
@@ -159,9 +171,11 @@ FEMB_HD CapReturn<T> cap_return_map(T st, T pt, T eve, T Kdt, T k, T kq, T c, T 
                 cap_residual(cand, st, pt, eve, Kdt, k, kq, c, ereg, g, inv_scale, rn, Jn);
                 const T rrn = rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2];
                 if (isfinite(rn[0]) && isfinite(rn[1]) && isfinite(rn[2]) && rrn <= (T(1) - alpha / T(10000)) * rr) {
+#pragma unroll
                     for (int i = 0; i < 3; ++i) {
                         x[i] = cand[i];
                         r[i] = rn[i];
+#pragma unroll
                         for (int j = 0; j < 3; ++j) J[i][j] = Jn[i][j];
                     }
                     accepted = true;
