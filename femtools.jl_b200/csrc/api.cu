@@ -39,6 +39,8 @@ struct femb200_handle {
     size_t mask_cap = 0;
     uint8_t* d_tmask = nullptr;
     size_t tmask_cap = 0;
+    uint8_t* d_cpmask = nullptr;   // Dirichlet bits of the cell-pressure solve
+    size_t cpmask_cap = 0;
     std::string err;
     bool tables_ready = false;
     // profiling: event pairs per kernel class, folded into totals when the pool fills
@@ -1496,12 +1498,14 @@ int cp_preconditioner(femb200_handle* h, const femb200_cell_pressure_problem* p)
     return FEMB200_OK;
 }
 
-int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int which, const double* geo_c = nullptr) {
+int cp_residuals(femb200_handle* h, const femb200_cell_pressure_problem* p, int which, const double* geo_c = nullptr,
+                 bool rv_zeroed = false) {
     CpArgs a = cp_args(p);
     a.geo_c = geo_c;
     if (which & 1) CK(launch_cp_pressure_residual(a, h->num_sms, h->stream));
     if (which & 2) {
-        for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(double) * p->nnodes, h->stream));
+        if (!rv_zeroed)
+            for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(p->Rv[c], 0, sizeof(double) * p->nnodes, h->stream));
         CK(launch_cp_momentum_residual(a, h->num_sms, h->stream));
     }
     return FEMB200_OK;
@@ -1678,6 +1682,7 @@ int femb200_destroy(femb200_handle* h) {
     if (h->h_partials) cudaFreeHost(h->h_partials);
     if (h->d_mask) cudaFree(h->d_mask);
     if (h->d_tmask) cudaFree(h->d_tmask);
+    if (h->d_cpmask) cudaFree(h->d_cpmask);
     if (h->d_geo_c) cudaFree(h->d_geo_c);
     if (h->d_flag) cudaFree(h->d_flag);
     if (h->h_flag) cudaFreeHost(h->h_flag);
@@ -1941,24 +1946,45 @@ int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_p
         CK(cudaStreamSynchronize(s));
         if (*h->h_flag == 0) geo_c = static_cast<const double*>(h->d_geo_c);
     }
-    // the first residual sees the prescribed boundary velocities too
+    // the first residual sees the prescribed boundary velocities too; the velocity step
+    // leaves the constrained entries (bit k of the mask) at these values
     for (int k = 0; k < 3; ++k) CK(launch_dirichlet<double>(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k], s));
+    if ((size_t)nn > h->cpmask_cap) {
+        if (h->d_cpmask) cudaFree(h->d_cpmask);
+        h->d_cpmask = nullptr;
+        CK(cudaMalloc(&h->d_cpmask, (size_t)nn));
+        h->cpmask_cap = (size_t)nn;
+    }
+    CK(cudaMemsetAsync(h->d_cpmask, 0, (size_t)nn, s));
+    for (int k = 0; k < 3; ++k)
+        if (p->bc_n[k] > 0) CK(launch_build_mask(h->d_cpmask, p->bc_dofs[k], p->bc_n[k], k, s));
+    CpVelArgs va;
+    for (int k = 0; k < 3; ++k) {
+        va.v[k] = p->v[k];
+        va.Rv[k] = p->Rv[k];
+        va.diag[k] = p->diagonal[k];
+        va.load[k] = p->load[k];
+    }
+    va.mask = h->d_cpmask;
+    va.n = nn;
+    va.step = c->velocity_step;
+    bool rv_zeroed = false;   // the previous velocity step left Rv zeroed
     const int nb = cp_mean_blocks(h->num_sms);
     RC(ensure_partials(h, nb));
     double err_v = INFINITY, err_P = INFINITY, err = INFINITY;
     int64_t iter = 0, hist = 0;
     for (int64_t it = 1; it <= c->max_iterations; ++it) {
         iter = it;
+        const bool check = it % c->check_interval == 0 || it == c->max_iterations;
         RC(cp_residuals(h, p, 1, geo_c));
         CK(launch_cp_pressure_update(p->P, p->RP, p->pressure_mass, nels, c->pressure_step, h->d_partials, nb, s));
-        RC(cp_residuals(h, p, 2, geo_c));
-        for (int k = 0; k < 3; ++k) {
-            if (p->load[k]) CK(launch_cp_subtract(p->Rv[k], p->load[k], nn, s));
-            CK(launch_dirichlet<double>(p->Rv[k], p->bc_dofs[k], nullptr, p->bc_n[k], s));
-            CK(launch_cp_velocity_update(p->v[k], p->Rv[k], p->diagonal[k], nn, c->velocity_step, s));
-            CK(launch_dirichlet<double>(p->v[k], p->bc_dofs[k], p->bc_vals[k], p->bc_n[k], s));
-        }
-        if (!(it % c->check_interval == 0 || it == c->max_iterations)) continue;
+        RC(cp_residuals(h, p, 2, geo_c, rv_zeroed));
+        // between checks nothing reads Rv after the step: it is zeroed there for the next
+        // momentum residual; a check iteration keeps it for the norms (and the caller)
+        va.zero = check ? 0 : 1;
+        CK(launch_cp_velocity_step(va, s));
+        rv_zeroed = !check;
+        if (!check) continue;
         err_v = 0;
         for (int k = 0; k < 3; ++k) {
             double ss = 0;

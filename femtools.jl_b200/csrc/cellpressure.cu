@@ -55,7 +55,7 @@ FEMB_D double warp_sum_d(double x) {
 // AFF: every cell is affine and a.geo_c holds one J⁻¹ and |det J| per cell (dΩ_q =
 // |det J|·ω_q), read once per element instead of at every point.
 template <bool MOM, bool AFF>
-__global__ void __launch_bounds__(CPS_THREADS) cp_residual_sf_kernel(const CpArgs a) {
+__global__ void __launch_bounds__(CPS_THREADS, AFF ? 3 : 2) cp_residual_sf_kernel(const CpArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
@@ -238,14 +238,18 @@ __global__ void __launch_bounds__(256) cp_pressure_mean_kernel(double* P, int64_
         P[4 * e] -= pm;
 }
 
-__global__ void cp_velocity_update_kernel(double* v, const double* R, const double* diag, int64_t n, double step) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[i] -= step * R[i] / diag[i];
-}
-
-__global__ void cp_subtract_kernel(double* R, const double* load, int64_t n) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        R[i] -= load[i];
+__global__ void cp_velocity_step_kernel(const CpVelArgs a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned m = a.mask[i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double r = a.Rv[c][i];
+            if (a.load[c]) r -= __ldg(a.load[c] + i);
+            if ((m >> c) & 1u) r = 0.0;
+            else a.v[c][i] -= a.step * r / __ldg(a.diag[c] + i);
+            a.Rv[c][i] = a.zero ? 0.0 : r;
+        }
+    }
 }
 
 // Connectivity in 1..nnodes and phases in 1..nphases, before any kernel gathers by them.
@@ -349,16 +353,9 @@ cudaError_t launch_cp_pressure_update(double* P, const double* RP, const double*
     return cudaGetLastError();
 }
 
-cudaError_t launch_cp_velocity_update(double* v, const double* R, const double* diag, int64_t n, double step,
-                                      cudaStream_t st) {
+cudaError_t launch_cp_velocity_step(const CpVelArgs& a, cudaStream_t st) {
     count_launch();
-    cp_velocity_update_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(v, R, diag, n, step);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cp_subtract(double* R, const double* load, int64_t n, cudaStream_t st) {
-    count_launch();
-    cp_subtract_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(R, load, n);
+    cp_velocity_step_kernel<<<grid_for(a.n, 256, 148 * 8), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -195,9 +195,22 @@ cudaError_t launch_cp_validate(const int32_t* el2n, const int32_t* phases, int64
                                int* bad, cudaStream_t st);
 cudaError_t launch_cp_pressure_update(double* P, const double* RP, const double* M, int64_t nels, double step,
                                       double* partials, int nb, cudaStream_t st);
-cudaError_t launch_cp_velocity_update(double* v, const double* R, const double* diag, int64_t n, double step,
-                                      cudaStream_t st);
-cudaError_t launch_cp_subtract(double* R, const double* load, int64_t n, cudaStream_t st);
+// The momentum step of one relaxation iteration for the three components at once: Rv_c
+// less the load (where given), zero at the entries bit c of mask constrains, and
+// v_c −= step·Rv_c/diagonal_c at the others (the constrained velocities keep their
+// prescribed values). With zero set, Rv is left zeroed for the next momentum residual
+// instead of holding this residual.
+struct CpVelArgs {
+    double* v[3];
+    double* Rv[3];
+    const double* diag[3];
+    const double* load[3];
+    const uint8_t* mask;
+    int64_t n;
+    double step;
+    int zero;
+};
+cudaError_t launch_cp_velocity_step(const CpVelArgs& a, cudaStream_t st);
 
 // Element-averaged strain-rate and stress diagnostics (postprocess.cu).
 template <class T, class TG>
