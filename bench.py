@@ -273,6 +273,11 @@ def adjoint_mode(args, fem):
                                           max_iterations=2_000_000, iter_max=2_000_000, max_ph_iterations=1000,
                                           throw_on_failure=False)
     e2.record()
+    torch.cuda.synchronize()
+    # the gradient once untimed (first launches load their modules), then timed
+    (dr.viscosity_ip * fem.viscosity_sensitivity(dr, dt, lam_v, lam_P)).reshape(mesh.nels, mesh.nq).sum(dim=1)
+    e2b = ev()
+    e2b.record()
     sens = fem.viscosity_sensitivity(dr, dt, lam_v, lam_P)
     grad = (dr.viscosity_ip * sens).reshape(mesh.nels, mesh.nq).sum(dim=1)
     e3.record()
@@ -311,7 +316,7 @@ def adjoint_mode(args, fem):
                     "converged": bool(stf["converged"]), "thermal_iterations": stf["thermal_iterations"]},
         "adjoint": {"ms": e1.elapsed_time(e2), "iterations": sta["iter"], "itPH": sta["itPH"],
                     "converged": bool(sta["converged"]), "err": sta["err"]},
-        "gradient_ms": e2.elapsed_time(e3), "J": J,
+        "gradient_ms": e2b.elapsed_time(e3), "J": J,
         "fd": {"elements": int(kfd), "tolerance": args.fd_tolerance, "ms": e3.elapsed_time(e4),
                "iterations": fd_iters, "per_h": fd_out},
         "scope": "T frozen at the converged coupled state in the adjoint and the differences",

@@ -72,9 +72,10 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_adjoint_kernel(AdjArgs<T> a
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
     // lanes 27..31 carry no element; they work in a private scratch slot (3)
-    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * H27_ELEM_SMEM;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * H27_ELEM_SMEM) + (warp * 4 + s) * 28;
+    using LY = H27Layout<T>;   // stage layout (bank-conflict-free in FP64)
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : LY::IDLE_M, m1 = m % 3, m2 = m / 3;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * LY::SLOT;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * LY::SLOT) + (warp * 4 + s) * 28;
 
     Tab1D<T> tb; tb.load();
     const T dt = a.dt;
@@ -132,21 +133,21 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_adjoint_kernel(AdjArgs<T> a
 
         // ---- reference gradients (and the λ value) at the owned points ----
         T gl[3][3][3], gv[3][3][3], lval[3][3];
-        h27_gradient(tb, lv, E, m1, m2, gl);
+        h27_gradient<T, LY>(tb, lv, E, m1, m2, gl);
         {
-            const T* E1 = E + 162;   // stage-Y output: the ξη-interpolated λ is the third block
+            const T* E1 = E + 6 * LY::K1;   // stage-Y output: the ξη-interpolated λ is the third block
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     T acc = T(0);
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) acc += tb.B[q][k] * E1[(c * 3 + 2) * 27 + tidx(m1, m2, k)];
+                    for (int k = 0; k < 3; ++k) acc += tb.B[q][k] * E1[(c * 3 + 2) * LY::K2 + LY::l2(m1, m2, k)];
                     lval[c][q] = acc;
                 }
         }
         __syncwarp();
-        h27_gradient(tb, vv, E, m1, m2, gv);
+        h27_gradient<T, LY>(tb, vv, E, m1, m2, gv);
 
         // ---- s = (∂Rv/∂Pnum)ᵀλv = −∫ N^P ∇·λv over the owned points ----
         T NPq[3][4];
@@ -167,7 +168,8 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_adjoint_kernel(AdjArgs<T> a
 #pragma unroll
             for (int p = 0; p < 4; ++p) sp[p] -= NPq[qz][p] * divl * dO;
         }
-        T* RPs = E + 460;
+        T* RPs = E + 6 * LY::K1 + 9 * LY::K2;   // after the gradient's stages
+        static_assert(6 * LY::K1 + 9 * LY::K2 + 36 <= LY::SLOT, "mode reduction scratch");
 #pragma unroll
         for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = sp[p];
         __syncwarp();
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_adjoint_kernel(AdjArgs<T> a
         __syncwarp();
         if (!a.out_dv[0]) continue;
         T R[3][3];
-        h27_transpose(tb, Fb, zero3, gvec, E, m1, m2, R);
+        h27_transpose<T, true, LY>(tb, Fb, zero3, gvec, E, m1, m2, R);
         if (act) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_adjoint_kernel(AdjArgs<T> a
 template <class T>
 cudaError_t launch_hex27_adjoint(const AdjArgs<T>& args, int num_sms, cudaStream_t st) {
     const int wpb = H27_THREADS / 32;
-    const size_t smem = (size_t)wpb * 4 * H27_ELEM_SMEM * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
+    const size_t smem = (size_t)wpb * 4 * H27Layout<T>::SLOT * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(hex27_adjoint_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

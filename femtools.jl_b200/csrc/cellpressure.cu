@@ -60,9 +60,11 @@ __global__ void __launch_bounds__(CPS_THREADS, AFF ? 3 : 2) cp_residual_sf_kerne
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
-    // lanes 27..31 carry no element; they work in a private scratch slot (3)
-    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    double* E = reinterpret_cast<double*>(smem_raw) + ((size_t)warp * 4 + s) * H27_ELEM_SMEM;
+    // lanes 27..31 carry no element; they work in a private scratch slot (3) on the line
+    // the bank-conflict-free stage layout leaves them
+    using LY = H27Fp64Banked;
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : LY::IDLE_M, m1 = m % 3, m2 = m / 3;
+    double* E = reinterpret_cast<double*>(smem_raw) + ((size_t)warp * 4 + s) * LY::SLOT;
     Tab1D<double> tb; tb.load();
     const double gvec[3] = {a.g[0], a.g[1], a.g[2]};
     const double xi = c_tab.qx[m1], et = c_tab.qx[m2];
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(CPS_THREADS, AFF ? 3 : 2) cp_residual_sf_kerne
             for (int c = 0; c < 3; ++c) v[c][i] = act ? a.v[c][node[i]] : 0.0;
         }
         double g[3][3][3];
-        h27_gradient(tb, v, E, m1, m2, g);
+        h27_gradient<double, LY>(tb, v, E, m1, m2, g);
         if constexpr (!MOM) {
             double rp[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -96,7 +98,8 @@ __global__ void __launch_bounds__(CPS_THREADS, AFF ? 3 : 2) cp_residual_sf_kerne
                 const double ze = c_tab.qx[qz];
                 rp[0] += f; rp[1] += xi * f; rp[2] += et * f; rp[3] += ze * f;
             }
-            double* RPs = E + 460;
+            double* RPs = E + 6 * LY::K1 + 9 * LY::K2;   // after the gradient's stages
+            static_assert(6 * LY::K1 + 9 * LY::K2 + 36 <= LY::SLOT, "mode reduction scratch");
 #pragma unroll
             for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = rp[p];
             __syncwarp();
@@ -145,7 +148,7 @@ __global__ void __launch_bounds__(CPS_THREADS, AFF ? 3 : 2) cp_residual_sf_kerne
                     for (int d = 0; d < 3; ++d) F[c][d][qz] = dO * (Ji[d] * sg[0][c] + Ji[d + 3] * sg[1][c] + Ji[d + 6] * sg[2][c]);
             }
             double R[3][3];
-            h27_transpose(tb, F, beta_q, gvec, E, m1, m2, R);
+            h27_transpose<double, true, LY>(tb, F, beta_q, gvec, E, m1, m2, R);
             if (act) {
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
@@ -272,7 +275,7 @@ inline unsigned grid_for(int64_t n, int t, int cap) {
 }  // namespace
 
 namespace {
-size_t cps_smem() { return (size_t)(CPS_THREADS / 32) * 4 * H27_ELEM_SMEM * sizeof(double); }
+size_t cps_smem() { return (size_t)(CPS_THREADS / 32) * 4 * H27Fp64Banked::SLOT * sizeof(double); }
 
 template <bool MOM, bool AFF>
 cudaError_t launch_cp_sf(const CpArgs& a, int num_sms, cudaStream_t st) {

@@ -14,6 +14,7 @@
 //   after stage Y    : y-line (m1, ·, m2)
 //   quadrature stage : z-line (m1, m2, ·)  — quadrature points q = m1 + 3m2 + 9qz
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 
 namespace femb {
@@ -21,6 +22,38 @@ namespace femb {
 constexpr int H27_ELEM_SMEM = 540;   // scalars of stage scratch per element
 
 FEMB_D int tidx(int i, int j, int k) { return i + 3 * j + 9 * k; }
+
+// Layouts of the stage buffers. A buffer holds blocks of one 3×3×3 grid; it is written
+// along one line orientation and read along another. Buffers of the first kind (the
+// gradient's x-stage, the transpose's y-stage) use l1 in blocks of K1 words, those of
+// the second kind (the gradient's y-stage, the transpose's z-stage) l2 in blocks of K2.
+// H27Compact is i + 3j + 9k for both. H27Fp64Banked is for FP64 element slots 539
+// words apart with the idle lanes on m = 2 of a fourth slot: 3i + 4j + 9k and
+// 3i + 2j + 9k, found by exhaustive search over the two access orientations of each
+// buffer kind (FP64 shared accesses go as two half-warps over 16 eight-byte banks);
+// a gradient and a transpose take 480 wavefronts instead of the compact layout's 807
+// (384 is the floor).
+struct H27Compact {
+    static constexpr int K1 = 27, K2 = 27;
+    static constexpr int SLOT = H27_ELEM_SMEM, IDLE_M = 0;
+    static FEMB_D int l1(int i, int j, int k) { return i + 3 * j + 9 * k; }
+    static FEMB_D int l2(int i, int j, int k) { return i + 3 * j + 9 * k; }
+};
+struct H27Fp64Banked {
+    static constexpr int K1 = 33, K2 = 29;
+    static constexpr int SLOT = 539, IDLE_M = 2;
+    static FEMB_D int l1(int i, int j, int k) { return 3 * i + 4 * j + 9 * k; }
+    static FEMB_D int l2(int i, int j, int k) { return 3 * i + 2 * j + 9 * k; }
+};
+// words of stage scratch a layout needs per element slot
+template <class LY> constexpr int h27_stage_words() {
+    return (6 * LY::K1 + 9 * LY::K2) > (10 * LY::K2 + 7 * LY::K1) ? (6 * LY::K1 + 9 * LY::K2)
+                                                                   : (10 * LY::K2 + 7 * LY::K1);
+}
+static_assert(h27_stage_words<H27Compact>() <= H27_ELEM_SMEM, "compact stage layout");
+static_assert(h27_stage_words<H27Fp64Banked>() <= H27Fp64Banked::SLOT, "banked stage layout");
+// the layout of the four-slot kernels (three elements and the idle lanes per warp)
+template <class T> using H27Layout = std::conditional_t<sizeof(T) == 8, H27Fp64Banked, H27Compact>;
 
 // 1-D basis tables read straight from constant memory: every index in the stage
 // code is a compile-time constant, so they become constant-bank operands and take
@@ -47,7 +80,7 @@ struct Tab1D {
 // Reference gradients of the three velocity components at the three quadrature
 // points of the owned z-line. v[c][i]: node values on the owned x-line.
 // Output g[c][d][qz], d = ξ, η, ζ.
-template <class T>
+template <class T, class LY = H27Compact>
 FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m2, T g[3][3][3], bool wr = true) {
     // stage X: contract x (thread owns x-line (·, m1, m2))
 #pragma unroll
@@ -57,27 +90,30 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
             T x0 = t.B[q][0] * v[c][0] + t.B[q][1] * v[c][1] + t.B[q][2] * v[c][2];
             T x1 = t.Dd[q][0] * v[c][0] + t.Dd[q][1] * v[c][1] + t.Dd[q][2] * v[c][2];
             if (wr) {
-                E[(c * 2 + 0) * 27 + tidx(q, m1, m2)] = x0;
-                E[(c * 2 + 1) * 27 + tidx(q, m1, m2)] = x1;
+                E[(c * 2 + 0) * LY::K1 + LY::l1(q, m1, m2)] = x0;
+                E[(c * 2 + 1) * LY::K1 + LY::l1(q, m1, m2)] = x1;
             }
         }
     __syncwarp();
     // stage Y: thread owns y-line (qx = m1, ·, k = m2)
-    T* E1 = E + 162;
+    T* E1 = E + 6 * LY::K1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         T X0[3], X1[3];
 #pragma unroll
-        for (int j = 0; j < 3; ++j) { X0[j] = E[(c * 2 + 0) * 27 + tidx(m1, j, m2)]; X1[j] = E[(c * 2 + 1) * 27 + tidx(m1, j, m2)]; }
+        for (int j = 0; j < 3; ++j) {
+            X0[j] = E[(c * 2 + 0) * LY::K1 + LY::l1(m1, j, m2)];
+            X1[j] = E[(c * 2 + 1) * LY::K1 + LY::l1(m1, j, m2)];
+        }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const T y0 = t.B[q][0] * X1[0] + t.B[q][1] * X1[1] + t.B[q][2] * X1[2];
             const T y1 = t.Dd[q][0] * X0[0] + t.Dd[q][1] * X0[1] + t.Dd[q][2] * X0[2];
             const T y2 = t.B[q][0] * X0[0] + t.B[q][1] * X0[1] + t.B[q][2] * X0[2];
             if (wr) {
-                E1[(c * 3 + 0) * 27 + tidx(m1, q, m2)] = y0;
-                E1[(c * 3 + 1) * 27 + tidx(m1, q, m2)] = y1;
-                E1[(c * 3 + 2) * 27 + tidx(m1, q, m2)] = y2;
+                E1[(c * 3 + 0) * LY::K2 + LY::l2(m1, q, m2)] = y0;
+                E1[(c * 3 + 1) * LY::K2 + LY::l2(m1, q, m2)] = y1;
+                E1[(c * 3 + 2) * LY::K2 + LY::l2(m1, q, m2)] = y2;
             }
         }
     }
@@ -88,9 +124,9 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
         T A[3], Bv[3], Cv[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            A[k] = E1[(c * 3 + 0) * 27 + tidx(m1, m2, k)];
-            Bv[k] = E1[(c * 3 + 1) * 27 + tidx(m1, m2, k)];
-            Cv[k] = E1[(c * 3 + 2) * 27 + tidx(m1, m2, k)];
+            A[k] = E1[(c * 3 + 0) * LY::K2 + LY::l2(m1, m2, k)];
+            Bv[k] = E1[(c * 3 + 1) * LY::K2 + LY::l2(m1, m2, k)];
+            Cv[k] = E1[(c * 3 + 2) * LY::K2 + LY::l2(m1, m2, k)];
         }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -105,7 +141,7 @@ FEMB_D void h27_gradient(const Tab1D<T>& t, const T v[3][3], T* E, int m1, int m
 // Transposed contraction: nodal residual R[c][ix] on the owned x-line from the
 // reference-frame fluxes F[c][d][qz] and the body-force density beta[qz]
 // (R_c(a) = Σ_q Σ_d ∂_d N_a(q) F_cd(q) − g_c Σ_q N_a(q) β(q)).
-template <class T, bool BODY = true>
+template <class T, bool BODY = true, class LY = H27Compact>
 FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3], const T gvec[3], T* E,
                           int m1, int m2, T R[3][3], bool wr = true) {
     // Z^T: thread owns z-line (qx = m1, qy = m2)
@@ -117,29 +153,29 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
             const T z1 = t.B[0][iz] * F[c][1][0] + t.B[1][iz] * F[c][1][1] + t.B[2][iz] * F[c][1][2];
             const T z2 = t.Dd[0][iz] * F[c][2][0] + t.Dd[1][iz] * F[c][2][1] + t.Dd[2][iz] * F[c][2][2];
             if (wr) {
-                E[(c * 3 + 0) * 27 + tidx(m1, m2, iz)] = z0;
-                E[(c * 3 + 1) * 27 + tidx(m1, m2, iz)] = z1;
-                E[(c * 3 + 2) * 27 + tidx(m1, m2, iz)] = z2;
+                E[(c * 3 + 0) * LY::K2 + LY::l2(m1, m2, iz)] = z0;
+                E[(c * 3 + 1) * LY::K2 + LY::l2(m1, m2, iz)] = z1;
+                E[(c * 3 + 2) * LY::K2 + LY::l2(m1, m2, iz)] = z2;
             }
         }
     if constexpr (BODY) {
 #pragma unroll
         for (int iz = 0; iz < 3; ++iz) {
             const T zb = t.B[0][iz] * beta[0] + t.B[1][iz] * beta[1] + t.B[2][iz] * beta[2];
-            if (wr) E[9 * 27 + tidx(m1, m2, iz)] = zb;
+            if (wr) E[9 * LY::K2 + LY::l2(m1, m2, iz)] = zb;
         }
     }
     __syncwarp();
     // Y^T: thread owns y-line (qx = m1, ·, iz = m2)
-    T* E1 = E + 270;
+    T* E1 = E + 10 * LY::K2;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         T TA[3], TB[3], TC[3];
 #pragma unroll
         for (int qy = 0; qy < 3; ++qy) {
-            TA[qy] = E[(c * 3 + 0) * 27 + tidx(m1, qy, m2)];
-            TB[qy] = E[(c * 3 + 1) * 27 + tidx(m1, qy, m2)];
-            TC[qy] = E[(c * 3 + 2) * 27 + tidx(m1, qy, m2)];
+            TA[qy] = E[(c * 3 + 0) * LY::K2 + LY::l2(m1, qy, m2)];
+            TB[qy] = E[(c * 3 + 1) * LY::K2 + LY::l2(m1, qy, m2)];
+            TC[qy] = E[(c * 3 + 2) * LY::K2 + LY::l2(m1, qy, m2)];
         }
 #pragma unroll
         for (int iy = 0; iy < 3; ++iy) {
@@ -147,19 +183,19 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
             const T u1 = (t.Dd[0][iy] * TB[0] + t.Dd[1][iy] * TB[1] + t.Dd[2][iy] * TB[2]) +
                          (t.B[0][iy] * TC[0] + t.B[1][iy] * TC[1] + t.B[2][iy] * TC[2]);
             if (wr) {
-                E1[(c * 2 + 0) * 27 + tidx(m1, iy, m2)] = u0;
-                E1[(c * 2 + 1) * 27 + tidx(m1, iy, m2)] = u1;
+                E1[(c * 2 + 0) * LY::K1 + LY::l1(m1, iy, m2)] = u0;
+                E1[(c * 2 + 1) * LY::K1 + LY::l1(m1, iy, m2)] = u1;
             }
         }
     }
     if constexpr (BODY) {
         T TD[3];
 #pragma unroll
-        for (int qy = 0; qy < 3; ++qy) TD[qy] = E[9 * 27 + tidx(m1, qy, m2)];
+        for (int qy = 0; qy < 3; ++qy) TD[qy] = E[9 * LY::K2 + LY::l2(m1, qy, m2)];
 #pragma unroll
         for (int iy = 0; iy < 3; ++iy) {
             const T ub = t.B[0][iy] * TD[0] + t.B[1][iy] * TD[1] + t.B[2][iy] * TD[2];
-            if (wr) E1[6 * 27 + tidx(m1, iy, m2)] = ub;
+            if (wr) E1[6 * LY::K1 + LY::l1(m1, iy, m2)] = ub;
         }
     }
     __syncwarp();
@@ -168,7 +204,7 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
     if constexpr (BODY) {
         T UD[3];
 #pragma unroll
-        for (int qx = 0; qx < 3; ++qx) UD[qx] = E1[6 * 27 + tidx(qx, m1, m2)];
+        for (int qx = 0; qx < 3; ++qx) UD[qx] = E1[6 * LY::K1 + LY::l1(qx, m1, m2)];
 #pragma unroll
         for (int ix = 0; ix < 3; ++ix) body[ix] = t.B[0][ix] * UD[0] + t.B[1][ix] * UD[1] + t.B[2][ix] * UD[2];
     }
@@ -176,7 +212,10 @@ FEMB_D void h27_transpose(const Tab1D<T>& t, const T F[3][3][3], const T beta[3]
     for (int c = 0; c < 3; ++c) {
         T UA[3], UB[3];
 #pragma unroll
-        for (int qx = 0; qx < 3; ++qx) { UA[qx] = E1[(c * 2 + 0) * 27 + tidx(qx, m1, m2)]; UB[qx] = E1[(c * 2 + 1) * 27 + tidx(qx, m1, m2)]; }
+        for (int qx = 0; qx < 3; ++qx) {
+            UA[qx] = E1[(c * 2 + 0) * LY::K1 + LY::l1(qx, m1, m2)];
+            UB[qx] = E1[(c * 2 + 1) * LY::K1 + LY::l1(qx, m1, m2)];
+        }
 #pragma unroll
         for (int ix = 0; ix < 3; ++ix)
             R[c][ix] = (t.Dd[0][ix] * UA[0] + t.Dd[1][ix] * UA[1] + t.Dd[2][ix] * UA[2]) +

@@ -22,9 +22,10 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
     const bool lane_ok = lane < 27;
     // lanes 27..31 carry no element; they work in a private scratch slot (3) so
     // their (discarded) stage writes never touch an element's shared memory.
-    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
-    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * H27_ELEM_SMEM;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * H27_ELEM_SMEM) + (warp * 4 + s) * 28;
+    using LY = H27Layout<T>;   // stage layout (bank-conflict-free in FP64)
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : LY::IDLE_M, m1 = m % 3, m2 = m / 3;
+    T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * LY::SLOT;
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * LY::SLOT) + (warp * 4 + s) * 28;
 
     Tab1D<T> tb; tb.load();
     const T dt = a.dt;
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
 
         // ---- reference gradients at the owned quadrature points ----
         T g[3][3][3];
-        h27_gradient(tb, v, E, m1, m2, g);
+        h27_gradient<T, LY>(tb, v, E, m1, m2, g);
 
         // physical gradients and geometry at the three owned points
         T gp[3][3][3];   // gp[qz][c][k] = ∂v_c/∂x_k
@@ -133,7 +134,8 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
 #pragma unroll
             for (int p = 0; p < 4; ++p) rp[p] += NPq[qz][p] * f;
         }
-        T* RPs = E + 460;
+        T* RPs = E + 6 * LY::K1 + 9 * LY::K2;   // after the gradient's stages
+        static_assert(6 * LY::K1 + 9 * LY::K2 + 36 <= LY::SLOT, "mode reduction scratch");
 #pragma unroll
         for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = rp[p];
         __syncwarp();
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
         if (!a.do_momentum) continue;
 
         T R[3][3];
-        h27_transpose(tb, F, beta_q, gvec, E, m1, m2, R);
+        h27_transpose<T, true, LY>(tb, F, beta_q, gvec, E, m1, m2, R);
         if (act) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(H27_THREADS) hex27_residual_kernel(H27Args<T, 
 template <class T, class TG>
 cudaError_t launch_hex27_residual(const H27Args<T, TG>& args, int num_sms, cudaStream_t st) {
     const int wpb = H27_THREADS / 32;
-    const size_t smem = (size_t)wpb * 4 * H27_ELEM_SMEM * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
+    const size_t smem = (size_t)wpb * 4 * H27Layout<T>::SLOT * sizeof(T) + (size_t)wpb * 4 * 28 * sizeof(int);
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(hex27_residual_kernel<T, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
