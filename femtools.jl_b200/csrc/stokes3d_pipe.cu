@@ -25,7 +25,20 @@ namespace femb {
 // 27-value gradient/flux lines of each thread), 16 in FP32.
 template <class T> struct PipeThreads { static constexpr int value = 256; };
 template <> struct PipeThreads<float> { static constexpr int value = 512; };
-constexpr int PL_STAGE = 500;       // stage scratch per element slot (≥ 496)
+// Stage scratch per element slot and the layout of its buffers: FP64 uses the
+// bank-conflict-free H27Fp64Banked buffers with slots 523 words apart and the idle lanes
+// reading along line m = 0 of slot 2 (480 shared wavefronts per gradient + transpose in
+// place of 750); FP32 keeps i + 3j + 9k in 500-word slots.
+template <class T> struct PipeStage {
+    using LY = H27Compact;
+    static constexpr int WORDS = 500, IDLE_S = 0, IDLE_M = 0;
+};
+template <> struct PipeStage<double> {
+    using LY = H27Fp64Banked;
+    static constexpr int WORDS = 523, IDLE_S = 2, IDLE_M = 0;
+};
+static_assert(h27_stage_words<H27Compact>() <= PipeStage<float>::WORDS &&
+              h27_stage_words<H27Fp64Banked>() <= PipeStage<double>::WORDS, "pipe stage scratch");
 // Load buffer of one element slot: per-point fields (τ_old, 6 × 27; or, in the
 // incremental sweep, the base trial stress and yield value, 7 × 27), the affine
 // geometry (10) and the pressure-DoF data (32).
@@ -127,8 +140,11 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
     const bool lane_ok = lane < 27;
-    // lanes 27..31 carry no element: they follow slot 0's reads but never write
-    const int s = lane_ok ? lane / 9 : 0, m = lane_ok ? lane % 9 : 0, m1 = m % 3, m2 = m / 3;
+    // lanes 27..31 carry no element: they follow one slot's reads but never write
+    using PS = PipeStage<T>;
+    using LY = typename PS::LY;
+    constexpr int PL_STAGE = PS::WORDS;
+    const int s = lane_ok ? lane / 9 : PS::IDLE_S, m = lane_ok ? lane % 9 : PS::IDLE_M, m1 = m % 3, m2 = m / 3;
     T* base_w = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (3 * PL_STAGE + 3 * L::BUF);
     T* E = base_w + s * PL_STAGE;
     T* BUF = base_w + 3 * PL_STAGE;
@@ -239,7 +255,7 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
         const T* D = B + L::DOF;
 
         T g[3][3][3];
-        h27_gradient(tb, v, E, m1, m2, g, lane_ok);
+        h27_gradient<T, LY>(tb, v, E, m1, m2, g, lane_ok);
 
         // ---- pressure residual ----
         T rp[4] = {T(0), T(0), T(0), T(0)};
@@ -294,7 +310,8 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
         }
         // element sums of RP: lane m < 4 of each element sums component m, computes
         // its Pnum = γP·RP/M_P and shares it with the element's other lanes
-        T* RPs = E + 460;
+        T* RPs = E + 6 * LY::K1 + 9 * LY::K2;   // after the gradient's stages
+        static_assert(6 * LY::K1 + 9 * LY::K2 + 36 <= PL_STAGE, "RP scratch");
         if (lane_ok) {
 #pragma unroll
             for (int p = 0; p < 4; ++p) RPs[m * 4 + p] = rp[p];
@@ -456,7 +473,7 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
         id_next = load_ids(a, base + 2 * stride, s, m, tn_own, lane_ok);
         if (!a.do_momentum) continue;
         T R[3][3];
-        h27_transpose(tb, g, beta_q, gvec, E, m1, m2, R, lane_ok);
+        h27_transpose<T, true, LY>(tb, g, beta_q, gvec, E, m1, m2, R, lane_ok);
         if (act) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
@@ -503,7 +520,8 @@ cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t n
 template <class T, bool INCR>
 size_t pipe_smem_bytes() {
     const int wpb = PipeThreads<T>::value / 32;
-    return (size_t)wpb * (3 * PL_STAGE + 3 * PipeLayout<INCR>::BUF) * sizeof(T) + (size_t)wpb * 3 * 28 * sizeof(int);
+    return (size_t)wpb * (3 * PipeStage<T>::WORDS + 3 * PipeLayout<INCR>::BUF) * sizeof(T) +
+           (size_t)wpb * 3 * 28 * sizeof(int);
 }
 
 template <class T, bool INCR>
