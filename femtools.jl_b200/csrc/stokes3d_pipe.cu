@@ -48,6 +48,19 @@ template <bool INCR> struct PipeLayout {
     static constexpr int DOF = GEO + 10;
     static constexpr int BUF = INCR ? 232 : 208;
 };
+// Words between the load buffers of consecutive element slots: the buffer rounded up to
+// 9 modulo the bank count (16 eight-byte banks per half-warp in FP64, 32 four-byte banks
+// in FP32), so that the three slots' point reads (offsets m1 + 3m2 of each slot) and
+// their geometry broadcasts fall in distinct banks.
+template <class T, bool INCR> constexpr int pipe_buf() {
+    constexpr int banks = sizeof(T) == 8 ? 16 : 32;
+    constexpr int b = PipeLayout<INCR>::BUF;
+    return b + ((9 - b % banks) % banks + banks) % banks;
+}
+static_assert(pipe_buf<double, false>() % 16 == 9 && pipe_buf<double, true>() % 16 == 9 &&
+              pipe_buf<float, false>() % 32 == 9 && pipe_buf<float, true>() % 32 == 9 &&
+              pipe_buf<double, false>() >= PipeLayout<false>::BUF && pipe_buf<float, true>() >= PipeLayout<true>::BUF,
+              "load-buffer stride");
 enum { PT_TWOE, PT_TWOE_EL, PT_RHO0, PT_ALPHA, PT_BETA, PT_CC, PT_SPHI, PT_INVDEN, PT_INVBULKDT, PT_BULK, PT_FIELDS };
 
 namespace {
@@ -96,7 +109,7 @@ FEMB_D void issue_prefetch(const H27Args<T, T>& a, const T* geo_c, const GroupId
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) vn[c][i] = ld(a.v[c] + id.node[i]);
-    T* B = buf + s * L::BUF;
+    T* B = buf + s * pipe_buf<T, INCR>();
     if constexpr (INCR) {
 #pragma unroll
         for (int c = 0; c < 7; ++c)
@@ -145,10 +158,11 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
     using LY = typename PS::LY;
     constexpr int PL_STAGE = PS::WORDS;
     const int s = lane_ok ? lane / 9 : PS::IDLE_S, m = lane_ok ? lane % 9 : PS::IDLE_M, m1 = m % 3, m2 = m / 3;
-    T* base_w = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (3 * PL_STAGE + 3 * L::BUF);
+    constexpr int SB = pipe_buf<T, INCR>();
+    T* base_w = reinterpret_cast<T*>(smem_raw) + (size_t)warp * (3 * PL_STAGE + 3 * SB);
     T* E = base_w + s * PL_STAGE;
     T* BUF = base_w + 3 * PL_STAGE;
-    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * (3 * PL_STAGE + 3 * L::BUF)) +
+    int* PH = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)wpb * (3 * PL_STAGE + 3 * SB)) +
               (warp * 3 + s) * 28;
     const int sl = s;
 
@@ -217,7 +231,7 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
         const bool act = id.act;
         const int64_t ec = act ? base + s : 0;
 
-        const T* B = BUF + sl * L::BUF;
+        const T* B = BUF + sl * SB;
         // ---- phases ----
         int p0 = id.phase;
         bool uniform = true;
@@ -520,7 +534,7 @@ cudaError_t launch_compress_geometry(const TG* geo_v, const TG* geo_P, int64_t n
 template <class T, bool INCR>
 size_t pipe_smem_bytes() {
     const int wpb = PipeThreads<T>::value / 32;
-    return (size_t)wpb * (3 * PipeStage<T>::WORDS + 3 * PipeLayout<INCR>::BUF) * sizeof(T) +
+    return (size_t)wpb * (3 * PipeStage<T>::WORDS + 3 * pipe_buf<T, INCR>()) * sizeof(T) +
            (size_t)wpb * 3 * 28 * sizeof(int);
 }
 
