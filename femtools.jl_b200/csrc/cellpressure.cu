@@ -229,11 +229,20 @@ __global__ void __launch_bounds__(256) cp_pressure_update_kernel(double* P, cons
 
 // P(1, e) −= Σ P·M / Σ M, every block reducing the nb partials in the same order.
 __global__ void __launch_bounds__(256) cp_pressure_mean_kernel(double* P, int64_t nels, const double* partials, int nb) {
+    __shared__ double red[8][2];
     __shared__ double mean;
+    // every block reduces the partials itself (in a fixed order), all threads at once
+    double t0 = 0, t1 = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) { t0 += partials[2 * k]; t1 += partials[2 * k + 1]; }
+    t0 = warp_sum_d(t0);
+    t1 = warp_sum_d(t1);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { red[w][0] = t0; red[w][1] = t1; }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        double t0 = 0, t1 = 0;
-        for (int k = 0; k < nb; ++k) { t0 += partials[2 * k]; t1 += partials[2 * k + 1]; }
-        mean = t0 / t1;
+        double s0 = 0, s1 = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { s0 += red[k][0]; s1 += red[k][1]; }
+        mean = s0 / s1;
     }
     __syncthreads();
     const double pm = mean;
