@@ -25,16 +25,23 @@ constexpr int JAC_BP = 4 * 81;                 // ∂RP_p/∂v_(b,j)
 // per component block); with slots 1025 ≡ 1 (mod 32) words apart and the idle lanes
 // on m = 8, every stage access of the warp hits 28 distinct banks. The geometry
 // slots, 306 ≡ 18 (mod 32) words apart, are conflict-free for the same lane map.
-// FP64 keeps the compact h27 stage layout (its slots already fill three blocks per SM).
+// FP64 uses the bank-conflict-free h27 stage buffers (H27Fp64Banked) for the gradient
+// and the column loop's transposes, with element slots 859 ≡ 539 (mod 16) words apart,
+// geometry slots 307 ≡ 3 (mod 16) apart and the idle lanes on m = 2: 480 shared
+// wavefronts per gradient + transpose instead of the compact layout's 1 152 in 864-word
+// slots, and two per geometry read instead of four.
 constexpr int JAC_LA = 9 * 45;                 // stage-1 scratch: 9 blocks
 template <class T>
 struct JacSmem {
     static constexpr bool strided = sizeof(T) == 4;
-    static constexpr int stage = strided ? JAC_LA + 6 * 45 : H27_ELEM_SMEM;   // BP follows the stage scratch
-    static constexpr int e_stride = strided ? 1025 : H27_ELEM_SMEM + JAC_BP;
-    static constexpr int g_stride = strided ? 306 : JAC_GEO;
-    static_assert(stage + JAC_BP <= e_stride && stage >= H27_ELEM_SMEM && g_stride >= JAC_GEO, "slot layout");
-    static_assert(!strided || (e_stride % 32 == 1 && g_stride % 32 == 18), "bank layout");
+    using LY = std::conditional_t<strided, H27Compact, H27Fp64Banked>;   // h27 stage buffers
+    static constexpr int stage = strided ? JAC_LA + 6 * 45 : h27_stage_words<H27Fp64Banked>();   // BP follows
+    static constexpr int e_stride = strided ? 1025 : 859;
+    static constexpr int g_stride = strided ? 306 : 307;
+    static constexpr int idle_m = strided ? 8 : H27Fp64Banked::IDLE_M;
+    static_assert(stage + JAC_BP <= e_stride && stage >= h27_stage_words<LY>() && g_stride >= JAC_GEO, "slot layout");
+    static_assert(strided ? (e_stride % 32 == 1 && g_stride % 32 == 18)
+                          : (e_stride % 16 == H27Fp64Banked::SLOT % 16 && g_stride % 16 == 3), "bank layout");
 };
 
 FEMB_D int jla(int i, int j, int k) { return 3 * i + 9 * j + 10 * k; }
@@ -96,8 +103,8 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     const bool lane_ok = lane < 27;
     // lanes 27..31 carry no element; they work in a private scratch slot (3) so
     // their (discarded) stage writes never touch an element's shared memory.
-    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : 8, m1 = m % 3, m2 = m / 3;
     using L = JacSmem<T>;
+    const int s = lane_ok ? lane / 9 : 3, m = lane_ok ? lane % 9 : L::idle_m, m1 = m % 3, m2 = m / 3;
     T* E = reinterpret_cast<T*>(smem_raw) + ((size_t)warp * 4 + s) * L::e_stride;
     T* GEO = reinterpret_cast<T*>(smem_raw) + (size_t)wpb * 4 * L::e_stride + ((size_t)warp * 4 + s) * L::g_stride;
     T* BP = E + L::stage;
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
         }
 
         T g[3][3][3];
-        h27_gradient(tb, v, E, m1, m2, g);
+        h27_gradient<T, typename L::LY>(tb, v, E, m1, m2, g);
 
         // primal state at the owned points with η_pc
         // per point: ηve, λ, the trial stress and the reciprocals the 81 columns use
@@ -274,7 +281,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
             }
             T Rp[3][3];
             if constexpr (L::strided) jac_transpose<T>(tb, Fp, E, m1, m2, Rp);
-            else h27_transpose<T, false>(tb, Fp, zero3, zero3, E, m1, m2, Rp);
+            else h27_transpose<T, false, typename L::LY>(tb, Fp, zero3, zero3, E, m1, m2, Rp);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 }
                 T dR[3][3];
                 if constexpr (L::strided) jac_transpose<T>(tb, Fd, E, m1, m2, dR);
-                else h27_transpose<T, false>(tb, Fd, zero3, zero3, E, m1, m2, dR);
+                else h27_transpose<T, false, typename L::LY>(tb, Fd, zero3, zero3, E, m1, m2, dR);
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
