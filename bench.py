@@ -118,7 +118,11 @@ class ClockSampler:
     def __init__(self, index):
         self.proc = None
         self.index = index
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        # the raw samples go to FEMB_CLOCKS_DIR when set (a folder the caller keeps), else
+        # to the system temporary directory; the JSON line carries their summary
+        import tempfile
+        out_dir = os.environ.get("FEMB_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_rank{index}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
