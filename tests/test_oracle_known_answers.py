@@ -3,7 +3,8 @@
 Each case restates a FEMTools.jl test: the element-level closed forms of
 test/test_stokes.jl (one-point elements with J⁻¹ = I), the pressure scaling and
 hydrostatic solve of test/test_stokes_quadrature_viscosity.jl, the positive
-Hex27 modal mass of test/test_mixed_mesh.jl, the bulk-viscous closed form of
+Hex27 modal mass of test/test_mixed_mesh.jl, the body-force / EOS and pressure-rate
+cases of test/test_stokes.jl:718-776 on its one-point triangle, the bulk-viscous closed form of
 test/test_solver_convergence_api.jl and the shear-heating closed form of
 test/test_coupled_solver.jl. Where the reference test uses a triangle element
 the oracle lacks (T6/T7), the same closed form is checked on Q9 or Hex27 meshes:
@@ -238,3 +239,61 @@ def test_jacobian_diagnostics_match_finite_differences(plastic):
     dg = np.abs(np.diag(J)).reshape(3, n)
     np.testing.assert_allclose(np.array(rows), rs, rtol=1e-5)
     np.testing.assert_allclose(np.array(diag), dg, rtol=1e-5)
+
+
+# test/test_stokes.jl:718-870: the momentum residual's body-force and EOS branch on the
+# reference test's one-point linear triangle (N = ⅓ at the centroid, ∂N∂x = 0, dΩ = 0.5,
+# P interpolated with the same ⅓ weights), so that Rv = −N ρ(T, P) g dΩ.
+THIRD = [[1 / 3, 1 / 3, 1 / 3]]
+
+
+def _body_force(eta, alpha, rho0, K, g, P=(0.0, 0.0, 0.0), T=(0.0, 0.0, 0.0), phv=None):
+    mat = SM(eta=eta, G=(math.inf,) * len(eta), alpha=alpha, rho0=rho0, K=K, g=g, Tref=0.0)
+    R, _, _ = oh.element_custom(2, THIRD, np.zeros((1, 3, 2)), [0.5], THIRD, np.zeros(6), list(P), mat,
+                                dt=1.0, T=list(T), phv=phv)
+    return R
+
+
+@pytest.mark.parametrize("name, kw, rx, ry", [
+    ("zero gravity vanishes", dict(eta=(1.0,), alpha=(0.0,), rho0=(3.0,), K=(math.inf,), g=(0.0, 0.0)), 0.0, 0.0),
+    ("body force with T = Tref", dict(eta=(1.0,), alpha=(0.0,), rho0=(3.0,), K=(math.inf,), g=(0.0, -10.0)), 0.0, 5.0),
+    ("horizontal body force", dict(eta=(1.0,), alpha=(0.0,), rho0=(2.0,), K=(math.inf,), g=(5.0, 0.0)), -5 / 3, 0.0),
+    ("thermal EOS reduces density", dict(eta=(1.0,), alpha=(0.1,), rho0=(4.0,), K=(math.inf,), g=(0.0, -10.0),
+                                         T=(1.0, 1.0, 1.0)), 0.0, 6.0),
+    ("pressure EOS increases density", dict(eta=(1.0,), alpha=(0.0,), rho0=(2.0,), K=(4.0,), g=(0.0, -10.0),
+                                            P=(2.0, 2.0, 2.0)), 0.0, 5.0),
+    ("two-phase body force", dict(eta=(1.0, 1.0), alpha=(0.0, 0.0), rho0=(1.0, 3.0), K=(math.inf, math.inf),
+                                  g=(0.0, -6.0), phv=[1, 1, 2]), 0.0, 5 / 3),
+])
+def test_body_force_and_eos(name, kw, rx, ry):
+    R = _body_force(**kw)
+    np.testing.assert_allclose(R[0], [rx] * 3, rtol=1e-14, atol=1e-14)
+    np.testing.assert_allclose(R[1], [ry] * 3, rtol=1e-14, atol=1e-14)
+
+
+def test_pressure_rates_interpolate_nodal_increments():
+    # test/test_stokes.jl:736-752 (FP64): with zero velocity the continuity residual is the
+    # storage and thermal-expansion rate at the point, RP = N^P · rate · dΩ
+    Nv = np.array([0.2, 0.3, 0.5])
+    P, P0 = np.array([3.0, 5.0, 8.0]), np.array([1.0, 2.0, 3.0])
+    T, T0 = np.array([7.0, 4.0, 2.0]), np.array([2.0, 1.0, 1.0])
+    dt, eta_b, alpha, dO = 2.0, 4.0, 0.25, 0.5
+    mat = SM(eta=(1.0,), eta_b=(eta_b,), alpha=(alpha,), g=(0.0, 0.0))
+    _, RP, _ = oh.element_custom(2, [Nv], np.zeros((1, 3, 2)), [dO], [Nv], np.zeros(6), P, mat, dt=dt,
+                                 P0=P0, T=T, T0=T0)
+    rate = -Nv @ (P - P0) / (eta_b * dt) + alpha * Nv @ (T - T0) / dt
+    np.testing.assert_allclose(RP, Nv * rate * dO, rtol=1e-14)
+
+
+def test_finite_elastic_bulk_modulus_replaces_bulk_viscosity():
+    # test/test_stokes.jl:754-776: K = 8 in place of ηb = 4 in the storage term
+    Nv = np.array([0.2, 0.3, 0.5])
+    P, P0 = np.array([3.0, 5.0, 8.0]), np.array([1.0, 2.0, 3.0])
+    mat = SM(eta=(1.0,), eta_b=(4.0,), K=(8.0,), alpha=(0.0,), g=(0.0, 0.0))
+    common = dict(dt=2.0, P0=P0, T=np.zeros(3), T0=np.zeros(3))
+    _, RPk, _ = oh.element_custom(2, [Nv], np.zeros((1, 3, 2)), [0.5], [Nv], np.zeros(6), P, mat, finite_K=True,
+                                  **common)
+    _, RPb, _ = oh.element_custom(2, [Nv], np.zeros((1, 3, 2)), [0.5], [Nv], np.zeros(6), P, mat, **common)
+    np.testing.assert_allclose(RPk, Nv * (-(Nv @ (P - P0)) / (8.0 * 2.0) * 0.5), rtol=1e-14)
+    np.testing.assert_allclose(RPb, Nv * (-(Nv @ (P - P0)) / (4.0 * 2.0) * 0.5), rtol=1e-14)
+    assert not np.allclose(RPk, RPb)
