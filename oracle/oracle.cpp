@@ -780,7 +780,26 @@ void thermal_assemble(const femb200_thermal_problem* tp, double dt, double Tref,
     else thermal_assemble_t<9>(tp, dt, Tref, jac);
 }
 
-// shear_heating_element / shear_dissipation (shear_heating.jl:47-103).
+// shear_dissipation (shear_heating.jl:79-103): stress power less elastic power at one
+// point; g[i][k] = ∂v_i/∂x_k, stresses in assembler order (xx, yy, xy) or
+// (xx, yy, zz, xy, xz, yz); plane strain carries τzz = −(τxx + τyy) in the elastic term.
+double shear_dissipation(int dim, const double* tau, const double* o, const double g[3][3], double inv2Gdt) {
+    if (dim == 3) {
+        const double power = tau[0] * g[0][0] + tau[1] * g[1][1] + tau[2] * g[2][2] + tau[3] * (g[0][1] + g[1][0]) +
+                             tau[4] * (g[0][2] + g[2][0]) + tau[5] * (g[1][2] + g[2][1]);
+        const double elastic = (tau[0] * (tau[0] - o[0]) + tau[1] * (tau[1] - o[1]) + tau[2] * (tau[2] - o[2]) +
+                                2 * (tau[3] * (tau[3] - o[3]) + tau[4] * (tau[4] - o[4]) + tau[5] * (tau[5] - o[5]))) *
+                               inv2Gdt;
+        return power - elastic;
+    }
+    const double tzz = -(tau[0] + tau[1]), tzzo = -(o[0] + o[1]);
+    const double power = tau[0] * g[0][0] + tau[1] * g[1][1] + tau[2] * (g[0][1] + g[1][0]);
+    const double elastic = (tau[0] * (tau[0] - o[0]) + tau[1] * (tau[1] - o[1]) + tzz * (tzz - tzzo) +
+                            2 * tau[2] * (tau[2] - o[2])) * inv2Gdt;
+    return power - elastic;
+}
+
+// shear_heating_element (shear_heating.jl:47-73).
 void shear_heating_impl(const femb200_stokes_problem* p, double dt, double* phi) {
     const Tables& t = tables_for(p->dim);
     const int DD = p->dim;
@@ -803,28 +822,14 @@ void shear_heating_impl(const femb200_stokes_problem* p, double dt, double* phi)
             double g[3][3];
             for (int i = 0; i < DD; ++i)
                 for (int k = 0; k < DD; ++k) { double s = 0; for (int a = 0; a < el.NV; ++a) s += dNdx[a][k] * v[i][a]; g[i][k] = s; }
-            double out;
+            double tau[6];
             if (DD == 3) {
-                double tau[6];
                 stress3d<double>(g, etave, inv2Gdt, el.told[q], plp, Peq, tau, nullptr);
-                const double* o = el.told[q];
-                double power = tau[0] * g[0][0] + tau[1] * g[1][1] + tau[2] * g[2][2] + tau[3] * (g[0][1] + g[1][0]) +
-                               tau[4] * (g[0][2] + g[2][0]) + tau[5] * (g[1][2] + g[2][1]);
-                double elastic = (tau[0] * (tau[0] - o[0]) + tau[1] * (tau[1] - o[1]) + tau[2] * (tau[2] - o[2]) +
-                                  2 * (tau[3] * (tau[3] - o[3]) + tau[4] * (tau[4] - o[4]) + tau[5] * (tau[5] - o[5]))) * inv2Gdt;
-                out = power - elastic;
             } else {
                 double g2[2][2] = {{g[0][0], g[0][1]}, {g[1][0], g[1][1]}};
-                double tau[3];
                 stress2d<double>(g2, etave, inv2Gdt, el.told[q], plp, Peq, tau, nullptr);
-                const double* o = el.told[q];
-                double tzz = -(tau[0] + tau[1]), tzzo = -(o[0] + o[1]);
-                double power = tau[0] * g[0][0] + tau[1] * g[1][1] + tau[2] * (g[0][1] + g[1][0]);
-                double elastic = (tau[0] * (tau[0] - o[0]) + tau[1] * (tau[1] - o[1]) + tzz * (tzz - tzzo) +
-                                  2 * tau[2] * (tau[2] - o[2])) * inv2Gdt;
-                out = power - elastic;
             }
-            phi[(int64_t)el.NQ * e + q] = out;
+            phi[(int64_t)el.NQ * e + q] = shear_dissipation(DD, tau, el.told[q], g, inv2Gdt);
         }
     }
 }
@@ -1587,6 +1592,17 @@ int orc_stokes_viscosity_sensitivity(const femb200_stokes_problem* p, double dt,
     if (p->dim != 3) { g_last_error = "the adjoint oracle is 3-D (Hex27) only"; return FEMB200_EUNSUPPORTED; }
     viscosity_sensitivity_impl(p, dt, finite_K, with_pnum != 0, lam_v, lam_P, out_eta_ip);
     return FEMB200_OK;
+}
+
+// shear_dissipation at one point: g is ∂v_i/∂x_k row-major (dim × dim).
+int orc_shear_dissipation(int dim, const double* tau, const double* tau_old, const double* grad, double inv2Gdt,
+                          double* out) {
+    if (dim != 2 && dim != 3) return FEMB200_EINVAL;
+    double g[3][3] = {{0}};
+    for (int i = 0; i < dim; ++i)
+        for (int k = 0; k < dim; ++k) g[i][k] = grad[i * dim + k];
+    *out = shear_dissipation(dim, tau, tau_old, g, inv2Gdt);
+    return 0;
 }
 
 int orc_shear_heating(const femb200_stokes_problem* p, double dt, double* phi) {

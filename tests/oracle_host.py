@@ -60,6 +60,7 @@ def lib():
             "orc_solve_thermal": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.ThermalControlsC), _P(abi.ThermalStatsC)]),
             "orc_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64]),
             "orc_shear_heating": (C.c_int, [_P(abi.StokesProblemC), C.c_double, _vp]),
+            "orc_shear_dissipation": (C.c_int, [C.c_int, _vp, _vp, _vp, C.c_double, _vp]),
             "orc_stokes_adjoint_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
                                                       _vp * 3, _vp, _vp * 3, _vp]),
             "orc_stokes_viscosity_sensitivity": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
@@ -497,3 +498,11 @@ def cap_invariants(s, p, k, kq, c, pT):
     F, At, Ap = np.empty(len(s)), np.empty(len(s)), np.empty(len(s))
     assert lib().orc_cap_invariants(len(s), ptr(s), ptr(p), k, kq, c, pT, ptr(F), ptr(At), ptr(Ap)) == 0
     return F, At, Ap
+
+
+def shear_dissipation(dim, tau, tau_old, grad, inv2Gdt):
+    """orc_shear_dissipation: stress power less elastic power at one point."""
+    t, o, g = (np.ascontiguousarray(x, dtype=np.float64).ravel() for x in (tau, tau_old, grad))
+    out = np.zeros(1)
+    check(lib().orc_shear_dissipation(dim, ptr(t), ptr(o), ptr(g), inv2Gdt, ptr(out)))
+    return float(out[0])

@@ -297,3 +297,18 @@ def test_finite_elastic_bulk_modulus_replaces_bulk_viscosity():
     np.testing.assert_allclose(RPk, Nv * (-(Nv @ (P - P0)) / (8.0 * 2.0) * 0.5), rtol=1e-14)
     np.testing.assert_allclose(RPb, Nv * (-(Nv @ (P - P0)) / (4.0 * 2.0) * 0.5), rtol=1e-14)
     assert not np.allclose(RPk, RPb)
+
+
+def test_3d_shear_dissipation_identities():
+    # test/test_coupled_solver.jl:122-136: viscous simple shear vx = γ̇ y dissipates η γ̇²,
+    # and a plane flow embedded in 3-D dissipates as in plane strain
+    eta, gd = 2.0, 0.3
+    grad = [[0.0, gd, 0.0], [0.0, 0.0, 0.0], [0.0, 0.0, 0.0]]
+    tau = [0.0, 0.0, 0.0, eta * gd, 0.0, 0.0]
+    assert oh.shear_dissipation(3, tau, tau, grad, 0.0) == pytest.approx(eta * gd ** 2, rel=1e-14)
+    t2, t2o = [0.7, -0.4, 0.3], [0.2, 0.1, -0.5]
+    g2 = [[0.4, -0.2], [0.6, -0.1]]
+    embed = lambda t: [t[0], t[1], -(t[0] + t[1]), t[2], 0.0, 0.0]
+    g3 = [[0.4, -0.2, 0.0], [0.6, -0.1, 0.0], [0.0, 0.0, 0.0]]
+    assert oh.shear_dissipation(3, embed(t2), embed(t2o), g3, 1.7) == \
+        pytest.approx(oh.shear_dissipation(2, t2, t2o, g2, 1.7), rel=1e-14)
