@@ -207,3 +207,44 @@ def test_drucker_prager_cap_parameters():
         fem.DruckerPragerCap((phi,), (psi,), (C,), (1.0,), (0.1,), (4.0,))
     with pytest.raises(ValueError, match="cap radius is not positive"):
         fem.DruckerPragerCap((phi,), (psi,), (1.0,), (-5.0,), (0.1,), (4.0,))
+
+
+def _grad_F(t, P, g, h=1e-5):
+    F = lambda a, b: fem.cap_yield_function(a, b, CAP_k, CAP_c, g)
+    return (F(t + h, P) - F(t - h, P)) / (2 * h), (F(t, P + h) - F(t, P - h)) / (2 * h)
+
+
+def test_yield_gradient_has_magnitude_a_and_is_continuous():
+    # test/test_drucker_prager_cap.jl:175-212
+    g = fem.cap_geometry(CAP_k, CAP_kq, CAP_c, CAP_pT)
+    for t, P in ((2 * g.tau_d, g.p_d + 10.0), (0.2 * g.tau_d, CAP_pT - 0.5), (g.tau_d, g.p_d + 0.05),
+                 (g.tau_d, g.p_d - 0.05)):
+        dt, dP = _grad_F(t, P, g)
+        assert math.hypot(dt, dP) == pytest.approx(g.a, rel=1e-6)
+    dt, dP = _grad_F(2 * g.tau_d, g.p_d + 10.0, g)
+    assert dt == pytest.approx(1.0, rel=1e-6) and dP == pytest.approx(-CAP_k, rel=1e-6)
+    t, P = 0.2 * g.tau_d, CAP_pT - 0.5
+    R = math.hypot(t, P - g.p_y)
+    dt, dP = _grad_F(t, P, g)
+    assert dt == pytest.approx(g.a * t / R, rel=1e-6) and dP == pytest.approx(g.a * (P - g.p_y) / R, rel=1e-6)
+    dtp, dPp = _grad_F(g.tau_d, g.p_d + 1e-4, g)
+    dtm, dPm = _grad_F(g.tau_d, g.p_d - 1e-4, g)
+    assert dtp == pytest.approx(dtm, rel=1e-4) and dPp == pytest.approx(dPm, rel=1e-4)
+    assert dtp == pytest.approx(1.0, rel=1e-4) and dPp == pytest.approx(-CAP_k, rel=1e-4)
+
+
+def test_pa_scale_geometry():
+    # test/test_drucker_prager_cap.jl:233-253 (FP64): C = 10 MPa, tensile strength 5 MPa
+    k, kq = math.sin(math.radians(30)), math.sin(math.radians(10))
+    c, pT = 10.0e6 * math.cos(math.radians(30)), -5.0e6
+    g = fem.cap_geometry(k, kq, c, pT)
+    tol = math.sqrt(np.finfo(np.float64).eps)
+    assert g.R_y == pytest.approx(g.p_y - pT, rel=1e-12)
+    assert g.R_y == pytest.approx((k * g.p_y + c) / g.a, rel=tol)
+    assert g.tau_d == pytest.approx(k * g.p_d + c, rel=tol)
+    assert abs(fem.cap_yield_function(0.0, pT, k, c, g)) <= tol * g.R_y
+    # the oracle's return at that scale: a hydrostatic tension beyond pT comes back to the cap
+    ret = oh.cap_update(0, 0.0, 2 * pT, 1.0e10, 4.0e10, k, kq, c, pT, 0.0)
+    assert ret["converged"][0] and ret["lambda"][0] > 0
+    F, _, _ = fem.cap_invariants(ret["tau_II"][0], ret["P"][0], k, kq, c, pT)
+    assert abs(F) <= 1e-12 * abs(pT)
