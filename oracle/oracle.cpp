@@ -1594,6 +1594,39 @@ int orc_stokes_viscosity_sensitivity(const femb200_stokes_problem* p, double dt,
     return FEMB200_OK;
 }
 
+// One synthetic thermal element (the reference's integrate_residual unit-test setup):
+// nq points with shape values N (nq × nv), physical gradients dNdx (nq × nv × dim) and
+// weights dOmega; nodal T, T0, source, P and 1-based phases; the material of tp.
+int orc_thermal_element_custom(int dim, int nv, int nq, const double* N, const double* dNdx, const double* dOmega,
+                               const double* T, const double* T0, const double* src, const double* P,
+                               const int32_t* ph, const femb200_thermal_problem* tp, double dt, double Tref,
+                               double* R_out) {
+    if (nv > 27 || nq > 27 || (dim != 2 && dim != 3)) return FEMB200_EINVAL;
+    static thread_local Tables t;
+    std::memset(&t, 0, sizeof(t));
+    t.dim = dim; t.nv = nv; t.nq = nq;
+    for (int q = 0; q < nq; ++q)
+        for (int a = 0; a < nv; ++a) {
+            t.N[q][a] = N[q * nv + a];
+            for (int j = 0; j < dim; ++j) t.dN[q][a][j] = dNdx[(q * nv + a) * dim + j];
+        }
+    std::vector<double> geo((size_t)nq * (dim * dim + 1), 0.0);
+    for (int q = 0; q < nq; ++q) {
+        for (int d = 0; d < dim; ++d) geo[q * (dim * dim + 1) + d + dim * d] = 1.0;
+        geo[q * (dim * dim + 1) + dim * dim] = dOmega[q];
+    }
+    TElem el;
+    std::memset(&el, 0, sizeof(el));
+    el.NV = nv; el.NQ = nq; el.D = dim; el.geo = geo.data(); el.hasPhi = false;
+    for (int a = 0; a < nv; ++a) {
+        el.T0[a] = T0[a]; el.s[a] = src ? src[a] : 0.0; el.P[a] = P ? P[a] : 0.0; el.ph[a] = ph ? ph[a] - 1 : 0;
+    }
+    double Re[27];
+    thermal_element<double>(t, el, tp, T, dt, Tref, Re);
+    for (int a = 0; a < nv; ++a) R_out[a] = Re[a];
+    return 0;
+}
+
 // shear_dissipation at one point: g is ∂v_i/∂x_k row-major (dim × dim).
 int orc_shear_dissipation(int dim, const double* tau, const double* tau_old, const double* grad, double inv2Gdt,
                           double* out) {

@@ -61,6 +61,8 @@ def lib():
             "orc_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64]),
             "orc_shear_heating": (C.c_int, [_P(abi.StokesProblemC), C.c_double, _vp]),
             "orc_shear_dissipation": (C.c_int, [C.c_int, _vp, _vp, _vp, C.c_double, _vp]),
+            "orc_thermal_element_custom": (C.c_int, [C.c_int] * 3 + [_vp] * 8 + [_P(abi.ThermalProblemC), C.c_double,
+                                                                                C.c_double, _vp]),
             "orc_stokes_adjoint_residual": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
                                                       _vp * 3, _vp, _vp * 3, _vp]),
             "orc_stokes_viscosity_sensitivity": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int32,
@@ -506,3 +508,22 @@ def shear_dissipation(dim, tau, tau_old, grad, inv2Gdt):
     out = np.zeros(1)
     check(lib().orc_shear_dissipation(dim, ptr(t), ptr(o), ptr(g), inv2Gdt, ptr(out)))
     return float(out[0])
+
+
+def thermal_element_custom(dim, N, dNdx, dOmega, T, T0, src, P, phases, k, Cp, rho0, alpha, K, dt=1.0, Tref=0.0):
+    """One synthetic thermal element through the oracle (integrate_residual's unit-test setup)."""
+    N = np.ascontiguousarray(N, dtype=np.float64)
+    nq, nv = N.shape
+    arr = lambda x: np.ascontiguousarray(x, dtype=np.float64)
+    tp = abi.ThermalProblemC()
+    for name, vals in (("k", k), ("Cp", Cp), ("rho0", rho0), ("alpha", alpha), ("K", K)):
+        field = getattr(tp, name)
+        for i, v in enumerate(vals):
+            field[i] = v
+    tp.nphases = len(k)
+    args = [arr(dNdx), arr(dOmega), arr(T), arr(T0), arr(src), arr(P)]
+    ph = np.ascontiguousarray(phases, dtype=np.int32)
+    R = np.zeros(nv)
+    check(lib().orc_thermal_element_custom(dim, nv, nq, ptr(N), *[ptr(a) for a in args], ptr(ph), C.byref(tp),
+                                           dt, Tref, ptr(R)))
+    return R

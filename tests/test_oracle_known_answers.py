@@ -4,7 +4,8 @@ Each case restates a FEMTools.jl test: the element-level closed forms of
 test/test_stokes.jl (one-point elements with J⁻¹ = I), the pressure scaling and
 hydrostatic solve of test/test_stokes_quadrature_viscosity.jl, the positive
 Hex27 modal mass of test/test_mixed_mesh.jl, the body-force / EOS and pressure-rate
-cases of test/test_stokes.jl:718-776 on its one-point triangle, the bulk-viscous closed form of
+cases of test/test_stokes.jl:718-776 on its one-point triangle, the thermal element cases of
+test/test_heat_diffusion_residual.jl, the bulk-viscous closed form of
 test/test_solver_convergence_api.jl and the shear-heating closed form of
 test/test_coupled_solver.jl. Where the reference test uses a triangle element
 the oracle lacks (T6/T7), the same closed form is checked on Q9 or Hex27 meshes:
@@ -312,3 +313,31 @@ def test_3d_shear_dissipation_identities():
     g3 = [[0.4, -0.2, 0.0], [0.6, -0.1, 0.0], [0.0, 0.0, 0.0]]
     assert oh.shear_dissipation(3, embed(t2), embed(t2o), g3, 1.7) == \
         pytest.approx(oh.shear_dissipation(2, t2, t2o, g2, 1.7), rel=1e-14)
+
+
+# test/test_heat_diffusion_residual.jl:1-58: the thermal element residual (integrate_residual)
+# on a two-node one-point element.
+def _thermal(N, dNdx, P, phases, K, Tref, k=(1.0,), Cp=(1.0,), rho0=(2.0,), alpha=(0.01,)):
+    return oh.thermal_element_custom(2, [N], [dNdx], [1.0], [300.0, 300.0], [300.0, 300.0], [1.0, 1.0], P,
+                                     phases, k, Cp, rho0, alpha, K, dt=1.0, Tref=Tref)
+
+
+def test_thermal_residual_reference_temperature():
+    zero = [[0.0, 0.0], [0.0, 0.0]]
+    r1 = _thermal([0.5, 0.5], zero, [0.0, 0.0], [1, 1], (100.0,), 300.0)
+    r2 = _thermal([0.5, 0.5], zero, [0.0, 0.0], [1, 1], (100.0,), 250.0)
+    np.testing.assert_allclose(r1, [0.25, 0.25], rtol=1e-14)
+    np.testing.assert_allclose(r2, 2 * r1, rtol=1e-14)
+
+
+def test_thermal_incompressible_limit_with_negative_shape_values():
+    # a negative shape value makes an interpolated K = ∞ give ∞ − ∞; interpolating 1/K keeps
+    # the incompressible limit finite, for one phase or two, and a stiff finite K approaches it
+    N, g, P = [-0.25, 1.25], [[0.0, 1.0], [0.0, -1.0]], [1.0e6, 1.0e6]
+    inc = _thermal(N, g, P, [1, 1], (math.inf,), 300.0)
+    assert np.isfinite(inc).all()
+    two = _thermal(N, g, P, [1, 2], (math.inf, math.inf), 300.0, k=(1.0, 1.0), Cp=(1.0, 1.0), rho0=(2.0, 2.0),
+                   alpha=(0.01, 0.01))
+    np.testing.assert_allclose(two, inc, rtol=1e-14)
+    stiff = _thermal(N, g, P, [1, 1], (1.0e30,), 300.0)
+    np.testing.assert_allclose(stiff, inc, rtol=1e-12)
