@@ -3,7 +3,8 @@ femtools_b200.cap to the reference's own tests (test/test_drucker_prager_cap.jl)
 JustRelax return-map rows (tests/golden/cap_justrelax.json, made from that file by
 tests/golden/make_cap_fixtures.py) at rtol 1e-12, the closed forms and residual identities
 of the coupled return, the geometry identities of the cap surface, and the parameter checks
-of DruckerPragerCap. CPU only."""
+of DruckerPragerCap, and the Popov 2-D material point (test/test_popov_2d_material_point.jl).
+CPU only."""
 import json
 import math
 import os
@@ -248,3 +249,30 @@ def test_pa_scale_geometry():
     assert ret["converged"][0] and ret["lambda"][0] > 0
     F, _, _ = fem.cap_invariants(ret["tau_II"][0], ret["P"][0], k, kq, c, pT)
     assert abs(F) <= 1e-12 * abs(pT)
+
+
+def test_popov_2d_material_point():
+    # test/test_popov_2d_material_point.jl: ϕ = 30°, ψ = 0, C = 20, pT = −1, ηve = 1, Kb·Δt = 64,
+    # η_reg = 0.1
+    phi = math.radians(30.0)
+    k, kq, c, pT = math.sin(phi), 0.0, 20.0 * math.cos(phi), -1.0
+    g = fem.cap_geometry(k, kq, c, pT)
+    assert abs(fem.cap_yield_function(0.0, pT, k, c, g)) <= 1e-12
+    el = oh.cap_update(0, 0.0, -0.5, 1.0, 64.0, k, kq, c, pT, 0.1)
+    assert el["converged"][0] and el["lambda"][0] == 0.0 and el["P"][0] == -0.5
+    y = oh.cap_update(0, 0.0, -1.2, 1.0, 64.0, k, kq, c, pT, 0.1)
+    assert y["converged"][0] and y["lambda"][0] > 0 and -1.2 < y["P"][0] < pT
+    # the plane-strain local update of a zero trial stress (η = G = Δt = 1: ηve = ½) returns
+    # the same pressure, with the stress left at zero
+    lu = oh.cap_update(3, np.zeros(3), -1.2, 0.5, 64.0, k, kq, c, pT, 0.1)
+    assert (lu["tau"][0] == 0).all() and lu["P"][0] == pytest.approx(y["P"][0], rel=1e-12)
+    # cohesion softening: C = 20, C_min = 5, H_C = −3
+    assert fem.softened_cohesion(20.0, 5.0, -3.0, 0.0) == 20.0
+    assert fem.softened_cohesion(20.0, 5.0, -3.0, 2.0) == 14.0
+    assert fem.softened_cohesion(20.0, 5.0, -3.0, 10.0) == 5.0
+    soft = fem.DruckerPragerCap((phi,), (0.0,), (20.0,), (pT,), (0.1,), (64.0,), C_min=(5.0,), H_C=(-3.0,))
+    assert soft.C_min == (5.0,) and soft.H_C == (-3.0,)
+    Cs = fem.softened_cohesion(soft.C[0], soft.C_min[0], soft.H_C[0], 2.0)
+    ps = oh.cap_update(3, np.zeros(3), -1.2, 0.5, 64.0, k, kq, Cs * soft.cos_phi[0], pT, 0.1)
+    ref = oh.cap_update(0, 0.0, -1.2, 1.0, 64.0, k, kq, 14.0 * math.cos(phi), pT, 0.1)
+    assert ps["P"][0] == pytest.approx(ref["P"][0], rel=1e-12)
