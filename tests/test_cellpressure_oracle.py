@@ -134,3 +134,35 @@ def test_oracle_adjoint_is_the_transposed_sparse_solve():
     lam[free] = spla.spsolve(A[free][:, free].T.tocsc(), objective[free])
     lv = lam[: 3 * nn].reshape(-1, 3)
     assert np.linalg.norm(np.stack(hs.v, axis=1) - lv) <= 1e-6 * np.linalg.norm(lv)
+
+
+def test_prescribed_velocities_enter_the_first_residual():
+    # test/test_stokes_3d_boundary_values.jl: one Hex27 cell, every boundary node prescribed
+    # (vx = x, vy = vz = 0), no gravity; one iteration with a check must not report
+    # convergence from the all-zero start, and a start that already carries the prescribed
+    # values gives the same first iteration
+    mesh = fem.structured_mixed_mesh(3, (1, 1, 1))
+    x = mesh.coords
+    gamma = np.nonzero(np.any((np.abs(x) < 1e-12) | (np.abs(x - 1.0) < 1e-12), axis=1))[0]
+    dofs = (gamma + 1).astype(np.int32)
+    vals = [x[gamma, 0].copy(), np.zeros(len(gamma)), np.zeros(len(gamma))]
+    bc = [(dofs, vals[c]) for c in range(3)]
+    ph = np.ones(1, dtype=np.int32)
+    kw = dict(check_interval=1, max_iterations=1)
+    hs = oh.HostCellPressure(mesh, (1.0,), (1.0,), (0.0, 0.0, 0.0), ph)
+    with pytest.raises(fem._abi.FemB200Error, match="3-D Stokes solve did not converge"):
+        hs.solve(bc, **kw)
+    hs = oh.HostCellPressure(mesh, (1.0,), (1.0,), (0.0, 0.0, 0.0), ph)
+    st = hs.solve(bc, throw_on_failure=False, **kw)
+    assert not st.converged and st.reached_total_iter and st.err_P > 1e-5
+    for c in range(3):
+        assert (hs.v[c][gamma] == vals[c]).all()
+    v0 = [np.zeros(mesh.nnodes) for _ in range(3)]
+    for c in range(3):
+        v0[c][gamma] = vals[c]
+    hc = oh.HostCellPressure(mesh, (1.0,), (1.0,), (0.0, 0.0, 0.0), ph, v=v0)
+    stc = hc.solve(bc, throw_on_failure=False, **kw)
+    assert stc.err_P == pytest.approx(st.err_P, rel=1e-14)
+    np.testing.assert_allclose(hc.P, hs.P, rtol=1e-14, atol=1e-300)
+    for c in range(3):
+        np.testing.assert_allclose(hc.v[c], hs.v[c], rtol=1e-14, atol=1e-300)
