@@ -1,6 +1,7 @@
 """The oracle's lithostatic-pressure path (LithostaticPressureDR), pinned to the known
 answers of the reference's test/test_lithostatic_pressure.jl (element residual,
-parameters, stiffness term, EOS Jacobian, multi-phase density) and to the exact
+parameters, stiffness term, EOS Jacobian, multi-phase density, the finite incompressible
+limit) and to the exact
 hydrostatic solution P = ρ|g|(1 − height) that Q2 elements reproduce."""
 import math
 
@@ -64,3 +65,13 @@ def test_non_convergence_message():
     with pytest.raises(fem._abi.FemB200Error, match="Lithostatic pressure DR solver did not converge after 1 "):
         hs.solve((top, np.zeros(len(top))), Tref=0.0, g=(0.0, -1.0), tolerance=0.0, max_iterations=1,
                  check_interval=1)
+
+
+def test_incompressible_limit_stays_finite():
+    # test/test_lithostatic_pressure.jl:186-206: with a negative shape value, K = ∞ stays finite
+    # (1/K is interpolated) and a stiff finite K approaches it
+    N, P, g = [[-0.25, 1.25]], [1.0e6, 1.0e6], (0.0, -9.81)
+    inc, _, _ = oh.lithostatic_element(N, G1, [1.0], P, (300.0, 300.0), (1, 1), (2.0,), (0.1,), (math.inf,), 300.0, g)
+    assert np.isfinite(inc).all()
+    stiff, _, _ = oh.lithostatic_element(N, G1, [1.0], P, (300.0, 300.0), (1, 1), (2.0,), (0.1,), (1.0e30,), 300.0, g)
+    np.testing.assert_allclose(stiff, inc, rtol=1e-12)
