@@ -41,6 +41,9 @@ struct femb200_handle {
     size_t tmask_cap = 0;
     uint8_t* d_cpmask = nullptr;   // Dirichlet bits of the cell-pressure solve
     size_t cpmask_cap = 0;
+    // device address of the allocation-free solve's scratch array, looked up by the
+    // first femb200_solve_thermal_noalloc call on this handle
+    unsigned char* noalloc_base = nullptr;
     std::string err;
     bool tables_ready = false;
     // profiling: event pairs per kernel class, folded into totals when the pool fills
@@ -495,6 +498,11 @@ int build_mask(femb200_handle* h, const femb200_stokes_problem* p) {
 }
 
 inline double julia_eps(double x) { x = std::fabs(x); return std::nextafter(x, INFINITY) - x; }
+// max / min with Julia's semantics: NaN when either argument is NaN. std::max and
+// std::min return their first argument when a comparison with NaN fails, which would
+// hide a NaN residual from the reference's isnan / isfinite exits.
+inline double jl_max(double a, double b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::max(a, b); }
+inline double jl_min(double a, double b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::min(a, b); }
 
 void cheb(double dtau, double lmin, double c_fact, double& a, double& b) {
     const double c = 2 * std::sqrt(lmin) * c_fact;
@@ -724,16 +732,16 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
             double s;
             RC(sumsq<T>(h, static_cast<const T*>(p->Rv[k]), (const T*)nullptr, nn, s));
             comps[k] = std::sqrt(s) / (2 * sq_nn);
-            err_v = std::max(err_v, std::sqrt(s));
+            err_v = jl_max(err_v, std::sqrt(s));
         }
         err_v /= 2 * sq_nn;
         push_hist((double)iter, err_v, err_P, comps);
         if (itPH == 1) { err_P0 = err_P + julia_eps(err_P); err_v0 = err_v + julia_eps(err_v); }
         else if (itPH == 2) err_P0 = err_P + julia_eps(err_P);
         const double err_v_rel = err_v / err_v0, err_P_rel = err_P / err_P0;
-        err_abs = std::max(err_v, err_P);
-        err_rel = std::max(err_v_rel, err_P_rel);
-        err = std::min(err_abs, err_rel);
+        err_abs = jl_max(err_v, err_P);
+        err_rel = jl_max(err_v_rel, err_P_rel);
+        err = jl_min(err_abs, err_rel);
         if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_ENAN; }
         if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_EKABOOM; }
         if (err < eps && thermal_converged) { converged = true; break; }
@@ -777,10 +785,10 @@ int solve_dyrel(femb200_handle* h, const femb200_stokes_problem* p, const femb20
                 double s[RED_SLOTS];
                 RC(fetch_sums(h, nb, RED_SLOTS, s));
                 double ev = 0, cmp[3] = {0, 0, 0};
-                for (int k = 0; k < D; ++k) { ev = std::max(ev, std::sqrt(s[3 * k])); cmp[k] = std::sqrt(s[3 * k]) / (2 * sq_nn); }
+                for (int k = 0; k < D; ++k) { ev = jl_max(ev, std::sqrt(s[3 * k])); cmp[k] = std::sqrt(s[3 * k]) / (2 * sq_nn); }
                 ev /= 2 * sq_nn;
                 if (iter == nout) err_v00 = ev + julia_eps(ev);
-                err = ev <= eps ? ev : std::max(ev / err_v00, ev);
+                err = ev <= eps ? ev : jl_max(ev / err_v00, ev);
                 if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_ENAN; }
                 if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_EKABOOM; }
                 if (c->history) {
@@ -1082,15 +1090,15 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             double sv;
             RC(sumsq<T>(h, static_cast<const T*>(p->Rv[k]), (const T*)nullptr, nn, sv));
             comps[k] = std::sqrt(sv) / (2 * sq_nn);
-            err_v = std::max(err_v, std::sqrt(sv));
+            err_v = jl_max(err_v, std::sqrt(sv));
         }
         err_v /= 2 * sq_nn;
         push_hist((double)iter, err_v, err_P, comps);
         if (itPH == 1) { err_P0 = err_P + julia_eps(err_P); err_v0 = err_v + julia_eps(err_v); }
         else if (itPH == 2) err_P0 = err_P + julia_eps(err_P);
-        err_abs = std::max(err_v, err_P);
-        err_rel = std::max(err_v / err_v0, err_P / err_P0);
-        err = std::min(err_abs, err_rel);
+        err_abs = jl_max(err_v, err_P);
+        err_rel = jl_max(err_v / err_v0, err_P / err_P0);
+        err = jl_min(err_abs, err_rel);
         if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_ENAN; }
         if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in outer loop at PH=%lld", (long long)itPH); h->err = b; return FEMB200_EKABOOM; }
         if (err < eps) { converged = true; break; }
@@ -1127,10 +1135,10 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
                 double sr[RED_SLOTS];
                 RC(fetch_sums(h, nb, RED_SLOTS, sr));
                 double ev = 0, cmp[3] = {0, 0, 0};
-                for (int k = 0; k < D; ++k) { ev = std::max(ev, std::sqrt(sr[3 * k])); cmp[k] = std::sqrt(sr[3 * k]) / (2 * sq_nn); }
+                for (int k = 0; k < D; ++k) { ev = jl_max(ev, std::sqrt(sr[3 * k])); cmp[k] = std::sqrt(sr[3 * k]) / (2 * sq_nn); }
                 ev /= 2 * sq_nn;
                 if (iter == nout) err_v00 = ev + julia_eps(ev);
-                err = ev <= eps ? ev : std::max(ev / err_v00, ev);
+                err = ev <= eps ? ev : jl_max(ev / err_v00, ev);
                 if (std::isnan(err)) { char b[96]; std::snprintf(b, sizeof b, "NaN detected in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_ENAN; }
                 if (err > 1e10) { char b[96]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); h->err = b; return FEMB200_EKABOOM; }
                 if (c->history) {
@@ -1351,7 +1359,7 @@ int solve_adjoint_impl(femb200_handle* h, const femb200_stokes_problem* p, const
         for (int k = 0; k < 3; ++k) {
             double sv;
             RC(sumsq<T>(h, Res[k], (const T*)nullptr, nn, sv));
-            ev = std::max(ev, std::sqrt(sv));
+            ev = jl_max(ev, std::sqrt(sv));
         }
         ev /= sq_nn;
         return FEMB200_OK;
@@ -1374,10 +1382,10 @@ int solve_adjoint_impl(femb200_handle* h, const femb200_stokes_problem* p, const
         RC(velocity_error(err_v));
         RC(pressure_error(err_P));
         if (itPH == 1) { err_v0 = err_v + julia_eps(err_v); err_P0 = err_P + julia_eps(err_P); }
-        err = std::max(std::min(err_v, err_v / err_v0), std::min(err_P, err_P / err_P0));
+        err = jl_max(jl_min(err_v, err_v / err_v0), jl_min(err_P, err_P / err_P0));
         if (std::isnan(err)) { h->err = "NaN detected in the adjoint solve"; return FEMB200_ENAN; }
         if (err < tol) { converged = true; break; }
-        const double target_v = std::max(err_v * rel_drop, tol);
+        const double target_v = jl_max(err_v * rel_drop, tol);
         int64_t inner = 0;
         while (err_v > target_v && inner < iter_max && iter < total_max) {
             ++inner; ++iter;
@@ -1417,7 +1425,7 @@ int solve_adjoint_impl(femb200_handle* h, const femb200_stokes_problem* p, const
         RC(assemble());
         RC(velocity_error(err_v));
         RC(pressure_error(err_P));
-        err = std::max(std::min(err_v, err_v / err_v0), std::min(err_P, err_P / err_P0));
+        err = jl_max(jl_min(err_v, err_v / err_v0), jl_min(err_P, err_P / err_P0));
     }
     CK(cudaStreamSynchronize(s));
     st->itPH = itPH_done; st->iter = iter; st->err = err; st->err_v = err_v; st->err_P = err_P;
@@ -1989,12 +1997,12 @@ int femb200_solve_cell_pressure(femb200_handle* h, const femb200_cell_pressure_p
         for (int k = 0; k < 3; ++k) {
             double ss = 0;
             RC(sumsq<double>(h, p->Rv[k], nullptr, nn, ss));
-            err_v = std::max(err_v, std::sqrt(ss));
+            err_v = jl_max(err_v, std::sqrt(ss));
         }
         double sp = 0;
         RC(sumsq<double>(h, p->RP, nullptr, 4 * nels, sp));
         err_P = std::sqrt(sp);
-        err = std::max(err_v, err_P);
+        err = jl_max(err_v, err_P);
         if (!std::isfinite(err)) { h->err = "non-finite residual in 3-D Stokes solve"; return FEMB200_ENONFINITE; }
         if (c->history && hist < c->history_capacity) {
             c->history[3 * hist] = (double)it;
@@ -2243,8 +2251,6 @@ constexpr int NA_MAX_BLOCKS = 1024;
 constexpr size_t NA_PARTIALS = (size_t)NA_MAX_BLOCKS * RED_SLOTS;   // doubles
 constexpr size_t NA_RESULT = 16;                                     // doubles
 constexpr size_t NA_BYTES = (NA_PARTIALS + NA_RESULT) * sizeof(double) + (size_t)NA_MAX_NODES;
-constexpr int NA_MAX_DEVICES = 64;
-
 }  // namespace
 
 // Layout: [block partials | reduced slots | one mask byte per node]. In host code
@@ -2253,17 +2259,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
 namespace {
 
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_base[NA_MAX_DEVICES] = {};
-
 struct NoallocScratch {
     double* partials;
     double* result;
     uint8_t* mask;
 };
 
-// Device address of the scratch array on the handle's device, looked up once per
-// device (the first call on a device does it; it must not fall inside a capture).
+// Device address of the scratch array, looked up by the first call on a handle
+// (with the handle's device current; it must not fall inside a capture) and kept
+// in the handle. A handle made after cudaDeviceReset looks it up again, in the
+// reloaded module.
 int noalloc_scratch(femb200_handle* h, NoallocScratch& s) {
     int dev = -1;
     CK(cudaGetDevice(&dev));
@@ -2272,18 +2277,12 @@ int noalloc_scratch(femb200_handle* h, NoallocScratch& s) {
                  ") is not the handle's device (" + std::to_string(h->device) + ")";
         return FEMB200_EINVAL;
     }
-    if (dev < 0 || dev >= NA_MAX_DEVICES) { h->err = "femb200_solve_thermal_noalloc: device ordinal out of range"; return FEMB200_EINVAL; }
-    unsigned char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_base[dev]) {
-            void* p = nullptr;
-            CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-            g_noalloc_base[dev] = static_cast<unsigned char*>(p);
-        }
-        base = g_noalloc_base[dev];
+    if (!h->noalloc_base) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        h->noalloc_base = static_cast<unsigned char*>(p);
     }
-    s.partials = reinterpret_cast<double*>(base);
+    s.partials = reinterpret_cast<double*>(h->noalloc_base);
     s.result = s.partials + NA_PARTIALS;
     s.mask = reinterpret_cast<uint8_t*>(s.result + NA_RESULT);
     return FEMB200_OK;
@@ -2361,7 +2360,14 @@ int femb200_solve_thermal_noalloc(femb200_handle* h, const femb200_thermal_probl
     // the mask region keeps the previous call's bits: clear it before setting this call's
     CK(cudaMemsetAsync(s.mask, 0, (size_t)n, h->stream));
     if (t->bc_n > 0) CK(launch_build_mask(s.mask, t->bc_dofs, t->bc_n, 0, h->stream));
-    const int nbk = std::min(red_blocks(h, n), NA_MAX_BLOCKS);
+    // the block split of femb200_solve_thermal (4 per SM) must fit the scratch
+    // partials, or the sums would be ordered differently from that solve's
+    const int nbk = red_blocks(h, n);
+    if (nbk > NA_MAX_BLOCKS) {
+        h->err = "femb200_solve_thermal_noalloc: " + std::to_string(nbk) + " reduction blocks (4 per SM) exceed the " +
+                 std::to_string(NA_MAX_BLOCKS) + " the fixed scratch holds";
+        return FEMB200_EUNSUPPORTED;
+    }
     double a = 0, b = 0, nr0 = 0, last = NAN, lmax = 0;
     for (int64_t it = 1; it <= c->max_iterations; ++it) {
         const bool dj = (it % c->check_interval == 0) || it == 1;

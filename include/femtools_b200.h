@@ -657,9 +657,13 @@ int femb200_profile_read(femb200_handle* h, double* ms, int64_t* launches);
  * - Inputs, outputs and status are those of femb200_solve_thermal (FP64 only).
  * - t->nnodes above FEMB200_NOALLOC_MAX_NODES is rejected with FEMB200_EINVAL
  *   before any work is queued.
- * - The first call on a device looks up the scratch array's device address
- *   (cudaGetSymbolAddress, with that device current; it must be the handle's
- *   device). Make that first call before any stream capture begins.
+ * - The first call on a handle looks up the scratch array's device address
+ *   (cudaGetSymbolAddress, with the handle's device current) and keeps it in the
+ *   handle. Make that first call before any stream capture begins. After
+ *   cudaDeviceReset, create new handles: the array may then sit elsewhere.
+ * - The reductions use femb200_solve_thermal's split of 4 blocks per SM; a GPU
+ *   with more than 256 SMs is rejected with FEMB200_EUNSUPPORTED, since that
+ *   split no longer fits the fixed scratch.
  * - Every call, on every stream and handle of the process, shares the one array,
  *   and the array keeps the last call's contents; each call clears the part that
  *   must start at zero. Calls that overlap on the GPU (other streams, other host
