@@ -1,8 +1,8 @@
 """Writes cap_justrelax.json: the pinned JustRelax tensile-cap return-map rows of the
 reference's test/test_drucker_prager_cap.jl ("Pinned JustRelax cap fixtures"), read from
-that file's text. Run where the reference checkout is present:
+that file's text. Run where a FEMTools.jl checkout is present, naming its root:
 
-    python tests/golden/make_cap_fixtures.py [path/to/FEMTools.jl]
+    python tests/golden/make_cap_fixtures.py path/to/FEMTools.jl
 
 Each row: (ψ in degrees, η_reg, s_trial, p_trial, τII, P, λ, θdot) for C = η = G = Δt = 1,
 K = 4, ϕ = 30°, pT = −0.5 and ηve = 0.5 (the reference calls
@@ -34,4 +34,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_cap_fixtures.py path/to/FEMTools.jl")
+    main(sys.argv[1])
