@@ -28,6 +28,11 @@ thread_local std::string g_last_error;
 inline const double* D(const void* p) { return static_cast<const double*>(p); }
 // Julia's eps(x): the spacing of floats at |x|.
 inline double julia_eps(double x) { x = std::fabs(x); return std::nextafter(x, INFINITY) - x; }
+// max / min with Julia's semantics: NaN when either argument is NaN. std::max and
+// std::min return their first argument when a comparison with NaN fails, which would
+// hide a NaN residual from the reference's isnan / isfinite exits.
+inline double jl_max(double a, double b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::max(a, b); }
+inline double jl_min(double a, double b) { return (std::isnan(a) || std::isnan(b)) ? NAN : std::min(a, b); }
 inline double* Dm(void* p) { return static_cast<double*>(p); }
 
 // _phase_at (src/utils.jl:70-72): returns a 0-based phase index.
@@ -371,15 +376,17 @@ void momentum_residual_impl(const femb200_stokes_problem* p, double dt, bool wit
 }
 
 // Augmented Jacobian diagnostics (momentum_residuals.jl:929-970, 1044-1117).
+// Elements [e0, e1) only when a range is given (the timed CPU sample assembles the
+// full-size arrays one block of elements at a time).
 template <int NVT>
-void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K) {
+void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K, int64_t e0, int64_t e1) {
     using DU = Dual<NVT>;
     const Tables& t = tables_for(p->dim);
     const int NV = t.nv, DD = p->dim;
-    std::vector<double> buf((size_t)p->nels * NV * DD * 2);
+    std::vector<double> buf((size_t)(e1 - e0) * NV * DD * 2);
     const double* bulk = bulk_table(p, finite_K);
 #pragma omp parallel for schedule(dynamic, 16)
-    for (int64_t e = 0; e < p->nels; ++e) {
+    for (int64_t e = e0; e < e1; ++e) {
         Elem el; gather(p, e, el);
         // The diagnostics read dr.P0 for the pressure storage term (DR.jl:468).
         el.P0_ip = false;
@@ -415,7 +422,7 @@ void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K) {
                     if (i == j) diag[i][a] = std::fabs(R[i][a].d[a]);
                 }
         }
-        double* o = &buf[(size_t)e * NV * DD * 2];
+        double* o = &buf[(size_t)(e - e0) * NV * DD * 2];
         for (int i = 0; i < DD; ++i)
             for (int a = 0; a < NV; ++a) { o[(i * NV + a) * 2] = rows[i][a]; o[(i * NV + a) * 2 + 1] = diag[i][a]; }
     }
@@ -423,8 +430,8 @@ void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K) {
         std::fill(Dm(p->dRdv[c]), Dm(p->dRdv[c]) + p->nnodes, 0.0);
         std::fill(Dm(p->PC[c]), Dm(p->PC[c]) + p->nnodes, 0.0);
     }
-    for (int64_t e = 0; e < p->nels; ++e) {
-        const double* o = &buf[(size_t)e * NV * DD * 2];
+    for (int64_t e = e0; e < e1; ++e) {
+        const double* o = &buf[(size_t)(e - e0) * NV * DD * 2];
         for (int i = 0; i < DD; ++i)
             for (int a = 0; a < NV; ++a) {
                 int64_t n = p->el2n[(int64_t)NV * e + a] - 1;
@@ -434,9 +441,10 @@ void jacobian_impl_t(const femb200_stokes_problem* p, double dt, int finite_K) {
     }
 }
 
-void jacobian_impl(const femb200_stokes_problem* p, double dt, int finite_K) {
-    if (p->dim == 3) jacobian_impl_t<27>(p, dt, finite_K);
-    else jacobian_impl_t<9>(p, dt, finite_K);
+void jacobian_impl(const femb200_stokes_problem* p, double dt, int finite_K, int64_t e0 = 0, int64_t e1 = -1) {
+    if (e1 < 0) e1 = p->nels;
+    if (p->dim == 3) jacobian_impl_t<27>(p, dt, finite_K, e0, e1);
+    else jacobian_impl_t<9>(p, dt, finite_K, e0, e1);
 }
 
 // ---- adjoint checks -----------------------------------------------------------
@@ -859,6 +867,40 @@ struct Coupled {
     double* phi;   // nq × nels or null
 };
 
+// The Stokes part of one inner DR iteration (DR.jl:664-698): pressure residual,
+// Pnum = γP·RP/M_P, momentum residual with Pnum, the Dirichlet pins of Rv and of the
+// rate, the negated Chebyshev velocity update (helpers.jl:31-41) and the pins of v.
+void stokes_inner_step(const femb200_stokes_problem* p, double dt, int finite_K, const double alpha[3],
+                       const double beta[3]) {
+    const int DD = p->dim;
+    const int64_t nn = p->nnodes, nP = p->nnodesP;
+    pressure_residual_impl(p, dt, finite_K);
+    for (int64_t i = 0; i < nP; ++i) Dm(p->Pnum)[i] = D(p->gammaP)[i] * D(p->RP)[i] / D(p->M_P)[i];
+    momentum_residual_impl(p, dt, true);
+    for (int k = 0; k < DD; ++k) {
+        if (p->body_force[k]) for (int64_t i = 0; i < nn; ++i) Dm(p->Rv[k])[i] -= D(p->body_force[k])[i];
+        dirichlet(Dm(p->Rv[k]), p->bc_dofs[k], nullptr, p->bc_n[k]);
+    }
+    for (int k = 0; k < DD; ++k) dirichlet(Dm(p->rate[k]), p->bc_dofs[k], nullptr, p->bc_n[k]);
+    for (int k = 0; k < DD; ++k) {
+        double* r = Dm(p->rate[k]); double* v = Dm(p->v[k]);
+        const double* R = D(p->Rv[k]); const double* PC = D(p->PC[k]);
+        double na = -alpha[k];
+        for (int64_t i = 0; i < nn; ++i) { double nr = beta[k] * r[i] + R[i] / PC[i]; r[i] = nr; v[i] += na * nr; }
+    }
+    for (int k = 0; k < DD; ++k) dirichlet(Dm(p->v[k]), p->bc_dofs[k], D(p->bc_vals[k]), p->bc_n[k]);
+}
+
+// The velocity error and the per-component λmin of a check (DR.jl:700-726).
+double stokes_check_norms(const femb200_stokes_problem* p, const double alpha[3], double lmin[3]) {
+    const int DD = p->dim;
+    const int64_t nn = p->nnodes;
+    double ev = 0; for (int k = 0; k < DD; ++k) ev = jl_max(ev, norm2(D(p->Rv[k]), nn));
+    ev /= 2 * std::sqrt((double)nn);
+    for (int k = 0; k < DD; ++k) lmin[k] = stokes_lmin(alpha[k], D(p->rate[k]), D(p->Rv[k]), D(p->Rv0[k]), D(p->PC[k]), nn);
+    return ev;
+}
+
 // _solve_stokes_dyrel! (src/stokes/solvers/DR.jl:348-802).
 int solve_dyrel(const femb200_stokes_problem* p, const femb200_stokes_controls* c, femb200_stokes_stats* st,
                 Coupled* cp) {
@@ -928,15 +970,15 @@ int solve_dyrel(const femb200_stokes_problem* p, const femb200_stokes_controls* 
             double s = 0; for (int64_t i = 0; i < nP; ++i) { double r = D(p->RP)[i] / D(p->M_P)[i]; s += r * r; }
             err_P = std::sqrt(s) / std::sqrt((double)nP);
         }
-        err_v = 0; for (int k = 0; k < DD; ++k) err_v = std::max(err_v, norm2(D(p->Rv[k]), nn));
+        err_v = 0; for (int k = 0; k < DD; ++k) err_v = jl_max(err_v, norm2(D(p->Rv[k]), nn));
         err_v /= 2 * std::sqrt((double)nn);
         push_hist((double)iter, err_v, err_P);
         if (itPH == 1) { err_P0 = err_P + julia_eps(err_P); err_v0 = err_v + julia_eps(err_v); }
         else if (itPH == 2) { err_P0 = err_P + julia_eps(err_P); }
         double err_v_rel = err_v / err_v0, err_P_rel = err_P / err_P0;
-        err_abs = std::max(err_v, err_P);
-        err_rel = std::max(err_v_rel, err_P_rel);
-        err = std::min(err_abs, err_rel);
+        err_abs = jl_max(err_v, err_P);
+        err_rel = jl_max(err_v_rel, err_P_rel);
+        err = jl_min(err_abs, err_rel);
         if (std::isnan(err)) { char b[128]; std::snprintf(b, sizeof b, "NaN detected in outer loop at PH=%lld", (long long)itPH); g_last_error = b; return FEMB200_ENAN; }
         if (err > 1e10) { char b[128]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in outer loop at PH=%lld", (long long)itPH); g_last_error = b; return FEMB200_EKABOOM; }
         if (err < eps && thermal_converged) { converged = true; break; }
@@ -980,35 +1022,19 @@ int solve_dyrel(const femb200_stokes_problem* p, const femb200_stokes_controls* 
                     shear_heat();
                 }
             }
-            pressure_residual_impl(p, dt, finite_K);
-            for (int64_t i = 0; i < nP; ++i) Dm(p->Pnum)[i] = D(p->gammaP)[i] * D(p->RP)[i] / D(p->M_P)[i];
-            momentum_residual_impl(p, dt, true);
-            for (int k = 0; k < DD; ++k) {
-                if (p->body_force[k]) for (int64_t i = 0; i < nn; ++i) Dm(p->Rv[k])[i] -= D(p->body_force[k])[i];
-                dirichlet(Dm(p->Rv[k]), p->bc_dofs[k], nullptr, p->bc_n[k]);
-            }
-            for (int k = 0; k < DD; ++k) dirichlet(Dm(p->rate[k]), p->bc_dofs[k], nullptr, p->bc_n[k]);
             // update_stokes_velocity! with the negated Chebyshev step (DR.jl:692-695, helpers.jl:31-41)
-            for (int k = 0; k < DD; ++k) {
-                double* r = Dm(p->rate[k]); double* v = Dm(p->v[k]);
-                const double* R = D(p->Rv[k]); const double* PC = D(p->PC[k]);
-                double na = -alpha[k];
-                for (int64_t i = 0; i < nn; ++i) { double nr = beta[k] * r[i] + R[i] / PC[i]; r[i] = nr; v[i] += na * nr; }
-            }
-            for (int k = 0; k < DD; ++k) dirichlet(Dm(p->v[k]), p->bc_dofs[k], D(p->bc_vals[k]), p->bc_n[k]);
+            stokes_inner_step(p, dt, finite_K, alpha, beta);
             if (do_check) {
-                double ev = 0; for (int k = 0; k < DD; ++k) ev = std::max(ev, norm2(D(p->Rv[k]), nn));
-                ev /= 2 * std::sqrt((double)nn);
+                double lmin[3];
+                const double ev = stokes_check_norms(p, alpha, lmin);
                 if (iter == nout) err_v00 = ev + julia_eps(ev);
-                err = ev <= eps ? ev : std::max(ev / err_v00, ev);
+                err = ev <= eps ? ev : jl_max(ev / err_v00, ev);
                 if (std::isnan(err)) { char b[128]; std::snprintf(b, sizeof b, "NaN detected in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); g_last_error = b; return FEMB200_ENAN; }
                 if (err > 1e10) { char b[128]; std::snprintf(b, sizeof b, "Kaboom! Error > 1e10 in inner loop PH=%lld PT=%lld", (long long)itPH, (long long)itPT); g_last_error = b; return FEMB200_EKABOOM; }
                 {
                     double s = 0; for (int64_t i = 0; i < nP; ++i) { double r = D(p->RP)[i] / D(p->M_P)[i]; s += r * r; }
                     push_hist((double)iter, ev, std::sqrt(s) / std::sqrt((double)nP));
                 }
-                double lmin[3];
-                for (int k = 0; k < DD; ++k) lmin[k] = stokes_lmin(alpha[k], D(p->rate[k]), D(p->Rv[k]), D(p->Rv0[k]), D(p->PC[k]), nn);
                 if (!freeze) {
                     ++jac_assemblies;
                     jacobian_impl(&pj, dt, finite_K);
@@ -1313,12 +1339,12 @@ int cp_solve_impl(const femb200_cell_pressure_problem* p, const femb200_cell_pre
         for (int k = 0; k < 3; ++k) {
             double ss = 0;
             for (int64_t i = 0; i < p->nnodes; ++i) ss += p->Rv[k][i] * p->Rv[k][i];
-            err_v = std::max(err_v, std::sqrt(ss));
+            err_v = jl_max(err_v, std::sqrt(ss));
         }
         double sp = 0;
         for (int64_t i = 0; i < 4 * p->nels; ++i) sp += p->RP[i] * p->RP[i];
         err_P = std::sqrt(sp);
-        err = std::max(err_v, err_P);
+        err = jl_max(err_v, err_P);
         if (!std::isfinite(err)) { g_last_error = "non-finite residual in 3-D Stokes solve"; return FEMB200_ENONFINITE; }
         if (c->history && hist < c->history_capacity) {
             c->history[3 * hist] = (double)it; c->history[3 * hist + 1] = err_v; c->history[3 * hist + 2] = err_P;
@@ -1519,6 +1545,35 @@ int orc_store_stress(const femb200_stokes_problem* p, double dt) {
 
 int orc_solve_stokes(const femb200_stokes_problem* p, const femb200_stokes_controls* c, femb200_stokes_stats* st) {
     return solve_stokes_impl(p, c, st, nullptr);
+}
+
+// Timed CPU sample of the solve: `iterations` inner DR iterations exactly as the
+// solve runs them (stokes_inner_step, with the given Chebyshev steps and the
+// preconditioner already in p->PC), then, when `check` is set, one check's work
+// without its Jacobian assembly: Rv → Rv0 before the last iteration, the velocity
+// error and λmin. Returns the velocity error of the check (0 without one) in *err_v.
+int orc_dr_iterations(const femb200_stokes_problem* p, double dt, int32_t finite_K, const double* alpha,
+                      const double* beta, int64_t iterations, int32_t check, double* err_v) {
+    int rc = check_problem(p); if (rc) return rc;
+    double ev = 0;
+    for (int64_t it = 1; it <= iterations; ++it) {
+        const bool last_check = check && it == iterations;
+        if (last_check)
+            for (int k = 0; k < p->dim; ++k) std::copy(D(p->Rv[k]), D(p->Rv[k]) + p->nnodes, Dm(p->Rv0[k]));
+        stokes_inner_step(p, dt, finite_K, alpha, beta);
+        if (last_check) { double lmin[3]; ev = stokes_check_norms(p, alpha, lmin); }
+    }
+    if (err_v) *err_v = ev;
+    return 0;
+}
+
+// The Jacobian diagnostics assembled from elements [e0, e1) into the full-size
+// dRdv / PC arrays (zeroed first), the assembly of the solve restricted to a block.
+int orc_jacobian_range(const femb200_stokes_problem* p, double dt, int32_t finite_K, int64_t e0, int64_t e1) {
+    int rc = check_problem(p); if (rc) return rc;
+    if (e0 < 0 || e1 > p->nels || e0 > e1) { g_last_error = "element range outside 0:nels"; return FEMB200_EINVAL; }
+    jacobian_impl(p, dt, finite_K, e0, e1);
+    return 0;
 }
 
 int orc_thermal_residual(const femb200_thermal_problem* t, double dt, double Tref, int32_t jac) {

@@ -56,6 +56,9 @@ def lib():
             "orc_pressure_scaling": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_double, C.c_int32]),
             "orc_store_stress": (C.c_int, [_P(abi.StokesProblemC), C.c_double]),
             "orc_solve_stokes": (C.c_int, [_P(abi.StokesProblemC), _P(abi.StokesControlsC), _P(abi.StokesStatsC)]),
+            "orc_dr_iterations": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, _vp, _vp, C.c_int64,
+                                            C.c_int32, _vp]),
+            "orc_jacobian_range": (C.c_int, [_P(abi.StokesProblemC), C.c_double, C.c_int32, C.c_int64, C.c_int64]),
             "orc_thermal_residual": (C.c_int, [_P(abi.ThermalProblemC), C.c_double, C.c_double, C.c_int32]),
             "orc_solve_thermal": (C.c_int, [_P(abi.ThermalProblemC), _P(abi.ThermalControlsC), _P(abi.ThermalStatsC)]),
             "orc_transfer_temperature": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64]),
@@ -171,6 +174,21 @@ class HostStokes:
 
     def jacobian_diagnostics(self, dt, finite_K=False):
         check(lib().orc_jacobian_diagnostics(C.byref(self.struct()), dt, int(finite_K)))
+
+    def jacobian_range(self, dt, e0, e1, finite_K=False):
+        """The Jacobian diagnostics of elements [e0, e1) into the full-size arrays."""
+        check(lib().orc_jacobian_range(C.byref(self.struct()), dt, int(finite_K), int(e0), int(e1)))
+
+    def dr_iterations(self, dt, alpha, beta, iterations, check_norms=False, finite_K=False):
+        """`iterations` inner DR iterations of the solve's loop with fixed Chebyshev steps
+        (the preconditioner already in PC), plus one check's norms and λmin when asked;
+        returns the check's velocity error."""
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        ev = C.c_double(0.0)
+        check(lib().orc_dr_iterations(C.byref(self.struct()), dt, int(finite_K), ptr(a), ptr(b), int(iterations),
+                                      int(check_norms), C.byref(ev)))
+        return ev.value
 
     def store_stress(self, dt):
         check(lib().orc_store_stress(C.byref(self.struct()), dt))

@@ -164,3 +164,18 @@ def test_adjoint_and_material_gradients_match_the_sparse_system():
         assert abs(grads["viscosity_gradient"][p] - fd_eta) <= 1e-4 * max(abs(fd_eta), 1e-12)
     # the forward state is untouched by the adjoint solve
     assert np.allclose(host(dr.v[2]), x[:nv].reshape(-1, 3)[:, 2], atol=1e-6 * np.abs(x[:nv]).max())
+
+
+def test_nan_velocity_raises_the_non_finite_exit():
+    # src/stokes/solvers/DR.jl:1041-1044: max(maximum(norm, Rv), norm(RP)) carries a NaN
+    # into isfinite(err); the oracle stops with the same message
+    case, dr, hs = states(n=2, seed=1, random=False)
+    node = int(np.setdiff1d(np.arange(1, case.mesh.nnodes + 1), case.mesh.boundary_nodes)[0]) - 1
+    dr.v[1][node] = float("nan")
+    hs.v[1][node] = np.nan
+    with pytest.raises(abi.FemB200Error) as ref:
+        hs.solve(case.bc, tolerance=1e-8, max_iterations=1000, check_interval=100)
+    with pytest.raises(abi.FemB200Error) as got:
+        fem.solve_cell_pressure(dr, case.bc, tolerance=1e-8, max_iterations=1000, check_interval=100)
+    assert got.value.code == ref.value.code == abi.ENONFINITE
+    assert str(got.value) == str(ref.value) == "non-finite residual in 3-D Stokes solve"

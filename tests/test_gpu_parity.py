@@ -304,3 +304,46 @@ def test_colored_thermal_assembly_matches_atomic(dim):
     for got, ref, host, what in zip((th.R, th.dRdT, th.PC), atomic, (ht.R, ht.dRdT, ht.PC), ("R", "∂R∂T", "PC")):
         close(got, ref.cpu().numpy(), rtol=1e-12, atol_rel=1e-14, what=what + " colored vs atomic")
         close(got, host, rtol=1e-9, what=what + " colored vs oracle")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("where", ["tau_old", "vy"])
+def test_nan_input_raises_the_reference_nan_exit(precision, where):
+    # src/stokes/solvers/DR.jl:570-575: Julia's max / min carry a NaN residual into
+    # isnan(err); a NaN in one velocity component or one stress-history point must not
+    # be hidden by the max over components. The oracle raises the same message.
+    case = vep_layers_case(n=2, seed=0)
+    dr, hs = case.device_state(fem), case.host_state(oh)
+    if where == "tau_old":
+        dr.tau_old[0][5] = float("nan")
+        hs.tau_old[0][5] = np.nan
+    else:
+        interior = np.setdiff1d(np.arange(1, case.mesh.nnodes + 1), case.mesh.boundary_nodes)
+        dr.v[1][int(interior[0]) - 1] = float("nan")
+        hs.v[1][interior[0] - 1] = np.nan
+    kw = dict(dt=case.dt, tolerance=1e-8, check_interval=50, throw_on_failure=False)
+    with pytest.raises(abi.FemB200Error) as ref:
+        hs.solve(**kw)
+    with pytest.raises(abi.FemB200Error) as got:
+        fem.solve(dr, case.bc_device(), precision=precision, **kw)
+    assert got.value.code == ref.value.code == abi.ENAN
+    assert str(got.value) == str(ref.value) == "NaN detected in outer loop at PH=1"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_unstable_pseudo_time_step_raises_kaboom(precision):
+    # DR.jl:711-712: a CFL far above the stability limit grows the velocity error past
+    # 1e10 by the first check; the oracle stops at the same check with the same message.
+    case = vep_layers_case(n=2, seed=0)
+    dr, hs = case.device_state(fem), case.host_state(oh)
+    kw = dict(dt=case.dt, tolerance=1e-8, check_interval=50, throw_on_failure=False, cfl_v=4.0)
+    with pytest.raises(abi.FemB200Error) as ref:
+        hs.solve(**kw)
+    with pytest.raises(abi.FemB200Error) as got:
+        fem.solve(dr, case.bc_device(), precision=precision, **kw)
+    assert got.value.code == ref.value.code == abi.EKABOOM
+    assert str(ref.value) == "Kaboom! Error > 1e10 in inner loop PH=1 PT=50"
+    if precision == "fp64":
+        assert str(got.value) == str(ref.value)
+    else:
+        assert str(got.value).startswith("Kaboom! Error > 1e10 in inner loop PH=1 PT=")
