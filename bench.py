@@ -29,6 +29,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "time-to-1e-8 residual, 3D Q2 Stokes 64³: chosen vs plain FP64 DR; HBM GB/s"
 
+# DR path of the 64³ solve of this workload, measured by this file's plain FP64 arm on
+# a B200: the CPU reference time is extrapolated along it (the oracle and the device
+# take the same path: equal iteration counts at 32³, `--mode parity`).
+PATH_64 = {"iterations": 12300, "itPH": 89, "jacobian_assemblies": 124, "check_interval": 100}
+# DRAM bytes read + written by one launch of the chosen method's hot kernel at 64³,
+# from the ncu capture summarised in profiles/hex27_incr_kernel_vep64.md.
+TRAFFIC = {(64, "mixed"): 299135488}
+
 
 def load_package():
     import importlib.util
@@ -177,35 +185,89 @@ def max_over_ranks(x, world, device="cuda"):
     return t.item()
 
 
-def cpu_baseline_estimate(case, iterations, jac_assemblies, threads=None):
-    """Time-to-solution of the CPU restatement of the reference (the oracle), from a
-    bounded sample: two fused residual sweeps on the full mesh, one Jacobian-diagnostics
-    assembly on an 8³ sub-mesh scaled by the element ratio, extrapolated with the GPU
-    run's iteration and assembly counts (both implementations take the same path)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_host as oh
-    from cases import vep_layers_case
-    L = oh.lib()
-    if threads:
-        L.orc_set_num_threads(threads)
-    cores = L.orc_num_threads()
-    hs = case.host_state(oh)
-    hs.pressure_scaling(50.0, case.dt)
-    t0 = time.perf_counter()
-    hs.stokes_residuals(case.dt)
-    hs.stokes_residuals(case.dt)
-    t_res = (time.perf_counter() - t0) / 2
-    small = vep_layers_case(n=8, seed=0)
-    hsm = small.host_state(oh)
-    hsm.pressure_scaling(50.0, small.dt)
-    t0 = time.perf_counter()
-    hsm.jacobian_diagnostics(small.dt)
-    t_jac = (time.perf_counter() - t0) * case.mesh.nels / small.mesh.nels
-    est = iterations * t_res + jac_assemblies * t_jac
-    sample = (f"2 fused residual sweeps at {case.mesh.nel} ({t_res:.3f} s each) + Jacobian diagnostics on "
-              f"8³ scaled ×{case.mesh.nels // small.mesh.nels} ({t_jac:.2f} s per assembly), extrapolated to "
-              f"{iterations} iterations and {jac_assemblies} assemblies")
-    return est, cores, sample
+def cpu_model():
+    """The host CPU's model name (first /proc/cpuinfo entry) and logical core count."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return name, os.cpu_count()
+
+
+class CpuSample:
+    """Timed sample of the CPU restatement of the reference (the oracle, OpenMP on all
+    host cores) on one workload, for extrapolating its time to solution.
+
+    Setup (untimed): the host state, M_P/γP and one full Jacobian assembly (the
+    preconditioner of the iterations and their Chebyshev steps). One `step()` then
+    times, on the full mesh, `block` whole inner DR iterations of the solve's own loop
+    (pressure residual, Pnum, momentum residual, Dirichlet pins, velocity update), one
+    more iteration with a check's work (Rv → Rv0, velocity error, λmin; no Jacobian)
+    and the Jacobian assembly of one of `parts` equal blocks of the elements into the
+    full-size arrays; successive steps take the blocks in turn. `estimate()` prices a
+    solve's path with the step's figures:
+    iterations·t_iter + checks·t_check + assemblies·parts·t_part + itPH·t_iter."""
+
+    def __init__(self, case, block=8, parts=8, threads=None):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_host as oh
+        L = oh.lib()
+        if threads:
+            L.orc_set_num_threads(threads)
+        self.cores = L.orc_num_threads()
+        self.case, self.block, self.parts = case, block, parts
+        self.hs = case.host_state(oh)
+        self.hs.pressure_scaling(50.0, case.dt)
+        self.hs.jacobian_diagnostics(case.dt)
+        lmax = [float(np.max(self.hs.dRdv[c] / self.hs.PC[c])) for c in range(case.mesh.dim)]
+        dtau = [2.0 / math.sqrt(x) * 0.98 for x in lmax]
+        self.alpha = [d * d for d in dtau]      # Chebyshev step with λmin = 0 (c = 0)
+        self.beta = [1.0] * case.mesh.dim
+        self.v0 = [x.copy() for x in self.hs.v]
+        self.k = 0
+
+    def step(self):
+        hs, dt, m = self.hs, self.case.dt, self.case.mesh
+        for c in range(m.dim):          # every step samples the same state
+            hs.v[c][:] = self.v0[c]
+            hs.rate[c][:] = 0.0
+        t0 = time.perf_counter()
+        hs.dr_iterations(dt, self.alpha, self.beta, self.block)
+        t1 = time.perf_counter()
+        hs.dr_iterations(dt, self.alpha, self.beta, 1, check_norms=True)
+        t2 = time.perf_counter()
+        e0 = m.nels * (self.k % self.parts) // self.parts
+        e1 = m.nels * (self.k % self.parts + 1) // self.parts
+        hs.jacobian_range(dt, e0, e1)
+        t3 = time.perf_counter()
+        self.k += 1
+        t_iter = (t1 - t0) / self.block
+        return {"t_iter": t_iter, "t_check": max(t2 - t1 - t_iter, 0.0), "t_jacobian": (t3 - t2) * self.parts,
+                "sampled_s": t3 - t0}
+
+    @staticmethod
+    def estimate(fig, path):
+        checks = path["iterations"] // path["check_interval"]
+        return (path["iterations"] * fig["t_iter"] + checks * fig["t_check"]
+                + path["jacobian_assemblies"] * fig["t_jacobian"] + path["itPH"] * fig["t_iter"])
+
+    def describe(self, fig):
+        return (f"oracle (C++ FP64 restatement of the reference CPU path, {self.cores} threads) on the full "
+                f"{self.case.mesh.nel} mesh: {self.block} whole DR iterations ({fig['t_iter']:.3f} s each), one "
+                f"check ({fig['t_check']:.3f} s) and 1/{self.parts} of a Jacobian assembly "
+                f"({fig['t_jacobian']:.2f} s per full assembly) per step")
+
+
+def cpu_baseline_estimate(case, path, steps=1, threads=None):
+    """Time to solution of the oracle along `path`, from `steps` CpuSample steps."""
+    smp = CpuSample(case, threads=threads)
+    figs = [smp.step() for _ in range(steps)]
+    fig = {k: statistics.mean(f[k] for f in figs) for k in figs[0]}
+    return CpuSample.estimate(fig, path), smp.cores, smp.describe(fig) + f", extrapolated along {path}"
 
 
 def sweep_mode(args, fem, case, dr, lib, h):
@@ -623,25 +685,190 @@ def timeloop_mode(args, fem):
     return 0
 
 
+def _rel(a, b):
+    """Relative L2 difference ‖a − b‖ / ‖b‖ of two numpy arrays."""
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+def _mean_free(P, M):
+    """P without its M_P-weighted mean (pressure is compared up to a constant)."""
+    return P - float(np.sum(P * M) / np.sum(M))
+
+
+def parity_mode(args, fem):
+    """Parity at the configurations' own sizes, against the FP64 oracle on all host cores.
+
+    3-D (the layered visco-elasto-plastic case, --n, `--tl-steps` time steps with
+    P0 ← P and τ_old ← τ): the device FP64 solve, the device mixed-precision solve and
+    the oracle's solve, each from the same state to min(err_abs, err_rel) < tol
+    (src/stokes/solvers/DR.jl:568-586); reported per step: iteration counts, relative
+    L2 errors of v, P (also without its M_P-weighted mean) and τ against the oracle,
+    and the wall times. The oracle's measured time is compared with the CpuSample
+    extrapolation along the oracle's own path (the model the 64³ reference figure uses).
+    2-D (the inclusion case at --n2d, FP64): the device solve against the oracle's.
+    Prints one JSON line."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    out = {"mode": "parity", "tolerance": args.tolerance, "check_interval": args.check_interval}
+    name, nproc = cpu_model()
+    out["host"] = {"cpu_model": name, "nproc": nproc, "oracle_threads": oh.lib().orc_num_threads()}
+    stream = torch.cuda.current_stream()
+
+    def gpu_solve(dr, bc, **kw):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        st = fem.solve(dr, bc, **kw)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return st, ev0.elapsed_time(ev1) / 1e3
+
+    keys = ("iter", "itPH", "jacobian_assemblies", "converged", "err")
+    if args.n > 0:
+        case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
+        bc = case.bc_device()
+        d64, dmx, hs = case.device_state(), case.device_state(), case.host_state(oh)
+        kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
+                  max_iterations=args.max_iterations, iter_max=args.max_iterations)
+        # warm-up of the device code paths on a copy, so the timed solves carry no first-launch costs
+        warm = case.device_state()
+        fem.solve(warm, bc, **dict(kw, max_iterations=200, iter_max=200))
+        fem.solve(warm, bc, **dict(kw, max_iterations=200, iter_max=200, precision="mixed"))
+        del warm
+        steps = []
+        for step in range(args.tl_steps):
+            s64, t64 = gpu_solve(d64, bc, **kw)
+            smx, tmx = gpu_solve(dmx, bc, precision="mixed", **kw)
+            t0 = time.perf_counter()
+            sor = hs.solve(**kw)
+            tor = time.perf_counter() - t0
+            fem.update_stokes_current_stress(d64, case.dt)
+            fem.update_stokes_current_stress(dmx, case.dt)
+            hs.store_stress(case.dt)
+            torch.cuda.synchronize()
+            host = lambda dr: {"v": np.concatenate([x.cpu().numpy() for x in dr.v]), "P": dr.P.cpu().numpy(),
+                               "tau": np.concatenate([x.cpu().numpy() for x in dr.tau])}
+            ref = {"v": np.concatenate(hs.v), "P": hs.P.copy(), "tau": np.concatenate(hs.tau)}
+            row = {"step": step + 1, "oracle": {k: sor[k] for k in keys}, "oracle_s": tor}
+            for label, dr, st, t in (("gpu_fp64", d64, s64, t64), ("gpu_mixed", dmx, smx, tmx)):
+                f = host(dr)
+                row[label] = {k: st[k] for k in keys}
+                row[label]["seconds"] = t
+                row[label]["rel_err_vs_oracle"] = {
+                    "v": _rel(f["v"], ref["v"]), "P": _rel(f["P"], ref["P"]),
+                    "P_mean_free": _rel(_mean_free(f["P"], hs.M_P), _mean_free(ref["P"], hs.M_P)),
+                    "tau": _rel(f["tau"], ref["tau"])}
+            steps.append(row)
+            print(json.dumps({"parity_step": row}), flush=True)
+            # the time-step driver: P0 ← P, τ_old ← τ on all three
+            for dr in (d64, dmx):
+                dr.P0.copy_(dr.P)
+                for c in range(6):
+                    dr.tau_old[c].copy_(dr.tau[c])
+            hs.P0[:] = hs.P
+            for c in range(6):
+                hs.tau_old[c][:] = hs.tau[c]
+        first = steps[0]["oracle"]
+        path = {"iterations": first["iter"], "itPH": first["itPH"], "jacobian_assemblies": first["jacobian_assemblies"],
+                "check_interval": args.check_interval}
+        # the extrapolation model on the same workload, priced along the oracle's own path of step 1
+        est, cores, sample = cpu_baseline_estimate(fem.configs.vep_layers_case(n=args.n, seed=args.seed), path, steps=3)
+        out["vep3d"] = {"workload": f"vep-layers-hex27-{args.n}^3 x {args.tl_steps} steps", "steps": steps,
+                        "cpu_model_check": {"measured_s": steps[0]["oracle_s"], "extrapolated_s": est,
+                                            "model_error": est / steps[0]["oracle_s"] - 1.0, "sample": sample}}
+    if args.n2d > 0:
+        case = fem.configs.inclusion_2d_case(n=args.n2d)
+        kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=50, throw_on_failure=False,
+                  max_iterations=args.max_iterations, iter_max=args.max_iterations)
+        ref = inclusion_oracle(args, case, oh, kw)
+        dr = case.device_state()
+        st, tg = gpu_solve(dr, case.bc_device(), **kw)
+        f = {"v": np.concatenate([x.cpu().numpy() for x in dr.v]), "P": dr.P.cpu().numpy()}
+        out["inclusion2d"] = {
+            "workload": f"inclusion-q9-{args.n2d}^2", "check_interval": 50,
+            "oracle": ref["stats"], "oracle_s": ref["seconds"], "oracle_host": ref["host"],
+            "gpu_fp64": dict({k: st[k] for k in ("iter", "itPH", "converged", "err")}, seconds=tg),
+            "rel_err_vs_oracle": {"v": _rel(f["v"], ref["v"]), "P": _rel(f["P"], ref["P"]),
+                                  "P_mean_free": _rel(_mean_free(f["P"], ref["M_P"]), _mean_free(ref["P"], ref["M_P"]))}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def inclusion_oracle(args, case, oh, kw):
+    """The oracle's solve of the 2-D inclusion case: loaded from --oracle2d (an .npz
+    this function wrote with --oracle-only, possibly on another host), or run here."""
+    if args.oracle2d and os.path.exists(args.oracle2d) and not args.oracle_only:
+        z = np.load(args.oracle2d, allow_pickle=False)
+        meta = json.loads(str(z["meta"]))
+        if meta["n"] != args.n2d or meta["tolerance"] != args.tolerance:
+            raise SystemExit(f"{args.oracle2d} holds n={meta['n']}, tolerance={meta['tolerance']}")
+        return {"v": z["v"], "P": z["P"], "M_P": z["M_P"], "stats": meta["stats"], "seconds": meta["seconds"],
+                "host": meta["host"]}
+    hs = case.host_state(oh)
+    t0 = time.perf_counter()
+    sor = hs.solve(**kw)
+    sec = time.perf_counter() - t0
+    name, nproc = cpu_model()
+    res = {"v": np.concatenate(hs.v), "P": hs.P.copy(), "M_P": hs.M_P.copy(),
+           "stats": {k: sor[k] for k in ("iter", "itPH", "converged", "err")}, "seconds": sec,
+           "host": {"cpu_model": name, "nproc": nproc, "oracle_threads": oh.lib().orc_num_threads()}}
+    if args.oracle2d:
+        meta = {"n": args.n2d, "tolerance": args.tolerance, "stats": res["stats"], "seconds": sec, "host": res["host"]}
+        np.savez(args.oracle2d, v=res["v"], P=res["P"], M_P=res["M_P"], meta=json.dumps(meta))
+    return res
+
+
+def workload_config(args, case, world=1):
+    """The `config` object of both arms' JSON lines: the workload only, no run results."""
+    m = case.mesh
+    return {"workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
+            "tolerance": args.tolerance, "check_interval": args.check_interval, "dt": case.dt,
+            "nels": m.nels, "nnodes": m.nnodes, "nnodesP": m.nnodesP,
+            "l2": "inputs larger than L2 (geometry alone %.0f MB)" % (m.geo_v.nbytes / 1e6),
+            "parallelism": f"replicas{world}"}
+
+
 def run_reference(args):
+    """--impl reference: the reference's CPU path on this host (the oracle, its C++ FP64
+    restatement, all host cores) on the same workload. Julia cannot run here, so this is
+    the stand-in the reference's CPU KernelAbstractions path is timed by. Every step is
+    one bounded CpuSample step on the full mesh; the value is the solve's time
+    extrapolated along the measured DR path (PATH_64, or --ref-* for other sizes)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     fem = load_package()
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
-    iters, jacs = args.ref_iterations, args.ref_jacobians
-    times = []
-    for _ in range(args.warmup + args.steps):
-        est, cores, sample = cpu_baseline_estimate(case, iters, jacs)
-        times.append(est)
-    t = statistics.mean(times[args.warmup:])
+    if args.ref_iterations > 0:
+        path = {"iterations": args.ref_iterations, "itPH": args.ref_itph, "jacobian_assemblies": args.ref_jacobians,
+                "check_interval": args.check_interval}
+    elif args.n == 64 and args.seed == 0 and args.check_interval == PATH_64["check_interval"]:
+        path = dict(PATH_64)
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": "no measured DR path for this size; pass --ref-iterations, "
+                          "--ref-itph and --ref-jacobians"}))
+        return 0
+    smp = CpuSample(case)
+    figs = []
+    for i in range(args.warmup + args.steps):
+        f = smp.step()
+        if i >= args.warmup:
+            figs.append(f)
+    fig = {k: statistics.mean(f[k] for f in figs) for k in figs[0]}
+    t = CpuSample.estimate(fig, path)
+    name, nproc = cpu_model()
     line = {
         "impl": "reference", "metric": METRIC, "value": t, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
-                   "tolerance": 1e-8},
-        "cpu_baseline": {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
+        "method": "oracle: C++ FP64 restatement of the reference's CPU path (Julia is not available here)",
+        "config": workload_config(args, case),
+        "value_kind": "extrapolated: the timed per-step sample priced along the measured DR path",
+        "path": path,
+        "sample_figures_s": fig,
+        "cpu_baseline": {"value": t, "unit": "s", "cores": smp.cores, "kind": "port", "sample": smp.describe(fig),
+                         "cpu_model": name, "nproc": nproc},
         "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -664,8 +891,9 @@ def main():
     ap.add_argument("--tolerance", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iterations", type=int, default=0,
-                    help="iteration count of the GPU run used to scale the reference sample")
+                    help="DR iterations of the path the reference sample is priced along (default: PATH_64)")
     ap.add_argument("--ref-jacobians", type=int, default=0)
+    ap.add_argument("--ref-itph", type=int, default=0)
     ap.add_argument("--max-iterations", type=int, default=2_000_000,
                     help="cap on DR iterations per solve (profiling runs of a few sweeps)")
     ap.add_argument("--adjoint-dt", type=float, default=1e-2)
@@ -676,20 +904,28 @@ def main():
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
     ap.add_argument("--tl-steps", type=int, default=10)
-    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap"],
+    ap.add_argument("--n2d", type=int, default=0, help="parity mode: size of the 2-D inclusion case (0: skip)")
+    ap.add_argument("--oracle2d", default="", help="parity mode: .npz of the 2-D oracle solve (read, or written "
+                    "with --oracle-only)")
+    ap.add_argument("--oracle-only", action="store_true", help="parity mode: run and save the 2-D oracle solve only")
+    ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap",
+                             "parity"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
-        if args.ref_iterations <= 0:
-            # the same solve's path on the GPU measured at 64³ (iterations, Jacobian assemblies)
-            prev = os.path.join(ROOT, "profiles", "bench_path.json")
-            if os.path.exists(prev):
-                d = json.load(open(prev))
-                args.ref_iterations, args.ref_jacobians = d["iterations"], d["jacobian_assemblies"]
-            else:
-                print(json.dumps({"impl": "reference", "unavailable": "no measured iteration path to scale the sample"}))
-                return 0
         return run_reference(args)
+    if args.mode == "parity" and args.oracle_only:
+        # the CPU half of the 2-D parity check, on a host without a GPU
+        fem = load_package()
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_host as oh
+        case = fem.configs.inclusion_2d_case(n=args.n2d)
+        kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=50, throw_on_failure=False,
+                  max_iterations=args.max_iterations, iter_max=args.max_iterations)
+        ref = inclusion_oracle(args, case, oh, kw)
+        print(json.dumps({"mode": "parity-oracle-2d", "n": args.n2d, "stats": ref["stats"], "seconds": ref["seconds"],
+                          "host": ref["host"]}), flush=True)
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -720,6 +956,8 @@ def main():
         return lithostatic_mode(args, fem)
     if args.mode == "cap":
         return cap_mode(args, fem)
+    if args.mode == "parity":
+        return parity_mode(args, fem)
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     dr = case.device_state()
     bc = case.bc_device()
@@ -845,31 +1083,29 @@ def main():
                  "kernel_ms": {"residual": pm[0], "jacobian": pm[1], "node_update": pm[2]},
                  "residual_avg_ms": pm[0] / max(pn[0], 1),
                  "field_rel_err_chosen_vs_fp64": err}
-    path_iters, path_jacs = (plain["iterations"], plain["jacobian_assemblies"]) if plain else (iters, jacs)
+    if plain:
+        path = {"iterations": plain["iterations"], "itPH": plain["itPH"],
+                "jacobian_assemblies": plain["jacobian_assemblies"], "check_interval": args.check_interval}
+    else:
+        path = {"iterations": iters, "itPH": st["itPH"], "jacobian_assemblies": jacs,
+                "check_interval": args.check_interval}
 
     peak, peak_kind = measured_peaks()
     mixed = args.precision == "mixed"
     nbytes = incremental_kernel_bytes(case) if mixed else residual_kernel_bytes(case, itemsize=8, geo_itemsize=8)
     res_avg_ms = prof_ms[0] / max(prof_n[0], 1)
     achieved = nbytes / (res_avg_ms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "residual_traffic.json")
-    if os.path.exists(tp):
-        d = json.load(open(tp))
-        if d.get("n") == args.n and d.get("precision") == args.precision:
-            traffic = d.get("bytes_per_launch")
+    traffic = TRAFFIC.get((args.n, args.precision))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        est, cores, sample = cpu_baseline_estimate(case, path_iters, path_jacs)
-        cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample}
+        # a bounded sample: two CpuSample steps (about 20 s of CPU work at 64³)
+        est, cores, sample = cpu_baseline_estimate(case, path, steps=2)
+        name, nproc = cpu_model()
+        cpu = {"value": est, "unit": "s", "cores": cores, "kind": "port", "sample": sample, "cpu_model": name,
+               "nproc": nproc}
 
     if rank == 0:
-        os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
-        if args.n == 64 and (plain or args.precision == "fp64"):
-            json.dump({"iterations": path_iters, "jacobian_assemblies": path_jacs,
-                       "itPH": plain["itPH"] if plain else st["itPH"]},
-                      open(os.path.join(ROOT, "profiles", "bench_path.json"), "w"))
         if mixed:
             kernel = "hex27_incr_kernel (thread-per-element FP32 incremental sweep: RP, Pnum, Rv increments)"
         elif mesh_is_affine(case.mesh):
@@ -881,17 +1117,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {
-                "workload": f"vep-layers-hex27-{args.n}^3", "nel": [args.n] * 3, "seed": args.seed,
-                "method": "mixed precision (FP32 increments, FP64 outer steps)" if mixed else "plain FP64 DR",
-                "precision": args.precision, "tolerance": args.tolerance, "check_interval": args.check_interval,
-                "dt": case.dt, "iterations": iters, "itPH": st["itPH"], "jacobian_assemblies": jacs,
-                "fp64_outer_sweeps": st.get("defect_corrections", 0),
-                "converged": bool(st["converged"]), "err": st["err"],
-                "nels": case.mesh.nels, "nnodes": case.mesh.nnodes, "nnodesP": case.mesh.nnodesP,
-                "l2": "inputs larger than L2 (geometry alone %.0f MB)" % (case.mesh.geo_v.nbytes / 1e6),
-                "parallelism": f"replicas{world}",
-            },
+            "method": "mixed precision (FP32 increments, FP64 outer steps)" if mixed else "plain FP64 DR",
+            "config": workload_config(args, case, world),
+            "path": {"iterations": iters, "itPH": st["itPH"], "jacobian_assemblies": jacs,
+                     "fp64_outer_sweeps": st.get("defect_corrections", 0), "converged": bool(st["converged"]),
+                     "err": st["err"]},
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": (plain["value"] / t_step) if plain else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
