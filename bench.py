@@ -73,13 +73,15 @@ def mesh_is_affine(mesh, tol=1e-12):
     return bool(ok)
 
 
-def incremental_kernel_bytes(case):
+def incremental_kernel_bytes(case, stress_reads=None):
     """Algorithmic bytes of one FP32 incremental sweep of the mixed-precision solve
     (hex27_incr_kernel): δv, the tiled connectivity, FP32 affine geometry, the two
-    element phases, δP, the Pnum scale γP/M_P of the element's DoFs, the base trial
-    stress and yield value of every integration point (7 × 27 FP32), the RP increment
-    written and the Rv read-modify-write (FP32). The pressure DoFs are numbered 4e + p
-    on the structured mesh, so no DoF table is read."""
+    element phases, δP, the Pnum scale γP/M_P of the element's DoFs, the base yield
+    value of every integration point (27 FP32), the base trial stress (6 FP32) of the
+    points the elastic bound does not settle (`stress_reads` per launch, measured by
+    the library's counter; every point when None), the RP increment written and the
+    Rv read-modify-write (FP32). The pressure DoFs are numbered 4e + p on the
+    structured mesh, so no DoF table is read."""
     m = case.mesh
     nels, nn, nP = m.nels, m.nnodes, m.nnodesP
     b = 3 * nn * 4                         # δv
@@ -88,7 +90,8 @@ def incremental_kernel_bytes(case):
     b += 2 * 4 * nels                      # phases of the velocity nodes and of the pressure DoFs
     b += nP * 4                            # δP
     b += 4 * 4 * nels                      # γP/M_P
-    b += 7 * 27 * 4 * nels                 # base trial stress and yield value
+    b += 27 * 4 * nels                     # base yield value
+    b += 6 * 4 * (27 * nels if stress_reads is None else stress_reads)   # base trial stress where read
     b += nP * 4                            # RP increment written
     b += 2 * 3 * nn * 4                    # Rv atomic read-modify-write
     return b
@@ -400,12 +403,15 @@ def warmstart_mode(args, fem):
     rows_out = []
     res = fem.warmstart.shear_band_warm_start(n=args.n, nsteps=args.ws_steps, ntrain=args.ws_train,
                                               epochs=args.ws_epochs, seed=args.seed, tolerance=args.tolerance,
+                                              check_interval=args.check_interval, online_steps=args.ws_online,
                                               log=(lambda r: rows_out.append(r)))
     test = [r for r in res["rows"] if "learned_iter" in r]
     mean = lambda k: float(np.mean([r[k] for r in test])) if test else None
     tot = lambda k: float(np.sum([r[k] for r in test])) if test else None
     line = {
         "mode": "warmstart", "workload": f"shear-band-q9-{args.n}^2", "n": args.n, "steps": args.ws_steps,
+        "check_interval": args.check_interval, "online_adam_steps": args.ws_online,
+        "online_train_ms_mean": mean("online_train_ms") if args.ws_online else 0.0,
         "train_steps": args.ws_train, "epochs": args.ws_epochs, "train_ms": res["train_ms"],
         "train_loss_first_last": [res["train_loss"][0], res["train_loss"][-1]] if res["train_loss"] else None,
         "gain": res["gain"], "test_steps": len(test),
@@ -903,6 +909,7 @@ def main():
     ap.add_argument("--ws-steps", type=int, default=200)
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
+    ap.add_argument("--ws-online", type=int, default=0, help="Adam steps on the newest converged pairs per solved step")
     ap.add_argument("--tl-steps", type=int, default=10)
     ap.add_argument("--n2d", type=int, default=0, help="parity mode: size of the 2-D inclusion case (0: skip)")
     ap.add_argument("--oracle2d", default="", help="parity mode: .npz of the 2-D oracle solve (read, or written "
@@ -1015,7 +1022,10 @@ def main():
     barrier()
     ms_profiled = ev0.elapsed_time(ev1)
     lib.femb200_profile_read(h, prof_ms, prof_n)
+    counters = (C.c_int64 * fem._abi.COUNTER_COUNT)()
+    lib.femb200_profile_counters(h, counters, fem._abi.COUNTER_COUNT)
     lib.femb200_profile(h, 0)
+    stress_reads = counters[fem._abi.COUNTER_STRESS_READS] / max(prof_n[0], 1)
     t_step = ms_total / 1e3 / args.steps
     t_step = max_over_ranks(t_step, world)
 
@@ -1092,7 +1102,8 @@ def main():
 
     peak, peak_kind = measured_peaks()
     mixed = args.precision == "mixed"
-    nbytes = incremental_kernel_bytes(case) if mixed else residual_kernel_bytes(case, itemsize=8, geo_itemsize=8)
+    nbytes = incremental_kernel_bytes(case, stress_reads) if mixed else residual_kernel_bytes(case, itemsize=8,
+                                                                                              geo_itemsize=8)
     res_avg_ms = prof_ms[0] / max(prof_n[0], 1)
     achieved = nbytes / (res_avg_ms / 1e3) / 1e9
     traffic = TRAFFIC.get((args.n, args.precision))
@@ -1127,7 +1138,9 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": res_avg_ms,
-                         "launches": int(prof_n[0]), "peak_kind": peak_kind},
+                         "launches": int(prof_n[0]), "peak_kind": peak_kind,
+                         "base_stress_reads_per_launch": stress_reads if mixed else None,
+                         "bytes_if_every_point_read_its_stress": incremental_kernel_bytes(case) if mixed else None},
             "kernel_ms": {"residual": prof_ms[0], "jacobian": prof_ms[1], "node_update": prof_ms[2],
                           "outer_fp64_sweeps": prof_ms[4], "profiled_solve": ms_profiled},
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

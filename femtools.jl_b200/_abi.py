@@ -233,6 +233,7 @@ SIGNATURES = {
                                         _P(StokesStatsC)]),
     "femb200_profile": (C.c_int, [_vp, C.c_int32]),
     "femb200_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_int64)]),
+    "femb200_profile_counters": (C.c_int, [_vp, _P(C.c_int64), C.c_int32]),
     "femb200_color_mesh": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, _vp, _P(C.c_int32)]),
     "femb200_color_groups": (C.c_int, [_vp, C.c_int64, C.c_int32, _vp, _vp]),
     "femb200_thermal_residual_colored": (C.c_int, [_vp, _P(ThermalProblemC), C.c_double, C.c_double, C.c_int32,
@@ -241,6 +242,7 @@ SIGNATURES = {
 }
 NOALLOC_MAX_NODES = 8388608   # FEMB200_NOALLOC_MAX_NODES
 PROF_RESIDUAL, PROF_JACOBIAN, PROF_NODE, PROF_ALL, PROF_OUTER, PROF_COUNT = range(6)
+COUNTER_STRESS_READS, COUNTER_SHARED_JACOBIANS, COUNTER_COUNT = 0, 1, 4
 
 _lib = None
 

@@ -54,6 +54,12 @@ struct femb200_handle {
     int64_t prof_n[FEMB200_PROF_COUNT] = {};
     int prof_sweep = FEMB200_PROF_RESIDUAL;   // class of launch_residual's sweeps
     unsigned long long launches_at_reset = 0;
+    // device counters of the profiled work (FEMB200_COUNTER_*), zeroed by femb200_profile
+    unsigned long long* d_counters = nullptr;
+    // shared elastic element Jacobians: one template per phase and the picked elements
+    void* d_jac_tmpl = nullptr;
+    int32_t* d_jac_pick = nullptr;
+    int jac_shared = 1;   // FEMB200_JAC_SHARED=0 at creation turns the shared Jacobians off
     // compressed affine geometry (one J⁻¹, |det J| per element), rebuilt per call
     void* d_geo_c = nullptr;
     size_t geo_c_cap = 0;
@@ -463,7 +469,29 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
         CK(cudaStreamSynchronize(h->stream));
         a.diag_geometry = *h->h_flag == 0;
     }
+    // one-phase cells: the elastic element Jacobian of each phase is computed once (on
+    // the phase's first element) and shared by every elastic element with the same inputs
+    const bool shared = p->dim == 3 && h->jac_shared && (!p->phases_v || p->phases_v_layout == FEMB200_PHASE_CELL);
     RC(prof_begin(h, FEMB200_PROF_JACOBIAN));
+    if (shared) {
+        if (!h->d_jac_tmpl) {
+            CK(cudaMalloc(&h->d_jac_tmpl, sizeof(JacTemplate<double>) * MAXPH));
+            CK(cudaMalloc(&h->d_jac_pick, sizeof(int32_t) * MAXPH));
+        }
+        CK(cudaMemsetAsync(h->d_jac_pick, 0x7f, sizeof(int32_t) * MAXPH, h->stream));   // JAC_NO_PICK
+        CK(launch_jac_pick(p->phases_v, p->nels, h->d_jac_pick, h->stream));
+        H27JacArgs<T, TG> b = a;
+        b.tmpl_mode = JAC_TMPL_BUILD;
+        b.tmpl = static_cast<JacTemplate<T>*>(h->d_jac_tmpl);
+        b.pick = h->d_jac_pick;
+        b.pick_nels = p->nels;
+        b.nels = MAXPH;
+        CK(launch_hex27_jacobian<T, TG>(b, h->num_sms, h->stream));
+        a.tmpl_mode = JAC_TMPL_USE;
+        a.tmpl = b.tmpl;
+        a.pick = b.pick;
+        a.shared_count = h->prof ? h->d_counters + FEMB200_COUNTER_SHARED_JACOBIANS : nullptr;
+    }
     if (p->dim == 3) CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
     else CK(launch_q9_jacobian<T, TG>(a, h->stream));
     RC(prof_end(h, FEMB200_PROF_JACOBIAN));
@@ -968,6 +996,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     at.pscale_t = m.pscale_t;
     for (int k = 0; k < 3; ++k) { at.dv[k] = m.dv[k]; at.R[k] = m.R[k]; at.g[k] = (float)p->mat.g[k]; }
     at.dP = m.dP; at.RPinc = m.RPinc;
+    at.stress_reads = h->prof ? h->d_counters + FEMB200_COUNTER_STRESS_READS : nullptr;
     at.nels = p->nels;
     at.plastic = p->mat.plastic;
     {
@@ -1654,12 +1683,16 @@ int femb200_create(femb200_handle** out) {
     // FEMB200_INCR_SWEEP=warp selects the warp-cooperative incremental sweep of the
     // mixed-precision solve (for comparisons); the default is thread-per-element
     if (const char* v = std::getenv("FEMB200_INCR_SWEEP")) h->use_incr_thread = std::strcmp(v, "warp") != 0;
+    // FEMB200_JAC_SHARED=0 assembles every element's Jacobian columns (for comparisons)
+    if (const char* v = std::getenv("FEMB200_JAC_SHARED")) h->jac_shared = std::strcmp(v, "0") != 0;
     *out = h;
     return FEMB200_OK;
 }
 
 int femb200_profile(femb200_handle* h, int32_t enable) {
     if (!h) return FEMB200_EINVAL;
+    if (!h->d_counters) CK(cudaMalloc(&h->d_counters, sizeof(unsigned long long) * FEMB200_COUNTER_COUNT));
+    CK(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned long long) * FEMB200_COUNTER_COUNT, h->stream));
     for (int k = 0; k < FEMB200_PROF_COUNT; ++k) {
         RC(prof_flush(h, k));
         h->prof_ms[k] = 0;
@@ -1667,6 +1700,17 @@ int femb200_profile(femb200_handle* h, int32_t enable) {
     }
     h->prof = enable != 0;
     h->launches_at_reset = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+    return FEMB200_OK;
+}
+
+int femb200_profile_counters(femb200_handle* h, int64_t* out, int32_t n) {
+    if (!h || !out || n < 0) return FEMB200_EINVAL;
+    unsigned long long c[FEMB200_COUNTER_COUNT] = {};
+    if (h->d_counters) {
+        CK(cudaMemcpyAsync(c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    for (int k = 0; k < n && k < FEMB200_COUNTER_COUNT; ++k) out[k] = (int64_t)c[k];
     return FEMB200_OK;
 }
 
@@ -1694,6 +1738,9 @@ int femb200_destroy(femb200_handle* h) {
     if (h->d_geo_c) cudaFree(h->d_geo_c);
     if (h->d_flag) cudaFree(h->d_flag);
     if (h->h_flag) cudaFreeHost(h->h_flag);
+    if (h->d_counters) cudaFree(h->d_counters);
+    if (h->d_jac_tmpl) cudaFree(h->d_jac_tmpl);
+    if (h->d_jac_pick) cudaFree(h->d_jac_pick);
     if (h->mixed.mem) cudaFree(h->mixed.mem);
     if (h->adj_mem) cudaFree(h->adj_mem);
     delete h;

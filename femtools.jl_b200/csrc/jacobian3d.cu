@@ -117,10 +117,14 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     const T EPS2 = eps2<T>();
     const T zero3[3] = {T(0), T(0), T(0)};
 
+    const bool build = a.tmpl_mode == JAC_TMPL_BUILD;
     const int64_t stride = (int64_t)gridDim.x * wpb * 3;
     for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
-        const int64_t e = base + (lane_ok ? s : 0);
-        const bool act = lane_ok && e < a.nels;
+        // building templates, slot k of the loop is phase k and its element pick[k]
+        const int64_t k = base + (lane_ok ? s : 0);
+        const bool picked = build && k < MAXPH && a.pick[k] >= 0 && a.pick[k] < a.pick_nels;
+        const int64_t e = build ? (picked ? (int64_t)a.pick[k] : 0) : k;
+        const bool act = lane_ok && (build ? picked : e < a.nels);
         const int64_t ec = act ? e : 0;
 
         int node[3];
@@ -257,10 +261,48 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 const T tII = sqrt((t[0] * t[0] + t[1] * t[1] + t[2] * t[2]) / T(2) + t[3] * t[3] + t[4] * t[4] + t[5] * t[5] + EPS2);
                 const T Fy = tII - cphi * C - sphi * Peq;
                 const T den = etave + ereg + Kb * dt * (-spsi) * (-sphi);
-                const T lam = Fy > T(0) ? Fy / den : T(0);
+                const T lam = Fy > T(0) && !build ? Fy / den : T(0);
                 plam[qz] = lam; pitII[qz] = T(1) / tII; pitIIs[qz] = T(1) / (tII + EPS2); piden[qz] = T(1) / den;
             }
         }
+
+        // a warp whose three elements are elastic here and carry their phase template's
+        // inputs bit for bit takes the template's rows (computed by this code on those inputs)
+        bool shared = false;
+        if (a.tmpl_mode == JAC_TMPL_USE) {
+            bool mine = !act;
+            if (act && uniform && p0 >= 0 && p0 < MAXPH) {
+                const JacTemplate<T>& tm = a.tmpl[p0];
+                bool ok = tm.valid != 0 && plam[0] == T(0) && plam[1] == T(0) && plam[2] == T(0) && eta_pc == tm.eta_pc;
+#pragma unroll
+                for (int p = 0; p < 4; ++p) ok = ok && gam[p] == tm.gam[p] && MPl[p] == tm.MP[p];
+#pragma unroll
+                for (int qz = 0; qz < 3; ++qz) {
+                    const int q = tidx(m1, m2, qz);
+#pragma unroll
+                    for (int r = 0; r < 11; ++r) ok = ok && GEO[q * 11 + r] == tm.geo[q * 11 + r];
+                }
+                mine = ok;
+            }
+            shared = __all_sync(0xffffffffu, mine || !lane_ok);
+            if (shared && a.shared_count) {
+                const unsigned n = __popc(__ballot_sync(0xffffffffu, act && m == 0));
+                if (lane == 0 && n) atomicAdd(a.shared_count, (unsigned long long)n);
+            }
+        }
+        T rows[3][3], diag[3][3];
+        if (shared) {
+            if (act) {
+                const JacTemplate<T>& tm = a.tmpl[p0];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        rows[c][i] = tm.rows[tidx(i, m1, m2) * 3 + c];
+                        diag[c][i] = tm.diag[tidx(i, m1, m2) * 3 + c];
+                    }
+            }
+        } else {
 
         // ∂RP_p/∂v_(b,j) = −Σ_q NP_p(q) ∂_j N_b(q) dΩ_P(q) for every column, via the
         // transposed contraction with a unit "pressure" flux per p.
@@ -289,7 +331,6 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
         }
         __syncwarp();
 
-        T rows[3][3], diag[3][3];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -381,7 +422,30 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                     }
             }
         }
-        if (act) {
+        }
+        if (act && build) {
+            JacTemplate<T>& tm = a.tmpl[k];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    tm.rows[tidx(i, m1, m2) * 3 + c] = rows[c][i];
+                    tm.diag[tidx(i, m1, m2) * 3 + c] = diag[c][i];
+                }
+#pragma unroll
+            for (int qz = 0; qz < 3; ++qz) {
+                const int q = tidx(m1, m2, qz);
+#pragma unroll
+                for (int r = 0; r < 11; ++r) tm.geo[q * 11 + r] = GEO[q * 11 + r];
+            }
+            if (m == 0) {
+#pragma unroll
+                for (int p = 0; p < 4; ++p) { tm.gam[p] = gam[p]; tm.MP[p] = MPl[p]; }
+                tm.eta_pc = eta_pc;
+                // only a one-phase element is a template; the flag is read by a later launch
+                tm.valid = uniform ? 1 : 0;
+            }
+        } else if (act) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -410,6 +474,22 @@ __global__ void geo_offdiag_kernel(const TG* geo_v, int64_t npts, int* flag) {
     }
 }
 }  // namespace
+
+namespace {
+__global__ void jac_pick_kernel(const int32_t* phv, int64_t nels, int32_t* pick) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nels; e += (int64_t)gridDim.x * blockDim.x) {
+        const int p = phv ? phv[e] - 1 : 0;
+        if (p >= 0 && p < MAXPH && e < JAC_NO_PICK) atomicMin(pick + p, (int32_t)e);
+    }
+}
+}  // namespace
+
+cudaError_t launch_jac_pick(const int32_t* phv, int64_t nels, int32_t* pick, cudaStream_t st) {
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((nels + 255) / 256, 148 * 8));
+    count_launch();
+    jac_pick_kernel<<<(unsigned)blocks, 256, 0, st>>>(phv, nels, pick);
+    return cudaGetLastError();
+}
 
 template <class TG>
 cudaError_t launch_geo_offdiag(const TG* geo_v, int64_t nels, int* flag, cudaStream_t st) {

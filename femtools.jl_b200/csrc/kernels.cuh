@@ -98,6 +98,9 @@ struct IncrArgs {
     int plastic;
     float g[3];
     IncrPhase ph[MAXPH];
+    // when set (profiling), the number of (element, point) pairs whose base trial stress
+    // the sweep read, i.e. that the elastic bound did not settle, is added here
+    unsigned long long* stress_reads;
 };
 // Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
 // copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.
@@ -240,6 +243,16 @@ cudaError_t launch_apply_guess(const T* vprev[2], const T* vcur[2], const T* Ppr
                                const int32_t* el2n, int64_t nnodes, int64_t nels, cudaStream_t st);
 
 // Augmented Jacobian diagnostics of Hex27 (row sums → dRdv, |diag| → PC).
+// Inputs and L1 row sums / |diagonal| of one phase's shared elastic element Jacobian
+// (rows indexed [tensor node · 3 + component]).
+template <class T>
+struct JacTemplate {
+    int32_t valid;
+    T geo[27 * 11];
+    T gam[4], MP[4], eta_pc;
+    T rows[81], diag[81];
+};
+
 template <class T, class TG>
 struct H27JacArgs {
     const int32_t* el2n;
@@ -263,9 +276,25 @@ struct H27JacArgs {
     int64_t nels;
     T dt;
     int diag_geometry;    // every J⁻¹ diagonal (the Hex27 kernel's DIAG specialisation)
+    // Shared element Jacobians (Hex27, one phase per cell): JAC_TMPL_BUILD computes, for
+    // the element pick[p] of each phase p, the diagnostics of its elastic linearisation
+    // and its inputs into tmpl[p]; JAC_TMPL_USE lets a warp whose three elements are
+    // all elastic at the current state and whose inputs equal their phase's template
+    // bit for bit take the template's rows instead of the 81 columns (the same code on
+    // the same inputs: identical results).
+    int tmpl_mode;
+    struct JacTemplate<T>* tmpl;
+    const int32_t* pick;
+    int64_t pick_nels;    // element count of the mesh the picks index (bound of every pick)
+    unsigned long long* shared_count;   // when set (profiling): elements that took a template
 };
+enum { JAC_TMPL_OFF = 0, JAC_TMPL_USE = 1, JAC_TMPL_BUILD = 2 };
+// fill of the pick array before launch_jac_pick (a byte-wise memset of 0x7f)
+constexpr int32_t JAC_NO_PICK = 0x7f7f7f7f;
 template <class TG>
 cudaError_t launch_geo_offdiag(const TG* geo_v, int64_t nels, int* flag, cudaStream_t st);
+// pick[p] ← the lowest element index whose cell phase is p + 1 (pick pre-filled with JAC_NO_PICK)
+cudaError_t launch_jac_pick(const int32_t* phv, int64_t nels, int32_t* pick, cudaStream_t st);
 
 template <class T, class TG>
 cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cudaStream_t st);

@@ -178,11 +178,17 @@ FEMB_D float ldg_stream(const float* ptr, uint64_t pol) {
     return v;
 }
 
-// Base data of one quadrature row (3 points × 7 fields, contiguous in the tiled
-// layout) into registers.
-FEMB_D void load_row(float (&r)[3 * BASE_FIELDS], const float* row, uint64_t pol) {
+// Yield values F of the base state at the three points of one quadrature row (field
+// 6 of each point in the tiled layout: one 128-byte line per point and warp).
+FEMB_D void load_row_F(float (&F)[3], const float* row, uint64_t pol) {
 #pragma unroll
-    for (int j = 0; j < 3 * BASE_FIELDS; ++j) r[j] = ldg_stream(row + j * 32, pol);
+    for (int j = 0; j < 3; ++j) F[j] = ldg_stream(row + (j * BASE_FIELDS + 6) * 32, pol);
+}
+
+FEMB_D float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // Per-element data of a tile, loaded one tile ahead (during the previous tile's
@@ -282,9 +288,12 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         }
         cp_async_commit();
     }
-    float pre[3 * BASE_FIELDS];
+    // yield values of the next row's points, loaded one row ahead; the trial stress of a
+    // point is read only where the elastic bound below does not settle the point
+    float preF[3] = {0.0f, 0.0f, 0.0f};
+    unsigned stress_reads = 0;
     const uint64_t pol = l2_evict_first();
-    if (plastic) load_row(pre, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane, pol);
+    if (plastic) load_row_F(preF, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane, pol);
     ElemData cur;
     load_elem<DIAG>(a, tile, lane, nslots, cur);
 
@@ -348,9 +357,10 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                 const float by[3] = {Lb(qy, 0), Lb(qy, 1), Lb(qy, 2)};
                 const float dy[3] = {Ld(qy, 0), Ld(qy, 1), Ld(qy, 2)};
                 const float et = gx(qy), wyz = gw(qy) * wz;
-                // base data of the next row (rows in (qz, qy) order, then the next tile's
-                // first row): each point's 7 registers are refilled as soon as the
-                // point has read them
+                // base data of this row and of the next one (rows in (qz, qy) order, then
+                // the next tile's first row): each point's F register is refilled as soon
+                // as the point has read it
+                const float* cur_row = a.base_t + (tile * 27 + 3 * (3 * qz + qy)) * BASE_FIELDS * 32 + lane;
                 const int rnext = 3 * qz + qy + 1;
                 const float* next_row = rnext < 9 ? a.base_t + (tile * 27 + 3 * rnext) * BASE_FIELDS * 32 + lane
                                                   : (has_next ? a.base_t + tnext * 27 * BASE_FIELDS * 32 + lane : nullptr);
@@ -441,15 +451,26 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
 #pragma unroll
                     for (int c = 0; c < 6; ++c) dtt[c] = twoe * ed[c];
                     if (plastic) {
+                        const float Fk = preF[qx];
+                        if (next_row) preF[qx] = ldg_stream(next_row + (qx * BASE_FIELDS + 6) * 32, pol);
+                        // Elastic bound: τII = sqrt(‖τ‖² + ε²) is 1-Lipschitz in the J2 norm
+                        // ‖τ‖² = ½Σ τ_ii² + Σ_{i<j} τ_ij², so the trial yield value satisfies
+                        // F(τb + δτ) ≤ F_k + ‖δτ‖ + sinϕ·|δP|. Where that bound (with a 1e-3
+                        // relative margin over the rounding of either path) stays negative,
+                        // base and trial are both elastic, the return leaves the increment
+                        // unchanged (dp_increment gives δτ exactly), and the base trial
+                        // stress is not needed.
+                        const float dd = 0.5f * (dtt[0] * dtt[0] + dtt[1] * dtt[1] + dtt[2] * dtt[2]) + dtt[3] * dtt[3] +
+                                         dtt[4] * dtt[4] + dtt[5] * dtt[5];
+                        const float reach = (sqrt_approx(dd) + fabsf(M.sphi * Pq)) * 1.001f + 1e-20f;
+                        if (Fk + reach < 0.0f) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
+                        } else {
+                        stress_reads += act ? 1u : 0u;
                         float tb[6];
 #pragma unroll
-                        for (int c = 0; c < 6; ++c) tb[c] = pre[qx * BASE_FIELDS + c];
-                        const float Fk = pre[qx * BASE_FIELDS + 6];
-                        if (next_row) {
-#pragma unroll
-                            for (int c = 0; c < BASE_FIELDS; ++c)
-                                pre[qx * BASE_FIELDS + c] = ldg_stream(next_row + (qx * BASE_FIELDS + c) * 32, pol);
-                        }
+                        for (int c = 0; c < 6; ++c) tb[c] = ldg_stream(cur_row + (qx * BASE_FIELDS + c) * 32, pol);
                         const float Jk = 0.5f * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] +
                                          tb[4] * tb[4] + tb[5] * tb[5];
                         if (Jk < 1e-6f * M.cC * M.cC) {
@@ -465,6 +486,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                             for (int c = 0; c < 6; ++c) tau[c] = o.tau[c];
                         } else {
                             dp_increment<float, true>(tb, Fk, dtt, Pq, twoe, M.sphi, inv_den, EPS2, tau);
+                        }
                         }
                     } else {
 #pragma unroll
@@ -569,6 +591,12 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         if (has_next) read_elem<DIAG>(a, tnext, lane, WS, cur);
     }
     cp_async_wait_all();
+    if (a.stress_reads) {
+        unsigned n = stress_reads;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+        if (lane == 0 && n) atomicAdd(a.stress_reads, (unsigned long long)n);
+    }
 }
 
 std::mutex g_inc_mutex;

@@ -255,6 +255,25 @@ class WarmStartNet:
         self.gain = min(max(num / den, 0.0), 1.0) if den > 0 else (1.0 if not Xv else 0.0)
         return hist
 
+    def train_online(self, pairs, H, W, steps=2, batch=4):
+        """`steps` Adam steps on the newest training pairs (X, T) of the time loop: each
+        batch holds the newest pair and up to batch − 1 earlier ones, so the network
+        follows the solver's converged history as the dynamics change."""
+        if not pairs or steps <= 0:
+            return
+        npix = H * W
+        n = len(pairs)
+        for k in range(steps):
+            idx = [n - 1] + [n - 2 - ((k * (batch - 1) + j) % max(n - 1, 1)) for j in range(min(batch - 1, n - 1))]
+            xb = torch.cat([pairs[i][0] for i in idx])
+            tb = torch.cat([pairs[i][1] for i in idx])
+            B = len(idx)
+            self.zero_grad()
+            out, acts = self.forward(xb, B, H, W, keep=True)
+            _, dy = self.loss_grad(out, tb, B * npix, 1.0 / (B * npix))
+            self.backward(acts, dy, B, H, W)
+            self.adam()
+
     def predict(self, Fp, Fc, H, W):
         out, _ = self.forward(self.make_input(Fp, Fc), 1, H, W)
         return out
@@ -281,7 +300,7 @@ def extrapolate_state(dr, bc_v, vprev, vcur, Pprev, Pcur):
 
 
 def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tolerance=1e-8, check_interval=100,
-                          log=None, online_gain=True, gain_window=5):
+                          log=None, online_gain=True, gain_window=5, online_steps=0, replay=8):
     """The learned-warm-start experiment on the 2-D shear-band time loop.
 
     Steps 1..ntrain run plain DR (each from the previous step's solution) and record
@@ -289,7 +308,10 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
     the same state is solved three times, each to `tolerance`: plain (from the
     previous solution), linear extrapolation 2·x_t − x_{t−1}, and extrapolation plus
     the network's correction; the trajectory continues with the plain solution, so
-    all three see identical histories. Returns per-step iteration counts and times."""
+    all three see identical histories. With `online_steps` > 0 the network keeps
+    training after every solved step: that many Adam steps on the newest `replay`
+    pairs of the converged history, their time charged to the network's arm.
+    Returns per-step iteration counts and times."""
     from . import configs
     case = configs.shear_band_2d_case(n=n, seed=seed)
     dr = case.device_state()
@@ -304,6 +326,7 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
     rows = []
     cal = []          # (⟨prediction, realised correction⟩, ⟨prediction, prediction⟩) per solved step
     pending = None
+    pairs = []        # (input, target) of the converged history since training, newest last
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     train_loss, train_ms = None, 0.0
 
@@ -364,6 +387,18 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
                 net.gain = min(max(num / den, 0.0), 1.0)
             row["gain"] = net.gain
             pending = None
+        if online_steps > 0 and step > ntrain and len(F) >= 3:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pairs.append((net.make_input(F[-3], F[-2]), net.make_target(F[-3], F[-2], F[-1])))
+            pairs = pairs[-replay:]
+            net.train_online(pairs, H, W, steps=online_steps)
+            e1.record()
+            torch.cuda.synchronize()
+            row["online_train_ms"] = e0.elapsed_time(e1)
+            if "learned_ms" in row:
+                row["learned_ms"] += row["online_train_ms"]
         hist_v.append([x.clone() for x in dr.v])
         hist_P.append(dr.P.clone())
         if len(hist_v) > 2:

@@ -635,6 +635,16 @@ int femb200_profile(femb200_handle* h, int32_t enable);
  * kernel class (arrays of FEMB200_PROF_COUNT). Synchronises the handle's stream. */
 int femb200_profile_read(femb200_handle* h, double* ms, int64_t* launches);
 
+/* Work counters of the profiled launches, since the last femb200_profile(h, 1):
+ * FEMB200_COUNTER_STRESS_READS = (element, integration point) pairs whose base
+ * trial stress the FP32 incremental sweep of the mixed-precision solve read; the
+ * others were settled by its elastic bound, which needs only the base yield value.
+ * FEMB200_COUNTER_SHARED_JACOBIANS = elements whose Jacobian diagnostics came from
+ * their phase's shared elastic element Jacobian instead of their own 81 columns.
+ * Writes min(n, FEMB200_COUNTER_COUNT) values. Synchronises the handle's stream. */
+enum { FEMB200_COUNTER_STRESS_READS = 0, FEMB200_COUNTER_SHARED_JACOBIANS = 1, FEMB200_COUNTER_COUNT = 4 };
+int femb200_profile_counters(femb200_handle* h, int64_t* out, int32_t n);
+
 /* ---- allocation-free thermal solve ---------------------------------------- */
 
 /* Largest thermal mesh (velocity-node count) femb200_solve_thermal_noalloc accepts. */

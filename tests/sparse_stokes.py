@@ -153,19 +153,21 @@ def linear_vep_case(n=3, seed=0, distort=True, phases="nodal"):
     return fem.configs.random_state_case(dim=3, n=n, seed=seed, phases=phases, plastic=False, distort=distort)
 
 
-def layered_solve_case(n=2, seed=0):
-    """The layered visco-elastic case of the benchmark without plasticity, on a mesh
-    whose interior nodes are perturbed (non-affine cells), with a random stress
-    history and old pressure: a well-posed linear problem to solve to convergence."""
+def layered_solve_case(n=2, seed=0, distort=True):
+    """The layered visco-elastic case of the benchmark without plasticity, with a
+    random stress history and old pressure: a well-posed linear problem to solve to
+    convergence; on a mesh whose interior nodes are perturbed (non-affine cells) when
+    `distort`, else on the box itself (affine cells, as the mixed-precision solve needs)."""
     case = fem.configs.vep_layers_case(n=n, seed=seed, plastic=False)
     rng = np.random.default_rng(seed + 50)
     mesh = case.mesh
-    h = 1.0 / (2 * n)
-    coords = mesh.coords.copy()
-    interior = np.all((coords > 1e-12) & (coords < 1 - 1e-12), axis=1)
-    coords[interior] += rng.uniform(-0.15 * h, 0.15 * h, size=(interior.sum(), 3))
-    mesh.coords = coords
-    mesh.geo_v, mesh.geo_P = fem.mesh.precompute_geometry(coords, mesh.el2n, fem.element_tables(3))
+    if distort:
+        h = 1.0 / (2 * n)
+        coords = mesh.coords.copy()
+        interior = np.all((coords > 1e-12) & (coords < 1 - 1e-12), axis=1)
+        coords[interior] += rng.uniform(-0.15 * h, 0.15 * h, size=(interior.sum(), 3))
+        mesh.coords = coords
+        mesh.geo_v, mesh.geo_P = fem.mesh.precompute_geometry(coords, mesh.el2n, fem.element_tables(3))
     case.tau_old = [0.3 * rng.standard_normal(mesh.nq * mesh.nels) for _ in range(6)]
     case.P0 = 0.3 * rng.standard_normal(mesh.nnodesP)
     return case

@@ -1,0 +1,71 @@
+"""Shared elastic element Jacobians in the Hex27 Jacobian diagnostics
+(assemble_augmented_momentum_jacobian_matrices_atomix!, momentum_residuals.jl:998-1117).
+
+With one phase per cell, the library computes the diagnostics of one element per
+phase from its elastic linearisation and lets every element that is elastic at the
+current state and has the same inputs bit for bit (geometry, γP, M_P, η_pc, phase)
+take that element's rows instead of its own 81 columns. The rows are the same code
+on the same inputs, so the assembly must equal the one without sharing (a handle
+created with FEMB200_JAC_SHARED=0) up to the atomic scatter order, and the oracle
+within the parity tolerance."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle_host as oh
+from cases import vep_layers_case
+from conftest import fem
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+abi = fem._abi
+
+
+def _full_handle():
+    lib = abi.load_library()
+    os.environ["FEMB200_JAC_SHARED"] = "0"
+    try:
+        h = C.c_void_p()
+        assert lib.femb200_create(C.byref(h)) == abi.OK
+    finally:
+        del os.environ["FEMB200_JAC_SHARED"]
+    assert lib.femb200_set_stream(h, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == abi.OK
+    return lib, h
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("seed", [0, 4])
+def test_shared_jacobians_equal_the_full_assembly(precision, seed):
+    # seed 0: no point yields at the initial state; seed 4: one layer yields
+    case = vep_layers_case(n=4, seed=seed)
+    tdt = torch.float64 if precision == "fp64" else torch.float32
+    dr = case.device_state(fem, dtype=tdt, geometry_dtype=tdt)
+    fem.assemble_viscosity_weighted_pressure_scaling(dr, 50.0, case.dt)
+    lib, h = fem.solver._Handle.get()
+    lib.femb200_profile(h, 1)
+    fem.assemble_augmented_momentum_jacobian(dr, case.dt)
+    cnt = (C.c_int64 * abi.COUNTER_COUNT)()
+    lib.femb200_profile_counters(h, cnt, abi.COUNTER_COUNT)
+    lib.femb200_profile(h, 0)
+    shared = cnt[abi.COUNTER_SHARED_JACOBIANS]
+    got = [x.double().cpu().numpy() for x in list(dr.dRdv) + list(dr.PC)]
+    lib2, h2 = _full_handle()
+    try:
+        assert lib2.femb200_jacobian_diagnostics(h2, C.byref(dr.problem()), float(case.dt), 0) == abi.OK
+        torch.cuda.synchronize()
+    finally:
+        lib2.femb200_destroy(h2)
+    full = [x.double().cpu().numpy() for x in list(dr.dRdv) + list(dr.PC)]
+    print(f"seed {seed} {precision}: {shared} of {case.mesh.nels} elements took their phase's shared Jacobian")
+    assert shared > 0
+    rtol = 1e-13 if precision == "fp64" else 2e-6
+    for g, f in zip(got, full):
+        np.testing.assert_allclose(g, f, rtol=rtol, atol=rtol * np.abs(f).max())
+    if precision == "fp64":
+        hs = case.host_state(oh)
+        hs.pressure_scaling(50.0, case.dt)
+        hs.jacobian_diagnostics(case.dt)
+        for g, r in zip(got, hs.dRdv + hs.PC):
+            np.testing.assert_allclose(g, r, rtol=1e-9, atol=1e-9 * np.abs(r).max())

@@ -162,3 +162,23 @@ def test_warm_started_time_loop_converges_to_the_plain_solution():
         assert r["learned_converged"]
         # both runs stop on the same FP64 test: the warm start changes the path, not the answer
         assert r["learned_vs_plain_rel"] < 1e-6, r
+
+
+def test_learned_start_saves_iterations_over_the_plain_start():
+    # BASELINE's learned-warm-start workload, small: the shear band at 32², trained on
+    # the first 14 converged steps and fine-tuned online on every later one. The start
+    # from extrapolation + network must take at least 25 % fewer DR iterations than the
+    # plain start over the test steps, and (the gain fades a network that does not help)
+    # no more than 5 % more than extrapolation alone; both shares are printed.
+    res = ws.shear_band_warm_start(n=32, nsteps=34, ntrain=14, epochs=60, seed=0, check_interval=50,
+                                   online_steps=2)
+    later = [r for r in res["rows"] if "learned_iter" in r]
+    assert len(later) == 20
+    plain = sum(r["plain_iter"] for r in later)
+    extrap = sum(r["extrap_iter"] for r in later)
+    learned = sum(r["learned_iter"] for r in later)
+    print(f"DR iterations over {len(later)} steps: plain {plain}, extrapolation {extrap}, network {learned} "
+          f"(network vs plain {learned / plain:.3f}, vs extrapolation {learned / extrap:.3f})")
+    assert all(r["learned_converged"] for r in later)
+    assert learned <= 0.75 * plain
+    assert learned <= 1.05 * extrap
