@@ -280,8 +280,8 @@ struct H27JacArgs {
     // the element pick[p] of each phase p, the diagnostics of its elastic linearisation
     // and its inputs into tmpl[p]; JAC_TMPL_USE lets a warp whose three elements are
     // all elastic at the current state and whose inputs equal their phase's template
-    // bit for bit take the template's rows instead of the 81 columns (the same code on
-    // the same inputs: identical results).
+    // take the template's rows instead of the 81 columns (the same code on the same
+    // inputs: bit for bit in FP64; within 4e-7 relative in FP32, jacobian3d.cu same_input).
     int tmpl_mode;
     struct JacTemplate<T>* tmpl;
     const int32_t* pick;

@@ -3,11 +3,12 @@
 
 With one phase per cell, the library computes the diagnostics of one element per
 phase from its elastic linearisation and lets every element that is elastic at the
-current state and has the same inputs bit for bit (geometry, γP, M_P, η_pc, phase)
-take that element's rows instead of its own 81 columns. The rows are the same code
-on the same inputs, so the assembly must equal the one without sharing (a handle
-created with FEMB200_JAC_SHARED=0) up to the atomic scatter order, and the oracle
-within the parity tolerance."""
+current state and has the same inputs (geometry, γP, M_P, η_pc, phase) take that
+element's rows instead of its own 81 columns: inputs bit for bit equal in FP64, within
+4e-7 relative in the FP32 diagnostics of the mixed-precision solve. The assembly must
+then equal the one without sharing (a handle created with FEMB200_JAC_SHARED=0) up to
+the atomic scatter order in FP64 and to FP32 rounding in FP32, and the oracle within
+the parity tolerance."""
 import ctypes as C
 import os
 
@@ -35,11 +36,21 @@ def _full_handle():
     return lib, h
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("seed", [0, 4])
-def test_shared_jacobians_equal_the_full_assembly(precision, seed):
-    # seed 0: no point yields at the initial state; seed 4: one layer yields
+def _case(seed, copy_geometry):
     case = vep_layers_case(n=4, seed=seed)
+    if copy_geometry:
+        # every cell carries the first cell's geometry bit for bit (what a generator that
+        # forms J from coordinate differences gives a uniform box)
+        m = case.mesh
+        m.geo_v = np.ascontiguousarray(np.broadcast_to(m.geo_v[:1], m.geo_v.shape))
+        m.geo_P = np.ascontiguousarray(np.broadcast_to(m.geo_P[:1], m.geo_P.shape))
+    return case
+
+
+@pytest.mark.parametrize("precision,copy_geometry", [("fp64", True), ("fp32", False), ("fp32", True)])
+@pytest.mark.parametrize("seed", [0, 4])
+def test_shared_jacobians_equal_the_full_assembly(precision, copy_geometry, seed):
+    case = _case(seed, copy_geometry)
     tdt = torch.float64 if precision == "fp64" else torch.float32
     dr = case.device_state(fem, dtype=tdt, geometry_dtype=tdt)
     fem.assemble_viscosity_weighted_pressure_scaling(dr, 50.0, case.dt)
@@ -58,9 +69,10 @@ def test_shared_jacobians_equal_the_full_assembly(precision, seed):
     finally:
         lib2.femb200_destroy(h2)
     full = [x.double().cpu().numpy() for x in list(dr.dRdv) + list(dr.PC)]
-    print(f"seed {seed} {precision}: {shared} of {case.mesh.nels} elements took their phase's shared Jacobian")
+    print(f"seed {seed} {precision} copied geometry {copy_geometry}: {shared} of {case.mesh.nels} elements took "
+          "their phase's shared Jacobian")
     assert shared > 0
-    rtol = 1e-13 if precision == "fp64" else 2e-6
+    rtol = 1e-13 if precision == "fp64" else 5e-6
     for g, f in zip(got, full):
         np.testing.assert_allclose(g, f, rtol=rtol, atol=rtol * np.abs(f).max())
     if precision == "fp64":
