@@ -469,9 +469,11 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
         CK(cudaStreamSynchronize(h->stream));
         a.diag_geometry = *h->h_flag == 0;
     }
-    // one-phase cells: the elastic element Jacobian of each phase is computed once (on
-    // the phase's first element) and shared by every elastic element with the same inputs
-    const bool shared = p->dim == 3 && h->jac_shared && (!p->phases_v || p->phases_v_layout == FEMB200_PHASE_CELL);
+    // FP32 diagnostics (the mixed-precision solve) on one-phase cells: the elastic element
+    // Jacobian of each phase is computed once (on the phase's first element) and shared by
+    // every elastic element whose inputs match it
+    const bool shared = std::is_same<T, float>::value && p->dim == 3 && h->jac_shared &&
+                        (!p->phases_v || p->phases_v_layout == FEMB200_PHASE_CELL);
     RC(prof_begin(h, FEMB200_PROF_JACOBIAN));
     if (shared) {
         if (!h->d_jac_tmpl) {

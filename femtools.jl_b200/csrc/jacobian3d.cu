@@ -93,13 +93,14 @@ FEMB_D void jac_transpose(const Tab1D<T>& t, const T F[3][3][3], T* E, int m1, i
     __syncwarp();
 }
 
-// Input match of an element against its phase's shared Jacobian. FP64 diagnostics share
-// only bit-identical inputs, so an FP64 assembly equals the unshared one; the FP32
-// diagnostics of the mixed-precision solve accept inputs within 4e-7 relative (about 3
-// ulp): structured generators form J = Σ dN_a·x_a, whose last bits vary with the element's
-// position, and the FP32 assembly carries rounding of that order anyway.
-FEMB_D bool same_input(double g, double t) { return g == t; }
-FEMB_D bool same_input(float g, float t) { return fabsf(g - t) <= 4e-7f * fabsf(t); }
+// Input match of an element against its phase's shared Jacobian (FP32 diagnostics of the
+// mixed-precision solve): within 4e-7 of `scale` (about 3 ulp; structured generators form
+// J = Σ dN_a·x_a, whose last bits vary with the element's position, and the FP32 assembly
+// carries rounding of that order anyway). `scale` is the entry itself, or for J⁻¹ entries
+// the largest |J⁻¹| of the point (its off-diagonals carry rounding residues near zero on
+// axis-aligned cells).
+FEMB_D bool same_input(float g, float t, float scale) { return fabsf(g - t) <= 4e-7f * scale; }
+FEMB_D bool same_input(double g, double t, double) { return g == t; }
 
 // DIAG: every J⁻¹ is diagonal (axis-aligned boxes); the gradient and flux transforms
 // are one product per entry.
@@ -125,7 +126,9 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     const T EPS2 = eps2<T>();
     const T zero3[3] = {T(0), T(0), T(0)};
 
-    const bool build = a.tmpl_mode == JAC_TMPL_BUILD;
+    // the shared element Jacobians exist in the FP32 diagnostics (the mixed-precision solve)
+    constexpr bool SHARE = sizeof(T) == 4;
+    const bool build = SHARE && a.tmpl_mode == JAC_TMPL_BUILD;
     const int64_t stride = (int64_t)gridDim.x * wpb * 3;
     for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
         // building templates, slot k of the loop is phase k and its element pick[k]
@@ -277,19 +280,27 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
         // a warp whose three elements are elastic here and carry their phase template's
         // inputs bit for bit takes the template's rows (computed by this code on those inputs)
         bool shared = false;
-        if (a.tmpl_mode == JAC_TMPL_USE) {
+        if (SHARE && a.tmpl_mode == JAC_TMPL_USE) {
             bool mine = !act;
             if (act && uniform && p0 >= 0 && p0 < MAXPH) {
                 const JacTemplate<T>& tm = a.tmpl[p0];
                 bool ok = tm.valid != 0 && plam[0] == T(0) && plam[1] == T(0) && plam[2] == T(0) &&
-                          same_input(eta_pc, tm.eta_pc);
+                          same_input(eta_pc, tm.eta_pc, fabs(tm.eta_pc));
 #pragma unroll
-                for (int p = 0; p < 4; ++p) ok = ok && same_input(gam[p], tm.gam[p]) && same_input(MPl[p], tm.MP[p]);
+                for (int p = 0; p < 4; ++p)
+                    ok = ok && same_input(gam[p], tm.gam[p], fabs(tm.gam[p])) && same_input(MPl[p], tm.MP[p], fabs(tm.MP[p]));
 #pragma unroll
                 for (int qz = 0; qz < 3; ++qz) {
                     const int q = tidx(m1, m2, qz);
+                    T jmax = T(0);
+                    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-                    for (int r = 0; r < 11; ++r) ok = ok && same_input(GEO[q * 11 + r], tm.geo[q * 11 + r]);
+                        for (int r = 0; r < 9; ++r) jmax = fmax(jmax, fabs(tm.geo[q * 11 + r]));
+                    }
+#pragma unroll
+                    for (int r = 0; r < 11; ++r)
+                        ok = ok && same_input(GEO[q * 11 + r], tm.geo[q * 11 + r],
+                                              sizeof(T) == 4 && r < 9 ? jmax : fabs(tm.geo[q * 11 + r]));
                 }
                 mine = ok;
             }
@@ -300,7 +311,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
             }
         }
         T rows[3][3], diag[3][3];
-        if (shared) {
+        if (SHARE && shared) {
             if (act) {
                 const JacTemplate<T>& tm = a.tmpl[p0];
 #pragma unroll
@@ -432,7 +443,7 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
             }
         }
         }
-        if (act && build) {
+        if (SHARE && act && build) {
             JacTemplate<T>& tm = a.tmpl[k];
 #pragma unroll
             for (int c = 0; c < 3; ++c)

@@ -276,12 +276,12 @@ struct H27JacArgs {
     int64_t nels;
     T dt;
     int diag_geometry;    // every J⁻¹ diagonal (the Hex27 kernel's DIAG specialisation)
-    // Shared element Jacobians (Hex27, one phase per cell): JAC_TMPL_BUILD computes, for
+    // Shared element Jacobians (Hex27 FP32 diagnostics, one phase per cell): JAC_TMPL_BUILD computes, for
     // the element pick[p] of each phase p, the diagnostics of its elastic linearisation
     // and its inputs into tmpl[p]; JAC_TMPL_USE lets a warp whose three elements are
     // all elastic at the current state and whose inputs equal their phase's template
-    // take the template's rows instead of the 81 columns (the same code on the same
-    // inputs: bit for bit in FP64; within 4e-7 relative in FP32, jacobian3d.cu same_input).
+    // take the template's rows instead of the 81 columns (the same code on inputs equal
+    // within 4e-7 relative, jacobian3d.cu same_input).
     int tmpl_mode;
     struct JacTemplate<T>* tmpl;
     const int32_t* pick;

@@ -1,14 +1,13 @@
 """Shared elastic element Jacobians in the Hex27 Jacobian diagnostics
 (assemble_augmented_momentum_jacobian_matrices_atomix!, momentum_residuals.jl:998-1117).
 
-With one phase per cell, the library computes the diagnostics of one element per
-phase from its elastic linearisation and lets every element that is elastic at the
-current state and has the same inputs (geometry, γP, M_P, η_pc, phase) take that
-element's rows instead of its own 81 columns: inputs bit for bit equal in FP64, within
-4e-7 relative in the FP32 diagnostics of the mixed-precision solve. The assembly must
-then equal the one without sharing (a handle created with FEMB200_JAC_SHARED=0) up to
-the atomic scatter order in FP64 and to FP32 rounding in FP32, and the oracle within
-the parity tolerance."""
+In the FP32 diagnostics of the mixed-precision solve, with one phase per cell, the
+library computes the diagnostics of one element per phase from its elastic
+linearisation and lets every element that is elastic at the current state and has the
+same inputs within 4e-7 relative (geometry, γP, M_P, η_pc, phase) take that element's
+rows instead of its own 81 columns. The assembly must then equal the one without
+sharing (a handle created with FEMB200_JAC_SHARED=0) to FP32 rounding, and the oracle
+within the FP32 parity tolerance. FP64 diagnostics never share."""
 import ctypes as C
 import os
 
@@ -47,7 +46,7 @@ def _case(seed, copy_geometry):
     return case
 
 
-@pytest.mark.parametrize("precision,copy_geometry", [("fp64", True), ("fp32", False), ("fp32", True)])
+@pytest.mark.parametrize("precision,copy_geometry", [("fp64", False), ("fp32", False), ("fp32", True)])
 @pytest.mark.parametrize("seed", [0, 4])
 def test_shared_jacobians_equal_the_full_assembly(precision, copy_geometry, seed):
     case = _case(seed, copy_geometry)
@@ -71,13 +70,13 @@ def test_shared_jacobians_equal_the_full_assembly(precision, copy_geometry, seed
     full = [x.double().cpu().numpy() for x in list(dr.dRdv) + list(dr.PC)]
     print(f"seed {seed} {precision} copied geometry {copy_geometry}: {shared} of {case.mesh.nels} elements took "
           "their phase's shared Jacobian")
-    assert shared > 0
+    assert (shared > 0) == (precision == "fp32")
     rtol = 1e-13 if precision == "fp64" else 5e-6
     for g, f in zip(got, full):
         np.testing.assert_allclose(g, f, rtol=rtol, atol=rtol * np.abs(f).max())
-    if precision == "fp64":
-        hs = case.host_state(oh)
-        hs.pressure_scaling(50.0, case.dt)
-        hs.jacobian_diagnostics(case.dt)
-        for g, r in zip(got, hs.dRdv + hs.PC):
-            np.testing.assert_allclose(g, r, rtol=1e-9, atol=1e-9 * np.abs(r).max())
+    hs = case.host_state(oh)
+    hs.pressure_scaling(50.0, case.dt)
+    hs.jacobian_diagnostics(case.dt)
+    tol = 1e-9 if precision == "fp64" else 2e-5
+    for g, r in zip(got, hs.dRdv + hs.PC):
+        np.testing.assert_allclose(g, r, rtol=tol, atol=tol * np.abs(r).max())
