@@ -60,6 +60,12 @@ struct femb200_handle {
     void* d_jac_tmpl = nullptr;
     int32_t* d_jac_pick = nullptr;
     int jac_shared = 1;   // FEMB200_JAC_SHARED=0 at creation turns the shared Jacobians off
+    // the diagonal-J⁻¹ test of the Jacobian diagnostics, valid for one public call (the
+    // geometry cannot change inside a solve): the call's serial and the geometry it tested
+    int64_t call_serial = 0;
+    int64_t geo_diag_serial = -1;
+    const void* geo_diag_ptr = nullptr;
+    int geo_diag = 0;
     // compressed affine geometry (one J⁻¹, |det J| per element), rebuilt per call
     void* d_geo_c = nullptr;
     size_t geo_c_cap = 0;
@@ -463,11 +469,16 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
             CK(cudaMalloc(&h->d_flag, sizeof(int)));
             CK(cudaMallocHost(&h->h_flag, sizeof(int)));
         }
-        CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-        CK(launch_geo_offdiag<TG>(a.geo_v, p->nels, h->d_flag, h->stream));
-        CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        a.diag_geometry = *h->h_flag == 0;
+        if (h->geo_diag_serial != h->call_serial || h->geo_diag_ptr != a.geo_v) {
+            CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+            CK(launch_geo_offdiag<TG>(a.geo_v, p->nels, h->d_flag, h->stream));
+            CK(cudaMemcpyAsync(h->h_flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            h->geo_diag = *h->h_flag == 0;
+            h->geo_diag_serial = h->call_serial;
+            h->geo_diag_ptr = a.geo_v;
+        }
+        a.diag_geometry = h->geo_diag;
     }
     // FP32 diagnostics (the mixed-precision solve) on one-phase cells: the elastic element
     // Jacobian of each phase is computed once (on the phase's first element) and shared by
@@ -1808,6 +1819,7 @@ int femb200_apply_dirichlet(femb200_handle* h, void* x, const int32_t* dofs, con
 
 int femb200_jacobian_diagnostics(femb200_handle* h, const femb200_stokes_problem* p, double dt, int32_t finite_K) {
     RC(check_problem(h, p));
+    ++h->call_serial;
     RC(upload_material(h, p->mat, finite_K, dt));
     return dispatch<DoJacobian>(p, h, p, dt);
 }
@@ -1836,6 +1848,7 @@ int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p, con
     RC(check_problem(h, p));
     RC(check_controls(h, c));
     if (!st) { h->err = "null stats"; return FEMB200_EINVAL; }
+    ++h->call_serial;
     RC(dispatch<DoSolve>(p, h, p, c, st, (Coupled*)nullptr));
     return finish_solve(h, c, st);
 }
@@ -2182,6 +2195,7 @@ int femb200_solve_stokes_adjoint(femb200_handle* h, const femb200_stokes_problem
     RC(check_adjoint_problem(h, p));
     RC(check_controls(h, c));
     if (!st || !objective_v || !lam_v || !lam_P) { h->err = "objective, λ and stats are required"; return FEMB200_EINVAL; }
+    ++h->call_serial;
     RC(solve_adjoint_impl(h, p, c, objective_v, lam_v, lam_P, st));
     if (c->throw_on_failure && !st->converged) {
         char b[160];
@@ -2265,6 +2279,7 @@ int femb200_solve_coupled(femb200_handle* h, femb200_thermal_problem* t, const f
     RC(check_controls(h, c));
     if (!t || !st) { h->err = "thermal problem and stats are required"; return FEMB200_EINVAL; }
     if (t->nnodes != p->nnodes) { h->err = "thermal mesh nodes must match the Stokes velocity-node layout"; return FEMB200_EINVAL; }
+    ++h->call_serial;
     if (t->dtype != p->dtype) { h->err = "thermal and Stokes states must share a precision"; return FEMB200_EINVAL; }
     if (shear_heating && !phi_scratch) { h->err = "shear heating needs an nq × nels scratch array"; return FEMB200_EINVAL; }
     const int64_t ntr = (int64_t)p->np * p->nels;

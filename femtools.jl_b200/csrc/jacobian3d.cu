@@ -497,10 +497,18 @@ __global__ void geo_offdiag_kernel(const TG* geo_v, int64_t npts, int* flag) {
 
 namespace {
 __global__ void jac_pick_kernel(const int32_t* phv, int64_t nels, int32_t* pick) {
+    // the block's lowest element per phase in shared memory, then one global atomic per
+    // phase and block (all elements of a phase contend on one word otherwise)
+    __shared__ int32_t smin[MAXPH];
+    for (int t = threadIdx.x; t < MAXPH; t += blockDim.x) smin[t] = JAC_NO_PICK;
+    __syncthreads();
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nels; e += (int64_t)gridDim.x * blockDim.x) {
         const int p = phv ? phv[e] - 1 : 0;
-        if (p >= 0 && p < MAXPH && e < JAC_NO_PICK) atomicMin(pick + p, (int32_t)e);
+        if (p >= 0 && p < MAXPH && e < JAC_NO_PICK) atomicMin(smin + p, (int32_t)e);
     }
+    __syncthreads();
+    for (int t = threadIdx.x; t < MAXPH; t += blockDim.x)
+        if (smin[t] != JAC_NO_PICK) atomicMin(pick + t, smin[t]);
 }
 }  // namespace
 

@@ -97,11 +97,12 @@ def test_adjoint_solve_matches_dense_oracle_adjoint():
     hs.gammaP[:] = dr.gammaP.cpu().numpy()
     hs.M_P[:] = dr.M_P.cpu().numpy()
     rl_v, rl_P = dense_adjoint(hs, ac.case.dt, obj, ac.case.bc)
-    assert rel(lam_v, rl_v) < 1e-6, rel(lam_v, rl_v)
-    assert rel([lam_P], [rl_P]) < 1e-6, rel([lam_P], [rl_P])
     sens = hs.viscosity_sensitivity(ac.case.dt, rl_v, rl_P)
     rgrad = (ac.eta_ip() * sens).reshape(hs.mesh.nels, hs.mesh.nq).sum(axis=1)
-    assert rel([grad], [rgrad]) < 1e-6
+    errs = (rel(lam_v, rl_v), rel([lam_P], [rl_P]), rel([grad], [rgrad]))
+    print(f"adjoint vs dense oracle adjoint: λv {errs[0]:.2e}, λP {errs[1]:.2e}, gradient {errs[2]:.2e}")
+    # the adjoint DR solve runs to 1e-12; its FP64 error against the direct solve is far below 1e-8
+    assert max(errs) < 1e-8, errs
 
 
 def test_adjoint_gradient_matches_central_differences():
