@@ -35,7 +35,7 @@ METRIC = "time-to-1e-8 residual, 3D Q2 Stokes 64³: chosen vs plain FP64 DR; HBM
 PATH_64 = {"iterations": 12300, "itPH": 89, "jacobian_assemblies": 124, "check_interval": 100}
 # DRAM bytes read + written by one launch of the chosen method's hot kernel at 64³,
 # from the ncu capture summarised in profiles/hex27_incr_kernel_vep64.md.
-TRAFFIC = {(64, "mixed"): 299135488}
+TRAFFIC = {(64, "mixed"): 127167488}
 
 
 def load_package():
@@ -404,13 +404,14 @@ def warmstart_mode(args, fem):
     res = fem.warmstart.shear_band_warm_start(n=args.n, nsteps=args.ws_steps, ntrain=args.ws_train,
                                               epochs=args.ws_epochs, seed=args.seed, tolerance=args.tolerance,
                                               check_interval=args.check_interval, online_steps=args.ws_online,
+                                              online_batch=args.ws_online_batch,
                                               log=(lambda r: rows_out.append(r)))
     test = [r for r in res["rows"] if "learned_iter" in r]
     mean = lambda k: float(np.mean([r[k] for r in test])) if test else None
     tot = lambda k: float(np.sum([r[k] for r in test])) if test else None
     line = {
         "mode": "warmstart", "workload": f"shear-band-q9-{args.n}^2", "n": args.n, "steps": args.ws_steps,
-        "check_interval": args.check_interval, "online_adam_steps": args.ws_online,
+        "check_interval": args.check_interval, "online_adam_steps": args.ws_online, "online_batch": args.ws_online_batch,
         "online_train_ms_mean": mean("online_train_ms") if args.ws_online else 0.0,
         "train_steps": args.ws_train, "epochs": args.ws_epochs, "train_ms": res["train_ms"],
         "train_loss_first_last": [res["train_loss"][0], res["train_loss"][-1]] if res["train_loss"] else None,
@@ -910,6 +911,7 @@ def main():
     ap.add_argument("--ws-train", type=int, default=50)
     ap.add_argument("--ws-epochs", type=int, default=300)
     ap.add_argument("--ws-online", type=int, default=0, help="Adam steps on the newest converged pairs per solved step")
+    ap.add_argument("--ws-online-batch", type=int, default=4)
     ap.add_argument("--tl-steps", type=int, default=10)
     ap.add_argument("--n2d", type=int, default=0, help="parity mode: size of the 2-D inclusion case (0: skip)")
     ap.add_argument("--oracle2d", default="", help="parity mode: .npz of the 2-D oracle solve (read, or written "
@@ -1102,8 +1104,9 @@ def main():
 
     peak, peak_kind = measured_peaks()
     mixed = args.precision == "mixed"
-    nbytes = incremental_kernel_bytes(case, stress_reads) if mixed else residual_kernel_bytes(case, itemsize=8,
-                                                                                              geo_itemsize=8)
+    # the survey's counting rule for one fused element pass (every array the sweep must touch,
+    # once, at its stored precision): FP32 for the chosen method's sweep, FP64 for the plain one
+    nbytes = residual_kernel_bytes(case, itemsize=4 if mixed else 8, geo_itemsize=4 if mixed else 8)
     res_avg_ms = prof_ms[0] / max(prof_n[0], 1)
     achieved = nbytes / (res_avg_ms / 1e3) / 1e9
     traffic = TRAFFIC.get((args.n, args.precision))
@@ -1139,8 +1142,9 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": res_avg_ms,
                          "launches": int(prof_n[0]), "peak_kind": peak_kind,
-                         "base_stress_reads_per_launch": stress_reads if mixed else None,
-                         "bytes_if_every_point_read_its_stress": incremental_kernel_bytes(case) if mixed else None},
+                         "bytes_rule": "fused element pass, stored precision, affine geometry (SURVEY 8d rule)",
+                         "kernel_read_bytes_per_launch": incremental_kernel_bytes(case, stress_reads) if mixed else None,
+                         "base_stress_reads_per_launch": stress_reads if mixed else None},
             "kernel_ms": {"residual": prof_ms[0], "jacobian": prof_ms[1], "node_update": prof_ms[2],
                           "outer_fp64_sweeps": prof_ms[4], "profiled_solve": ms_profiled},
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -292,6 +292,11 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     // point is read only where the elastic bound below does not settle the point
     float preF[3] = {0.0f, 0.0f, 0.0f};
     unsigned stress_reads = 0;
+    // Where yielding is possible (some lane of the warp needed a point's trial stress in
+    // the previous row) the next row's trial stresses are loaded a row ahead too, so that
+    // plastic regions do not wait on them point by point; elastic regions load none.
+    float preT[3][6] = {};
+    bool preT_ok = false, warp_plastic = false;
     const uint64_t pol = l2_evict_first();
     if (plastic) load_row_F(preF, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane, pol);
     ElemData cur;
@@ -364,6 +369,9 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                 const int rnext = 3 * qz + qy + 1;
                 const float* next_row = rnext < 9 ? a.base_t + (tile * 27 + 3 * rnext) * BASE_FIELDS * 32 + lane
                                                   : (has_next ? a.base_t + tnext * 27 * BASE_FIELDS * 32 + lane : nullptr);
+                // warp-uniform: the previous row needed a trial stress somewhere in the warp
+                const bool fetch = plastic && next_row && warp_plastic;
+                bool row_needed = false;
                 // η-contraction of the row: X = Σ_j L_j(η) W0, Y = Σ_j L'_j(η) W0, Z = Σ_j L_j(η) W1
                 float X[3][3], Y[3][3], Z[3][3];
 #pragma unroll
@@ -453,6 +461,14 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                     if (plastic) {
                         const float Fk = preF[qx];
                         if (next_row) preF[qx] = ldg_stream(next_row + (qx * BASE_FIELDS + 6) * 32, pol);
+                        float tbp[6];
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) tbp[c] = preT[qx][c];
+                        if (fetch) {
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) preT[qx][c] = ldg_stream(next_row + (qx * BASE_FIELDS + c) * 32, pol);
+                            stress_reads += act ? 1u : 0u;
+                        }
                         // Elastic bound: τII = sqrt(‖τ‖² + ε²) is 1-Lipschitz in the J2 norm
                         // ‖τ‖² = ½Σ τ_ii² + Σ_{i<j} τ_ij², so the trial yield value satisfies
                         // F(τb + δτ) ≤ F_k + ‖δτ‖ + sinϕ·|δP|. Where that bound (with a 1e-3
@@ -467,10 +483,16 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
 #pragma unroll
                             for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
                         } else {
-                        stress_reads += act ? 1u : 0u;
+                        row_needed = true;
                         float tb[6];
+                        if (preT_ok) {
 #pragma unroll
-                        for (int c = 0; c < 6; ++c) tb[c] = ldg_stream(cur_row + (qx * BASE_FIELDS + c) * 32, pol);
+                            for (int c = 0; c < 6; ++c) tb[c] = tbp[c];
+                        } else {
+                            stress_reads += act ? 1u : 0u;
+#pragma unroll
+                            for (int c = 0; c < 6; ++c) tb[c] = ldg_stream(cur_row + (qx * BASE_FIELDS + c) * 32, pol);
+                        }
                         const float Jk = 0.5f * (tb[0] * tb[0] + tb[1] * tb[1] + tb[2] * tb[2]) + tb[3] * tb[3] +
                                          tb[4] * tb[4] + tb[5] * tb[5];
                         if (Jk < 1e-6f * M.cC * M.cC) {
@@ -513,6 +535,8 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
 #pragma unroll
                     for (int i = 0; i < 3; ++i) Ab[i] = cfma(Lb(qx, i), bq, Ab[i]);
                 }
+                preT_ok = fetch;
+                warp_plastic = __any_sync(0xffffffffu, row_needed);
                 // contract the row over η: U0 += L_j(η) (A − g_c Ab) + L'_j(η) B, U1 += L_j(η) C
 #pragma unroll
                 for (int c = 0; c < 3; ++c)

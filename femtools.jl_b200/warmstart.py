@@ -300,7 +300,7 @@ def extrapolate_state(dr, bc_v, vprev, vcur, Pprev, Pcur):
 
 
 def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tolerance=1e-8, check_interval=100,
-                          log=None, online_gain=True, gain_window=5, online_steps=0, replay=8):
+                          log=None, online_gain=True, gain_window=5, online_steps=0, replay=8, online_batch=4):
     """The learned-warm-start experiment on the 2-D shear-band time loop.
 
     Steps 1..ntrain run plain DR (each from the previous step's solution) and record
@@ -310,7 +310,8 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
     the network's correction; the trajectory continues with the plain solution, so
     all three see identical histories. With `online_steps` > 0 the network keeps
     training after every solved step: that many Adam steps on the newest `replay`
-    pairs of the converged history, their time charged to the network's arm.
+    pairs of the converged history in batches of `online_batch`, their time charged to
+    the network's arm.
     Returns per-step iteration counts and times."""
     from . import configs
     case = configs.shear_band_2d_case(n=n, seed=seed)
@@ -393,7 +394,7 @@ def shear_band_warm_start(n=256, nsteps=200, ntrain=50, epochs=200, seed=0, tole
             e0.record()
             pairs.append((net.make_input(F[-3], F[-2]), net.make_target(F[-3], F[-2], F[-1])))
             pairs = pairs[-replay:]
-            net.train_online(pairs, H, W, steps=online_steps)
+            net.train_online(pairs, H, W, steps=online_steps, batch=online_batch)
             e1.record()
             torch.cuda.synchronize()
             row["online_train_ms"] = e0.elapsed_time(e1)
