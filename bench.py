@@ -703,6 +703,61 @@ def _mean_free(P, M):
     return P - float(np.sum(P * M) / np.sum(M))
 
 
+def field_subsample(case, seed=1234):
+    """Seeded index sets into the concatenated v (3·nnodes), P (nnodesP) and τ (6·27·nels)
+    of a 3-D case: up to 50 000, 50 000 and 100 000 entries, the same on every host."""
+    m = case.mesh
+    rng = np.random.default_rng(seed)
+    pick = lambda n, k: np.sort(rng.choice(n, size=min(n, k), replace=False))
+    return {"v": pick(3 * m.nnodes, 50_000), "P": pick(m.nnodesP, 50_000), "tau": pick(6 * m.nq * m.nels, 100_000)}
+
+
+def oracle_time_loop(args, fem):
+    """The oracle's time loop of the layered case (P0 ← P, τ_old ← τ between steps), saved
+    after every step to --oracle3d: per-step statistics and wall time, and the fields on the
+    seeded subsample (P also without its M_P-weighted mean)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_host as oh
+    case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
+    hs = case.host_state(oh)
+    sub = field_subsample(case)
+    kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
+              max_iterations=args.max_iterations, iter_max=args.max_iterations)
+    name, nproc = cpu_model()
+    meta = {"n": args.n, "seed": args.seed, "tolerance": args.tolerance, "check_interval": args.check_interval,
+            "host": {"cpu_model": name, "nproc": nproc, "oracle_threads": oh.lib().orc_num_threads()}, "steps": []}
+    arrays = {}
+    for step in range(args.tl_steps):
+        t0 = time.perf_counter()
+        st = hs.solve(**kw)
+        sec = time.perf_counter() - t0
+        hs.store_stress(case.dt)
+        v, P, tau = np.concatenate(hs.v), hs.P.copy(), np.concatenate(hs.tau)
+        Pmf = P - float(np.sum(P * hs.M_P) / np.sum(hs.M_P))
+        meta["steps"].append({"stats": {k: st[k] for k in ("iter", "itPH", "jacobian_assemblies", "converged", "err")},
+                              "seconds": sec})
+        arrays.update({f"v{step}": v[sub["v"]], f"P{step}": P[sub["P"]], f"Pmf{step}": Pmf[sub["P"]],
+                       f"tau{step}": tau[sub["tau"]]})
+        np.savez(args.oracle3d, meta=json.dumps(meta), **arrays)
+        print(json.dumps({"oracle_step": step + 1, **meta["steps"][-1]}), flush=True)
+        hs.P0[:] = hs.P
+        for c in range(6):
+            hs.tau_old[c][:] = hs.tau[c]
+    return 0
+
+
+def load_oracle_steps(args):
+    z = np.load(args.oracle3d, allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    if meta["n"] != args.n or meta["tolerance"] != args.tolerance or meta["check_interval"] != args.check_interval:
+        raise SystemExit(f"{args.oracle3d} holds another configuration: {meta}")
+    if len(meta["steps"]) < args.tl_steps:
+        raise SystemExit(f"{args.oracle3d} holds {len(meta['steps'])} steps, {args.tl_steps} asked")
+    steps = [dict(m, v=z[f"v{k}"], P=z[f"P{k}"], P_mean_free=z[f"Pmf{k}"], tau=z[f"tau{k}"])
+             for k, m in enumerate(meta["steps"])]
+    return {"steps": steps, "host": meta["host"]}
+
+
 def parity_mode(args, fem):
     """Parity at the configurations' own sizes, against the FP64 oracle on all host cores.
 
@@ -735,9 +790,12 @@ def parity_mode(args, fem):
     if args.n > 0:
         case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
         bc = case.bc_device()
-        d64, dmx, hs = case.device_state(), case.device_state(), case.host_state(oh)
+        d64, dmx = case.device_state(), case.device_state()
         kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
                   max_iterations=args.max_iterations, iter_max=args.max_iterations)
+        saved = load_oracle_steps(args) if args.oracle3d else None
+        hs = None if saved else case.host_state(oh)
+        sub = field_subsample(case) if saved else None
         # warm-up of the device code paths on a copy, so the timed solves carry no first-launch costs
         warm = case.device_state()
         fem.solve(warm, bc, **dict(kw, max_iterations=200, iter_max=200))
@@ -747,43 +805,62 @@ def parity_mode(args, fem):
         for step in range(args.tl_steps):
             s64, t64 = gpu_solve(d64, bc, **kw)
             smx, tmx = gpu_solve(dmx, bc, precision="mixed", **kw)
-            t0 = time.perf_counter()
-            sor = hs.solve(**kw)
-            tor = time.perf_counter() - t0
             fem.update_stokes_current_stress(d64, case.dt)
             fem.update_stokes_current_stress(dmx, case.dt)
-            hs.store_stress(case.dt)
             torch.cuda.synchronize()
             host = lambda dr: {"v": np.concatenate([x.cpu().numpy() for x in dr.v]), "P": dr.P.cpu().numpy(),
                                "tau": np.concatenate([x.cpu().numpy() for x in dr.tau])}
-            ref = {"v": np.concatenate(hs.v), "P": hs.P.copy(), "tau": np.concatenate(hs.tau)}
-            row = {"step": step + 1, "oracle": {k: sor[k] for k in keys}, "oracle_s": tor}
+            if saved:
+                o = saved["steps"][step]
+                row = {"step": step + 1, "oracle": o["stats"], "oracle_s": o["seconds"],
+                       "compared_on": {k: int(len(v)) for k, v in sub.items()}}
+            else:
+                t0 = time.perf_counter()
+                sor = hs.solve(**kw)
+                tor = time.perf_counter() - t0
+                hs.store_stress(case.dt)
+                ref = {"v": np.concatenate(hs.v), "P": hs.P.copy(), "tau": np.concatenate(hs.tau)}
+                row = {"step": step + 1, "oracle": {k: sor[k] for k in keys}, "oracle_s": tor}
             for label, dr, st, t in (("gpu_fp64", d64, s64, t64), ("gpu_mixed", dmx, smx, tmx)):
                 f = host(dr)
                 row[label] = {k: st[k] for k in keys}
                 row[label]["seconds"] = t
-                row[label]["rel_err_vs_oracle"] = {
-                    "v": _rel(f["v"], ref["v"]), "P": _rel(f["P"], ref["P"]),
-                    "P_mean_free": _rel(_mean_free(f["P"], hs.M_P), _mean_free(ref["P"], hs.M_P)),
-                    "tau": _rel(f["tau"], ref["tau"])}
+                if saved:
+                    o = saved["steps"][step]
+                    M = dr.M_P.cpu().numpy()
+                    Pmf = f["P"] - float(np.sum(f["P"] * M) / np.sum(M))
+                    row[label]["rel_err_vs_oracle"] = {
+                        "v": _rel(f["v"][sub["v"]], o["v"]), "P": _rel(f["P"][sub["P"]], o["P"]),
+                        "P_mean_free": _rel(Pmf[sub["P"]], o["P_mean_free"]), "tau": _rel(f["tau"][sub["tau"]], o["tau"])}
+                else:
+                    row[label]["rel_err_vs_oracle"] = {
+                        "v": _rel(f["v"], ref["v"]), "P": _rel(f["P"], ref["P"]),
+                        "P_mean_free": _rel(_mean_free(f["P"], hs.M_P), _mean_free(ref["P"], hs.M_P)),
+                        "tau": _rel(f["tau"], ref["tau"])}
             steps.append(row)
             print(json.dumps({"parity_step": row}), flush=True)
-            # the time-step driver: P0 ← P, τ_old ← τ on all three
+            # the time-step driver: P0 ← P, τ_old ← τ
             for dr in (d64, dmx):
                 dr.P0.copy_(dr.P)
                 for c in range(6):
                     dr.tau_old[c].copy_(dr.tau[c])
-            hs.P0[:] = hs.P
-            for c in range(6):
-                hs.tau_old[c][:] = hs.tau[c]
-        first = steps[0]["oracle"]
-        path = {"iterations": first["iter"], "itPH": first["itPH"], "jacobian_assemblies": first["jacobian_assemblies"],
-                "check_interval": args.check_interval}
-        # the extrapolation model on the same workload, priced along the oracle's own path of step 1
-        est, cores, sample = cpu_baseline_estimate(fem.configs.vep_layers_case(n=args.n, seed=args.seed), path, steps=3)
-        out["vep3d"] = {"workload": f"vep-layers-hex27-{args.n}^3 x {args.tl_steps} steps", "steps": steps,
-                        "cpu_model_check": {"measured_s": steps[0]["oracle_s"], "extrapolated_s": est,
-                                            "model_error": est / steps[0]["oracle_s"] - 1.0, "sample": sample}}
+            if hs is not None:
+                hs.P0[:] = hs.P
+                for c in range(6):
+                    hs.tau_old[c][:] = hs.tau[c]
+        out["vep3d"] = {"workload": f"vep-layers-hex27-{args.n}^3 x {args.tl_steps} steps", "steps": steps}
+        if saved:
+            out["vep3d"]["oracle_host"] = saved["host"]
+            out["vep3d"]["comparison"] = "relative L2 on seeded subsamples of the fields (field_subsample)"
+        else:
+            first = steps[0]["oracle"]
+            path = {"iterations": first["iter"], "itPH": first["itPH"],
+                    "jacobian_assemblies": first["jacobian_assemblies"], "check_interval": args.check_interval}
+            # the extrapolation model on the same workload, priced along the oracle's own path of step 1
+            est, cores, sample = cpu_baseline_estimate(fem.configs.vep_layers_case(n=args.n, seed=args.seed), path,
+                                                       steps=3)
+            out["vep3d"]["cpu_model_check"] = {"measured_s": steps[0]["oracle_s"], "extrapolated_s": est,
+                                               "model_error": est / steps[0]["oracle_s"] - 1.0, "sample": sample}
     if args.n2d > 0:
         case = fem.configs.inclusion_2d_case(n=args.n2d)
         kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=50, throw_on_failure=False,
@@ -916,13 +993,18 @@ def main():
     ap.add_argument("--n2d", type=int, default=0, help="parity mode: size of the 2-D inclusion case (0: skip)")
     ap.add_argument("--oracle2d", default="", help="parity mode: .npz of the 2-D oracle solve (read, or written "
                     "with --oracle-only)")
-    ap.add_argument("--oracle-only", action="store_true", help="parity mode: run and save the 2-D oracle solve only")
+    ap.add_argument("--oracle-only", action="store_true", help="parity mode: run and save the oracle's solves only")
+    ap.add_argument("--oracle3d", default="", help="parity mode: .npz of the 3-D oracle time loop (read, or written "
+                    "with --oracle-only)")
     ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap",
                              "parity"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "parity" and args.oracle_only and args.oracle3d:
+        # the CPU half of the 3-D time-loop parity check, on a host without a GPU
+        return oracle_time_loop(args, load_package())
     if args.mode == "parity" and args.oracle_only:
         # the CPU half of the 2-D parity check, on a host without a GPU
         fem = load_package()

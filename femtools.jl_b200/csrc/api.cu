@@ -60,6 +60,12 @@ struct femb200_handle {
     void* d_jac_tmpl = nullptr;
     int32_t* d_jac_pick = nullptr;
     int jac_shared = 1;   // FEMB200_JAC_SHARED=0 at creation turns the shared Jacobians off
+    // points of the FP32 sweeps that failed the elastic bound since the last check (device
+    // and pinned host word), and the sweep variant chosen from it: 1 = trial stresses
+    // prefetched row by row (regions that yield), 0 = read on demand (elastic regions)
+    unsigned long long* d_bound = nullptr;
+    unsigned long long* h_bound = nullptr;
+    int incr_pre = 0;
     // the diagonal-J⁻¹ test of the Jacobian diagnostics, valid for one public call (the
     // geometry cannot change inside a solve): the call's serial and the geometry it tested
     int64_t call_serial = 0;
@@ -1010,6 +1016,14 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     for (int k = 0; k < 3; ++k) { at.dv[k] = m.dv[k]; at.R[k] = m.R[k]; at.g[k] = (float)p->mat.g[k]; }
     at.dP = m.dP; at.RPinc = m.RPinc;
     at.stress_reads = h->prof ? h->d_counters + FEMB200_COUNTER_STRESS_READS : nullptr;
+    if (!h->d_bound) {
+        CK(cudaMalloc(&h->d_bound, sizeof(unsigned long long)));
+        CK(cudaMallocHost(&h->h_bound, sizeof(unsigned long long)));
+    }
+    CK(cudaMemsetAsync(h->d_bound, 0, sizeof(unsigned long long), s));
+    at.bound_failures = h->d_bound;
+    at.prefetch_stress = h->incr_pre;
+    int64_t sweeps_since_check = 0;
     at.nels = p->nels;
     at.plastic = p->mat.plastic;
     {
@@ -1056,6 +1070,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
         if (!prefilled)
             for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
         RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
+        ++sweeps_since_check;
         if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s));
         else CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
         RC(prof_end(h, FEMB200_PROF_RESIDUAL));
@@ -1175,7 +1190,18 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             RC(prof_end(h, FEMB200_PROF_NODE));
             if (do_check) {
                 double sr[RED_SLOTS];
+                // the elastic-bound failures of the sweeps since the last check travel with
+                // the check's own synchronisation
+                CK(cudaMemcpyAsync(h->h_bound, h->d_bound, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
                 RC(fetch_sums(h, nb, RED_SLOTS, sr));
+                if (thread_sweep && sweeps_since_check > 0) {
+                    // prefetch the trial stresses while more than 1e-3 of the points need them
+                    const double pts = (double)sweeps_since_check * 27.0 * (double)p->nels;
+                    h->incr_pre = (double)*h->h_bound > 1e-3 * pts ? 1 : 0;
+                    at.prefetch_stress = h->incr_pre;
+                    CK(cudaMemsetAsync(h->d_bound, 0, sizeof(unsigned long long), s));
+                    sweeps_since_check = 0;
+                }
                 double ev = 0, cmp[3] = {0, 0, 0};
                 for (int k = 0; k < D; ++k) { ev = jl_max(ev, std::sqrt(sr[3 * k])); cmp[k] = std::sqrt(sr[3 * k]) / (2 * sq_nn); }
                 ev /= 2 * sq_nn;
@@ -1752,6 +1778,8 @@ int femb200_destroy(femb200_handle* h) {
     if (h->d_flag) cudaFree(h->d_flag);
     if (h->h_flag) cudaFreeHost(h->h_flag);
     if (h->d_counters) cudaFree(h->d_counters);
+    if (h->d_bound) cudaFree(h->d_bound);
+    if (h->h_bound) cudaFreeHost(h->h_bound);
     if (h->d_jac_tmpl) cudaFree(h->d_jac_tmpl);
     if (h->d_jac_pick) cudaFree(h->d_jac_pick);
     if (h->mixed.mem) cudaFree(h->mixed.mem);

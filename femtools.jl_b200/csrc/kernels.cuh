@@ -99,8 +99,13 @@ struct IncrArgs {
     float g[3];
     IncrPhase ph[MAXPH];
     // when set (profiling), the number of (element, point) pairs whose base trial stress
-    // the sweep read, i.e. that the elastic bound did not settle, is added here
+    // the sweep read is added here
     unsigned long long* stress_reads;
+    // when set, the number of (element, point) pairs the elastic bound did not settle
+    unsigned long long* bound_failures;
+    // load every row's base trial stresses a row ahead (regions that yield) instead of
+    // reading them on demand where the bound fails (elastic regions)
+    int prefetch_stress;
 };
 // Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
 // copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.

@@ -253,7 +253,7 @@ FEMB_D void read_elem(const IncrArgs& a, int64_t tile, int lane, const float* S,
 
 // DIAG: every element's J⁻¹ is diagonal (axis-aligned boxes, the structured
 // generators' meshes), so the gradient and flux transforms are one product per entry.
-template <bool DIAG>
+template <bool DIAG, bool PRE>
 __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArgs a) {
     extern __shared__ float in_smem[];
     __shared__ IncrPhase PT[MAXPH];
@@ -292,12 +292,22 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     // point is read only where the elastic bound below does not settle the point
     float preF[3] = {0.0f, 0.0f, 0.0f};
     unsigned stress_reads = 0;
-    // Where yielding is possible (some lane of the warp needed a point's trial stress in
-    // the previous row) the next row's trial stresses are loaded a row ahead too, so that
-    // plastic regions do not wait on them point by point; elastic regions load none.
+    unsigned needed = 0;
+    // PRE (regions that yield): the trial stresses of the current row's points, loaded a
+    // row ahead like the yield values; without PRE they are read on demand where the
+    // elastic bound fails
     float preT[3][6] = {};
-    bool preT_ok = false, warp_plastic = false;
     const uint64_t pol = l2_evict_first();
+    if constexpr (PRE) {
+        if (plastic) {
+            const float* row0 = a.base_t + tile * 27 * BASE_FIELDS * 32 + lane;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) preT[j][c] = ldg_stream(row0 + (j * BASE_FIELDS + c) * 32, pol);
+            stress_reads += tile * 32 + lane < a.nels ? 3u : 0u;
+        }
+    }
     if (plastic) load_row_F(preF, a.base_t + tile * 27 * BASE_FIELDS * 32 + lane, pol);
     ElemData cur;
     load_elem<DIAG>(a, tile, lane, nslots, cur);
@@ -369,9 +379,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                 const int rnext = 3 * qz + qy + 1;
                 const float* next_row = rnext < 9 ? a.base_t + (tile * 27 + 3 * rnext) * BASE_FIELDS * 32 + lane
                                                   : (has_next ? a.base_t + tnext * 27 * BASE_FIELDS * 32 + lane : nullptr);
-                // warp-uniform: the previous row needed a trial stress somewhere in the warp
-                const bool fetch = plastic && next_row && warp_plastic;
-                bool row_needed = false;
+                const bool fetch = PRE && plastic && next_row;
                 // η-contraction of the row: X = Σ_j L_j(η) W0, Y = Σ_j L'_j(η) W0, Z = Σ_j L_j(η) W1
                 float X[3][3], Y[3][3], Z[3][3];
 #pragma unroll
@@ -483,9 +491,9 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
 #pragma unroll
                             for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
                         } else {
-                        row_needed = true;
+                        needed += act ? 1u : 0u;
                         float tb[6];
-                        if (preT_ok) {
+                        if constexpr (PRE) {
 #pragma unroll
                             for (int c = 0; c < 6; ++c) tb[c] = tbp[c];
                         } else {
@@ -535,8 +543,6 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
 #pragma unroll
                     for (int i = 0; i < 3; ++i) Ab[i] = cfma(Lb(qx, i), bq, Ab[i]);
                 }
-                preT_ok = fetch;
-                warp_plastic = __any_sync(0xffffffffu, row_needed);
                 // contract the row over η: U0 += L_j(η) (A − g_c Ab) + L'_j(η) B, U1 += L_j(η) C
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
@@ -621,6 +627,12 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
         if (lane == 0 && n) atomicAdd(a.stress_reads, (unsigned long long)n);
     }
+    if (a.bound_failures) {
+        unsigned n = needed;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+        if (lane == 0 && n) atomicAdd(a.bound_failures, (unsigned long long)n);
+    }
 }
 
 std::mutex g_inc_mutex;
@@ -642,12 +654,12 @@ cudaError_t launch_incr_tiles(const IncrTileSrc& src, int64_t nels, const IncrAr
             host_pnum_table(K);
             err = cudaMemcpyToSymbol(c_inc_K, K, sizeof(K));
             if (err != cudaSuccess) return err;
-            err = cudaFuncSetAttribute(hex27_incr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
-            if (err != cudaSuccess) return err;
-            err = cudaFuncSetAttribute(hex27_incr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
-            if (err != cudaSuccess) return err;
+            for (auto fn : {hex27_incr_kernel<false, false>, hex27_incr_kernel<true, false>, hex27_incr_kernel<false, true>,
+                            hex27_incr_kernel<true, true>}) {
+                err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           IN_WARPS * IN_SLOTS * 32 * (int)sizeof(float));
+                if (err != cudaSuccess) return err;
+            }
             g_inc_ready[dev] = true;
         }
     }
@@ -674,16 +686,16 @@ cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n
 cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
     const size_t smem = (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float);
     const int64_t ntiles = (a.nels + 31) / 32;
+    auto fn = a.diag_geometry ? (a.prefetch_stress ? hex27_incr_kernel<true, true> : hex27_incr_kernel<true, false>)
+                              : (a.prefetch_stress ? hex27_incr_kernel<false, true> : hex27_incr_kernel<false, false>);
     int per_sm = 2;
-    if (a.diag_geometry) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel<true>, IN_THREADS, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel<false>, IN_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, IN_THREADS, smem);
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (ntiles + IN_WARPS - 1) / IN_WARPS;
     blocks = std::min<int64_t>(blocks, (int64_t)num_sms * per_sm);
     if (blocks < 1) blocks = 1;
     count_launch();
-    if (a.diag_geometry) hex27_incr_kernel<true><<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
-    else hex27_incr_kernel<false><<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
+    fn<<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
