@@ -63,7 +63,7 @@ struct femb200_handle {
     // points of the FP32 sweeps that failed the elastic bound since the last check (device
     // and pinned host word), and the sweep variant chosen from it: 1 = trial stresses
     // prefetched row by row (regions that yield), 0 = read on demand (elastic regions)
-    unsigned long long* d_bound = nullptr;
+    unsigned long long* d_bound = nullptr;   // [0] bound failures, [1] bulk-copy wait failures of the FP32 sweep
     unsigned long long* h_bound = nullptr;
     int incr_pre = 0;
     // the diagonal-J⁻¹ test of the Jacobian diagnostics, valid for one public call (the
@@ -1017,11 +1017,12 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     at.dP = m.dP; at.RPinc = m.RPinc;
     at.stress_reads = h->prof ? h->d_counters + FEMB200_COUNTER_STRESS_READS : nullptr;
     if (!h->d_bound) {
-        CK(cudaMalloc(&h->d_bound, sizeof(unsigned long long)));
-        CK(cudaMallocHost(&h->h_bound, sizeof(unsigned long long)));
+        CK(cudaMalloc(&h->d_bound, 2 * sizeof(unsigned long long)));
+        CK(cudaMallocHost(&h->h_bound, 2 * sizeof(unsigned long long)));
     }
-    CK(cudaMemsetAsync(h->d_bound, 0, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(h->d_bound, 0, 2 * sizeof(unsigned long long), s));
     at.bound_failures = h->d_bound;
+    at.err_flag = reinterpret_cast<int*>(h->d_bound + 1);
     at.prefetch_stress = h->incr_pre;
     int64_t sweeps_since_check = 0;
     at.nels = p->nels;
@@ -1192,8 +1193,12 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
                 double sr[RED_SLOTS];
                 // the elastic-bound failures of the sweeps since the last check travel with
                 // the check's own synchronisation
-                CK(cudaMemcpyAsync(h->h_bound, h->d_bound, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+                CK(cudaMemcpyAsync(h->h_bound, h->d_bound, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
                 RC(fetch_sums(h, nb, RED_SLOTS, sr));
+                if (h->h_bound[1] != 0) {
+                    h->err = "the FP32 sweep gave up waiting for a bulk copy of its tile data";
+                    return FEMB200_ECUDA;
+                }
                 if (thread_sweep && sweeps_since_check > 0) {
                     // prefetch the trial stresses while more than 1e-3 of the points need them
                     const double pts = (double)sweeps_since_check * 27.0 * (double)p->nels;

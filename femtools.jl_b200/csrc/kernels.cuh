@@ -106,6 +106,7 @@ struct IncrArgs {
     // load every row's base trial stresses a row ahead (regions that yield) instead of
     // reading them on demand where the bound fails (elastic regions)
     int prefetch_stress;
+    int* err_flag;   // set (to 1) when a bulk-copy wait of the sweep gave up; its warp then stops
 };
 // Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
 // copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.

@@ -144,6 +144,34 @@ FEMB_D void cp_async4(float* dst, const float* src) {
 FEMB_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 FEMB_D void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Bulk copies (sm_90+ cp.async.bulk, one thread issues, completion counted in bytes on an
+// mbarrier) of the contiguous per-tile blocks: this GPU's global memory to the CTA's own
+// shared memory, no multicast.
+FEMB_D uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+FEMB_D void mbar_init(uint32_t m) { asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m) : "memory"); }
+// orders this thread's earlier shared-memory accesses before later bulk-copy writes
+FEMB_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+FEMB_D void mbar_expect(uint32_t m, unsigned bytes) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(m), "r"(bytes)
+                 : "memory");
+}
+FEMB_D void bulk_load(uint32_t dst, const void* src, unsigned bytes, uint32_t m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(m)
+                 : "memory");
+}
+// Waits until the barrier's phase `parity` has completed: at most 2^20 try_wait rounds,
+// each suspended for a bounded, implementation-defined time; false when it gave up.
+FEMB_D bool mbar_wait(uint32_t m, unsigned parity) {
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 20) && !done; ++it)
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done)
+                     : "r"(m), "r"(parity)
+                     : "memory");
+    return done != 0;
+}
+
 // Inputs and output of the FP64 return near the yield-surface apex, passed by value
 // so that the caller's arrays stay in registers on the common (FP32) path.
 struct ApexIn {
@@ -219,47 +247,45 @@ FEMB_D void load_elem(const IncrArgs& a, int64_t tile, int lane, int64_t nslots,
     d.phP = __ldg(a.phase_t + nslots + e);
 }
 
-// The next tile's per-element data into a thread's slots 31.. (slot s at S[s * 32]):
-// J⁻¹ (its diagonal when DIAG), det J, the two phase indices and, for linear pressure
-// numbering, δP at the element's four pressure DoFs.
-template <bool DIAG>
-FEMB_D void load_elem_async(const IncrArgs& a, int64_t tile, int lane, int64_t nslots, float* S) {
-    const int64_t e = tile * 32 + lane;
-    const float* gt = a.geo_t + tile * 10 * 32 + lane;
-    int s = 31;
-#pragma unroll
-    for (int r = 0; r < 9; ++r)
-        if (!DIAG || r % 4 == 0) cp_async4(S + (s++) * 32, gt + r * 32);
-    cp_async4(S + (s++) * 32, gt + 9 * 32);
-    cp_async4(S + (s++) * 32, reinterpret_cast<const float*>(a.phase_t + e));
-    cp_async4(S + (s++) * 32, reinterpret_cast<const float*>(a.phase_t + nslots + e));
+// The next tile's per-element data in a thread's slots 31.. (slot s at S[s * 32]): the
+// tile's ten geometry rows (J⁻¹ column-major, then |det J|) at 31..40 and its two phase
+// rows at 41, 42 arrive by bulk copy; for linear pressure numbering δP at the element's
+// four pressure DoFs goes to 43..46 by per-thread cp.async (its rows are element-major).
+FEMB_D void load_elem_dP_async(const IncrArgs& a, int64_t tile, int lane, float* S) {
     if (a.dofs_linear) {
 #pragma unroll
-        for (int p = 0; p < 4; ++p) cp_async4(S + (s + p) * 32, a.dP + elem_dof(a, tile, lane, p));
+        for (int p = 0; p < 4; ++p) cp_async4(S + (43 + p) * 32, a.dP + elem_dof(a, tile, lane, p));
     }
 }
 
 template <bool DIAG>
 FEMB_D void read_elem(const IncrArgs& a, int64_t tile, int lane, const float* S, ElemData& d) {
-    int s = 31;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) d.Ji[r] = (!DIAG || r % 4 == 0) ? S[(s++) * 32] : 0.0f;
-    d.detJ = S[(s++) * 32];
-    d.ph = __float_as_int(S[(s++) * 32]);
-    d.phP = __float_as_int(S[(s++) * 32]);
+    for (int r = 0; r < 9; ++r) d.Ji[r] = (!DIAG || r % 4 == 0) ? S[(31 + r) * 32] : 0.0f;
+    d.detJ = S[40 * 32];
+    d.ph = __float_as_int(S[41 * 32]);
+    d.phP = __float_as_int(S[42 * 32]);
 #pragma unroll
-    for (int p = 0; p < 4; ++p) d.dP[p] = a.dofs_linear ? S[(s + p) * 32] : __ldg(a.dP + elem_dof(a, tile, lane, p));
+    for (int p = 0; p < 4; ++p) d.dP[p] = a.dofs_linear ? S[(43 + p) * 32] : __ldg(a.dP + elem_dof(a, tile, lane, p));
 }
 
 // DIAG: every element's J⁻¹ is diagonal (axis-aligned boxes, the structured
 // generators' meshes), so the gradient and flux transforms are one product per entry.
 template <bool DIAG, bool PRE>
 __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArgs a) {
-    extern __shared__ float in_smem[];
+    extern __shared__ __align__(128) float in_smem[];
     __shared__ IncrPhase PT[MAXPH];
+    __shared__ __align__(8) uint64_t mbar_all[IN_WARPS];
     for (int t = threadIdx.x; t < MAXPH; t += blockDim.x) PT[t] = a.ph[t];
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t mbar = smem_addr(mbar_all + warp);
+    if (lane == 0) mbar_init(mbar);
+    fence_proxy_async();
+    __syncthreads();
+    unsigned mphase = 0;   // parity of the warp's barrier phase the next wait completes
+    // shared addresses of the warp's slot 0 (lane 0 first) and of its plane slots
+    const uint32_t sV = smem_addr(in_smem) + (uint32_t)(warp * IN_SLOTS * 32 * 4);
+    const uint32_t sWS = sV + 162 * 32 * 4;
     float* V = in_smem + (size_t)warp * IN_SLOTS * 32 + lane;   // slot s at V[s * 32]
     int* Vi = reinterpret_cast<int*>(V);
     float* RS = V + 81 * 32;
@@ -342,10 +368,14 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
             // the δv slots are free from here on: the next tile's connectivity goes
             // into the first 27 of them
             if (qz == 2 && has_next) {
-                const int32_t* nd = a.el2n_t + tnext * 27 * 32 + lane;
-#pragma unroll
-                for (int k = 0; k < 27; ++k) cp_async4(reinterpret_cast<float*>(Vi + k * 32), reinterpret_cast<const float*>(nd + k * 32));
-                cp_async_commit();
+                // every lane has read its δv slots: one bulk copy of the next tile's 27
+                // connectivity rows (3 456 B) into slots 0..26 of the warp
+                fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_expect(mbar, 27 * 32 * 4);
+                    bulk_load(sV, a.el2n_t + tnext * 27 * 32, 27 * 32 * 4, mbar);
+                }
             }
             // plane accumulators; the body-force term −g_c β carries the same L_k(ζ)
             // factor as the ξ/η fluxes and is folded into U0
@@ -359,7 +389,11 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                 if (qz == 2 && qy == 1 && has_next) {
                     // the connectivity has landed: gather the next tile's δv (slot k is
                     // read before the copy that overwrites it is issued)
-                    cp_async_wait_all();
+                    if (!__all_sync(0xffffffffu, mbar_wait(mbar, mphase))) {
+                        if (lane == 0) atomicExch(a.err_flag, 1);
+                        return;
+                    }
+                    mphase ^= 1u;
 #pragma unroll 9
                     for (int k = 0; k < 27; ++k) {
                         const int n = Vi[k * 32];
@@ -425,12 +459,22 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                         // the plane slots were last read by this row's η-contraction, whose
                         // values the first point consumed: the scatter's node indices and
                         // pressure scales go there, in flight during the last two points
-                        const int32_t* ndc = a.el2n_t + tile * 27 * 32 + lane;
-#pragma unroll
-                        for (int k = 0; k < 27; ++k) cp_async4(WS + k * 32, reinterpret_cast<const float*>(ndc + k * 32));
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) cp_async4(WS + (27 + p) * 32, a.pscale_t + (tile * 4 + p) * 32 + lane);
-                        if (has_next) load_elem_async<DIAG>(a, tnext, lane, nslots, WS);
+                        // bulk copies: the tile's connectivity (slots 0..26) and pressure
+                        // scales (27..30), the next tile's geometry rows (31..40) and phase
+                        // rows (41, 42); δP per thread
+                        fence_proxy_async();
+                        __syncwarp();
+                        if (lane == 0) {
+                            mbar_expect(mbar, (27 + 4) * 32 * 4 + (has_next ? 12 * 32 * 4 : 0));
+                            bulk_load(sWS, a.el2n_t + tile * 27 * 32, 27 * 32 * 4, mbar);
+                            bulk_load(sWS + 27 * 128, a.pscale_t + tile * 4 * 32, 4 * 32 * 4, mbar);
+                            if (has_next) {
+                                bulk_load(sWS + 31 * 128, a.geo_t + tnext * 10 * 32, 10 * 32 * 4, mbar);
+                                bulk_load(sWS + 41 * 128, a.phase_t + tnext * 32, 32 * 4, mbar);
+                                bulk_load(sWS + 42 * 128, a.phase_t + nslots + tnext * 32, 32 * 4, mbar);
+                            }
+                        }
+                        if (has_next) load_elem_dP_async(a, tnext, lane, WS);
                         cp_async_commit();
                     }
                     // physical gradient ∂δv_c/∂x_k = Σ_d gr[c][d] ∂ξ_d/∂x_k
@@ -570,6 +614,11 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
         }
         // ---- pressure residual and Pnum increments (element-local) ----
         cp_async_wait_all();
+        if (!__all_sync(0xffffffffu, mbar_wait(mbar, mphase))) {
+            if (lane == 0) atomicExch(a.err_flag, 1);
+            return;
+        }
+        mphase ^= 1u;
         float Pn[4];
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
