@@ -300,6 +300,76 @@ def sweep_mode(args, fem, case, dr, lib, h):
     return 0
 
 
+def scatter_order_mode(args, fem, case, dr, lib, h):
+    """The FP32 sweep's ordered scatter (one launch per tile colour) against its atomic
+    scatter on the mixed-precision solve: per-sweep time, whole-solve time, iterations, and
+    whether two solves of each kind repeat each other's path and fields."""
+    import torch
+    stream = torch.cuda.current_stream()
+    init = {"v": [x.clone() for x in dr.v], "P": dr.P.clone(), "P0": dr.P0.clone(),
+            "tau_old": [x.clone() for x in dr.tau_old]}
+
+    def reset():
+        for c in range(3):
+            dr.v[c].copy_(init["v"][c])
+        dr.P.copy_(init["P"])
+        dr.P0.copy_(init["P0"])
+        for c in range(6):
+            dr.tau_old[c].copy_(init["tau_old"][c])
+
+    kw = dict(dt=case.dt, tolerance=args.tolerance, check_interval=args.check_interval, throw_on_failure=False,
+              max_iterations=args.max_iterations, iter_max=args.max_iterations, precision="mixed")
+    bc = case.bc_device()
+    out = {"mode": "scatter-order", "n": args.n, "tolerance": args.tolerance}
+    fields = {}
+
+    def rel(x, y):
+        return _rel(x.double().cpu().numpy(), y.double().cpu().numpy())
+
+    try:
+        for ordered in (0, 1):
+            assert lib.femb200_set_ordered_scatter(h, ordered) == fem._abi.OK
+            name = "ordered" if ordered else "atomic"
+            reset()
+            fem.solve(dr, bc, **kw)   # warm-up
+            runs = []
+            for rep in range(2):
+                reset()
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                ev0.record(stream)
+                st = fem.solve(dr, bc, **kw)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                fem.update_stokes_current_stress(dr, case.dt)
+                f = {"v": torch.cat([x.clone() for x in dr.v]), "P": dr.P.clone(),
+                     "tau": torch.cat([x.clone() for x in dr.tau])}
+                fields[(name, rep)] = f
+                runs.append({"s": ev0.elapsed_time(ev1) / 1e3, "iterations": st["iter"], "itPH": st["itPH"],
+                             "err": st["err"]})
+            # per-sweep time from one more solve with events around every sweep
+            lib.femb200_profile(h, 1)
+            reset()
+            fem.solve(dr, bc, **kw)
+            prof_ms = (C.c_double * fem._abi.PROF_COUNT)()
+            prof_n = (C.c_int64 * fem._abi.PROF_COUNT)()
+            lib.femb200_profile_read(h, prof_ms, prof_n)
+            lib.femb200_profile(h, 0)
+            same = all(torch.equal(fields[(name, 0)][k], fields[(name, 1)][k]) for k in ("v", "P", "tau"))
+            out[name] = {"runs": runs, "sweep_ms": prof_ms[0] / max(prof_n[0], 1), "sweeps": int(prof_n[0]),
+                         "residual_ms_total": prof_ms[0], "jacobian_ms": prof_ms[1], "node_update_ms": prof_ms[2],
+                         "outer_fp64_ms": prof_ms[4], "two_runs_bitwise_equal": bool(same),
+                         "two_runs_rel_diff": {k: rel(fields[(name, 0)][k], fields[(name, 1)][k])
+                                                   for k in ("v", "P", "tau")}}
+    finally:
+        lib.femb200_set_ordered_scatter(h, 0)
+    out["ordered_vs_atomic_rel_diff"] = {k: rel(fields[("ordered", 0)][k], fields[("atomic", 0)][k])
+                                         for k in ("v", "P", "tau")}
+    out["sweep_cost"] = out["ordered"]["sweep_ms"] / out["atomic"]["sweep_ms"] - 1.0
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def adjoint_mode(args, fem):
     """Adjoint workload (coupled thermal–Stokes forward with shear heating on a Hex27 n³
     mesh, T-dependent viscosity η = exp(−0.1·T)·exp(δ_e)): the coupled forward solve,
@@ -997,7 +1067,7 @@ def main():
     ap.add_argument("--oracle3d", default="", help="parity mode: .npz of the 3-D oracle time loop (read, or written "
                     "with --oracle-only)")
     ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap",
-                             "parity"],
+                             "parity", "scatter-order"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -1055,6 +1125,8 @@ def main():
     lib, h = fem.solver._Handle.get()
     if args.mode == "sweep":
         return sweep_mode(args, fem, case, dr, lib, h)
+    if args.mode == "scatter-order":
+        return scatter_order_mode(args, fem, case, dr, lib, h)
     # device-resident initial state of every step
     init = {"v": [x.clone() for x in dr.v], "P": dr.P.clone(), "P0": dr.P0.clone(),
             "tau_old": [x.clone() for x in dr.tau_old]}

@@ -179,6 +179,7 @@ SIGNATURES = {
     "femb200_create": (C.c_int, [_P(_vp)]),
     "femb200_destroy": (C.c_int, [_vp]),
     "femb200_set_stream": (C.c_int, [_vp, _vp]),
+    "femb200_set_ordered_scatter": (C.c_int, [_vp, C.c_int32]),
     "femb200_last_error": (C.c_char_p, [_vp]),
     "femb200_version": (C.c_char_p, []),
     "femb200_pressure_residual": (C.c_int, [_vp, _P(StokesProblemC), C.c_double, C.c_int32]),

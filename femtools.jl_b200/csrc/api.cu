@@ -66,6 +66,18 @@ struct femb200_handle {
     unsigned long long* d_bound = nullptr;   // [0] bound failures, [1] bulk-copy wait failures of the FP32 sweep
     unsigned long long* h_bound = nullptr;
     int incr_pre = 0;
+    // ordered scatter of the FP32 sweep (femb200_set_ordered_scatter): the tiles sorted by
+    // colour (no two tiles of a colour share a node) and the start of each colour
+    int ordered_scatter = 0;
+    int32_t* d_tile_list = nullptr;
+    size_t tile_list_cap = 0;
+    std::vector<int64_t> tile_colour_start;
+    // the warp groups (three consecutive elements) of the pipelined sweep and the Jacobian
+    // diagnostics, sorted by colour, and the start of each colour
+    int32_t* d_group_list = nullptr;
+    size_t group_list_cap = 0;
+    std::vector<int64_t> group_colour_start;
+    bool ordered_active = false;   // set inside a mixed solve with the ordered scatter
     // the diagonal-J⁻¹ test of the Jacobian diagnostics, valid for one public call (the
     // geometry cannot change inside a solve): the call's serial and the geometry it tested
     int64_t call_serial = 0;
@@ -412,7 +424,16 @@ int launch_residual(femb200_handle* h, const femb200_stokes_problem* p, const H2
         H27Args<T, T> b;
         std::memcpy(&b, &a, sizeof(b));   // identical layout; the pipelined sweep reads geometry from d_geo_c
         b.geo_v = nullptr; b.geo_P = nullptr;
-        CK(launch_hex27_residual_pipe<T>(b, static_cast<const T*>(h->d_geo_c), h->num_sms, h->stream));
+        if (h->ordered_active) {
+            // one launch per colour of warp groups, in colour order
+            for (size_t c = 0; c + 1 < h->group_colour_start.size(); ++c) {
+                b.group_list = h->d_group_list + h->group_colour_start[c];
+                b.group_count = h->group_colour_start[c + 1] - h->group_colour_start[c];
+                CK(launch_hex27_residual_pipe<T>(b, static_cast<const T*>(h->d_geo_c), h->num_sms, h->stream));
+            }
+        } else {
+            CK(launch_hex27_residual_pipe<T>(b, static_cast<const T*>(h->d_geo_c), h->num_sms, h->stream));
+        }
     } else if (p->dim == 3) {
         CK(launch_hex27_residual<T, TG>(a, h->num_sms, h->stream));
     } else {
@@ -511,8 +532,17 @@ int jacobian_sweep(femb200_handle* h, const femb200_stokes_problem* p, double dt
         a.pick = b.pick;
         a.shared_count = h->prof ? h->d_counters + FEMB200_COUNTER_SHARED_JACOBIANS : nullptr;
     }
-    if (p->dim == 3) CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
-    else CK(launch_q9_jacobian<T, TG>(a, h->stream));
+    if (p->dim == 3 && h->ordered_active) {
+        for (size_t c = 0; c + 1 < h->group_colour_start.size(); ++c) {
+            a.group_list = h->d_group_list + h->group_colour_start[c];
+            a.group_count = h->group_colour_start[c + 1] - h->group_colour_start[c];
+            CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
+        }
+    } else if (p->dim == 3) {
+        CK(launch_hex27_jacobian<T, TG>(a, h->num_sms, h->stream));
+    } else {
+        CK(launch_q9_jacobian<T, TG>(a, h->stream));
+    }
     RC(prof_end(h, FEMB200_PROF_JACOBIAN));
     return FEMB200_OK;
 }
@@ -930,6 +960,82 @@ int ensure_mixed(femb200_handle* h, const femb200_stokes_problem* p) {
     return FEMB200_OK;
 }
 
+// Colours of the ordered scatter, for units of U consecutive elements (U = 32: the FP32
+// sweep's tiles; U = 3: the warp groups of the pipelined sweep and of the Jacobian
+// diagnostics), from the connectivity in tensor order (tn[27e + t], t = i + 3j + 9k,
+// 0-based). Greedy in unit order: a unit takes the lowest colour that no earlier unit
+// sharing one of its nodes holds. Inside a unit the kernels fold the ξ = −1 node of
+// line L (t = 3L) of element e + 1 into the ξ = +1 node (t = 3L + 2) of element e when
+// the two are one node; every other node of the unit must be distinct, so that within
+// one colour every node receives at most one addition. Returns the units sorted by
+// colour and the start of each colour (colours + 1 entries).
+int colour_units(femb200_handle* h, const std::vector<int32_t>& tn, int64_t nels, int64_t nnodes, int U,
+                 std::vector<int32_t>& order, std::vector<int64_t>& start) {
+    const int64_t nunits = (nels + U - 1) / U;
+    std::vector<uint64_t> used((size_t)nnodes, 0);
+    std::vector<int64_t> seen((size_t)nnodes, -1);
+    std::vector<int32_t> colour((size_t)nunits);
+    std::vector<int32_t> nodes;
+    nodes.reserve((size_t)27 * U);
+    int ncol = 0;
+    for (int64_t u = 0; u < nunits; ++u) {
+        nodes.clear();
+        uint64_t mask = 0;
+        for (int64_t e = u * U; e < std::min<int64_t>((u + 1) * U, nels); ++e)
+            for (int t = 0; t < 27; ++t) {
+                const int32_t n = tn[(size_t)(27 * e + t)];
+                if (n < 0 || n >= nnodes) {
+                    h->err = "ordered scatter: node index out of range in the connectivity";
+                    return FEMB200_EINVAL;
+                }
+                if (t % 3 == 0 && e > u * U && tn[(size_t)(27 * (e - 1) + t + 2)] == n) continue;
+                if (seen[(size_t)n] == u) {
+                    h->err = "ordered scatter needs consecutive elements whose only shared nodes are the ξ faces of "
+                             "neighbouring elements within each unit of " + std::to_string(U) +
+                             " elements (element " + std::to_string(e + 1) + " repeats a node of its unit)";
+                    return FEMB200_EUNSUPPORTED;
+                }
+                seen[(size_t)n] = u;
+                mask |= used[(size_t)n];
+                nodes.push_back(n);
+            }
+        if (~mask == 0) {
+            h->err = "ordered scatter: more than 64 colours";
+            return FEMB200_EUNSUPPORTED;
+        }
+        const int c = __builtin_ctzll(~mask);
+        colour[(size_t)u] = c;
+        ncol = std::max(ncol, c + 1);
+        for (int32_t n : nodes) used[(size_t)n] |= 1ull << c;
+    }
+    start.assign((size_t)ncol + 1, 0);
+    for (int64_t u = 0; u < nunits; ++u) ++start[(size_t)colour[(size_t)u] + 1];
+    for (int c = 0; c < ncol; ++c) start[(size_t)c + 1] += start[(size_t)c];
+    order.assign((size_t)nunits, 0);
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    for (int64_t u = 0; u < nunits; ++u) order[(size_t)fill[(size_t)colour[(size_t)u]]++] = (int32_t)u;
+    return FEMB200_OK;
+}
+
+// Uploads a unit order into a handle-owned device array, growing it when needed.
+int upload_order(femb200_handle* h, const std::vector<int32_t>& order, int32_t*& d, size_t& cap) {
+    if (cap < order.size()) {
+        if (d) CK(cudaFree(d));
+        d = nullptr;
+        cap = 0;
+        CK(cudaMalloc(&d, order.size() * sizeof(int32_t)));
+        cap = order.size();
+    }
+    CK(cudaMemcpyAsync(d, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    return FEMB200_OK;
+}
+
+// The handle's ordered-scatter state is valid for the duration of one solve.
+struct OrderedScope {
+    femb200_handle* h;
+    ~OrderedScope() { h->ordered_active = false; }
+};
+
 template <class TG>
 int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const femb200_stokes_controls* c,
                       femb200_stokes_stats* st) {
@@ -1061,6 +1167,32 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     const bool thread_sweep = (*h->h_flag & INCR_MIXED_PHASES) == 0 && h->use_incr_thread;
     at.dofs_linear = (*h->h_flag & INCR_DOFS_GENERAL) == 0;
     at.diag_geometry = (*h->h_flag & INCR_GEOMETRY_FULL) == 0;
+    // ordered scatter: every sweep and Jacobian assembly of this solve adds to each node
+    // at most once per launch (colours of tiles and of warp groups)
+    OrderedScope ordered_scope{h};
+    const bool ordered = h->ordered_scatter != 0;
+    if (ordered) {
+        if (!thread_sweep || !h->geo_c_valid) {
+            h->err = "ordered scatter needs the thread-per-element FP32 sweep and the pipelined FP64 sweep "
+                     "(one phase per cell, affine elements)";
+            return FEMB200_EUNSUPPORTED;
+        }
+        std::vector<int32_t> el2n_h((size_t)p->nels * 27);
+        CK(cudaMemcpyAsync(el2n_h.data(), p->el2n, el2n_h.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        int tn3[27];
+        for (int a3 = 0; a3 < 27; ++a3) tn3[(H27[a3][0] + 1) + 3 * (H27[a3][1] + 1) + 9 * (H27[a3][2] + 1)] = a3;
+        std::vector<int32_t> tn(el2n_h.size());
+        for (int64_t e = 0; e < p->nels; ++e)
+            for (int t = 0; t < 27; ++t) tn[(size_t)(27 * e + t)] = el2n_h[(size_t)(27 * e + tn3[t])] - 1;
+        std::vector<int32_t> order;
+        RC(colour_units(h, tn, p->nels, p->nnodes, 32, order, h->tile_colour_start));
+        RC(upload_order(h, order, h->d_tile_list, h->tile_list_cap));
+        RC(colour_units(h, tn, p->nels, p->nnodes, 3, order, h->group_colour_start));
+        RC(upload_order(h, order, h->d_group_list, h->group_list_cap));
+        CK(cudaStreamSynchronize(s));
+        h->ordered_active = true;
+    }
     // the thread-per-element sweep writes the increment of RP; RP itself is formed
     // where it is read (checks and the Powell–Hestenes pressure update)
     auto form_RP = [&]() -> int {
@@ -1072,7 +1204,17 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             for (int k = 0; k < D; ++k) CK(launch_copy<float>(m.R[k], m.Rk[k], nn, s));
         RC(prof_begin(h, FEMB200_PROF_RESIDUAL));
         ++sweeps_since_check;
-        if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s));
+        if (thread_sweep && ordered) {
+            // one launch per tile colour, in colour order: each node receives at most one
+            // addition per launch, so the increments do not depend on the atomics' order
+            for (size_t c = 0; c + 1 < h->tile_colour_start.size(); ++c) {
+                at.tile_list = h->d_tile_list + h->tile_colour_start[c];
+                at.tile_count = h->tile_colour_start[c + 1] - h->tile_colour_start[c];
+                CK(launch_hex27_incr(at, h->num_sms, s));
+            }
+            at.tile_list = nullptr;
+            at.tile_count = 0;
+        } else if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s));
         else CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
         RC(prof_end(h, FEMB200_PROF_RESIDUAL));
         return FEMB200_OK;
@@ -1787,6 +1929,8 @@ int femb200_destroy(femb200_handle* h) {
     if (h->h_bound) cudaFreeHost(h->h_bound);
     if (h->d_jac_tmpl) cudaFree(h->d_jac_tmpl);
     if (h->d_jac_pick) cudaFree(h->d_jac_pick);
+    if (h->d_tile_list) cudaFree(h->d_tile_list);
+    if (h->d_group_list) cudaFree(h->d_group_list);
     if (h->mixed.mem) cudaFree(h->mixed.mem);
     if (h->adj_mem) cudaFree(h->adj_mem);
     delete h;
@@ -1796,6 +1940,12 @@ int femb200_destroy(femb200_handle* h) {
 int femb200_set_stream(femb200_handle* h, void* stream) {
     if (!h) return FEMB200_EINVAL;
     h->stream = static_cast<cudaStream_t>(stream);
+    return FEMB200_OK;
+}
+
+int femb200_set_ordered_scatter(femb200_handle* h, int32_t on) {
+    if (!h) return FEMB200_EINVAL;
+    h->ordered_scatter = on != 0;
     return FEMB200_OK;
 }
 

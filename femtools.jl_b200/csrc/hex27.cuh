@@ -23,6 +23,26 @@ constexpr int H27_ELEM_SMEM = 540;   // scalars of stage scratch per element
 
 FEMB_D int tidx(int i, int j, int k) { return i + 3 * j + 9 * k; }
 
+// Ordered scatter of a warp's three elements (lane s·9 + m owns the x-line (·, m1, m2) of
+// element s; lanes 27..31 idle): where element s + 1's ξ = −1 node of the line is element
+// s's ξ = +1 node (consecutive elements along ξ), lane (s, m) adds that lane's node-0
+// values into its node-2 values, so the group adds to such a node once. Returns whether
+// this lane's node 0 went to the previous element's lane. Every lane of the warp calls it.
+template <class T>
+FEMB_D bool fold_next_element(const int node[3], bool act, int s, T (&R)[3][3]) {
+    const int lane = threadIdx.x & 31;
+    const int n0n = __shfl_down_sync(0xffffffffu, node[0], 9);
+    const int actn = __shfl_down_sync(0xffffffffu, (int)act, 9);
+    const bool fold = s < 2 && act && actn && n0n == node[2];
+    const bool folded = __shfl_up_sync(0xffffffffu, (int)fold, 9) && lane >= 9;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const T v0n = __shfl_down_sync(0xffffffffu, R[c][0], 9);
+        if (fold) R[c][2] += v0n;
+    }
+    return folded;
+}
+
 // Layouts of the stage buffers. A buffer holds blocks of one 3×3×3 grid; it is written
 // along one line orientation and read along another. Buffers of the first kind (the
 // gradient's x-stage, the transpose's y-stage) use l1 in blocks of K1 words, those of

@@ -129,8 +129,12 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
     // the shared element Jacobians exist in the FP32 diagnostics (the mixed-precision solve)
     constexpr bool SHARE = sizeof(T) == 4;
     const bool build = SHARE && a.tmpl_mode == JAC_TMPL_BUILD;
-    const int64_t stride = (int64_t)gridDim.x * wpb * 3;
-    for (int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3; base < a.nels; base += stride) {
+    // work item gk is group gk (three elements), or the gk-th group of the launch's list
+    const bool listed = a.group_list != nullptr && !build;
+    const int64_t gstride = (int64_t)gridDim.x * wpb;
+    const int64_t ngroups = listed ? a.group_count : (a.nels + 2) / 3;
+    for (int64_t gk = (int64_t)blockIdx.x * wpb + warp; gk < ngroups; gk += gstride) {
+        const int64_t base = listed ? 3 * (int64_t)__ldg(a.group_list + gk) : 3 * gk;
         // building templates, slot k of the loop is phase k and its element pick[k]
         const int64_t k = base + (lane_ok ? s : 0);
         const bool picked = build && k < MAXPH && a.pick[k] >= 0 && a.pick[k] < a.pick_nels;
@@ -465,14 +469,23 @@ __global__ void __launch_bounds__(JAC_THREADS) hex27_jacobian_kernel(H27JacArgs<
                 // only a one-phase element is a template; the flag is read by a later launch
                 tm.valid = uniform ? 1 : 0;
             }
-        } else if (act) {
+        } else {
+            // ordered scatter: each node of the group receives one addition (hex27.cuh)
+            bool folded = false;
+            if (listed) {
+                folded = fold_next_element(node, act, s, rows);
+                fold_next_element(node, act, s, diag);
+            }
+            if (act) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    atomic_add(a.dRdv[c] + node[i], rows[c][i]);
-                    atomic_add(a.PC[c] + node[i], diag[c][i]);
-                }
+                    for (int i = 0; i < 3; ++i)
+                        if (i > 0 || !folded) {
+                            atomic_add(a.dRdv[c] + node[i], rows[c][i]);
+                            atomic_add(a.PC[c] + node[i], diag[c][i]);
+                        }
+            }
         }
         __syncwarp();
     }
@@ -541,7 +554,8 @@ cudaError_t launch_hex27_jacobian(const H27JacArgs<T, TG>& args, int num_sms, cu
         cudaFuncSetAttribute(hex27_jacobian_kernel<T, TG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
-    const int64_t groups = (args.nels + 2) / 3;
+    const int64_t groups = (args.group_list && args.tmpl_mode != JAC_TMPL_BUILD) ? args.group_count : (args.nels + 2) / 3;
+    if (groups < 1) return cudaSuccess;
     int64_t blocks = (groups + wpb - 1) / wpb;
     const int64_t cap = (int64_t)num_sms * 32;
     if (blocks > cap) blocks = cap;

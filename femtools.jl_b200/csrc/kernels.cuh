@@ -52,6 +52,10 @@ struct H27Args {
     float* base_out;
     const float* base_in;
     const T* RP_base;
+    // the element groups this launch processes, in order (group g is elements 3g … 3g + 2;
+    // one colour of the ordered scatter, pipelined sweep only), or null for every group
+    const int32_t* group_list;
+    int64_t group_count;
 };
 
 template <class T, class TG>
@@ -107,6 +111,10 @@ struct IncrArgs {
     // reading them on demand where the bound fails (elastic regions)
     int prefetch_stress;
     int* err_flag;   // set (to 1) when a bulk-copy wait of the sweep gave up; its warp then stops
+    // the tiles this launch processes, in order (one colour of the ordered scatter), or
+    // null for every tile
+    const int32_t* tile_list;
+    int64_t tile_count;
 };
 // Builds el2n_t, dofs_t, geo_t (from the compressed per-element geometry FP32
 // copy), phase_t, pscale_t and, if eta is given (e·27 + q layout), eta_t of dst.
@@ -293,6 +301,9 @@ struct H27JacArgs {
     const int32_t* pick;
     int64_t pick_nels;    // element count of the mesh the picks index (bound of every pick)
     unsigned long long* shared_count;   // when set (profiling): elements that took a template
+    // as H27Args::group_list (Hex27; not read when building templates)
+    const int32_t* group_list;
+    int64_t group_count;
 };
 enum { JAC_TMPL_OFF = 0, JAC_TMPL_USE = 1, JAC_TMPL_BUILD = 2 };
 // fill of the pick array before launch_jac_pick (a byte-wise memset of 0x7f)

@@ -294,10 +294,14 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     const float EPS2 = (float)eps2<double>();
     const int64_t ntiles = (a.nels + 31) >> 5;
     const int64_t nslots = ntiles * 32;
-    const int64_t tstride = (int64_t)gridDim.x * IN_WARPS;
+    const int tstride = (int)gridDim.x * IN_WARPS;
     const bool plastic = a.plastic != 0;
-    int64_t tile = (int64_t)blockIdx.x * IN_WARPS + warp;
-    if (tile >= ntiles) return;
+    // work item wk is tile wk, or the wk-th tile of the launch's list (32-bit: 2^31 tiles
+    // would be 2^36 elements, more than a GPU's memory holds connectivity for)
+    const int nwork = (int)(a.tile_list ? a.tile_count : ntiles);
+    int wk = (int)blockIdx.x * IN_WARPS + warp;
+    if (wk >= nwork) return;
+    int64_t tile = a.tile_list ? __ldg(a.tile_list + wk) : wk;
 
     // Software pipeline across tiles: the next tile's connectivity (cp.async) and
     // δv gather (cp.async, indexed by it) run during the last quadrature plane, its
@@ -338,11 +342,11 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     ElemData cur;
     load_elem<DIAG>(a, tile, lane, nslots, cur);
 
-    for (; tile < ntiles; tile += tstride) {
+    for (; wk < nwork; wk += tstride) {
         const int64_t e = tile * 32 + lane;
         const bool act = e < a.nels;
-        const int64_t tnext = tile + tstride;
-        const bool has_next = tnext < ntiles;
+        const bool has_next = wk + tstride < nwork;
+        const int64_t tnext = !has_next ? 0 : a.tile_list ? __ldg(a.tile_list + wk + tstride) : wk + tstride;
         const IncrPhase M = PT[cur.ph];
         // storage term of the continuity residual: the phase of the pressure DoFs
         const float invbulkdt = PT[cur.phP].invbulkdt;
@@ -668,6 +672,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
             }
         }
         if (has_next) read_elem<DIAG>(a, tnext, lane, WS, cur);
+        tile = tnext;
     }
     cp_async_wait_all();
     if (a.stress_reads) {
@@ -734,7 +739,8 @@ cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n
 
 cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
     const size_t smem = (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float);
-    const int64_t ntiles = (a.nels + 31) / 32;
+    const int64_t ntiles = a.tile_list ? a.tile_count : (a.nels + 31) / 32;
+    if (ntiles < 1) return cudaSuccess;
     auto fn = a.diag_geometry ? (a.prefetch_stress ? hex27_incr_kernel<true, true> : hex27_incr_kernel<true, false>)
                               : (a.prefetch_stress ? hex27_incr_kernel<false, true> : hex27_incr_kernel<false, false>);
     int per_sm = 2;

@@ -204,12 +204,19 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
     const T EPS2 = INCR ? (T)eps2<double>() : eps2<T>();
     const bool nodal_phases = a.phv && a.phv_layout != FEMB200_PHASE_CELL;
 
-    const int64_t stride = (int64_t)gridDim.x * wpb * 3;
-    int64_t base = ((int64_t)blockIdx.x * wpb + warp) * 3;
+    // work item gk is group gk, or the gk-th group of the launch's list; its first element
+    // (a.nels past the end, which load_ids marks inactive)
+    const int64_t gstride = (int64_t)gridDim.x * wpb;
+    const int64_t ngroups = a.group_list ? a.group_count : (a.nels + 2) / 3;
+    auto group_base = [&](int64_t g) -> int64_t {
+        return g >= ngroups ? a.nels : a.group_list ? 3 * (int64_t)__ldg(a.group_list + g) : 3 * g;
+    };
+    int64_t gk = (int64_t)blockIdx.x * wpb + warp;
+    int64_t base = group_base(gk);
 
     // prologue: ids of the first two groups, loads of the first
     GroupIds id_cur = load_ids(a, base, s, m, tn_own, lane_ok);
-    GroupIds id_next = load_ids(a, base + stride, s, m, tn_own, lane_ok);
+    GroupIds id_next = load_ids(a, group_base(gk + gstride), s, m, tn_own, lane_ok);
     T vn[3][3];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -219,7 +226,7 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
     cp_commit();
     const bool do_qp = a.do_momentum || a.phi;
 
-    for (; base < a.nels; base += stride) {
+    for (; gk < ngroups; gk += gstride, base = group_base(gk)) {
         cp_wait_all();
         __syncwarp();
         T v[3][3];
@@ -481,18 +488,22 @@ __global__ void __launch_bounds__(PipeThreads<T>::value, 1) hex27_residual_pipe_
         }
         // every lane is done with this group's buffer: load the next group into it
         __syncwarp();
-        issue_prefetch<T, INCR>(a, geo_c, id_next, base + stride, s, m, m1, m2, BUF, vn);
+        issue_prefetch<T, INCR>(a, geo_c, id_next, group_base(gk + gstride), s, m, m1, m2, BUF, vn);
         cp_commit();
         id_cur = id_next;
-        id_next = load_ids(a, base + 2 * stride, s, m, tn_own, lane_ok);
+        id_next = load_ids(a, group_base(gk + 2 * gstride), s, m, tn_own, lane_ok);
         if (!a.do_momentum) continue;
         T R[3][3];
         h27_transpose<T, true, LY>(tb, g, beta_q, gvec, E, m1, m2, R, lane_ok);
+        // ordered scatter: the next element's ξ = −1 node of this line, when it is this
+        // element's ξ = +1 node, is added here, so a group adds to each node once
+        const bool folded = a.group_list ? fold_next_element(id.node, act, s, R) : false;
         if (act) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int i = 0; i < 3; ++i) atomic_add(a.Rv[c] + id.node[i], R[c][i]);
+                for (int i = 0; i < 3; ++i)
+                    if (i > 0 || !folded) atomic_add(a.Rv[c] + id.node[i], R[c][i]);
         }
     }
     cp_wait_all();
@@ -552,7 +563,8 @@ cudaError_t launch_pipe(const H27Args<T, T>& args, const T* geo_c, int num_sms, 
     constexpr int threads = PipeThreads<T>::value;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_residual_pipe_kernel<T, INCR>, threads, smem);
     if (per_sm < 1) per_sm = 1;
-    const int64_t groups = (args.nels + 2) / 3;
+    const int64_t groups = args.group_list ? args.group_count : (args.nels + 2) / 3;
+    if (groups < 1) return cudaSuccess;
     int64_t blocks = (groups + threads / 32 - 1) / (threads / 32);
     const int64_t cap = (int64_t)num_sms * per_sm;
     if (blocks > cap) blocks = cap;

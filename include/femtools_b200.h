@@ -348,6 +348,19 @@ int femb200_destroy(femb200_handle* h);
 /* Queue all work on `stream` (a cudaStream_t; NULL = legacy default stream).
  * Replaces CUDA.stream() of the Julia CUDABackend. */
 int femb200_set_stream(femb200_handle* h, void* stream);
+/* Ordered scatter for mixed-precision solves on this handle (on != 0; off at creation):
+ * a reproducible solve. The FP32 sweep runs once per colour of its tiles (32 consecutive
+ * elements), the FP64 sweep and the Jacobian diagnostics once per colour of their warp
+ * groups (3 consecutive elements); no two units of a colour share a node (greedy colours:
+ * 8 tile colours and 10 group colours at 64³), and inside a unit the ξ-face node shared by
+ * consecutive elements is added once. Every node then receives at most one atomic addition
+ * per launch, in a fixed order of launches, so two solves of the same inputs give the same
+ * iterations and fields bit for bit. Costs about a third of the solve time (64³). A solve
+ * returns FEMB200_EUNSUPPORTED when a unit's elements share other nodes (tiles that span
+ * several rows: fewer than 32 elements along ξ) or when the solve does not take the
+ * thread-per-element FP32 sweep. No reference counterpart: the reference's GPU scatter
+ * (Atomix, src/stokes/assemblers/momentum_residuals.jl:474-482) is unordered. */
+int femb200_set_ordered_scatter(femb200_handle* h, int32_t on);
 /* Message of the last failure on this handle (also the reference's error text). */
 const char* femb200_last_error(const femb200_handle* h);
 /* Build information: compiled architecture and version string. */
