@@ -35,7 +35,7 @@ METRIC = "time-to-1e-8 residual, 3D Q2 Stokes 64³: chosen vs plain FP64 DR; HBM
 PATH_64 = {"iterations": 12300, "itPH": 89, "jacobian_assemblies": 124, "check_interval": 100}
 # DRAM bytes read + written by one launch of the chosen method's hot kernel at 64³,
 # from the ncu capture summarised in profiles/hex27_incr_kernel_vep64.md.
-TRAFFIC = {(64, "mixed"): 127167488}
+TRAFFIC = {(64, "mixed"): 133528576}
 
 
 def load_package():

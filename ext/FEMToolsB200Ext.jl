@@ -366,7 +366,8 @@ function FEMTools.solve!(dr::CuStokesDR{D}, mesh::MixedMesh{D}, bc_v::NTuple{D, 
                          dt, pressure_factor = 50, viscosity = dr.η, scaling_viscosity = viscosity,
                          phases_v = dr.phases_v, plastic = nothing, finite_K = false, tolerance = 1.0e-6,
                          max_iterations = 50_000, check_interval = 50, throw_on_failure = true, workgroup = 256,
-                         precision = :fp64, body_force = nothing, P_old = nothing, kwargs...) where {D}
+                         precision = :fp64, body_force = nothing, P_old = nothing, ordered_scatter = false,
+                         kwargs...) where {D}
     if !ENABLED[]
         return invoke(FEMTools.solve!, Tuple{StokesDR{<:Any, D}, MixedMesh{D}, NTuple{D, DirichletBoundaryCondition}},
                       dr, mesh, bc_v; dt, pressure_factor, viscosity, scaling_viscosity, phases_v, plastic, finite_K,
@@ -377,10 +378,13 @@ function FEMTools.solve!(dr::CuStokesDR{D}, mesh::MixedMesh{D}, bc_v::NTuple{D, 
     c = Ref(stokes_controls(dr; dt, pressure_factor, tolerance, max_iterations, check_interval, finite_K,
                             throw_on_failure, precision, kwargs...))
     st = Ref{StokesStatsC}()
+    # ordered_scatter = true: a reproducible mixed-precision solve (colour-ordered scatter)
+    ccall((:femb200_set_ordered_scatter, LIB), Cint, (Ptr{Cvoid}, Int32), h.ptr, Int32(ordered_scatter))
     rc = GC.@preserve dr mesh bc_v viscosity phases_v body_force P_old begin
         ccall((:femb200_solve_stokes, LIB), Cint,
               (Ptr{Cvoid}, Ref{StokesProblemC}, Ref{StokesControlsC}, Ref{StokesStatsC}), h.ptr, p, c, st)
     end
+    ccall((:femb200_set_ordered_scatter, LIB), Cint, (Ptr{Cvoid}, Int32), h.ptr, Int32(0))
     rc == OK || throw_status(h, rc)
     return stats_tuple(st[])
 end

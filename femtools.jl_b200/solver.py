@@ -218,17 +218,19 @@ def _controls(dt, **kw):
 
 def solve(dr: StokesDR, bc_v, dt, pressure_factor=50.0, tolerance=1e-6, max_iterations=50_000, check_interval=50,
           throw_on_failure=True, finite_K=False, scaling_viscosity=None, history_capacity=0, precision="fp64",
-          **kwargs):
+          ordered_scatter=False, **kwargs):
     """solve!(dr::StokesDR, mesh, bc_v; dt, …) (src/stokes/solvers/DR.jl:302-337).
 
     Assembles M_P and γP, then runs the Powell–Hestenes/DYREL iteration. Returns
     the statistics as a dict; raises FemB200Error when the solve does not converge
-    and `throw_on_failure` is set, with the reference's message.
+    and `throw_on_failure` is set, with the reference's message. With
+    precision="mixed", ordered_scatter=True makes the solve reproducible bit for bit
+    (femb200_set_ordered_scatter: colour-ordered scatter, about a third slower).
     """
     return _solve(dr, bc_v, dt, True, pressure_factor=pressure_factor, tolerance=tolerance,
                   max_iterations=max_iterations, check_interval=check_interval, throw_on_failure=throw_on_failure,
                   finite_K=finite_K, scaling_viscosity=scaling_viscosity, history_capacity=history_capacity,
-                  precision=precision, **kwargs)
+                  precision=precision, ordered_scatter=ordered_scatter, **kwargs)
 
 
 def solve_stokes_dyrel(dr: StokesDR, bc_v, dt, ncheck=50, eps_tol=1e-6, iterMax=50_000, total_iterMax=50_000,
@@ -239,7 +241,8 @@ def solve_stokes_dyrel(dr: StokesDR, bc_v, dt, ncheck=50, eps_tol=1e-6, iterMax=
                   throw_on_failure=False, history_capacity=history_capacity, **kwargs)
 
 
-def _solve(dr, bc_v, dt, assemble_scaling, scaling_viscosity=None, history_capacity=0, precision="fp64", **kw):
+def _solve(dr, bc_v, dt, assemble_scaling, scaling_viscosity=None, history_capacity=0, precision="fp64",
+           ordered_scatter=False, **kw):
     lib, h = _Handle.get()
     kw.setdefault("cfl_v", dr.CFL_v)
     kw.setdefault("c_fact", dr.c_fact)
@@ -248,7 +251,11 @@ def _solve(dr, bc_v, dt, assemble_scaling, scaling_viscosity=None, history_capac
                         precision=abi.PRECISION_MIXED if precision == "mixed" else abi.PRECISION_FP64, **kw)
     st = abi.StokesStatsC()
     s = dr.problem(bc_v, scaling_viscosity)
-    rc = lib.femb200_solve_stokes(h, C.byref(s), C.byref(c), C.byref(st))
+    _check(lib, h, lib.femb200_set_ordered_scatter(h, 1 if ordered_scatter else 0))
+    try:
+        rc = lib.femb200_solve_stokes(h, C.byref(s), C.byref(c), C.byref(st))
+    finally:
+        lib.femb200_set_ordered_scatter(h, 0)
     _check(lib, h, rc)
     out = prob.stats_dict(st)
     out["iterations"] = out["iter"]

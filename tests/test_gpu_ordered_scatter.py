@@ -24,16 +24,11 @@ def rel_l2(a, b):
 
 
 def solve_mixed(case, ordered):
-    lib, h = fem.solver._Handle.get()
-    assert lib.femb200_set_ordered_scatter(h, 1 if ordered else 0) == abi.OK
-    try:
-        dr = case.device_state(fem)
-        st = fem.solve(dr, case.bc_device(), dt=case.dt, tolerance=1e-8, check_interval=100,
-                       throw_on_failure=False, precision="mixed")
-        fem.update_stokes_current_stress(dr, case.dt)
-        f = {"v": torch.cat([x.clone() for x in dr.v]), "P": dr.P.clone(), "tau": torch.cat([x.clone() for x in dr.tau])}
-    finally:
-        lib.femb200_set_ordered_scatter(h, 0)
+    dr = case.device_state(fem)
+    st = fem.solve(dr, case.bc_device(), dt=case.dt, tolerance=1e-8, check_interval=100,
+                   throw_on_failure=False, precision="mixed", ordered_scatter=ordered)
+    fem.update_stokes_current_stress(dr, case.dt)
+    f = {"v": torch.cat([x.clone() for x in dr.v]), "P": dr.P.clone(), "tau": torch.cat([x.clone() for x in dr.tau])}
     return st, f
 
 
