@@ -724,13 +724,17 @@ def timeloop_mode(args, fem):
     case = fem.configs.vep_layers_case(n=args.n, seed=args.seed)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def run(precision, extrapolate):
+    lib, h = fem.solver._Handle.get()
+
+    def run(precision, extrapolate, profile=False):
         dr = case.device_state()
         bc = case.bc_device()
         hist, rows = [], []
         for step in range(1, args.tl_steps + 1):
             dr.P0.copy_(dr.P)
             torch.cuda.synchronize()
+            if profile:
+                lib.femb200_profile(h, 1)
             ev0.record()
             if extrapolate and len(hist) == 2:
                 fem.warmstart.extrapolate_state(dr, bc, hist[0][0], hist[1][0], hist[0][1], hist[1][1])
@@ -739,6 +743,18 @@ def timeloop_mode(args, fem):
             ev1.record()
             torch.cuda.synchronize()
             rows.append({"step": step, "iter": st["iter"], "ms": ev0.elapsed_time(ev1), "converged": bool(st["converged"])})
+            if profile:
+                pm = (C.c_double * fem._abi.PROF_COUNT)()
+                pn = (C.c_int64 * fem._abi.PROF_COUNT)()
+                lib.femb200_profile_read(h, pm, pn)
+                cnt = (C.c_int64 * fem._abi.COUNTER_COUNT)()
+                lib.femb200_profile_counters(h, cnt, fem._abi.COUNTER_COUNT)
+                lib.femb200_profile(h, 0)
+                rows[-1]["kernel_ms"] = {"sweep": pm[0], "jacobian": pm[1], "node_update": pm[2], "outer_fp64": pm[4]}
+                rows[-1]["sweep_avg_us"] = pm[0] / max(pn[0], 1) * 1e3
+                rows[-1]["jacobian_assemblies"] = st["jacobian_assemblies"]
+                rows[-1]["stress_reads_per_sweep"] = cnt[fem._abi.COUNTER_STRESS_READS] / max(pn[0], 1)
+                rows[-1]["shared_jacobian_elements"] = int(cnt[fem._abi.COUNTER_SHARED_JACOBIANS])
             fem.update_stokes_current_stress(dr, case.dt)
             for c in range(6):
                 dr.tau_old[c].copy_(dr.tau[c])
@@ -758,6 +774,9 @@ def timeloop_mode(args, fem):
                                        "P": float(torch.linalg.norm(P - ref_P) / torch.linalg.norm(ref_P))}}
     tp = out["arms"]["plain_fp64"]["total_s"]
     out["speedup_vs_plain_fp64"] = {k: tp / a["total_s"] for k, a in out["arms"].items()}
+    if args.tl_profile:
+        # the mixed arm once more with CUDA events around every launch: the per-step split
+        out["mixed_profiled_steps"] = run("mixed", False, profile=True)[0]
     print(json.dumps(out), flush=True)
     return 0
 
@@ -1060,6 +1079,7 @@ def main():
     ap.add_argument("--ws-online", type=int, default=0, help="Adam steps on the newest converged pairs per solved step")
     ap.add_argument("--ws-online-batch", type=int, default=4)
     ap.add_argument("--tl-steps", type=int, default=10)
+    ap.add_argument("--tl-profile", action="store_true", help="timeloop mode: per-step kernel split of the mixed arm")
     ap.add_argument("--n2d", type=int, default=0, help="parity mode: size of the 2-D inclusion case (0: skip)")
     ap.add_argument("--oracle2d", default="", help="parity mode: .npz of the 2-D oracle solve (read, or written "
                     "with --oracle-only)")

@@ -23,6 +23,7 @@ namespace femb {
 __constant__ DevStokesMaterial c_mat;
 __constant__ DevTables c_tab;
 unsigned long long g_kernel_launches = 0;
+int g_pdl_enabled = 1;
 }  // namespace femb
 
 using namespace femb;
@@ -1170,6 +1171,9 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
     // ordered scatter: every sweep and Jacobian assembly of this solve adds to each node
     // at most once per launch (colours of tiles and of warp groups)
     OrderedScope ordered_scope{h};
+    // programmatic dependent launch of the sweep and the node update where every warp of
+    // the sweep takes at most one tile (measured: 10 % faster at 32³, 2 % slower at 64³)
+    const bool pdl = thread_sweep && (p->nels + 31) / 32 <= incr_warp_slots(h->num_sms);
     const bool ordered = h->ordered_scatter != 0;
     if (ordered) {
         if (!thread_sweep || !h->geo_c_valid) {
@@ -1210,11 +1214,11 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             for (size_t c = 0; c + 1 < h->tile_colour_start.size(); ++c) {
                 at.tile_list = h->d_tile_list + h->tile_colour_start[c];
                 at.tile_count = h->tile_colour_start[c + 1] - h->tile_colour_start[c];
-                CK(launch_hex27_incr(at, h->num_sms, s));
+                CK(launch_hex27_incr(at, h->num_sms, s, pdl));
             }
             at.tile_list = nullptr;
             at.tile_count = 0;
-        } else if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s));
+        } else if (thread_sweep) CK(launch_hex27_incr(at, h->num_sms, s, pdl));
         else CK(launch_hex27_residual_incr(ai, m.geo, h->num_sms, s));
         RC(prof_end(h, FEMB200_PROF_RESIDUAL));
         return FEMB200_OK;
@@ -1329,7 +1333,7 @@ int solve_dyrel_mixed(femb200_handle* h, const femb200_stokes_problem* p, const 
             na.fill = nout > 1;
             for (int k = 0; k < 3; ++k) na.Rfill[k] = m.Rk[k];
             RC(prof_begin(h, FEMB200_PROF_NODE));
-            CK(launch_node_update<float>(na, nb, s));
+            CK(launch_node_update<float>(na, nb, s, pdl));
             RC(prof_end(h, FEMB200_PROF_NODE));
             if (do_check) {
                 double sr[RED_SLOTS];
@@ -1871,6 +1875,9 @@ int femb200_create(femb200_handle** out) {
     if (const char* v = std::getenv("FEMB200_INCR_SWEEP")) h->use_incr_thread = std::strcmp(v, "warp") != 0;
     // FEMB200_JAC_SHARED=0 assembles every element's Jacobian columns (for comparisons)
     if (const char* v = std::getenv("FEMB200_JAC_SHARED")) h->jac_shared = std::strcmp(v, "0") != 0;
+    // FEMB200_PDL=0 launches the inner iteration's kernels without programmatic dependent
+    // launch (for comparisons; process-wide)
+    if (const char* v = std::getenv("FEMB200_PDL")) g_pdl_enabled = std::strcmp(v, "0") != 0;
     *out = h;
     return FEMB200_OK;
 }

@@ -72,6 +72,16 @@ template <> FEMB_HD float eps2<float>() { return 1.1920929e-07f * 1.1920929e-07f
 FEMB_D void atomic_add(double* p, double v) { atomicAdd(p, v); }
 FEMB_D void atomic_add(float* p, float v) { atomicAdd(p, v); }
 
+// Programmatic dependent launch (sm_90+) of the inner DR iteration's kernels: a kernel
+// launched with programmatic stream serialization may be scheduled while its predecessor
+// in the stream still runs. It waits here, before its first global-memory access, until
+// the predecessor grid has completed and its writes are visible, then lets its own
+// successor be scheduled. Without the launch attribute both are no-ops.
+FEMB_D void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Phase lookup for the three layouts (src/utils.jl:70-72); returns 0-based.
 FEMB_D int phase_of(const int32_t* ph, int layout, int64_t node1, int i, int64_t e, int n) {
     if (!ph) return 0;

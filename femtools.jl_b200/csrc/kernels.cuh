@@ -1,6 +1,7 @@
 // kernels.cuh — argument packs and launchers of the libfemtools_b200 kernels.
 #pragma once
 #include <limits>
+#include <utility>
 #include "common.cuh"
 
 namespace femb {
@@ -8,7 +9,29 @@ namespace femb {
 // Kernels launched by this library since the last profile reset (every launcher
 // adds one per launch); reported through femb200_profile_read.
 extern unsigned long long g_kernel_launches;
+// programmatic dependent launch of the inner iteration's kernels (launch_pdl); set from
+// FEMB200_PDL at handle creation
+extern int g_pdl_enabled;
 inline void count_launch() { __atomic_fetch_add(&g_kernel_launches, 1ull, __ATOMIC_RELAXED); }
+
+// Launches `kernel`, with programmatic stream serialization when `pdl` is set (the kernel
+// calls pdl_enter() before touching global memory), so that it is scheduled while its
+// predecessor drains.
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl && g_pdl_enabled ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 constexpr int H27_THREADS = 128;   // 4 warps × 3 elements per warp
 
@@ -136,7 +159,12 @@ struct IncrTileSrc {
 };
 cudaError_t launch_incr_tiles(const IncrTileSrc& src, int64_t nels, const IncrArgs& dst, int32_t* flags,
                               cudaStream_t st);
-cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st);
+// pdl: programmatic dependent launch (the mixed solve sets it when every warp of the sweep
+// processes at most one tile, where the gap between the sweep and the node update is a
+// sizeable part of an iteration)
+cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st, bool pdl = false);
+// tiles the FP32 sweep processes at once: resident warps on num_sms SMs
+int64_t incr_warp_slots(int num_sms);
 // out = x + y (FP32)
 cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n, cudaStream_t st);
 
@@ -362,7 +390,7 @@ struct NodeArgs {
 };
 
 template <class T>
-cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st);
+cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st, bool pdl = false);
 
 template <class T>
 cudaError_t launch_dirichlet(T* x, const int32_t* dofs, const T* vals, int64_t n, cudaStream_t st);

@@ -120,6 +120,7 @@ FEMB_D NodeOut node_comp(const NodeArgs<float>& a, int c, bool masked, float R, 
 // kernel needs no FP64 registers.
 template <bool REDUCE>
 __global__ void __launch_bounds__(NODE_THREADS, 2) node_update_f32x4_kernel(NodeArgs<float> a) {
+    pdl_enter();
     double acc[RED_SLOTS];
 #pragma unroll
     for (int s = 0; s < RED_SLOTS; ++s) acc[s] = 0.0;
@@ -297,7 +298,7 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 }  // namespace
 
 template <class T>
-cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st) {
+cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st, bool pdl) {
     count_launch();
     if constexpr (std::is_same<T, float>::value) {
         bool ok = aligned16(a.mask);
@@ -305,9 +306,8 @@ cudaError_t launch_node_update(const NodeArgs<T>& a, int blocks, cudaStream_t st
             ok = ok && aligned16(a.v[c]) && aligned16(a.rate[c]) && aligned16(a.Rv[c]) && aligned16(a.PC[c]) &&
                  aligned16(a.Rv0[c]) && aligned16(a.Rfill[c]);
         if (ok) {
-            if (a.reduce) node_update_f32x4_kernel<true><<<blocks, NODE_THREADS, 0, st>>>(a);
-            else node_update_f32x4_kernel<false><<<blocks, NODE_THREADS, 0, st>>>(a);
-            return cudaGetLastError();
+            return launch_pdl(pdl, a.reduce ? node_update_f32x4_kernel<true> : node_update_f32x4_kernel<false>,
+                              dim3((unsigned)blocks), dim3(NODE_THREADS), 0, st, a);
         }
     }
     node_update_kernel<T><<<blocks, NODE_THREADS, 0, st>>>(a);
@@ -396,7 +396,7 @@ cudaError_t launch_lmin_sums(const T* rate, const T* R, const T* R0, const T* PC
 }
 
 #define FEMB_INST(T)                                                                                                  \
-    template cudaError_t launch_node_update<T>(const NodeArgs<T>&, int, cudaStream_t);                               \
+    template cudaError_t launch_node_update<T>(const NodeArgs<T>&, int, cudaStream_t, bool);                               \
     template cudaError_t launch_dirichlet<T>(T*, const int32_t*, const T*, int64_t, cudaStream_t);                   \
     template cudaError_t launch_sumsq<T>(const T*, const T*, int64_t, double*, int, cudaStream_t);                   \
     template cudaError_t launch_ratio_max<T>(const T*, const T*, int64_t, double*, int, cudaStream_t);               \

@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
     extern __shared__ __align__(128) float in_smem[];
     __shared__ IncrPhase PT[MAXPH];
     __shared__ __align__(8) uint64_t mbar_all[IN_WARPS];
+    pdl_enter();
     for (int t = threadIdx.x; t < MAXPH; t += blockDim.x) PT[t] = a.ph[t];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t mbar = smem_addr(mbar_all + warp);
@@ -737,7 +738,14 @@ cudaError_t launch_add_f32(float* out, const float* x, const float* y, int64_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
+int64_t incr_warp_slots(int num_sms) {
+    int per_sm = 2;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hex27_incr_kernel<true, false>, IN_THREADS,
+                                                  (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float));
+    return (int64_t)num_sms * std::max(per_sm, 1) * IN_WARPS;
+}
+
+cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st, bool pdl) {
     const size_t smem = (size_t)IN_WARPS * IN_SLOTS * 32 * sizeof(float);
     const int64_t ntiles = a.tile_list ? a.tile_count : (a.nels + 31) / 32;
     if (ntiles < 1) return cudaSuccess;
@@ -750,8 +758,7 @@ cudaError_t launch_hex27_incr(const IncrArgs& a, int num_sms, cudaStream_t st) {
     blocks = std::min<int64_t>(blocks, (int64_t)num_sms * per_sm);
     if (blocks < 1) blocks = 1;
     count_launch();
-    fn<<<(unsigned)blocks, IN_THREADS, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(pdl, fn, dim3((unsigned)blocks), dim3(IN_THREADS), smem, st, a);
 }
 
 }  // namespace femb
