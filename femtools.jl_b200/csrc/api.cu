@@ -66,6 +66,10 @@ struct femb200_handle {
     // prefetched row by row (regions that yield), 0 = read on demand (elastic regions)
     unsigned long long* d_bound = nullptr;   // [0] bound failures, [1] bulk-copy wait failures of the FP32 sweep
     unsigned long long* h_bound = nullptr;
+    // tensor-core convolutions: device word set when a wait on the MMA completion gave up,
+    // and its pinned host mirror, refreshed after every convolution launch
+    int* d_conv_err = nullptr;
+    int* h_conv_err = nullptr;
     int incr_pre = 0;
     // ordered scatter of the FP32 sweep (femb200_set_ordered_scatter): the tiles sorted by
     // colour (no two tiles of a colour share a node) and the start of each colour
@@ -1934,6 +1938,8 @@ int femb200_destroy(femb200_handle* h) {
     if (h->d_counters) cudaFree(h->d_counters);
     if (h->d_bound) cudaFree(h->d_bound);
     if (h->h_bound) cudaFreeHost(h->h_bound);
+    if (h->d_conv_err) cudaFree(h->d_conv_err);
+    if (h->h_conv_err) cudaFreeHost(h->h_conv_err);
     if (h->d_jac_tmpl) cudaFree(h->d_jac_tmpl);
     if (h->d_jac_pick) cudaFree(h->d_jac_pick);
     if (h->d_tile_list) cudaFree(h->d_tile_list);
@@ -2043,6 +2049,29 @@ int femb200_solve_stokes(femb200_handle* h, const femb200_stokes_problem* p, con
     return finish_solve(h, c, st);
 }
 
+// The convolutions' error word: allocated and cleared on first use; a failure recorded by
+// an earlier launch is reported once its mirror has reached the host (at the latest at the
+// loss read-back, which synchronises the stream).
+static int conv_err_word(femb200_handle* h, int** dev) {
+    if (!h->d_conv_err) {
+        CK(cudaMalloc(&h->d_conv_err, sizeof(int)));
+        CK(cudaMallocHost(&h->h_conv_err, sizeof(int)));
+        *h->h_conv_err = 0;
+        CK(cudaMemsetAsync(h->d_conv_err, 0, sizeof(int), h->stream));
+    }
+    if (*h->h_conv_err != 0) {
+        h->err = "tensor-core convolution: a wait on the MMA completion gave up";
+        return FEMB200_ECUDA;
+    }
+    *dev = h->d_conv_err;
+    return FEMB200_OK;
+}
+
+static int conv_err_mirror(femb200_handle* h) {
+    CK(cudaMemcpyAsync(h->h_conv_err, h->d_conv_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    return FEMB200_OK;
+}
+
 int femb200_conv3x3_forward(femb200_handle* h, const void* in, const void* wt, const float* bias, const void* mask,
                             void* out, int32_t batch, int32_t height, int32_t width, int32_t ci, int32_t co,
                             int32_t mode) {
@@ -2053,8 +2082,14 @@ int femb200_conv3x3_forward(femb200_handle* h, const void* in, const void* wt, c
     if (!in || !wt || !out || (mode != 2 && !bias) || (mode == 2 && !mask) || batch < 1 || height < 1 || width < 1) {
         h->err = "conv3x3: missing array or empty grid"; return FEMB200_EINVAL;
     }
-    CK(launch_conv3x3(ci, co, mode, in, wt, bias, mask, out, batch, height, width, h->stream));
-    return FEMB200_OK;
+    if (height > 65535) { h->err = "conv3x3: height above 65535"; return FEMB200_EINVAL; }
+    if (((uintptr_t)in | (uintptr_t)wt | (uintptr_t)mask | (uintptr_t)out) & 15u) {
+        h->err = "conv3x3: in, wt, mask and out must be 16-byte aligned"; return FEMB200_EINVAL;
+    }
+    int* err = nullptr;
+    RC(conv_err_word(h, &err));
+    CK(launch_conv3x3(ci, co, mode, in, wt, bias, mask, out, batch, height, width, h->num_sms, err, h->stream));
+    return conv_err_mirror(h);
 }
 
 int femb200_conv3x3_weight_grad(femb200_handle* h, const void* in, const void* dy, float* dw, float* db, int32_t batch,
@@ -2062,8 +2097,11 @@ int femb200_conv3x3_weight_grad(femb200_handle* h, const void* in, const void* d
     if (!h) return FEMB200_EINVAL;
     if ((ci != 16 && ci != 32) || (co != 16 && co != 32)) { h->err = "conv3x3: ci and co must be 16 or 32"; return FEMB200_EUNSUPPORTED; }
     if (!in || !dy || !dw || batch < 1 || height < 1 || width < 1) { h->err = "conv3x3: missing array or empty grid"; return FEMB200_EINVAL; }
-    CK(launch_conv3x3_wgrad(ci, co, in, dy, dw, db, batch, height, width, h->num_sms, h->stream));
-    return FEMB200_OK;
+    if (((uintptr_t)in | (uintptr_t)dy) & 15u) { h->err = "conv3x3: in and dy must be 16-byte aligned"; return FEMB200_EINVAL; }
+    int* err = nullptr;
+    RC(conv_err_word(h, &err));
+    CK(launch_conv3x3_wgrad(ci, co, in, dy, dw, db, batch, height, width, h->num_sms, err, h->stream));
+    return conv_err_mirror(h);
 }
 
 int femb200_conv3x3_flip_weights(femb200_handle* h, const void* w, void* wT, int32_t ci, int32_t co) {
@@ -2084,6 +2122,10 @@ int femb200_mse_loss_grad(femb200_handle* h, const float* out, const float* targ
         double s;
         RC(fetch_sums(h, blocks, 1, &s));
         *loss = scale * s;
+        if (h->h_conv_err && *h->h_conv_err != 0) {
+            h->err = "tensor-core convolution: a wait on the MMA completion gave up";
+            return FEMB200_ECUDA;
+        }
     }
     return FEMB200_OK;
 }

@@ -4,227 +4,359 @@
 // time step's v/P from the solver's own converged history.
 //
 // Layout: activations NHWC BF16 with C ∈ {16, 32} channels (unused channels zero);
-// weights [co][9·ci + 8] BF16 (k = tap·ci + c, tap = 3·ky + kx; 8 padding entries per
-// row keep the B-fragment loads bank-conflict-free).
+// weights [co][9·ci + 8] BF16 (k = tap·ci + c, tap = 3·ky + kx; eight padding entries
+// per row).
 //
-// The convolution is an implicit GEMM on mma.sync.m16n8k16 (BF16 in, FP32 accumulate):
-// a 128-thread block owns an 8 × 16 output tile; the input tile with its one-pixel
-// halo (zero outside the grid) and the whole weight matrix are staged in shared
-// memory, each warp owns two output rows (two 16-pixel M tiles) and all output
-// channels, and the reduction runs over the 9 taps × ci. The data gradient is the
-// same kernel on the flipped, transposed weights with the ReLU mask of the layer
-// below applied in the epilogue; the weight gradient contracts the input patches
-// with the output gradient over the pixels (per block, then one atomic add per
-// weight and block).
+// Both contractions run on the sm_100a tensor cores (tcgen05.mma, kind::f16, BF16
+// operands from shared memory, FP32 accumulators in tensor memory):
+//
+// * convolution (forward, and the data gradient on the flipped transposed weights):
+//   an implicit GEMM with M = 128 output pixels (one segment of an image row),
+//   N = co and K = 9·ci. The three input rows of the segment with their one-pixel halo
+//   are staged once, 8 channels per 16-byte row of a core matrix, so that the A operand
+//   of tap (ky, kx) is the same staged block shifted by ky·130 + kx pixels: a start
+//   address in the descriptor, no im2col copy. One thread issues the 9·ci/16 MMAs.
+// * weight gradient: M = k (the 9·ci patch entries in 128-row tiles), N = co, K = the
+//   pixels of a 128-pixel segment; the patch matrix and the output gradient are staged
+//   per segment (pixel pairs per thread, row strides chosen so that the 32-bit stores of
+//   a warp fall in 32 different banks), the accumulators stay in tensor memory over all
+//   the segments a CTA visits, and each CTA adds its sums to dw once.
 #include <cuda_bf16.h>
 #include <algorithm>
 #include "kernels.cuh"
+#include "tc05.cuh"
 
 namespace femb {
 namespace {
 
-constexpr int CT_X = 16, CT_Y = 8, CONV_THREADS = 128;
-constexpr int HALO_X = CT_X + 2, HALO_Y = CT_Y + 2;
+using tc05::smem_u32;
 
-template <int C> constexpr int kpad() { return 9 * C + 8; }
-
-FEMB_D void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-FEMB_D uint32_t lds32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 FEMB_D uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
+FEMB_D float bf16_lo(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu))); }
+FEMB_D float bf16_hi(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16))); }
 
-// MODE 0: out = ReLU(conv + bias), BF16.  MODE 1: out = conv + bias, FP32.
-// MODE 2: out = conv where mask > 0 else 0, BF16 (data gradient through a ReLU; no bias).
-template <int CI, int CO, int MODE>
-__global__ void __launch_bounds__(CONV_THREADS) conv3x3_kernel(const __nv_bfloat16* __restrict__ in,
-                                                             const __nv_bfloat16* __restrict__ wt,
-                                                             const float* __restrict__ bias,
-                                                             const __nv_bfloat16* __restrict__ mask, void* out, int H,
-                                                             int W) {
-    constexpr int K = 9 * CI, KP = kpad<CI>(), PS = CI + 8;
-    __shared__ __align__(16) __nv_bfloat16 s_in[HALO_Y * HALO_X * PS];
-    __shared__ __align__(16) __nv_bfloat16 s_w[CO * KP];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int gid = lane >> 2, tig = lane & 3;
-    const int x0 = blockIdx.x * CT_X, y0 = blockIdx.y * CT_Y, b = blockIdx.z;
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(wt);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(s_w);
-        for (int i = tid; i < CO * KP / 2; i += CONV_THREADS) dst[i] = src[i];
-    }
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(in);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(s_in);
-        for (int i = tid; i < HALO_Y * HALO_X * (CI / 2); i += CONV_THREADS) {
-            const int pix = i / (CI / 2), cp = i % (CI / 2);
-            const int gy = y0 - 1 + pix / HALO_X, gx = x0 - 1 + pix % HALO_X;
-            uint32_t v = 0;
-            if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = src[(((int64_t)b * H + gy) * W + gx) * (CI / 2) + cp];
-            dst[pix * (PS / 2) + cp] = v;
-        }
-    }
-    __syncthreads();
-    float acc[2][CO / 8][4];
+constexpr int TC_THREADS = 128;              // 4 warps: warp w reads TMEM lanes 32w..32w+31
+constexpr int SEG = 128;                     // output pixels of one image-row segment (the MMA's M)
+constexpr int HALO = SEG + 2;                // staged input pixels per row
+constexpr int SLAB = 3 * HALO * 16;          // bytes of one 8-channel slab of the three staged rows
+
+FEMB_D void cp_async16(void* dst, const void* src, bool valid) {
+    // 16 bytes global → shared; zero-filled where `valid` is false (src is then not read)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+FEMB_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> FEMB_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// A segment: 128 consecutive pixels [x0, x0 + 128) of image row y of image b; segments
+// are numbered row by row (tile indices fit in 32 bits, checked on the host).
+struct Seg {
+    int b, y, x0;
+};
+FEMB_D Seg seg_of(int t, int nseg, int H) {
+    const int row = t / nseg;
+    return Seg{row / H, row % H, (t - row * nseg) * SEG};
+}
+
+// Stages the three input rows y − 1 .. y + 1 of a segment with their halo columns:
+// 8-channel slab s, row r, pixel xx (input column x0 − 1 + xx) at ((s·3 + r)·HALO + xx)·16
+// bytes, zero outside the grid. Consecutive threads copy consecutive 16-byte chunks of an
+// input row (the slabs of a pixel, then the next pixel), so each warp reads whole sectors.
+template <int CI>
+FEMB_D void stage_halo(uint8_t* dst, const __nv_bfloat16* in, Seg g, int H, int W, int tid) {
+    constexpr int NS = CI / 8, LOG = NS == 4 ? 2 : 1, PER_ROW = HALO * NS;
+    static_assert(NS == 2 || NS == 4, "16 or 32 channels");
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+    for (int r = 0; r < 3; ++r) {
+        const int gy = g.y - 1 + r;
+        const bool row = gy >= 0 && gy < H;
+        const __nv_bfloat16* rowp = in + ((int64_t)g.b * H + (row ? gy : 0)) * W * CI;
 #pragma unroll
-        for (int nt = 0; nt < CO / 8; ++nt)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[mt][nt][r] = 0.0f;
-#pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const int ky = tap / 3, kx = tap % 3;
-#pragma unroll
-        for (int c0 = 0; c0 < CI; c0 += 16) {
-            uint32_t a[2][4];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const int row = 2 * warp + mt;
-                const __nv_bfloat16* lo = s_in + ((row + ky) * HALO_X + gid + kx) * PS + c0 + tig * 2;
-                const __nv_bfloat16* hi = lo + 8 * PS;
-                a[mt][0] = lds32(lo);
-                a[mt][1] = lds32(hi);
-                a[mt][2] = lds32(lo + 8);
-                a[mt][3] = lds32(hi + 8);
-            }
-#pragma unroll
-            for (int nt = 0; nt < CO / 8; ++nt) {
-                const __nv_bfloat16* wp = s_w + (nt * 8 + gid) * KP + tap * CI + c0 + tig * 2;
-                const uint32_t b0 = lds32(wp), b1 = lds32(wp + 8);
-                mma16816(acc[0][nt], a[0], b0, b1);
-                mma16816(acc[1][nt], a[1], b0, b1);
-            }
-        }
-    }
-    static_assert(K % 16 == 0, "9·ci must be a multiple of 16");
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-        const int gy = y0 + 2 * warp + mt;
-        if (gy >= H) continue;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int gx = x0 + gid + 8 * half;
-            if (gx >= W) continue;
-            const int64_t pix = ((int64_t)b * H + gy) * W + gx;
-#pragma unroll
-            for (int nt = 0; nt < CO / 8; ++nt) {
-                const int co = nt * 8 + tig * 2;
-                float v0 = acc[mt][nt][2 * half], v1 = acc[mt][nt][2 * half + 1];
-                if constexpr (MODE == 0 || MODE == 1) { v0 += bias[co]; v1 += bias[co + 1]; }
-                if constexpr (MODE == 0) { v0 = fmaxf(v0, 0.0f); v1 = fmaxf(v1, 0.0f); }
-                if constexpr (MODE == 2) {
-                    const uint32_t m = *reinterpret_cast<const uint32_t*>(mask + pix * CO + co);
-                    if (!(__bfloat162float(__ushort_as_bfloat16((unsigned short)(m & 0xffffu))) > 0.0f)) v0 = 0.0f;
-                    if (!(__bfloat162float(__ushort_as_bfloat16((unsigned short)(m >> 16))) > 0.0f)) v1 = 0.0f;
-                }
-                if constexpr (MODE == 1) {
-                    *reinterpret_cast<float2*>(static_cast<float*>(out) + pix * CO + co) = make_float2(v0, v1);
-                } else {
-                    *reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(out) + pix * CO + co) =
-                        pack2(__float2bfloat16(v0), __float2bfloat16(v1));
-                }
+        for (int k = 0; k < (PER_ROW + TC_THREADS - 1) / TC_THREADS; ++k) {
+            const int i = tid + k * TC_THREADS;
+            if (i < PER_ROW) {
+                const int sl = i & (NS - 1), xx = i >> LOG;
+                const int gx = g.x0 - 1 + xx;
+                const bool v = row && gx >= 0 && gx < W;
+                cp_async16(dst + ((sl * 3 + r) * HALO + xx) * 16, v ? rowp + (int64_t)gx * CI + 8 * sl : in, v);
             }
         }
     }
 }
 
-// dW[co][tap·ci + c] += Σ_p X[p + (ky−1, kx−1)][c]·dY[p][co] over the grid (batch
-// included), on mma.sync with the pixels as the reduction dimension: tiles are
-// staged channel-major (X_T[c][iy][ix], dY_T[co][py][px]) so that consecutive pixels
-// are adjacent; the block accumulates in registers over all the tiles it visits and
-// adds its partial sums once.
-template <int CI, int CO>
-__global__ void __launch_bounds__(CONV_THREADS) conv3x3_wgrad_kernel(const __nv_bfloat16* __restrict__ x,
-                                                                   const __nv_bfloat16* __restrict__ dy, float* dw,
-                                                                   int B, int H, int W) {
-    constexpr int XS = 20, YS = 20;   // row strides of the staged tiles (halo width 18, tile width 16)
-    constexpr int MT = 9 * CI / 16, NT = CO / 8;
-    constexpr int MT_W = (MT + 3) / 4;   // M tiles per warp
-    constexpr int KP = kpad<CI>();
-    __shared__ __align__(16) __nv_bfloat16 s_x[CI * HALO_Y * XS];
-    __shared__ __align__(16) __nv_bfloat16 s_dy[CO * CT_Y * YS];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int gid = lane >> 2, tig = lane & 3;
-    float acc[MT_W][NT][4];
-#pragma unroll
-    for (int i = 0; i < MT_W; ++i)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[i][nt][r] = 0.0f;
-    const int tx_n = (W + CT_X - 1) / CT_X, ty_n = (H + CT_Y - 1) / CT_Y;
-    const int64_t ntile = (int64_t)B * tx_n * ty_n;
-    for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
-        const int b = (int)(t / ((int64_t)tx_n * ty_n));
-        const int rem = (int)(t % ((int64_t)tx_n * ty_n));
-        const int x0 = (rem % tx_n) * CT_X, y0 = (rem / tx_n) * CT_Y;
-        __syncthreads();
-        for (int i = tid; i < HALO_Y * HALO_X * CI; i += CONV_THREADS) {
-            const int pix = i / CI, c = i % CI;
-            const int iy = pix / HALO_X, ix = pix % HALO_X;
-            const int gy = y0 - 1 + iy, gx = x0 - 1 + ix;
-            __nv_bfloat16 v = __float2bfloat16(0.0f);
-            if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = x[(((int64_t)b * H + gy) * W + gx) * CI + c];
-            s_x[(c * HALO_Y + iy) * XS + ix] = v;
+// Shared memory of the convolution: the weights (16-byte chunk j of row co at
+// (j·co_n + co)·16), NSTAGE halo stages, the bias, the mbarrier and the TMEM address slot.
+constexpr int NSTAGE = 3;
+template <int CI, int CO> struct ConvSmem {
+    static constexpr int A = CI / 8 * SLAB;
+    static constexpr int B = 9 * CI / 8 * CO * 16;
+    static constexpr int BIAS = B + NSTAGE * A;
+    static constexpr int BAR = BIAS + CO * 4;
+    static constexpr int BYTES = BAR + 32;
+};
+
+// MODE 0: out = ReLU(conv + bias), BF16.  MODE 1: out = conv + bias, FP32.
+// MODE 2: out = conv where mask > 0 else 0, BF16 (data gradient through a ReLU; no bias).
+// Persistent: the CTA visits segments blockIdx.x, blockIdx.x + gridDim.x, ...; the halos
+// of the next two segments are in flight (cp.async into the other stages) while the current
+// one's MMAs and epilogue run. The MMAs of the three kernel rows accumulate separately
+// (consecutive MMAs are independent) and the epilogue adds the three.
+template <int CI, int CO, int MODE>
+__global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                               const __nv_bfloat16* __restrict__ wt,
+                                                               const float* __restrict__ bias,
+                                                               const __nv_bfloat16* __restrict__ mask, void* out, int B,
+                                                               int H, int W, int* err) {
+    using S = ConvSmem<CI, CO>;
+    // three accumulators, one per kernel row ky
+    constexpr uint32_t TCOLS = 3 * CO <= 64 ? 64 : 128;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* sB = smem;
+    uint8_t* sA = smem + S::B;   // stage k at sA + k·S::A
+    float* sbias = reinterpret_cast<float*>(smem + S::BIAS);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::BAR + 16);
+    const int tid = threadIdx.x, warp = tid >> 5;   // thread tid owns TMEM lane (pixel) tid
+    const int nseg = (W + SEG - 1) / SEG;
+    const int ntile = B * H * nseg;
+    if (warp == 0) tc05::tmem_alloc(smem_u32(tslot), TCOLS);
+    if (tid == 0) {
+        tc05::mbar_init(smem_u32(mbar));
+        tc05::fence_mbar_init();
+    }
+    if (tid < CO) sbias[tid] = MODE == 2 ? 0.0f : __ldg(bias + tid);
+    {
+        constexpr int KP8 = (9 * CI + 8) / 8;   // 16-byte chunks of a weight row
+        for (int i = tid; i < 9 * CI / 8 * CO; i += TC_THREADS) {
+            const int co = i % CO, j = i / CO;
+            cp_async16(sB + (j * CO + co) * 16, wt + (co * KP8 + j) * 8, true);
         }
-        for (int i = tid; i < CT_Y * CT_X * CO; i += CONV_THREADS) {
-            const int pix = i / CO, c = i % CO;
-            const int py = pix / CT_X, px = pix % CT_X;
-            const int gy = y0 + py, gx = x0 + px;
-            __nv_bfloat16 v = __float2bfloat16(0.0f);
-            if (gy < H && gx < W) v = dy[(((int64_t)b * H + gy) * W + gx) * CO + c];
-            s_dy[(c * CT_Y + py) * YS + px] = v;
-        }
+    }
+    const int G = (int)gridDim.x;
+    int t = blockIdx.x;
+    // prologue: the halos of the first two segments (the weights travel in the first group)
+#pragma unroll
+    for (int k = 0; k < NSTAGE - 1; ++k) {
+        if (t + k * G < ntile) stage_halo<CI>(sA + k * S::A, in, seg_of(t + k * G, nseg, H), H, W, tid);
+        cp_async_commit();
+    }
+    tc05::fence_before_sync();
+    __syncthreads();
+    tc05::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    constexpr uint32_t idesc = tc05::idesc_bf16_f32<SEG, CO>();
+    // descriptors of stage 0 and of the weights; offsets are added in 16-byte units to the
+    // start-address field (shared addresses stay below 2^18 bytes)
+    const uint64_t adesc0 = tc05::smem_desc(smem_u32(sA), SLAB, 128);
+    const uint64_t bdesc0 = tc05::smem_desc(smem_u32(sB), CO * 16, 128);
+    uint32_t phase = 0u;
+    int st = 0;   // stage of segment t
+    for (; t < ntile; t += G, st = st == NSTAGE - 1 ? 0 : st + 1) {
+        // the stage of the segment two ahead was last read by the MMAs of the previous one
+        const int ta = t + (NSTAGE - 1) * G;
+        const int sa = st == 0 ? NSTAGE - 1 : st - 1;
+        if (ta < ntile) stage_halo<CI>(sA + sa * S::A, in, seg_of(ta, nseg, H), H, W, tid);
+        cp_async_commit();
+        cp_async_wait<NSTAGE - 1>();   // every group but the two newest: this segment's halo
+        tc05::fence_async_smem();
+        tc05::fence_before_sync();
         __syncthreads();
-#pragma unroll 1
-        for (int py = 0; py < CT_Y; ++py) {
-            uint32_t bf[NT][2];
+        tc05::fence_after_sync();
+        if (tid == 0) {
+            const uint64_t ab = adesc0 + (uint64_t)(st * S::A / 16);
 #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const __nv_bfloat16* p = s_dy + ((nt * 8 + gid) * CT_Y + py) * YS + tig * 2;
-                bf[nt][0] = lds32(p);
-                bf[nt][1] = lds32(p + 8);
-            }
+            for (int kx = 0; kx < 3; ++kx)
 #pragma unroll
-            for (int i = 0; i < MT_W; ++i) {
-                const int mt = warp + 4 * i;
-                if (mt >= MT) break;
-                const int tap = (mt * 16) / CI, c0 = (mt * 16) % CI;
-                const int ky = tap / 3, kx = tap % 3;
-                uint32_t a[4];
+                for (int c0 = 0; c0 < CI; c0 += 16)
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int c = c0 + gid + ((r & 1) ? 8 : 0);
-                    const int px = tig * 2 + ((r & 2) ? 8 : 0);
-                    const __nv_bfloat16* p = s_x + (c * HALO_Y + py + ky) * XS + px + kx;
-                    a[r] = pack2(p[0], p[1]);
+                    for (int ky = 0; ky < 3; ++ky) {
+                        // rows m of tap (ky, kx): staged pixels ky·HALO + kx + m of slabs c0/8, c0/8 + 1
+                        const uint64_t ad = ab + (uint64_t)((c0 / 8) * (SLAB / 16) + ky * HALO + kx);
+                        const uint64_t bd = bdesc0 + (uint64_t)(((3 * ky + kx) * CI + c0) / 8 * CO);
+                        tc05::mma_bf16(tbase + ky * CO, ad, bd, idesc, kx > 0 || c0 > 0);
+                    }
+            tc05::commit(smem_u32(mbar));
+        }
+        const bool ok = __syncthreads_and(tid != 0 || tc05::mbar_poll(smem_u32(mbar), phase)) != 0;
+        phase ^= 1u;
+        if (!ok) {
+            if (tid == 0) atomicExch(err, 1);
+            break;
+        }
+        tc05::fence_after_sync();
+        float acc[CO / 16][16];
+#pragma unroll
+        for (int c = 0; c < CO / 16; ++c) {
+            const uint32_t ta0 = tbase + ((uint32_t)(warp * 32) << 16) + c * 16;
+            float a1[16], a2[16];
+            tc05::tmem_ld16(ta0, acc[c]);
+            tc05::tmem_ld16(ta0 + CO, a1);
+            tc05::tmem_ld16(ta0 + 2 * CO, a2);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[c][i] += a1[i] + a2[i];
+        }
+        // every thread's TMEM reads are done before the next segment's MMAs overwrite them
+        tc05::fence_before_sync();
+        const Seg cur = seg_of(t, nseg, H);
+        const int gx = cur.x0 + tid;
+        if (gx < W) {
+            const int64_t pix = ((int64_t)cur.b * H + cur.y) * W + gx;
+            if constexpr (MODE == 1) {
+                float4* o = reinterpret_cast<float4*>(static_cast<float*>(out) + pix * CO);
+#pragma unroll
+                for (int q = 0; q < CO / 4; ++q) {
+                    const int c = 4 * q;
+                    o[q] = make_float4(acc[c / 16][c % 16] + sbias[c], acc[c / 16][c % 16 + 1] + sbias[c + 1],
+                                       acc[c / 16][c % 16 + 2] + sbias[c + 2], acc[c / 16][c % 16 + 3] + sbias[c + 3]);
                 }
+            } else {
+                uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + pix * CO);
+                const uint4* mk = MODE == 2 ? reinterpret_cast<const uint4*>(mask + pix * CO) : nullptr;
 #pragma unroll
-                for (int nt = 0; nt < NT; ++nt) mma16816(acc[i][nt], a, bf[nt][0], bf[nt][1]);
+                for (int q = 0; q < CO / 8; ++q) {
+                    uint32_t w[4];
+                    uint4 m4 = make_uint4(0u, 0u, 0u, 0u);
+                    if constexpr (MODE == 2) m4 = __ldg(mk + q);
+                    const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const int c = 8 * q + 2 * h;
+                        float v0 = acc[c / 16][c % 16], v1 = acc[c / 16][c % 16 + 1];
+                        if constexpr (MODE == 0) {
+                            v0 = fmaxf(v0 + sbias[c], 0.0f);
+                            v1 = fmaxf(v1 + sbias[c + 1], 0.0f);
+                        }
+                        if constexpr (MODE == 2) {
+                            if (!(bf16_lo(mw[h]) > 0.0f)) v0 = 0.0f;
+                            if (!(bf16_hi(mw[h]) > 0.0f)) v1 = 0.0f;
+                        }
+                        w[h] = pack2(__float2bfloat16(v0), __float2bfloat16(v1));
+                    }
+                    o[q] = make_uint4(w[0], w[1], w[2], w[3]);
+                }
             }
         }
     }
-    // D rows: k = mt·16 + gid (+8); columns: co = nt·8 + tig·2 (+1)
-#pragma unroll
-    for (int i = 0; i < MT_W; ++i) {
-        const int mt = warp + 4 * i;
-        if (mt >= MT) break;
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-            const int k0 = mt * 16 + gid, co = nt * 8 + tig * 2;
-            atomicAdd(dw + (int64_t)co * KP + k0, acc[i][nt][0]);
-            atomicAdd(dw + (int64_t)(co + 1) * KP + k0, acc[i][nt][1]);
-            atomicAdd(dw + (int64_t)co * KP + k0 + 8, acc[i][nt][2]);
-            atomicAdd(dw + (int64_t)(co + 1) * KP + k0 + 8, acc[i][nt][3]);
-        }
+    cp_async_wait<0>();
+    tc05::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc05::tmem_dealloc(tbase, TCOLS);
+}
+
+// Weight gradient: for each tap, D_tap[c][co] += Σ_p X[p + (ky−1, kx−1)][c]·dY[p][co]
+// over a segment's 128 pixels. The MMA is MN-major on both operands: A (M = channel,
+// K = pixel) is the staged halo itself — slab s at SBO = SLAB, the tap as the start
+// address — and B (N = co, K = pixel) the staged output gradient ((co/8)·SEG + p)·16.
+// M is 128 rows while only the first ci are channels: the other rows read further into
+// shared memory (inside the CTA's allocation, 16·SLAB bytes from the stage start) and
+// fill accumulator rows that are never read. Accumulators: TMEM columns tap·co + n,
+// lanes 0..ci−1, kept over every segment the CTA visits.
+template <int CI, int CO> struct WgradSmem {
+    static constexpr int A = CI / 8 * SLAB;
+    static constexpr int BY = CO / 8 * SEG * 16;
+    static constexpr int STAGE = A + BY;
+    static constexpr int WINDOW = 16 * SLAB;                 // bytes an M = 128 operand spans
+    static constexpr int BYTES = STAGE + WINDOW + 32;        // the second stage's window ends here
+    static constexpr int COLS = 9 * CO;
+    static constexpr int TCOLS = COLS <= 256 ? 256 : 512;
+    static_assert(COLS <= 512 && CI <= 32, "accumulators in one TMEM allocation; channels in warp 0's lanes");
+};
+
+template <int CI, int CO>
+__global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                     const __nv_bfloat16* __restrict__ dy, float* dw,
+                                                                     int B, int H, int W, int* err) {
+    using S = WgradSmem<CI, CO>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::STAGE + S::WINDOW);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::STAGE + S::WINDOW + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nseg = (W + SEG - 1) / SEG;
+    const int ntile = B * H * nseg;
+    if (warp == 0) tc05::tmem_alloc(smem_u32(tslot), S::TCOLS);
+    if (tid == 0) {
+        tc05::mbar_init(smem_u32(mbar));
+        tc05::mbar_init(smem_u32(mbar + 1));
+        tc05::fence_mbar_init();
     }
+    // halo and the output gradient of the segment (consecutive threads: consecutive chunks)
+    auto stage = [&](Seg g, uint8_t* dst) {
+        stage_halo<CI>(dst, x, g, H, W, tid);
+        constexpr int NS = CO / 8, LOG = NS == 4 ? 2 : 1;
+        const __nv_bfloat16* rowp = dy + (((int64_t)g.b * H + g.y) * W + g.x0) * CO;
+#pragma unroll
+        for (int k = 0; k < SEG * NS / TC_THREADS; ++k) {
+            const int i = tid + k * TC_THREADS;
+            const int sl = i & (NS - 1), p = i >> LOG;
+            const bool v = g.x0 + p < W;
+            cp_async16(dst + S::A + (sl * SEG + p) * 16, v ? rowp + p * CO + 8 * sl : dy, v);
+        }
+    };
+    int t = blockIdx.x;
+    if (t < ntile) stage(seg_of(t, nseg, H), smem);
+    cp_async_commit();
+    tc05::fence_before_sync();
+    __syncthreads();
+    tc05::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    // A and B both MN-major (bits 15 and 16 of the instruction descriptor)
+    constexpr uint32_t idesc = tc05::idesc_bf16_f32<128, CO>() | (1u << 15) | (1u << 16);
+    const uint64_t adesc0 = tc05::smem_desc(smem_u32(smem), 128, SLAB);
+    const uint64_t bdesc0 = tc05::smem_desc(smem_u32(smem + S::A), 128, SEG * 16);
+    uint32_t phases = 0u;
+    bool ok = true, any = false;
+    for (int it = 0; t < ntile; ++it, t += gridDim.x) {
+        const int buf = it & 1;
+        const int tn = t + (int)gridDim.x;
+        if (tn < ntile) stage(seg_of(tn, nseg, H), smem + (buf ^ 1) * S::STAGE);
+        cp_async_commit();
+        cp_async_wait<1>();
+        tc05::fence_async_smem();
+        tc05::fence_before_sync();
+        __syncthreads();
+        tc05::fence_after_sync();
+        if (tid == 0) {
+            const uint64_t ab = adesc0 + (uint64_t)(buf * S::STAGE / 16), bb = bdesc0 + (uint64_t)(buf * S::STAGE / 16);
+            // K-step major: consecutive MMAs accumulate into different taps' columns
+#pragma unroll
+            for (int ks = 0; ks < SEG / 16; ++ks)
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap)
+                    tc05::mma_bf16(tbase + tap * CO, ab + (uint64_t)((tap / 3) * HALO + tap % 3 + 16 * ks),
+                                   bb + (uint64_t)(16 * ks), idesc, any || ks > 0);
+            tc05::commit(smem_u32(mbar + buf));
+        }
+        any = true;
+        // the stage is re-filled only after the MMAs that read it completed
+        ok = __syncthreads_and(tid != 0 || tc05::mbar_poll(smem_u32(mbar + buf), (phases >> buf) & 1u)) != 0;
+        phases ^= 1u << buf;
+        if (!ok) break;
+    }
+    cp_async_wait<0>();
+    if (ok && any) {
+        tc05::fence_after_sync();
+        if (warp == 0) {
+            constexpr int KP = 9 * CI + 8;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; ++tap)
+#pragma unroll
+                for (int c = 0; c < CO / 16; ++c) {
+                    float v[16];
+                    tc05::tmem_ld16(tbase + tap * CO + c * 16, v);
+                    if (lane < CI) {
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) atomicAdd(dw + (int64_t)(c * 16 + i) * KP + tap * CI + lane, v[i]);
+                    }
+                }
+        }
+    } else if (!ok && tid == 0) {
+        atomicExch(err, 1);
+    }
+    tc05::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc05::tmem_dealloc(tbase, S::TCOLS);
 }
 
 // db[co] += Σ_p dY[p][co]
@@ -307,35 +439,56 @@ __global__ void f32_to_bf16_kernel(const float* x, __nv_bfloat16* y, int64_t n) 
         y[i] = __float2bfloat16(x[i]);
 }
 
+// Dynamic shared memory above 48 KB needs the kernel attribute (a host-side setting).
 template <int CI, int CO, int MODE>
 cudaError_t conv_launch(const void* in, const void* wt, const float* bias, const void* mask, void* out, int B, int H,
-                        int W, cudaStream_t st) {
-    dim3 grid((W + CT_X - 1) / CT_X, (H + CT_Y - 1) / CT_Y, B);
+                        int W, int num_sms, int* err, cudaStream_t st) {
+    constexpr int smem = ConvSmem<CI, CO>::BYTES;
+    auto fn = conv3x3_tc_kernel<CI, CO, MODE>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    int per_sm = 1;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TC_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    const int64_t ntile = (int64_t)B * H * ((W + SEG - 1) / SEG);
+    if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(ntile, (int64_t)num_sms * std::max(per_sm, 1)));
     count_launch();
-    conv3x3_kernel<CI, CO, MODE><<<grid, CONV_THREADS, 0, st>>>(static_cast<const __nv_bfloat16*>(in),
-                                                                static_cast<const __nv_bfloat16*>(wt), bias,
-                                                                static_cast<const __nv_bfloat16*>(mask), out, H, W);
+    fn<<<(unsigned)blocks, TC_THREADS, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
+                                                   static_cast<const __nv_bfloat16*>(wt), bias,
+                                                   static_cast<const __nv_bfloat16*>(mask), out, B, H, W, err);
     return cudaGetLastError();
 }
 
 template <int CI, int CO>
 cudaError_t conv_mode(int mode, const void* in, const void* wt, const float* bias, const void* mask, void* out, int B,
-                      int H, int W, cudaStream_t st) {
-    if (mode == 0) return conv_launch<CI, CO, 0>(in, wt, bias, mask, out, B, H, W, st);
-    if (mode == 1) return conv_launch<CI, CO, 1>(in, wt, bias, mask, out, B, H, W, st);
-    return conv_launch<CI, CO, 2>(in, wt, bias, mask, out, B, H, W, st);
+                      int H, int W, int num_sms, int* err, cudaStream_t st) {
+    if (mode == 0) return conv_launch<CI, CO, 0>(in, wt, bias, mask, out, B, H, W, num_sms, err, st);
+    if (mode == 1) return conv_launch<CI, CO, 1>(in, wt, bias, mask, out, B, H, W, num_sms, err, st);
+    return conv_launch<CI, CO, 2>(in, wt, bias, mask, out, B, H, W, num_sms, err, st);
 }
 
 template <int CI, int CO>
-cudaError_t wgrad_launch(const void* x, const void* dy, float* dw, float* db, int B, int H, int W, int num_sms,
+cudaError_t wgrad_launch(const void* x, const void* dy, float* dw, float* db, int B, int H, int W, int num_sms, int* err,
                          cudaStream_t st) {
-    const int64_t ntile = (int64_t)B * ((W + CT_X - 1) / CT_X) * ((H + CT_Y - 1) / CT_Y);
-    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(ntile, (int64_t)num_sms * 8));
+    using S = WgradSmem<CI, CO>;
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         S::BYTES);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<CI, CO>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    int per_sm = 1;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_wgrad_tc_kernel<CI, CO>, TC_THREADS, S::BYTES);
+    if (e != cudaSuccess) return e;
+    const int64_t ntile = (int64_t)B * H * ((W + SEG - 1) / SEG);
+    if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(ntile, (int64_t)num_sms * std::max(per_sm, 1)));
     count_launch();
-    conv3x3_wgrad_kernel<CI, CO><<<(unsigned)blocks, CONV_THREADS, 0, st>>>(static_cast<const __nv_bfloat16*>(x),
-                                                                           static_cast<const __nv_bfloat16*>(dy), dw, B,
-                                                                           H, W);
-    cudaError_t e = cudaGetLastError();
+    conv3x3_wgrad_tc_kernel<CI, CO><<<(unsigned)blocks, TC_THREADS, S::BYTES, st>>>(
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, B, H, W, err);
+    e = cudaGetLastError();
     if (e != cudaSuccess || !db) return e;
     const int64_t npix = (int64_t)B * H * W;
     count_launch();
@@ -347,20 +500,20 @@ cudaError_t wgrad_launch(const void* x, const void* dy, float* dw, float* db, in
 }  // namespace
 
 cudaError_t launch_conv3x3(int ci, int co, int mode, const void* in, const void* wt, const float* bias,
-                           const void* mask, void* out, int B, int H, int W, cudaStream_t st) {
-    if (ci == 16 && co == 16) return conv_mode<16, 16>(mode, in, wt, bias, mask, out, B, H, W, st);
-    if (ci == 16 && co == 32) return conv_mode<16, 32>(mode, in, wt, bias, mask, out, B, H, W, st);
-    if (ci == 32 && co == 16) return conv_mode<32, 16>(mode, in, wt, bias, mask, out, B, H, W, st);
-    if (ci == 32 && co == 32) return conv_mode<32, 32>(mode, in, wt, bias, mask, out, B, H, W, st);
+                           const void* mask, void* out, int B, int H, int W, int num_sms, int* err, cudaStream_t st) {
+    if (ci == 16 && co == 16) return conv_mode<16, 16>(mode, in, wt, bias, mask, out, B, H, W, num_sms, err, st);
+    if (ci == 16 && co == 32) return conv_mode<16, 32>(mode, in, wt, bias, mask, out, B, H, W, num_sms, err, st);
+    if (ci == 32 && co == 16) return conv_mode<32, 16>(mode, in, wt, bias, mask, out, B, H, W, num_sms, err, st);
+    if (ci == 32 && co == 32) return conv_mode<32, 32>(mode, in, wt, bias, mask, out, B, H, W, num_sms, err, st);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_conv3x3_wgrad(int ci, int co, const void* x, const void* dy, float* dw, float* db, int B, int H, int W,
-                                 int num_sms, cudaStream_t st) {
-    if (ci == 16 && co == 16) return wgrad_launch<16, 16>(x, dy, dw, db, B, H, W, num_sms, st);
-    if (ci == 16 && co == 32) return wgrad_launch<16, 32>(x, dy, dw, db, B, H, W, num_sms, st);
-    if (ci == 32 && co == 16) return wgrad_launch<32, 16>(x, dy, dw, db, B, H, W, num_sms, st);
-    if (ci == 32 && co == 32) return wgrad_launch<32, 32>(x, dy, dw, db, B, H, W, num_sms, st);
+                                 int num_sms, int* err, cudaStream_t st) {
+    if (ci == 16 && co == 16) return wgrad_launch<16, 16>(x, dy, dw, db, B, H, W, num_sms, err, st);
+    if (ci == 16 && co == 32) return wgrad_launch<16, 32>(x, dy, dw, db, B, H, W, num_sms, err, st);
+    if (ci == 32 && co == 16) return wgrad_launch<32, 16>(x, dy, dw, db, B, H, W, num_sms, err, st);
+    if (ci == 32 && co == 32) return wgrad_launch<32, 32>(x, dy, dw, db, B, H, W, num_sms, err, st);
     return cudaErrorInvalidValue;
 }
 

@@ -199,10 +199,11 @@ template <class T>
 cudaError_t launch_hex27_adjoint(const AdjArgs<T>& args, int num_sms, cudaStream_t st);
 
 // ---- learned warm start (conv_bf16.cu, warmstart_fields.cu) ----
+// err: device word set to 1 when a tensor-core wait of the kernel gave up
 cudaError_t launch_conv3x3(int ci, int co, int mode, const void* in, const void* wt, const float* bias,
-                           const void* mask, void* out, int B, int H, int W, cudaStream_t st);
+                           const void* mask, void* out, int B, int H, int W, int num_sms, int* err, cudaStream_t st);
 cudaError_t launch_conv3x3_wgrad(int ci, int co, const void* x, const void* dy, float* dw, float* db, int B, int H, int W,
-                                 int num_sms, cudaStream_t st);
+                                 int num_sms, int* err, cudaStream_t st);
 cudaError_t launch_flip_weights(const void* w, void* wT, int ci, int co, cudaStream_t st);
 cudaError_t launch_mse(const float* out, const float* target, int nt, int co, float scale, void* dy, int64_t npix,
                        double* partials, int blocks, cudaStream_t st);

@@ -459,9 +459,13 @@ int femb200_solve_stokes_adjoint(femb200_handle* h, const femb200_stokes_problem
  * component) --------------------------------------------------------------------
  * A convolutional network over the node grid of a structured 2-D Q9/P1-disc mesh
  * predicts the next time step's correction to linear extrapolation of (vx, vy, P);
- * its BF16 tensor-core kernels (FP32 accumulation) and the field transfers are
- * below. Activations are NHWC BF16 with 16 or 32 channels; weights are
- * [co][9·ci + 8] (k = (3·ky + kx)·ci + c, eight padding entries per row). */
+ * its BF16 tensor-core kernels (tcgen05 MMAs with FP32 accumulation in tensor
+ * memory) and the field transfers are below. Activations are NHWC BF16 with 16 or 32
+ * channels; weights are [co][9·ci + 8] (k = (3·ky + kx)·ci + c, eight padding entries
+ * per row). The activation, weight and mask arrays are read and written 16 bytes at a
+ * time and must be 16-byte aligned (EINVAL otherwise). A tensor-core wait that gives
+ * up is reported as ECUDA by a later convolution call or by the loss read-back of
+ * femb200_mse_loss_grad. */
 
 /* 3×3 same-padded convolution (zero outside the grid), ci, co ∈ {16, 32}.
  * mode 0: out = ReLU(conv + bias) as BF16; 1: out = conv + bias as FP32;

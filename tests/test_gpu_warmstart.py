@@ -44,9 +44,10 @@ def call_conv(x, w, b, mask, B, H, W, ci, co_, mode):
 
 @pytest.mark.parametrize("ci,co_", [(16, 16), (16, 32), (32, 16), (32, 32)])
 @pytest.mark.parametrize("mode", [0, 1, 2])
-def test_conv_forward_matches_oracle(ci, co_, mode):
-    rng = np.random.default_rng(ci * 100 + co_ + mode)
-    B, H, W = 2, 11, 19     # not multiples of the 8 × 16 tile
+@pytest.mark.parametrize("W", [19, 150])
+def test_conv_forward_matches_oracle(ci, co_, mode, W):
+    rng = np.random.default_rng(ci * 100 + co_ + mode + W)
+    B, H = 2, 11     # one ragged 128-pixel row segment (W = 19), or a full one and a ragged one
     x = co.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
     w, b = rand_layer(rng, ci, co_)
     mask = co.bf16(rng.standard_normal((B, H, W, co_)).astype(np.float32)) if mode == 2 else None
@@ -62,9 +63,10 @@ def test_conv_forward_matches_oracle(ci, co_, mode):
 
 
 @pytest.mark.parametrize("ci,co_", [(16, 16), (16, 32), (32, 16), (32, 32)])
-def test_weight_gradient_matches_oracle(ci, co_):
-    rng = np.random.default_rng(7 + ci + co_)
-    B, H, W = 3, 13, 21
+@pytest.mark.parametrize("W", [21, 133])
+def test_weight_gradient_matches_oracle(ci, co_, W):
+    rng = np.random.default_rng(7 + ci + co_ + W)
+    B, H = 3, 13
     x = co.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
     dy = co.bf16(rng.standard_normal((B, H, W, co_)).astype(np.float32))
     lib, h = fem.solver._Handle.get()
@@ -80,6 +82,62 @@ def test_weight_gradient_matches_oracle(ci, co_):
     assert np.max(np.abs(gdw - rdw)) <= 1e-5 * np.max(np.abs(rdw))
     assert np.all(gdw[:, 9 * ci:] == 0)
     assert np.max(np.abs(host(db) - rdb)) <= 1e-5 * np.max(np.abs(rdb))
+
+
+@pytest.mark.parametrize("ci,co_,mode", [(32, 32, 0), (16, 16, 2), (32, 16, 1)])
+def test_conv_forward_many_segments_per_cta(ci, co_, mode):
+    # more 128-pixel segments than resident CTAs: every CTA runs its staging / MMA /
+    # epilogue pipeline over several segments and both halo stages
+    rng = np.random.default_rng(11 + ci + co_ + mode)
+    B, H, W = 2, 300, 150
+    x = co.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
+    w, b = rand_layer(rng, ci, co_)
+    mask = co.bf16(rng.standard_normal((B, H, W, co_)).astype(np.float32)) if mode == 2 else None
+    y = call_conv(dev_bf16(x), w, b if mode != 2 else None, dev_bf16(mask) if mode == 2 else None, B, H, W, ci, co_, mode)
+    ref = co.conv3x3(x, w, None if mode == 2 else b)
+    if mode == 0:
+        ref = np.maximum(ref, 0)
+    if mode == 2:
+        ref = ref * (mask > 0)
+    got = host(y).reshape(B, H, W, co_)
+    tol = 1e-5 if mode == 1 else 8e-3
+    assert np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref)), np.max(np.abs(got - ref))
+
+
+@pytest.mark.parametrize("ci,co_", [(32, 32), (16, 32)])
+def test_weight_gradient_many_segments_per_cta(ci, co_):
+    rng = np.random.default_rng(5 + ci + co_)
+    B, H, W = 2, 100, 133     # 400 segments: more than one CTA per SM can hold
+    x = co.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
+    dy = co.bf16(rng.standard_normal((B, H, W, co_)).astype(np.float32))
+    lib, h = fem.solver._Handle.get()
+    dw = torch.zeros(co_ * co.kpad(ci), dtype=torch.float32, device="cuda")
+    xd, dyd = dev_bf16(x), dev_bf16(dy)
+    rc = lib.femb200_conv3x3_weight_grad(h, ws._p(xd), ws._p(dyd), ws._p(dw), None, B, H, W, ci, co_)
+    assert rc == 0
+    torch.cuda.synchronize()
+    _, rdw, _ = co.conv3x3_backward(x, np.zeros((co_, co.kpad(ci))), dy)
+    gdw = host(dw).reshape(co_, co.kpad(ci))
+    assert np.max(np.abs(gdw - rdw)) <= 1e-5 * np.max(np.abs(rdw))
+
+
+def test_conv_rejects_misaligned_arrays():
+    # the tensor-core kernels move 16 bytes per access: a view two bytes into a buffer is
+    # refused before anything is launched
+    lib, h = fem.solver._Handle.get()
+    B, H, W, ci, co_ = 1, 4, 8, 16, 16
+    x = torch.zeros(B * H * W * ci + 8, dtype=torch.bfloat16, device="cuda")
+    wb = torch.zeros(co_ * co.kpad(ci), dtype=torch.bfloat16, device="cuda")
+    bb = torch.zeros(co_, dtype=torch.float32, device="cuda")
+    out = torch.empty(B * H * W * co_, dtype=torch.bfloat16, device="cuda")
+    rc = lib.femb200_conv3x3_forward(h, ws._p(x[1:]), ws._p(wb), ws._p(bb), None, ws._p(out), B, H, W, ci, co_, 0)
+    assert rc == 1 and b"16-byte aligned" in lib.femb200_last_error(h)
+    dw = torch.zeros(co_ * co.kpad(ci), dtype=torch.float32, device="cuda")
+    rc = lib.femb200_conv3x3_weight_grad(h, ws._p(x), ws._p(out[1:]), ws._p(dw), None, B, H, W, ci, co_)
+    assert rc == 1 and b"16-byte aligned" in lib.femb200_last_error(h)
+    rc = lib.femb200_conv3x3_forward(h, ws._p(x), ws._p(wb), ws._p(bb), None, ws._p(out), B, H, W, ci, co_, 0)
+    assert rc == 0, lib.femb200_last_error(h)
+    torch.cuda.synchronize()
 
 
 def test_network_gradient_matches_oracle():
