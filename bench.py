@@ -714,6 +714,47 @@ def lithostatic_mode(args, fem):
     return 0
 
 
+def conv_mode(args, fem):
+    """The learned warm start's network on its own: the (2n+1)² node grid of an n² Q9 mesh,
+    `--conv-batch` images; CUDA-event times of the 6-layer forward and of one training step
+    (forward, MSE, backward through the ReLU masks, Adam), after `--warmup` untimed repetitions,
+    averaged over `--steps`. Prints one JSON line."""
+    import torch
+    ws = fem.warmstart
+    B, H = args.conv_batch, 2 * args.n + 1
+    net = ws.WarmStartNet(seed=args.seed)
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    x = torch.randn(B * H * H * ws.IN_CH, device="cuda", generator=g).to(torch.bfloat16)
+    tgt = torch.randn(B * H * H * 3, device="cuda", generator=g)
+    npix = B * H * H
+
+    def forward():
+        net.forward(x, B, H, H)
+
+    def train_step():
+        net.zero_grad()
+        out, acts = net.forward(x, B, H, H, keep=True)
+        _, dy = net.loss_grad(out, tgt, npix, 1.0 / npix)
+        net.backward(acts, dy, B, H, H)
+        net.adam()
+
+    line = {"mode": "conv", "workload": f"warm-start-net-{B}x{H}^2", "batch": B, "grid": [H, H],
+            "layers": len(net.layers), "steps": args.steps, "warmup": args.warmup,
+            "kernels": "conv3x3_tc_kernel / conv3x3_wgrad_tc_kernel (tcgen05.mma kind::f16, FP32 in TMEM)"}
+    for name, fn in (("forward_ms", forward), ("train_step_ms", train_step)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        line[name] = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps(line))
+
+
 def timeloop_mode(args, fem):
     """Time loop of the layered visco-elasto-plastic case (BASELINE config 2 shape): each
     step P0 ← P, solve to the tolerance, τ_old ← τ. Arms, each on its own trajectory:
@@ -1086,8 +1127,9 @@ def main():
     ap.add_argument("--oracle-only", action="store_true", help="parity mode: run and save the oracle's solves only")
     ap.add_argument("--oracle3d", default="", help="parity mode: .npz of the 3-D oracle time loop (read, or written "
                     "with --oracle-only)")
+    ap.add_argument("--conv-batch", type=int, default=8, help="conv mode: images per batch")
     ap.add_argument("--mode", default="solve", choices=["solve", "sweep", "adjoint", "warmstart", "timeloop", "cellpressure", "lithostatic", "cap",
-                             "parity", "scatter-order"],
+                             "parity", "scatter-order", "conv"],
                     help="sweep: time K fused residual sweeps and K Jacobian assemblies on the initial state")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -1129,6 +1171,8 @@ def main():
         return adjoint_mode(args, fem)
     if args.mode == "warmstart":
         return warmstart_mode(args, fem)
+    if args.mode == "conv":
+        return conv_mode(args, fem)
     if args.mode == "timeloop":
         return timeloop_mode(args, fem)
     if args.mode == "cellpressure":

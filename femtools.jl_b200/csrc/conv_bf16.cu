@@ -37,10 +37,13 @@ FEMB_D uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
 FEMB_D float bf16_lo(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu))); }
 FEMB_D float bf16_hi(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16))); }
 
-constexpr int TC_THREADS = 128;              // 4 warps: warp w reads TMEM lanes 32w..32w+31
+constexpr int TC_THREADS = 128;              // weight gradient: 4 warps, warp w reads TMEM lanes 32w..32w+31
 constexpr int SEG = 128;                     // output pixels of one image-row segment (the MMA's M)
 constexpr int HALO = SEG + 2;                // staged input pixels per row
-constexpr int SLAB = 3 * HALO * 16;          // bytes of one 8-channel slab of the three staged rows
+constexpr int SLAB = 3 * HALO * 16;          // bytes of one 8-channel slab of three staged rows
+constexpr int FROWS = 4;                     // output rows of a convolution tile
+constexpr int FSLAB = (FROWS + 2) * HALO * 16;   // bytes of one 8-channel slab of its staged rows
+constexpr int FWD_THREADS = 256;             // 8 warps: warp w reads TMEM lanes 32·(w mod 4)..
 
 FEMB_D void cp_async16(void* dst, const void* src, bool valid) {
     // 16 bytes global → shared; zero-filled where `valid` is false (src is then not read)
@@ -50,47 +53,49 @@ FEMB_D void cp_async16(void* dst, const void* src, bool valid) {
 FEMB_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> FEMB_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// A segment: 128 consecutive pixels [x0, x0 + 128) of image row y of image b; segments
-// are numbered row by row (tile indices fit in 32 bits, checked on the host).
+// A tile: rows [y, y + ROWS) × pixels [x0, x0 + 128) of image b; tiles are numbered row
+// block by row block (tile indices fit in 32 bits, checked on the host).
 struct Seg {
     int b, y, x0;
 };
-FEMB_D Seg seg_of(int t, int nseg, int H) {
-    const int row = t / nseg;
-    return Seg{row / H, row % H, (t - row * nseg) * SEG};
+template <int ROWS>
+FEMB_D Seg seg_of(int t, int nseg, int nrb) {
+    const int rb = t / nseg;
+    return Seg{rb / nrb, (rb % nrb) * ROWS, (t - rb * nseg) * SEG};
 }
 
-// Stages the three input rows y − 1 .. y + 1 of a segment with their halo columns:
-// 8-channel slab s, row r, pixel xx (input column x0 − 1 + xx) at ((s·3 + r)·HALO + xx)·16
-// bytes, zero outside the grid. Consecutive threads copy consecutive 16-byte chunks of an
-// input row (the slabs of a pixel, then the next pixel), so each warp reads whole sectors.
-template <int CI>
+// Stages the NR input rows y − 1 .. y + NR − 2 of a tile with their halo columns: 8-channel
+// slab s, row r, pixel xx (input column x0 − 1 + xx) at ((s·NR + r)·HALO + xx)·16 bytes,
+// zero outside the grid. Consecutive threads copy consecutive 16-byte chunks of an input
+// row (the slabs of a pixel, then the next pixel), so each warp reads whole sectors.
+template <int CI, int NR, int NTH>
 FEMB_D void stage_halo(uint8_t* dst, const __nv_bfloat16* in, Seg g, int H, int W, int tid) {
     constexpr int NS = CI / 8, LOG = NS == 4 ? 2 : 1, PER_ROW = HALO * NS;
     static_assert(NS == 2 || NS == 4, "16 or 32 channels");
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
+    for (int r = 0; r < NR; ++r) {
         const int gy = g.y - 1 + r;
         const bool row = gy >= 0 && gy < H;
         const __nv_bfloat16* rowp = in + ((int64_t)g.b * H + (row ? gy : 0)) * W * CI;
 #pragma unroll
-        for (int k = 0; k < (PER_ROW + TC_THREADS - 1) / TC_THREADS; ++k) {
-            const int i = tid + k * TC_THREADS;
+        for (int k = 0; k < (PER_ROW + NTH - 1) / NTH; ++k) {
+            const int i = tid + k * NTH;
             if (i < PER_ROW) {
                 const int sl = i & (NS - 1), xx = i >> LOG;
                 const int gx = g.x0 - 1 + xx;
                 const bool v = row && gx >= 0 && gx < W;
-                cp_async16(dst + ((sl * 3 + r) * HALO + xx) * 16, v ? rowp + (int64_t)gx * CI + 8 * sl : in, v);
+                cp_async16(dst + ((sl * NR + r) * HALO + xx) * 16, v ? rowp + (int64_t)gx * CI + 8 * sl : in, v);
             }
         }
     }
 }
 
 // Shared memory of the convolution: the weights (16-byte chunk j of row co at
-// (j·co_n + co)·16), NSTAGE halo stages, the bias, the mbarrier and the TMEM address slot.
+// (j·co_n + co)·16), NSTAGE halo stages of FROWS + 2 rows, the bias, the mbarrier and the
+// TMEM address slot.
 constexpr int NSTAGE = 3;
 template <int CI, int CO> struct ConvSmem {
-    static constexpr int A = CI / 8 * SLAB;
+    static constexpr int A = CI / 8 * FSLAB;
     static constexpr int B = 9 * CI / 8 * CO * 16;
     static constexpr int BIAS = B + NSTAGE * A;
     static constexpr int BAR = BIAS + CO * 4;
@@ -99,28 +104,32 @@ template <int CI, int CO> struct ConvSmem {
 
 // MODE 0: out = ReLU(conv + bias), BF16.  MODE 1: out = conv + bias, FP32.
 // MODE 2: out = conv where mask > 0 else 0, BF16 (data gradient through a ReLU; no bias).
-// Persistent: the CTA visits segments blockIdx.x, blockIdx.x + gridDim.x, ...; the halos
-// of the next two segments are in flight (cp.async into the other stages) while the current
-// one's MMAs and epilogue run. The MMAs of the three kernel rows accumulate separately
-// (consecutive MMAs are independent) and the epilogue adds the three.
+// A tile is FROWS output rows × 128 pixels: FROWS + 2 staged input rows serve all of them
+// (1.5 staged rows per output row instead of 3). Output row u of the tile accumulates in
+// TMEM columns u·co.., from A blocks that start ((u + ky)·HALO + kx) staged pixels into
+// the stage. Persistent: the CTA visits tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the
+// halos of the next two tiles are in flight (cp.async into the other stages) while the
+// current one's MMAs and epilogue run. Warps w and w + 4 share TMEM lane quadrant w and
+// write rows 0, 1 and 2, 3 of the tile.
 template <int CI, int CO, int MODE>
-__global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ in,
-                                                               const __nv_bfloat16* __restrict__ wt,
-                                                               const float* __restrict__ bias,
-                                                               const __nv_bfloat16* __restrict__ mask, void* out, int B,
-                                                               int H, int W, int* err) {
+__global__ void __launch_bounds__(FWD_THREADS) conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                                const __nv_bfloat16* __restrict__ wt,
+                                                                const float* __restrict__ bias,
+                                                                const __nv_bfloat16* __restrict__ mask, void* out, int B,
+                                                                int H, int W, int* err) {
     using S = ConvSmem<CI, CO>;
-    // three accumulators, one per kernel row ky
-    constexpr uint32_t TCOLS = 3 * CO <= 64 ? 64 : 128;
+    constexpr uint32_t TCOLS = FROWS * CO <= 64 ? 64 : 128;
+    static_assert(FROWS * CO <= 128 && FWD_THREADS == 2 * 128 && FROWS == 4, "two rows per warp");
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* sB = smem;
     uint8_t* sA = smem + S::B;   // stage k at sA + k·S::A
     float* sbias = reinterpret_cast<float*>(smem + S::BIAS);
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::BAR);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::BAR + 16);
-    const int tid = threadIdx.x, warp = tid >> 5;   // thread tid owns TMEM lane (pixel) tid
-    const int nseg = (W + SEG - 1) / SEG;
-    const int ntile = B * H * nseg;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quad = warp & 3, half = warp >> 2;   // TMEM lanes 32·quad.., tile rows 2·half, 2·half + 1
+    const int nseg = (W + SEG - 1) / SEG, nrb = (H + FROWS - 1) / FROWS;
+    const int ntile = B * nrb * nseg;
     if (warp == 0) tc05::tmem_alloc(smem_u32(tslot), TCOLS);
     if (tid == 0) {
         tc05::mbar_init(smem_u32(mbar));
@@ -129,17 +138,18 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloa
     if (tid < CO) sbias[tid] = MODE == 2 ? 0.0f : __ldg(bias + tid);
     {
         constexpr int KP8 = (9 * CI + 8) / 8;   // 16-byte chunks of a weight row
-        for (int i = tid; i < 9 * CI / 8 * CO; i += TC_THREADS) {
+        for (int i = tid; i < 9 * CI / 8 * CO; i += FWD_THREADS) {
             const int co = i % CO, j = i / CO;
             cp_async16(sB + (j * CO + co) * 16, wt + (co * KP8 + j) * 8, true);
         }
     }
     const int G = (int)gridDim.x;
     int t = blockIdx.x;
-    // prologue: the halos of the first two segments (the weights travel in the first group)
+    // prologue: the halos of the first two tiles (the weights travel in the first group)
 #pragma unroll
     for (int k = 0; k < NSTAGE - 1; ++k) {
-        if (t + k * G < ntile) stage_halo<CI>(sA + k * S::A, in, seg_of(t + k * G, nseg, H), H, W, tid);
+        if (t + k * G < ntile)
+            stage_halo<CI, FROWS + 2, FWD_THREADS>(sA + k * S::A, in, seg_of<FROWS>(t + k * G, nseg, nrb), H, W, tid);
         cp_async_commit();
     }
     tc05::fence_before_sync();
@@ -149,17 +159,17 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloa
     constexpr uint32_t idesc = tc05::idesc_bf16_f32<SEG, CO>();
     // descriptors of stage 0 and of the weights; offsets are added in 16-byte units to the
     // start-address field (shared addresses stay below 2^18 bytes)
-    const uint64_t adesc0 = tc05::smem_desc(smem_u32(sA), SLAB, 128);
+    const uint64_t adesc0 = tc05::smem_desc(smem_u32(sA), FSLAB, 128);
     const uint64_t bdesc0 = tc05::smem_desc(smem_u32(sB), CO * 16, 128);
     uint32_t phase = 0u;
-    int st = 0;   // stage of segment t
+    int st = 0;   // stage of tile t
     for (; t < ntile; t += G, st = st == NSTAGE - 1 ? 0 : st + 1) {
-        // the stage of the segment two ahead was last read by the MMAs of the previous one
+        // the stage of the tile two ahead was last read by the MMAs of the previous one
         const int ta = t + (NSTAGE - 1) * G;
         const int sa = st == 0 ? NSTAGE - 1 : st - 1;
-        if (ta < ntile) stage_halo<CI>(sA + sa * S::A, in, seg_of(ta, nseg, H), H, W, tid);
+        if (ta < ntile) stage_halo<CI, FROWS + 2, FWD_THREADS>(sA + sa * S::A, in, seg_of<FROWS>(ta, nseg, nrb), H, W, tid);
         cp_async_commit();
-        cp_async_wait<NSTAGE - 1>();   // every group but the two newest: this segment's halo
+        cp_async_wait<NSTAGE - 1>();   // every group but the two newest: this tile's halo
         tc05::fence_async_smem();
         tc05::fence_before_sync();
         __syncthreads();
@@ -167,15 +177,16 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloa
         if (tid == 0) {
             const uint64_t ab = adesc0 + (uint64_t)(st * S::A / 16);
 #pragma unroll
-            for (int kx = 0; kx < 3; ++kx)
+            for (int tap = 0; tap < 9; ++tap)
 #pragma unroll
                 for (int c0 = 0; c0 < CI; c0 += 16)
 #pragma unroll
-                    for (int ky = 0; ky < 3; ++ky) {
-                        // rows m of tap (ky, kx): staged pixels ky·HALO + kx + m of slabs c0/8, c0/8 + 1
-                        const uint64_t ad = ab + (uint64_t)((c0 / 8) * (SLAB / 16) + ky * HALO + kx);
-                        const uint64_t bd = bdesc0 + (uint64_t)(((3 * ky + kx) * CI + c0) / 8 * CO);
-                        tc05::mma_bf16(tbase + ky * CO, ad, bd, idesc, kx > 0 || c0 > 0);
+                    for (int u = 0; u < FROWS; ++u) {
+                        // rows m of output row u, tap (ky, kx): staged pixels (u + ky)·HALO + kx + m
+                        // of slabs c0/8, c0/8 + 1
+                        const uint64_t ad = ab + (uint64_t)((c0 / 8) * (FSLAB / 16) + (u + tap / 3) * HALO + tap % 3);
+                        const uint64_t bd = bdesc0 + (uint64_t)((tap * CI + c0) / 8 * CO);
+                        tc05::mma_bf16(tbase + u * CO, ad, bd, idesc, tap > 0 || c0 > 0);
                     }
             tc05::commit(smem_u32(mbar));
         }
@@ -186,23 +197,19 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloa
             break;
         }
         tc05::fence_after_sync();
-        float acc[CO / 16][16];
+        const Seg cur = seg_of<FROWS>(t, nseg, nrb);
+        const int gx = cur.x0 + quad * 32 + lane;
 #pragma unroll
-        for (int c = 0; c < CO / 16; ++c) {
-            const uint32_t ta0 = tbase + ((uint32_t)(warp * 32) << 16) + c * 16;
-            float a1[16], a2[16];
-            tc05::tmem_ld16(ta0, acc[c]);
-            tc05::tmem_ld16(ta0 + CO, a1);
-            tc05::tmem_ld16(ta0 + 2 * CO, a2);
+        for (int uu = 0; uu < 2; ++uu) {
+            const int u = 2 * half + uu;
+            float acc[CO / 16][16];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) acc[c][i] += a1[i] + a2[i];
-        }
-        // every thread's TMEM reads are done before the next segment's MMAs overwrite them
-        tc05::fence_before_sync();
-        const Seg cur = seg_of(t, nseg, H);
-        const int gx = cur.x0 + tid;
-        if (gx < W) {
-            const int64_t pix = ((int64_t)cur.b * H + cur.y) * W + gx;
+            for (int c = 0; c < CO / 16; ++c)
+                tc05::tmem_ld16(tbase + ((uint32_t)(quad * 32) << 16) + u * CO + c * 16, acc[c]);
+            const int gy = cur.y + u;
+            if (gx >= W || gy >= H) continue;
+            const int64_t pix = ((int64_t)cur.b * H + gy) * W + gx;
+            {
             if constexpr (MODE == 1) {
                 float4* o = reinterpret_cast<float4*>(static_cast<float*>(out) + pix * CO);
 #pragma unroll
@@ -237,7 +244,10 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_tc_kernel(const __nv_bfloa
                     o[q] = make_uint4(w[0], w[1], w[2], w[3]);
                 }
             }
+            }
         }
+        // every thread's TMEM reads are done before the next tile's MMAs overwrite them
+        tc05::fence_before_sync();
     }
     cp_async_wait<0>();
     tc05::fence_before_sync();
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv
     }
     // halo and the output gradient of the segment (consecutive threads: consecutive chunks)
     auto stage = [&](Seg g, uint8_t* dst) {
-        stage_halo<CI>(dst, x, g, H, W, tid);
+        stage_halo<CI, 3, TC_THREADS>(dst, x, g, H, W, tid);
         constexpr int NS = CO / 8, LOG = NS == 4 ? 2 : 1;
         const __nv_bfloat16* rowp = dy + (((int64_t)g.b * H + g.y) * W + g.x0) * CO;
 #pragma unroll
@@ -295,7 +305,7 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv
         }
     };
     int t = blockIdx.x;
-    if (t < ntile) stage(seg_of(t, nseg, H), smem);
+    if (t < ntile) stage(seg_of<1>(t, nseg, H), smem);
     cp_async_commit();
     tc05::fence_before_sync();
     __syncthreads();
@@ -310,7 +320,7 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv
     for (int it = 0; t < ntile; ++it, t += gridDim.x) {
         const int buf = it & 1;
         const int tn = t + (int)gridDim.x;
-        if (tn < ntile) stage(seg_of(tn, nseg, H), smem + (buf ^ 1) * S::STAGE);
+        if (tn < ntile) stage(seg_of<1>(tn, nseg, H), smem + (buf ^ 1) * S::STAGE);
         cp_async_commit();
         cp_async_wait<1>();
         tc05::fence_async_smem();
@@ -450,13 +460,13 @@ cudaError_t conv_launch(const void* in, const void* wt, const float* bias, const
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     int per_sm = 1;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TC_THREADS, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FWD_THREADS, smem);
     if (e != cudaSuccess) return e;
-    const int64_t ntile = (int64_t)B * H * ((W + SEG - 1) / SEG);
+    const int64_t ntile = (int64_t)B * ((H + FROWS - 1) / FROWS) * ((W + SEG - 1) / SEG);
     if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(ntile, (int64_t)num_sms * std::max(per_sm, 1)));
     count_launch();
-    fn<<<(unsigned)blocks, TC_THREADS, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
+    fn<<<(unsigned)blocks, FWD_THREADS, smem, st>>>(static_cast<const __nv_bfloat16*>(in),
                                                    static_cast<const __nv_bfloat16*>(wt), bias,
                                                    static_cast<const __nv_bfloat16*>(mask), out, B, H, W, err);
     return cudaGetLastError();
