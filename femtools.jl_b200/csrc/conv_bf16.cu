@@ -8,19 +8,20 @@
 // per row).
 //
 // Both contractions run on the sm_100a tensor cores (tcgen05.mma, kind::f16, BF16
-// operands from shared memory, FP32 accumulators in tensor memory):
+// operands from shared memory, FP32 accumulators in tensor memory), on tiles of four output
+// rows × 128 pixels: the six staged input rows of a tile serve all four, which halves the
+// bytes moved from L2 into shared memory per output pixel against one-row tiles.
 //
-// * convolution (forward, and the data gradient on the flipped transposed weights):
-//   an implicit GEMM with M = 128 output pixels (one segment of an image row),
-//   N = co and K = 9·ci. The three input rows of the segment with their one-pixel halo
-//   are staged once, 8 channels per 16-byte row of a core matrix, so that the A operand
-//   of tap (ky, kx) is the same staged block shifted by ky·130 + kx pixels: a start
-//   address in the descriptor, no im2col copy. One thread issues the 9·ci/16 MMAs.
-// * weight gradient: M = k (the 9·ci patch entries in 128-row tiles), N = co, K = the
-//   pixels of a 128-pixel segment; the patch matrix and the output gradient are staged
-//   per segment (pixel pairs per thread, row strides chosen so that the 32-bit stores of
-//   a warp fall in 32 different banks), the accumulators stay in tensor memory over all
-//   the segments a CTA visits, and each CTA adds its sums to dw once.
+// * convolution (forward, and the data gradient on the flipped transposed weights): an
+//   implicit GEMM per output row with M = 128 pixels, N = co and K = 9·ci. The staged rows
+//   keep 8 channels per 16-byte row of a core matrix, so that the A operand of tap (ky, kx)
+//   is the staged block shifted by (u + ky)·130 + kx pixels: a start address in the
+//   descriptor, no im2col copy. One thread issues the MMAs of the tile's four rows.
+// * weight gradient: per tap an MMA with M = channel, N = co, K = the 128 pixels of one
+//   row, both operands MN-major, reading the staged rows directly; the accumulators stay in
+//   tensor memory over all the tiles a CTA visits, and each CTA adds its sums to dw once.
+// Both kernels are persistent and stage the next tiles with cp.async while the current
+// one's MMAs and epilogue run.
 #include <cuda_bf16.h>
 #include <algorithm>
 #include "kernels.cuh"
@@ -37,10 +38,8 @@ FEMB_D uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
 FEMB_D float bf16_lo(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w & 0xffffu))); }
 FEMB_D float bf16_hi(uint32_t w) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(w >> 16))); }
 
-constexpr int TC_THREADS = 128;              // weight gradient: 4 warps, warp w reads TMEM lanes 32w..32w+31
 constexpr int SEG = 128;                     // output pixels of one image-row segment (the MMA's M)
 constexpr int HALO = SEG + 2;                // staged input pixels per row
-constexpr int SLAB = 3 * HALO * 16;          // bytes of one 8-channel slab of three staged rows
 constexpr int FROWS = 4;                     // output rows of a convolution tile
 constexpr int FSLAB = (FROWS + 2) * HALO * 16;   // bytes of one 8-channel slab of its staged rows
 constexpr int FWD_THREADS = 256;             // 8 warps: warp w reads TMEM lanes 32·(w mod 4)..
@@ -256,56 +255,88 @@ __global__ void __launch_bounds__(FWD_THREADS) conv3x3_tc_kernel(const __nv_bflo
 }
 
 // Weight gradient: for each tap, D_tap[c][co] += Σ_p X[p + (ky−1, kx−1)][c]·dY[p][co]
-// over a segment's 128 pixels. The MMA is MN-major on both operands: A (M = channel,
-// K = pixel) is the staged halo itself — slab s at SBO = SLAB, the tap as the start
-// address — and B (N = co, K = pixel) the staged output gradient ((co/8)·SEG + p)·16.
-// M is 128 rows while only the first ci are channels: the other rows read further into
-// shared memory (inside the CTA's allocation, 16·SLAB bytes from the stage start) and
-// fill accumulator rows that are never read. Accumulators: TMEM columns tap·co + n,
-// lanes 0..ci−1, kept over every segment the CTA visits.
+// over the pixels of a tile of FROWS rows × 128. The MMA is MN-major on both operands.
+// A (M = channel, K = pixel) is the staged input itself, stored row-major by slabs —
+// staged row r, slab s, pixel xx at ((r·ns + s)·HALO + xx)·16 — so that for output row u
+// and tap (ky, kx) the block starts ((u + ky)·ns·HALO + kx) pixels in and its channel
+// groups lie HALO·16 bytes apart. B (N = co, K = pixel) is the staged output gradient,
+// ((u·co/8 + s)·SEG + p)·16. M is 128 rows while only the first ci are channels: the other
+// rows read further into the stage (inside the CTA's allocation) and fill accumulator rows
+// that are never read. Accumulators: TMEM columns tap·co + n, lanes 0..ci−1, kept over
+// every tile the CTA visits.
+constexpr int WG_THREADS = 256;
 template <int CI, int CO> struct WgradSmem {
-    static constexpr int A = CI / 8 * SLAB;
-    static constexpr int BY = CO / 8 * SEG * 16;
+    static constexpr int NS = CI / 8, NSO = CO / 8, NR = FROWS + 2;
+    static constexpr int A = NR * NS * HALO * 16;            // staged input rows
+    static constexpr int BY = FROWS * NSO * SEG * 16;        // staged output gradient
     static constexpr int STAGE = A + BY;
-    static constexpr int WINDOW = 16 * SLAB;                 // bytes an M = 128 operand spans
-    static constexpr int BYTES = STAGE + WINDOW + 32;        // the second stage's window ends here
+    // last byte an A block can reach from its stage's start, plus one
+    static constexpr int REACH = ((FROWS + 1) * NS * HALO + 2 + SEG - 16) * 16 + 15 * HALO * 16 + 256;
+    static constexpr int TAIL = REACH > STAGE ? REACH - STAGE : 0;
+    static constexpr int BYTES = 2 * STAGE + TAIL + 32;
     static constexpr int COLS = 9 * CO;
     static constexpr int TCOLS = COLS <= 256 ? 256 : 512;
     static_assert(COLS <= 512 && CI <= 32, "accumulators in one TMEM allocation; channels in warp 0's lanes");
 };
 
+// Stages the input rows of a tile for the weight gradient (row-major slabs, see above).
+template <int CI>
+FEMB_D void stage_rows_wg(uint8_t* dst, const __nv_bfloat16* in, Seg g, int H, int W, int tid) {
+    constexpr int NS = CI / 8, LOG = NS == 4 ? 2 : 1, PER_ROW = HALO * NS;
+#pragma unroll
+    for (int r = 0; r < FROWS + 2; ++r) {
+        const int gy = g.y - 1 + r;
+        const bool row = gy >= 0 && gy < H;
+        const __nv_bfloat16* rowp = in + ((int64_t)g.b * H + (row ? gy : 0)) * W * CI;
+#pragma unroll
+        for (int k = 0; k < (PER_ROW + WG_THREADS - 1) / WG_THREADS; ++k) {
+            const int i = tid + k * WG_THREADS;
+            if (i < PER_ROW) {
+                const int sl = i & (NS - 1), xx = i >> LOG;
+                const int gx = g.x0 - 1 + xx;
+                const bool v = row && gx >= 0 && gx < W;
+                cp_async16(dst + ((r * NS + sl) * HALO + xx) * 16, v ? rowp + (int64_t)gx * CI + 8 * sl : in, v);
+            }
+        }
+    }
+}
+
 template <int CI, int CO>
-__global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
+__global__ void __launch_bounds__(WG_THREADS) conv3x3_wgrad_tc_kernel(const __nv_bfloat16* __restrict__ x,
                                                                      const __nv_bfloat16* __restrict__ dy, float* dw,
                                                                      int B, int H, int W, int* err) {
     using S = WgradSmem<CI, CO>;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::STAGE + S::WINDOW);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + S::STAGE + S::WINDOW + 16);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * S::STAGE + S::TAIL);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 2 * S::STAGE + S::TAIL + 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nseg = (W + SEG - 1) / SEG;
-    const int ntile = B * H * nseg;
+    const int nseg = (W + SEG - 1) / SEG, nrb = (H + FROWS - 1) / FROWS;
+    const int ntile = B * nrb * nseg;
     if (warp == 0) tc05::tmem_alloc(smem_u32(tslot), S::TCOLS);
     if (tid == 0) {
         tc05::mbar_init(smem_u32(mbar));
         tc05::mbar_init(smem_u32(mbar + 1));
         tc05::fence_mbar_init();
     }
-    // halo and the output gradient of the segment (consecutive threads: consecutive chunks)
+    // input rows and the output gradient of a tile (consecutive threads: consecutive chunks)
     auto stage = [&](Seg g, uint8_t* dst) {
-        stage_halo<CI, 3, TC_THREADS>(dst, x, g, H, W, tid);
-        constexpr int NS = CO / 8, LOG = NS == 4 ? 2 : 1;
-        const __nv_bfloat16* rowp = dy + (((int64_t)g.b * H + g.y) * W + g.x0) * CO;
+        stage_rows_wg<CI>(dst, x, g, H, W, tid);
+        constexpr int LOG = S::NSO == 4 ? 2 : 1;
 #pragma unroll
-        for (int k = 0; k < SEG * NS / TC_THREADS; ++k) {
-            const int i = tid + k * TC_THREADS;
-            const int sl = i & (NS - 1), p = i >> LOG;
-            const bool v = g.x0 + p < W;
-            cp_async16(dst + S::A + (sl * SEG + p) * 16, v ? rowp + p * CO + 8 * sl : dy, v);
+        for (int u = 0; u < FROWS; ++u) {
+            const bool row = g.y + u < H;
+            const __nv_bfloat16* rowp = dy + (((int64_t)g.b * H + (row ? g.y + u : 0)) * W + g.x0) * CO;
+#pragma unroll
+            for (int k = 0; k < SEG * S::NSO / WG_THREADS; ++k) {
+                const int i = tid + k * WG_THREADS;
+                const int sl = i & (S::NSO - 1), p = i >> LOG;
+                const bool v = row && g.x0 + p < W;
+                cp_async16(dst + S::A + ((u * S::NSO + sl) * SEG + p) * 16, v ? rowp + p * CO + 8 * sl : dy, v);
+            }
         }
     };
     int t = blockIdx.x;
-    if (t < ntile) stage(seg_of<1>(t, nseg, H), smem);
+    if (t < ntile) stage(seg_of<FROWS>(t, nseg, nrb), smem);
     cp_async_commit();
     tc05::fence_before_sync();
     __syncthreads();
@@ -313,14 +344,14 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv
     const uint32_t tbase = *tslot;
     // A and B both MN-major (bits 15 and 16 of the instruction descriptor)
     constexpr uint32_t idesc = tc05::idesc_bf16_f32<128, CO>() | (1u << 15) | (1u << 16);
-    const uint64_t adesc0 = tc05::smem_desc(smem_u32(smem), 128, SLAB);
+    const uint64_t adesc0 = tc05::smem_desc(smem_u32(smem), 128, HALO * 16);
     const uint64_t bdesc0 = tc05::smem_desc(smem_u32(smem + S::A), 128, SEG * 16);
-    uint32_t phases = 0u;
+    uint32_t phases = 0u;   // bit k: parity of the next completion of mbarrier k
     bool ok = true, any = false;
     for (int it = 0; t < ntile; ++it, t += gridDim.x) {
         const int buf = it & 1;
         const int tn = t + (int)gridDim.x;
-        if (tn < ntile) stage(seg_of<1>(tn, nseg, H), smem + (buf ^ 1) * S::STAGE);
+        if (tn < ntile) stage(seg_of<FROWS>(tn, nseg, nrb), smem + (buf ^ 1) * S::STAGE);
         cp_async_commit();
         cp_async_wait<1>();
         tc05::fence_async_smem();
@@ -329,13 +360,16 @@ __global__ void __launch_bounds__(TC_THREADS) conv3x3_wgrad_tc_kernel(const __nv
         tc05::fence_after_sync();
         if (tid == 0) {
             const uint64_t ab = adesc0 + (uint64_t)(buf * S::STAGE / 16), bb = bdesc0 + (uint64_t)(buf * S::STAGE / 16);
-            // K-step major: consecutive MMAs accumulate into different taps' columns
-#pragma unroll
+            // consecutive MMAs accumulate into different taps' columns
+#pragma unroll 1
             for (int ks = 0; ks < SEG / 16; ++ks)
 #pragma unroll
-                for (int tap = 0; tap < 9; ++tap)
-                    tc05::mma_bf16(tbase + tap * CO, ab + (uint64_t)((tap / 3) * HALO + tap % 3 + 16 * ks),
-                                   bb + (uint64_t)(16 * ks), idesc, any || ks > 0);
+                for (int u = 0; u < FROWS; ++u)
+#pragma unroll
+                    for (int tap = 0; tap < 9; ++tap)
+                        tc05::mma_bf16(tbase + tap * CO,
+                                       ab + (uint64_t)((u + tap / 3) * S::NS * HALO + tap % 3 + 16 * ks),
+                                       bb + (uint64_t)(u * S::NSO * SEG + 16 * ks), idesc, any || ks > 0 || u > 0);
             tc05::commit(smem_u32(mbar + buf));
         }
         any = true;
@@ -490,13 +524,13 @@ cudaError_t wgrad_launch(const void* x, const void* dy, float* dw, float* db, in
     e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<CI, CO>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     int per_sm = 1;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_wgrad_tc_kernel<CI, CO>, TC_THREADS, S::BYTES);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_wgrad_tc_kernel<CI, CO>, WG_THREADS, S::BYTES);
     if (e != cudaSuccess) return e;
-    const int64_t ntile = (int64_t)B * H * ((W + SEG - 1) / SEG);
+    const int64_t ntile = (int64_t)B * ((H + FROWS - 1) / FROWS) * ((W + SEG - 1) / SEG);
     if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(ntile, (int64_t)num_sms * std::max(per_sm, 1)));
     count_launch();
-    conv3x3_wgrad_tc_kernel<CI, CO><<<(unsigned)blocks, TC_THREADS, S::BYTES, st>>>(
+    conv3x3_wgrad_tc_kernel<CI, CO><<<(unsigned)blocks, WG_THREADS, S::BYTES, st>>>(
         static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, B, H, W, err);
     e = cudaGetLastError();
     if (e != cudaSuccess || !db) return e;
