@@ -254,16 +254,17 @@ __global__ void __launch_bounds__(FWD_THREADS) conv3x3_tc_kernel(const __nv_bflo
     if (warp == 0) tc05::tmem_dealloc(tbase, TCOLS);
 }
 
-// Weight gradient: for each tap, D_tap[c][co] += Σ_p X[p + (ky−1, kx−1)][c]·dY[p][co]
-// over the pixels of a tile of FROWS rows × 128. The MMA is MN-major on both operands.
-// A (M = channel, K = pixel) is the staged input itself, stored row-major by slabs —
-// staged row r, slab s, pixel xx at ((r·ns + s)·HALO + xx)·16 — so that for output row u
-// and tap (ky, kx) the block starts ((u + ky)·ns·HALO + kx) pixels in and its channel
-// groups lie HALO·16 bytes apart. B (N = co, K = pixel) is the staged output gradient,
-// ((u·co/8 + s)·SEG + p)·16. M is 128 rows while only the first ci are channels: the other
-// rows read further into the stage (inside the CTA's allocation) and fill accumulator rows
-// that are never read. Accumulators: TMEM columns tap·co + n, lanes 0..ci−1, kept over
-// every tile the CTA visits.
+// Weight gradient: dW[co][(3·ky + kx)·ci + c] = Σ_p X[p + (ky−1, kx−1)][c]·dY[p][co] over
+// the pixels of tiles of FROWS rows × 128. The MMA is MN-major on both operands. A
+// (M = 128 rows, K = pixel) is the staged input itself, stored row-major by slabs — staged
+// row r, slab s, pixel xx at ((r·ns + s)·HALO + xx)·16 — so that consecutive 8-channel groups
+// lie one staged row apart (HALO·16 bytes): an A block that starts at output row u's first
+// input row and column kx holds, in rows ky·ci + c, the input of kernel row ky for every ky
+// at once. B (N = co, K = pixel) is the staged output gradient of row u,
+// ((u·co/8 + s)·SEG + p)·16. One MMA per (row, kx, K step) thus accumulates all three kernel
+// rows of column kx into TMEM columns kx·co + n, lanes ky·ci + c; rows 3·ci.. of the block
+// read further into the stage (inside the CTA's allocation) and fill accumulator rows that
+// are never read. The accumulators stay in tensor memory over every tile the CTA visits.
 constexpr int WG_THREADS = 256;
 template <int CI, int CO> struct WgradSmem {
     static constexpr int NS = CI / 8, NSO = CO / 8, NR = FROWS + 2;
@@ -271,12 +272,12 @@ template <int CI, int CO> struct WgradSmem {
     static constexpr int BY = FROWS * NSO * SEG * 16;        // staged output gradient
     static constexpr int STAGE = A + BY;
     // last byte an A block can reach from its stage's start, plus one
-    static constexpr int REACH = ((FROWS + 1) * NS * HALO + 2 + SEG - 16) * 16 + 15 * HALO * 16 + 256;
+    static constexpr int REACH = ((FROWS - 1) * NS * HALO + 2 + SEG - 16) * 16 + 15 * HALO * 16 + 256;
     static constexpr int TAIL = REACH > STAGE ? REACH - STAGE : 0;
     static constexpr int BYTES = 2 * STAGE + TAIL + 32;
-    static constexpr int COLS = 9 * CO;
-    static constexpr int TCOLS = COLS <= 256 ? 256 : 512;
-    static_assert(COLS <= 512 && CI <= 32, "accumulators in one TMEM allocation; channels in warp 0's lanes");
+    static constexpr int COLS = 3 * CO;
+    static constexpr int TCOLS = COLS <= 64 ? 64 : 128;
+    static_assert(3 * CI <= 128, "the three kernel rows of a column in one M = 128 block");
 };
 
 // Stages the input rows of a tile for the weight gradient (row-major slabs, see above).
@@ -360,15 +361,14 @@ __global__ void __launch_bounds__(WG_THREADS) conv3x3_wgrad_tc_kernel(const __nv
         tc05::fence_after_sync();
         if (tid == 0) {
             const uint64_t ab = adesc0 + (uint64_t)(buf * S::STAGE / 16), bb = bdesc0 + (uint64_t)(buf * S::STAGE / 16);
-            // consecutive MMAs accumulate into different taps' columns
+            // consecutive MMAs accumulate into different kernel columns' accumulators
 #pragma unroll 1
             for (int ks = 0; ks < SEG / 16; ++ks)
 #pragma unroll
                 for (int u = 0; u < FROWS; ++u)
 #pragma unroll
-                    for (int tap = 0; tap < 9; ++tap)
-                        tc05::mma_bf16(tbase + tap * CO,
-                                       ab + (uint64_t)((u + tap / 3) * S::NS * HALO + tap % 3 + 16 * ks),
+                    for (int kx = 0; kx < 3; ++kx)
+                        tc05::mma_bf16(tbase + kx * CO, ab + (uint64_t)(u * S::NS * HALO + kx + 16 * ks),
                                        bb + (uint64_t)(u * S::NSO * SEG + 16 * ks), idesc, any || ks > 0 || u > 0);
             tc05::commit(smem_u32(mbar + buf));
         }
@@ -381,17 +381,20 @@ __global__ void __launch_bounds__(WG_THREADS) conv3x3_wgrad_tc_kernel(const __nv
     cp_async_wait<0>();
     if (ok && any) {
         tc05::fence_after_sync();
-        if (warp == 0) {
+        // accumulator row m = ky·ci + c sits in TMEM lane m: warp w < 4 reads lanes 32w..
+        const int m = warp * 32 + lane, ky = m / CI, ch = m % CI;
+        if (warp < 4 && warp * 32 < 3 * CI) {
             constexpr int KP = 9 * CI + 8;
 #pragma unroll 1
-            for (int tap = 0; tap < 9; ++tap)
+            for (int kx = 0; kx < 3; ++kx)
 #pragma unroll
                 for (int c = 0; c < CO / 16; ++c) {
                     float v[16];
-                    tc05::tmem_ld16(tbase + tap * CO + c * 16, v);
-                    if (lane < CI) {
+                    tc05::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + kx * CO + c * 16, v);
+                    if (ky < 3) {
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) atomicAdd(dw + (int64_t)(c * 16 + i) * KP + tap * CI + lane, v[i]);
+                        for (int i = 0; i < 16; ++i)
+                            atomicAdd(dw + (int64_t)(c * 16 + i) * KP + (3 * ky + kx) * CI + ch, v[i]);
                     }
                 }
         }
