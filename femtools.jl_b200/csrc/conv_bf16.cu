@@ -24,6 +24,7 @@
 // one's MMAs and epilogue run.
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <mutex>
 #include "kernels.cuh"
 #include "tc05.cuh"
 
@@ -486,18 +487,46 @@ __global__ void f32_to_bf16_kernel(const float* x, __nv_bfloat16* y, int64_t n) 
         y[i] = __float2bfloat16(x[i]);
 }
 
-// Dynamic shared memory above 48 KB needs the kernel attribute (a host-side setting).
+// Dynamic shared memory above 48 KB needs the kernel attribute (a host-side setting, made on
+// every call so that it survives a context reset); the resident blocks per SM that the
+// attributes give are queried once per kernel and device.
+struct LaunchCache {
+    const void* fn;
+    int dev, per_sm;
+};
+std::mutex g_launch_mutex;
+LaunchCache g_launch_cache[128];
+int g_launch_entries = 0;
+
+template <class... KArgs>
+cudaError_t prepare_kernel(void (*fn)(KArgs...), int threads, int smem, int& per_sm) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_launch_mutex);
+    for (int i = 0; i < g_launch_entries; ++i)
+        if (g_launch_cache[i].fn == (const void*)fn && g_launch_cache[i].dev == dev) {
+            per_sm = g_launch_cache[i].per_sm;
+            return cudaSuccess;
+        }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = std::max(per_sm, 1);
+    if (g_launch_entries < 128) g_launch_cache[g_launch_entries++] = LaunchCache{(const void*)fn, dev, per_sm};
+    return cudaSuccess;
+}
+
 template <int CI, int CO, int MODE>
 cudaError_t conv_launch(const void* in, const void* wt, const float* bias, const void* mask, void* out, int B, int H,
                         int W, int num_sms, int* err, cudaStream_t st) {
     constexpr int smem = ConvSmem<CI, CO>::BYTES;
     auto fn = conv3x3_tc_kernel<CI, CO, MODE>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
     int per_sm = 1;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FWD_THREADS, smem);
+    cudaError_t e = prepare_kernel(fn, FWD_THREADS, smem, per_sm);
     if (e != cudaSuccess) return e;
     const int64_t ntile = (int64_t)B * ((H + FROWS - 1) / FROWS) * ((W + SEG - 1) / SEG);
     if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
@@ -521,13 +550,8 @@ template <int CI, int CO>
 cudaError_t wgrad_launch(const void* x, const void* dy, float* dw, float* db, int B, int H, int W, int num_sms, int* err,
                          cudaStream_t st) {
     using S = WgradSmem<CI, CO>;
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<CI, CO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         S::BYTES);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<CI, CO>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
     int per_sm = 1;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_wgrad_tc_kernel<CI, CO>, WG_THREADS, S::BYTES);
+    cudaError_t e = prepare_kernel(conv3x3_wgrad_tc_kernel<CI, CO>, WG_THREADS, S::BYTES, per_sm);
     if (e != cudaSuccess) return e;
     const int64_t ntile = (int64_t)B * ((H + FROWS - 1) / FROWS) * ((W + SEG - 1) / SEG);
     if (ntile >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
