@@ -213,12 +213,6 @@ FEMB_D void load_row_F(float (&F)[3], const float* row, uint64_t pol) {
     for (int j = 0; j < 3; ++j) F[j] = ldg_stream(row + (j * BASE_FIELDS + 6) * 32, pol);
 }
 
-FEMB_D float sqrt_approx(float x) {
-    float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
 // Per-element data of a tile, loaded one tile ahead (during the previous tile's
 // scatter) so that its latency is hidden.
 struct ElemData {
@@ -535,8 +529,9 @@ __global__ void __launch_bounds__(IN_THREADS, 2) hex27_incr_kernel(const IncrArg
                         // stress is not needed.
                         const float dd = 0.5f * (dtt[0] * dtt[0] + dtt[1] * dtt[1] + dtt[2] * dtt[2]) + dtt[3] * dtt[3] +
                                          dtt[4] * dtt[4] + dtt[5] * dtt[5];
-                        const float reach = (sqrt_approx(dd) + fabsf(M.sphi * Pq)) * 1.001f + 1e-20f;
-                        if (Fk + reach < 0.0f) {
+                        // (sqrt(dd) + |sinϕ·δP|)·1.001 + 1e-20 < −F_k, compared on squares
+                        const float lim = -(Fk + 1e-20f) * 0.999000999f - fabsf(M.sphi * Pq);
+                        if (lim > 0.0f && dd < lim * lim) {
 #pragma unroll
                             for (int c = 0; c < 6; ++c) tau[c] = dtt[c];
                         } else {
