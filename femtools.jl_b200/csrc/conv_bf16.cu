@@ -164,12 +164,7 @@ __global__ void __launch_bounds__(FWD_THREADS) conv3x3_tc_kernel(const __nv_bflo
     uint32_t phase = 0u;
     int st = 0;   // stage of tile t
     for (; t < ntile; t += G, st = st == NSTAGE - 1 ? 0 : st + 1) {
-        // the stage of the tile two ahead was last read by the MMAs of the previous one
-        const int ta = t + (NSTAGE - 1) * G;
-        const int sa = st == 0 ? NSTAGE - 1 : st - 1;
-        if (ta < ntile) stage_halo<CI, FROWS + 2, FWD_THREADS>(sA + sa * S::A, in, seg_of<FROWS>(ta, nseg, nrb), H, W, tid);
-        cp_async_commit();
-        cp_async_wait<NSTAGE - 1>();   // every group but the two newest: this tile's halo
+        cp_async_wait<NSTAGE - 2>();   // every group but the newest: this tile's halo
         tc05::fence_async_smem();
         tc05::fence_before_sync();
         __syncthreads();
@@ -190,6 +185,12 @@ __global__ void __launch_bounds__(FWD_THREADS) conv3x3_tc_kernel(const __nv_bflo
                     }
             tc05::commit(smem_u32(mbar));
         }
+        // while the MMAs run: the tile two ahead goes into the stage the previous tile's
+        // (completed) MMAs read
+        const int ta = t + (NSTAGE - 1) * G;
+        const int sa = st == 0 ? NSTAGE - 1 : st - 1;
+        if (ta < ntile) stage_halo<CI, FROWS + 2, FWD_THREADS>(sA + sa * S::A, in, seg_of<FROWS>(ta, nseg, nrb), H, W, tid);
+        cp_async_commit();
         const bool ok = __syncthreads_and(tid != 0 || tc05::mbar_poll(smem_u32(mbar), phase)) != 0;
         phase ^= 1u;
         if (!ok) {
@@ -352,10 +353,7 @@ __global__ void __launch_bounds__(WG_THREADS) conv3x3_wgrad_tc_kernel(const __nv
     bool ok = true, any = false;
     for (int it = 0; t < ntile; ++it, t += gridDim.x) {
         const int buf = it & 1;
-        const int tn = t + (int)gridDim.x;
-        if (tn < ntile) stage(seg_of<FROWS>(tn, nseg, nrb), smem + (buf ^ 1) * S::STAGE);
-        cp_async_commit();
-        cp_async_wait<1>();
+        cp_async_wait<0>();   // this tile's rows
         tc05::fence_async_smem();
         tc05::fence_before_sync();
         __syncthreads();
@@ -373,6 +371,11 @@ __global__ void __launch_bounds__(WG_THREADS) conv3x3_wgrad_tc_kernel(const __nv
                                        bb + (uint64_t)(u * S::NSO * SEG + 16 * ks), idesc, any || ks > 0 || u > 0);
             tc05::commit(smem_u32(mbar + buf));
         }
+        // while the MMAs run: the next tile goes into the other stage, whose MMAs (the
+        // previous tile's) have completed
+        const int tn = t + (int)gridDim.x;
+        if (tn < ntile) stage(seg_of<FROWS>(tn, nseg, nrb), smem + (buf ^ 1) * S::STAGE);
+        cp_async_commit();
         any = true;
         // the stage is re-filled only after the MMAs that read it completed
         ok = __syncthreads_and(tid != 0 || tc05::mbar_poll(smem_u32(mbar + buf), (phases >> buf) & 1u)) != 0;
