@@ -9,8 +9,9 @@
 // after the first; consecutive groups of 8 rows lie SBO bytes apart. Addresses, LBO
 // and SBO are multiples of 16 bytes.
 //
-// Every wait on an mbarrier is bounded: after 2^20 try_wait rounds it gives up and the
-// caller records the failure in an error word and still frees its TMEM.
+// Every wait on an mbarrier is bounded (mbar_poll gives up after 2^22 test_wait polls) and
+// reports whether it gave up; the caller then records the failure in an error word and
+// still frees its TMEM.
 #pragma once
 #include <stdint.h>
 #include "common.cuh"
@@ -27,9 +28,9 @@ FEMB_D uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16 with BF16 A and B (both K-major) and an FP32
-// accumulator: D format at bits 4–5, A/B formats at 7–9 / 10–12, N/8 at 17–22, M/16
-// at 24–28.
+// Instruction descriptor of kind::f16 with BF16 A and B and an FP32 accumulator: D format
+// at bits 4–5, A/B formats at 7–9 / 10–12, N/8 at 17–22, M/16 at 24–28; both operands
+// K-major (bits 15 and 16 select MN-major for A and B).
 template <int M, int N>
 FEMB_HD constexpr uint32_t idesc_bf16_f32() {
     static_assert(M == 128 && N % 16 == 0 && N >= 16 && N <= 256, "cta_group::1, M = 128 shapes only");
@@ -65,17 +66,6 @@ FEMB_D void commit(uint32_t mbar) {
 
 FEMB_D void mbar_init(uint32_t m) { asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m) : "memory"); }
 FEMB_D void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-// true once the barrier's phase `parity` has completed; false after 2^20 rounds
-FEMB_D bool mbar_wait(uint32_t m, uint32_t parity) {
-    uint32_t done = 0;
-    for (int it = 0; it < (1 << 20) && !done; ++it)
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(done)
-                     : "r"(m), "r"(parity)
-                     : "memory");
-    return done != 0;
-}
-
 // Polling form for a completion that is only a few hundred cycles away (the MMAs just
 // issued): mbarrier.test_wait never suspends the thread, so the caller resumes as soon as
 // the phase completes; false after 2^22 polls.
